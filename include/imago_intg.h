@@ -1,0 +1,210 @@
+/*
+ * imago_intg.h -- C ABI of the B200 integral setup for Imago.
+ *
+ * This library replaces the four integral builds that Imago's setupSCF
+ * (src/imago/imago.F90:103-377) calls:
+ *
+ *   gaussOverlapOL      src/imago/integrals.F90:151   (called imago.F90:262)
+ *   gaussOverlapKE      src/imago/integrals.F90:656   (called imago.F90:268)
+ *   gaussOverlapNP      src/imago/integrals.F90:1531  (called imago.F90:284)
+ *   elecPotGaussOverlap src/imago/integrals.F90:2357  (called imago.F90:293)
+ *
+ * Each build sums the two- or three-centre Gaussian integrals over lattice
+ * images within the reference's cutoffs, phases them onto every k-point,
+ * core-orthogonalises the valence-valence block and writes it packed exactly
+ * as orthoOL/ortho (integrals.F90:3608-3911, intgOrtho.F90:115-213) hand it to
+ * HDF5:
+ *
+ *   packed[k][idx][2], idx = j*(j+1)/2 + i for 0 <= i <= j < valeDim
+ *   (the Fortran column-major upper triangle, (re, im) pairs), with
+ *   |x| < 1e-10 set to 0 when coreDim > 0 (intgOrtho.F90:185-190).
+ *
+ * The OL build also returns coreValeOL (integrals.F90:3686-3694 writes it as
+ * separate real and imaginary datasets): cv_re[k][v][c], cv_im[k][v][c],
+ * i.e. a column-major (coreDim, valeDim) matrix per k.
+ * EP output is ordered by potential term as the reference numbers them
+ * (potTypes(t)%cumulAlphaSum + alphaIndex, integrals.F90:3778):
+ * ep_packed[term][k][idx][2].
+ *
+ * All arrays are plain FP64; all indices in the system description are the
+ * reference's 1-based ones.  Every entry point returns an imago status code;
+ * imago_strerror() gives the message the reference would have written to
+ * fort.20 before `stop`.
+ */
+#ifndef IMAGO_INTG_H
+#define IMAGO_INTG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  They replace the reference's `stop` statements. */
+enum imago_status {
+  IMAGO_OK = 0,
+  IMAGO_ERR_INVALID = 1,      /* malformed system description (input.f90 checks) */
+  IMAGO_ERR_CELL_LIST = 2,    /* "More lattice points needed", integrals.F90:378-383 */
+  IMAGO_ERR_NEED_OVERLAP = 3, /* KE/NP/EP requested before OL while coreDim > 0 */
+  IMAGO_ERR_NOMEM = 4,        /* host or device allocation failed */
+  IMAGO_ERR_CUDA = 5,         /* a CUDA call failed */
+  IMAGO_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
+  IMAGO_ERR_NO_DEVICE = 7,    /* no CUDA device of compute capability 10.0 */
+  IMAGO_ERR_RANGE = 8         /* argument outside the supported range */
+};
+
+/* Matrix selection bits for imago_intg_build. */
+enum imago_matrix {
+  IMAGO_OL = 1u, /* overlap, timeStamp 8 */
+  IMAGO_KE = 2u, /* kinetic energy, timeStamp 9 */
+  IMAGO_NP = 4u, /* nuclear potential, timeStamp 10 */
+  IMAGO_EP = 8u  /* every electronic potential term, timeStamp 11 */
+};
+
+/*
+ * System description: the module data that setupSCF has read before the
+ * integral calls (atomTypes, atomSites, potTypes, potSites, realVectors,
+ * kPoints, logBasisFnThresh).
+ */
+typedef struct imago_system {
+  /* realVectors(xyz, abc) in bohr, column-major: real_vectors[3*abc + xyz]
+   * (lattice.f90:163, CELL_VECTORS). */
+  double real_vectors[9];
+  /* BASISFUNCTION_AND_ELECTROSTATIC_CUTOFFS (input.f90:327-346). */
+  double basis_fn_convg;
+  double electro_convg;
+
+  /* Atom types (atomicTypes.f90:132-361). */
+  int num_atom_types;
+  const int *type_element;        /* elementID per type (1-based) */
+  const int *type_num_orb_alphas; /* NUM_ALPHA_S_P_D_F: [4*t + l] */
+  const double *type_alphas;      /* ALPHAS: numOrbAlphas(1) per type, concatenated */
+  const int *type_num_core_fns;   /* radial functions per type (core) */
+  const int *type_num_vale_fns;   /* radial functions per type (valence) */
+  const int *fn_l;                /* QN_l per radial fn, per type core fns then
+                                     valence fns, concatenated over types */
+  const double *fn_coeffs;        /* numOrbAlphas(l+1) coefficients per radial
+                                     fn, same order as fn_l */
+
+  /* Atom sites (atomicSites.f90:85-132). */
+  int num_atom_sites;
+  const int *site_type;           /* atomTypeAssn (1-based) */
+  const double *site_pos;         /* cartPos: [3*s + xyz], bohr */
+
+  /* Potential types (potTypes.f90:86-195). */
+  int num_pot_types;
+  const int *pot_type_element;
+  const double *pot_type_nuc_charge;
+  const double *pot_type_nuc_alpha;
+  const int *pot_type_num_alphas;
+  const double *pot_type_alphas;  /* numAlphas per type, concatenated, ascending */
+
+  /* Potential sites (potSites.f90:40-86): sites of one type consecutive,
+   * types in ascending order. */
+  int num_pot_sites;
+  const int *pot_site_type;
+  const double *pot_site_pos;     /* [3*s + xyz], bohr */
+
+  /* k-points in fractional reciprocal-cell (abc) coordinates, as listed in
+   * fort.15 or made by imago_kpoint_mesh (kpoints.f90:195-440). */
+  int num_kpoints;
+  const double *kpoints_abc;      /* [3*k + abc] */
+} imago_system;
+
+typedef struct imago_opts {
+  int device;            /* CUDA device ordinal */
+  void *stream;          /* cudaStream_t to run on; NULL: a private stream */
+  int outputs_on_device; /* 1: output pointers are device memory */
+  size_t scratch_bytes;  /* device scratch budget; 0: a quarter of free memory */
+} imago_opts;
+
+typedef struct imago_out {
+  double *ol_packed; /* [nk][nPacked][2] */
+  double *ol_cv_re;  /* [nk][valeDim][coreDim] */
+  double *ol_cv_im;  /* [nk][valeDim][coreDim] */
+  double *ke_packed; /* [nk][nPacked][2] */
+  double *np_packed; /* [nk][nPacked][2] */
+  double *ep_packed; /* [potDim][nk][nPacked][2] */
+} imago_out;
+
+/* Sizes of a created context. */
+typedef struct imago_dims {
+  int vale_dim;      /* valeDim (atomicSites.f90:172-186) */
+  int core_dim;      /* coreDim */
+  int num_kpoints;
+  int pot_dim;       /* potDim: sum of potential alphas over types */
+  int num_cells;     /* numCellsReal (lattice.f90:310-444) */
+  long long packed;  /* valeDim*(valeDim+1)/2 */
+  long long num_pair_images;  /* (atom pair, lattice image) units within cutoffs */
+  long long num_shell_pairs;  /* screened primitive (pair, image, alpha1, alpha2) */
+} imago_dims;
+
+typedef struct imago_ctx imago_ctx;
+
+/* Validate the system, build the lattice cell list, k-points, phase
+ * factors and screening tables, and stage them on the device.  Replaces the
+ * setup that setupSCF does before the integral calls
+ * (imago.F90:185-258: initializeLattice, initializeFindVec,
+ * initializeKPoints, renormalizeBasis, makeAlphaDist, makeAlphaNucDist,
+ * makeAlphaPotDist). */
+int imago_intg_create(const imago_system *sys, const imago_opts *opts,
+                      imago_ctx **out_ctx);
+
+/* Fill *dims for a created context. */
+int imago_intg_dims(const imago_ctx *ctx, imago_dims *dims);
+
+/* Overlap: replaces gaussOverlapOL + orthoOL (integrals.F90:151-652,
+ * 3608-3745).  Must run first when coreDim > 0: the context keeps
+ * coreValeOL on the device for the other builds' orthogonalisation. */
+int imago_gauss_overlap_ol(imago_ctx *ctx, double *packed, double *cv_re,
+                           double *cv_im);
+
+/* Kinetic energy: replaces gaussOverlapKE + ortho(2)
+ * (integrals.F90:656-1090). */
+int imago_gauss_overlap_ke(imago_ctx *ctx, double *packed);
+
+/* Nuclear potential: replaces gaussOverlapNP + nuclearPE + ortho(3)
+ * (integrals.F90:1531-1942, 2533-2698). */
+int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
+
+/* Every electronic potential term: replaces elecPotGaussOverlap,
+ * gaussOverlapEP, electronicPE and ortho(4) for all potDim terms
+ * (integrals.F90:1946-2531, 2700-2858). */
+int imago_elec_pot_gauss_overlap(imago_ctx *ctx, double *packed);
+
+/* All matrices selected by `which` (IMAGO_OL|IMAGO_KE|IMAGO_NP|IMAGO_EP)
+ * in one call; OL runs first. */
+int imago_intg_build(imago_ctx *ctx, unsigned which, const imago_out *out);
+
+/* Device time in milliseconds of the stages of the last build:
+ * ms[0..3] = OL, KE, NP, EP (timeStamps.f90:45-48 labels 8-11). */
+int imago_intg_stage_ms(const imago_ctx *ctx, double ms[4]);
+
+void imago_intg_destroy(imago_ctx *ctx);
+
+const char *imago_strerror(int status);
+
+/* Monkhorst-Pack style mesh of kpoints.f90:837-899 without symmetry
+ * folding (the P1 case): k_abc = -1/2 + (i - 1 + shift)/n for each axis,
+ * a-major.  Writes n[0]*n[1]*n[2] points to kpoints_abc[3*k + abc]. */
+int imago_kpoint_mesh(const int n[3], const double shift[3],
+                      double *kpoints_abc);
+
+/*
+ * Primitive integrals on the device, for checking the kernels against the
+ * reference's generated primitives (gaussIntegrals.f90).  kind: 0 overlap
+ * (overlap2CIntg), 1 kinetic (kinetic2CIntg), 2 three-centre overlap
+ * (electron3CIntg), 3 three-centre nuclear (nuclear3CIntg), 4 Boys function
+ * (boys, F_0..F_6 of params[0]).  Record r reads
+ *   params[r*12 + 0..11] = a1, a2, a3, A[3], B[3], C[3]
+ * and cls[2*r + 0..1] = l of atom 1 and atom 2 (0..3); it writes
+ * sh[r*256 + i*16 + j] = reference sh(i+1, j+1).  Host pointers.
+ */
+int imago_prim_eval(int kind, int n, const double *params, const int *cls,
+                    double *sh);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMAGO_INTG_H */

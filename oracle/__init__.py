@@ -1,0 +1,188 @@
+"""ctypes access to the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA integral path.  It is
+imported by tests/, by __graft_entry__.smoke() and by bench.py's CPU
+baseline leg, never by the imago_b200 package.  See oracle.h for what it
+restates and how its parity is pinned.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from imago_b200.system import ImagoDimsC
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        for name in ("orc_overlap2c", "orc_kinetic2c"):
+            f = getattr(L, name)
+            f.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D,
+                          ctypes.c_int, ctypes.c_int, _D]
+            f.restype = None
+        for name in ("orc_electron3c", "orc_nuclear3c"):
+            f = getattr(L, name)
+            f.argtypes = [ctypes.c_double] * 3 + [_D, _D, _D, ctypes.c_int,
+                                                  ctypes.c_int, _D]
+            f.restype = None
+        L.orc_boys.argtypes = [ctypes.c_double, _D]
+        L.orc_boys.restype = None
+        L.orc_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.orc_create.restype = ctypes.c_int
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_destroy.restype = None
+        L.orc_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ImagoDimsC)]
+        L.orc_set_sampling.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_set_sampling.restype = None
+        L.orc_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
+        L.orc_gauss_overlap_ke.argtypes = [ctypes.c_void_p, _D]
+        L.orc_gauss_overlap_np.argtypes = [ctypes.c_void_p, _D]
+        L.orc_elec_pot_gauss_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                                 ctypes.c_int, _D]
+        L.orc_last_times.argtypes = [ctypes.c_void_p, _D, _D]
+        L.orc_last_times.restype = None
+        L.orc_num_cells.argtypes = [ctypes.c_void_p]
+        L.orc_cells.argtypes = [ctypes.c_void_p, _D, _D]
+        L.orc_cells.restype = None
+        L.orc_kpoints_xyz.argtypes = [ctypes.c_void_p, _D]
+        L.orc_kpoints_xyz.restype = None
+        L.orc_find_lattice_vector.argtypes = [ctypes.c_void_p, _D, _D]
+        L.orc_find_lattice_vector.restype = None
+        L.orc_last_counts.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_longlong)] * 3
+        L.orc_last_counts.restype = None
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def primitive(kind, la, lb, a1, a2, a3, A, B, C):
+    """Reference-layout sh block (nsh(la) x nsh(lb)) from the oracle.
+    kind: overlap, kinetic, electron3c, nuclear3c."""
+    L = lib()
+    sh = np.zeros(256)
+    A = np.ascontiguousarray(A, float)
+    B = np.ascontiguousarray(B, float)
+    C = np.ascontiguousarray(C, float)
+    if kind == "overlap":
+        L.orc_overlap2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
+    elif kind == "kinetic":
+        L.orc_kinetic2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
+    elif kind == "electron3c":
+        L.orc_electron3c(a1, a2, a3, _p(A), _p(B), _p(C), la, lb, _p(sh))
+    elif kind == "nuclear3c":
+        L.orc_nuclear3c(a1, a2, a3, _p(A), _p(B), _p(C), la, lb, _p(sh))
+    else:
+        raise ValueError(kind)
+    n1, n2 = (la + 1) ** 2, (lb + 1) ** 2
+    return sh.reshape(16, 16)[:n1, :n2].copy()
+
+
+def boys(T):
+    F = np.zeros(7)
+    lib().orc_boys(float(T), _p(F))
+    return F
+
+
+class OracleBuild:
+    """The reference's four integral builds restated on the CPU."""
+
+    def __init__(self, system, stride=1, nthreads=0):
+        self.system = system
+        self._cs, self._keep = system.to_c()
+        self._ctx = ctypes.c_void_p()
+        st = lib().orc_create(ctypes.byref(self._cs), ctypes.byref(self._ctx))
+        if st != 0:
+            raise RuntimeError(f"orc_create failed with status {st}")
+        lib().orc_set_sampling(self._ctx, stride, nthreads)
+        d = ImagoDimsC()
+        lib().orc_dims(self._ctx, ctypes.byref(d))
+        self.vale_dim, self.core_dim = d.vale_dim, d.core_dim
+        self.nk, self.pot_dim, self.num_cells = d.num_kpoints, d.pot_dim, d.num_cells
+        self.npacked = int(d.packed)
+
+    def close(self):
+        if self._ctx:
+            lib().orc_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _packed(self, n=1):
+        return np.zeros((n, self.nk, self.npacked, 2))
+
+    def _check(self, st, what):
+        if st != 0:
+            raise RuntimeError(f"{what} failed with status {st}")
+
+    def overlap(self):
+        out = self._packed()
+        cre = np.zeros((self.nk, self.vale_dim, max(self.core_dim, 1)))
+        cim = np.zeros_like(cre)
+        self._check(lib().orc_gauss_overlap_ol(self._ctx, _p(out), _p(cre), _p(cim)), "OL")
+        return out[0], cre[:, :, :self.core_dim], cim[:, :, :self.core_dim]
+
+    def kinetic(self):
+        out = self._packed()
+        self._check(lib().orc_gauss_overlap_ke(self._ctx, _p(out)), "KE")
+        return out[0]
+
+    def nuclear(self):
+        out = self._packed()
+        self._check(lib().orc_gauss_overlap_np(self._ctx, _p(out)), "NP")
+        return out[0]
+
+    def elec_pot(self, lo=0, hi=None):
+        hi = self.pot_dim if hi is None else hi
+        out = self._packed(hi - lo)
+        self._check(lib().orc_elec_pot_gauss_overlap(self._ctx, lo, hi, _p(out)), "EP")
+        return out
+
+    def last_times(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        lib().orc_last_times(self._ctx, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def last_counts(self):
+        x = [ctypes.c_longlong() for _ in range(3)]
+        lib().orc_last_counts(self._ctx, *[ctypes.byref(v) for v in x])
+        return tuple(v.value for v in x)
+
+    def cells(self):
+        n = lib().orc_num_cells(self._ctx)
+        d, s = np.zeros((n, 3)), np.zeros(n)
+        lib().orc_cells(self._ctx, _p(d), _p(s))
+        return d, s
+
+    def kpoints_xyz(self):
+        k = np.zeros((self.nk, 3))
+        lib().orc_kpoints_xyz(self._ctx, _p(k))
+        return k
+
+    def nearest_lattice_vector(self, v):
+        v = np.ascontiguousarray(v, float)
+        o = np.zeros(3)
+        lib().orc_find_lattice_vector(self._ctx, _p(v), _p(o))
+        return o

@@ -1,0 +1,59 @@
+"""The CPU oracle's primitives against the reference's own generated
+kernels (tests/golden/primitives.json, made by executing
+src/imago/gaussIntegrals.f90 statement by statement)."""
+import numpy as np
+import pytest
+
+import oracle
+
+KINDS = ("overlap", "kinetic", "electron3c", "nuclear3c")
+# Relative to the largest element of the block.  The oracle uses its own
+# recursions, so the two agree to rounding; 1e-12 leaves room for the
+# nuclear higher classes (observed <= 1.2e-13).
+RTOL = 1e-12
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_primitives_match_reference_kernels(golden, kind):
+    n = 0
+    for r in golden["records"]:
+        if kind not in r:
+            continue
+        ref = np.array(r[kind])
+        got = oracle.primitive(kind, r["la"], r["lb"], r["a1"], r["a2"],
+                               r["a3"], r["A"], r["B"], r["C"])
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.abs(got - ref).max() <= RTOL * scale, (kind, r["la"], r["lb"])
+        n += 1
+    assert n >= 64
+
+
+def test_boys_bit_exact_with_reference(golden):
+    # Same branch structure, same single-precision series constants and the
+    # same operation order as gaussIntegrals.f90:16080-16221.
+    for row in golden["boys"]:
+        F = oracle.boys(row["T"])
+        assert np.array_equal(F, np.array(row["F"])), row["T"]
+
+
+def test_boys_reference_deviation_from_exact():
+    # The reference's series constants are single precision, so F_6(0) is
+    # not 1/13; the oracle keeps that.
+    F = oracle.boys(0.0)
+    assert abs(F[6] - 1.0 / 13.0) > 1e-9
+    assert abs(F[6] - 1.0 / 13.0) < 1e-7
+
+
+def test_closed_forms_s_s():
+    a1, a2, a3 = 0.7, 1.9, 3.1
+    A, B, C = np.array([0.1, 0.2, -0.3]), np.array([1.0, -0.4, 0.5]), np.array([0.3, 0.9, 0.2])
+    z, xi = a1 + a2, a1 * a2 / (a1 + a2)
+    d2 = ((A - B) ** 2).sum()
+    S = (np.pi / z) ** 1.5 * np.exp(-xi * d2)
+    assert oracle.primitive("overlap", 0, 0, a1, a2, 0, A, B, C)[0, 0] == pytest.approx(S, rel=1e-14)
+    assert oracle.primitive("kinetic", 0, 0, a1, a2, 0, A, B, C)[0, 0] == pytest.approx(
+        xi * (3 - 2 * xi * d2) * S, rel=1e-13)
+    z3 = z + a3
+    P = (a1 * A + a2 * B) / z
+    E = (np.pi / z3) ** 1.5 * np.exp(-xi * d2 - z * a3 / z3 * ((P - C) ** 2).sum())
+    assert oracle.primitive("electron3c", 0, 0, a1, a2, a3, A, B, C)[0, 0] == pytest.approx(E, rel=1e-14)
