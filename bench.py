@@ -1,0 +1,373 @@
+"""Integral-build benchmark: Imago's SCF integral setup on B200.
+
+Workload (one "step"): the full integral setup of the jittered 8-atom
+silicon conventional cell with an s,p,d basis of 20 even-tempered
+primitives, 20 potential terms and an 8x8x8 k-mesh: the overlap, kinetic,
+nuclear and all 20 electronic-potential matrices, lattice-summed,
+Bloch-phased onto 512 k-points, core-orthogonalised and packed as the
+reference hands them to SCF.  Inputs are synthetic (seeded positions and
+synthesised contraction coefficients; the reference's basis database is not
+available).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Our arm times K builds on the device (CUDA events on the library's stream,
+L2 flushed between steps, outputs resident in HBM), then the same build end
+to end through the C ABI with host buffers.  The reference arm times the
+CPU restatement of the reference's algorithm (oracle/, all host threads) on
+a bounded sample of the same workload and scales it to one build.
+Under torchrun each rank builds its own independently jittered cell (weak
+scaling, no collective on the data path).
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "integral build time (OL+KE+NP+20 EP, 512 k-points)"
+UNIT = "s"
+WORKLOAD = ("Si8 conventional cell, jitter N(0,0.02 A), s,p,d basis 20 "
+            "primitives (20/20/14/0), 20 potential terms, 8x8x8 k")
+
+
+def system_for_rank(rank):
+    from imago_b200 import configs
+    return configs.silicon_cubic8(seed=2 + rank)
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ algorithmic --
+def algorithmic_flops(g):
+    """Per-build FLOPs of the dense stages, from the screened work counts:
+    lattice-to-k sum: 4 flops per (k, unit block element), per matrix;
+    orthogonalisation: Y = X_cv - X_cc S/2 (8 C^2 V per k) and the packed
+    update S^H Y + Y^H S (16 C per packed element per k), per matrix."""
+    nmat = 3 + g.pot_dim
+    V, C, nk = g.vale_dim, g.core_dim, g.nk
+    m_elems = g.block_elements
+    bloch = 4.0 * nk * m_elems * nmat
+    ortho = nk * (8.0 * C * C * V + 16.0 * C * g.npacked) * nmat
+    return {"bloch": bloch, "ortho": ortho}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 dense throughput of this GPU (cuBLAS DGEMM 8192^3)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+# ------------------------------------------------------------- CPU legs --
+def cpu_sample_build(system, pair_stride, k_stride, nthreads):
+    """Time the oracle on 1/pair_stride of the atom pairs and 1/k_stride of
+    the k-points in the orthogonalisation, scaled to one full build."""
+    import oracle
+    from imago_b200.system import ImagoSystem  # noqa: F401
+    sub = system
+    ob = oracle.OracleBuild(sub, stride=pair_stride, nthreads=nthreads)
+    loops = ortho = 0.0
+    ob.overlap()
+    lo, ot = ob.last_times(); loops += lo; ortho += ot
+    ob.kinetic()
+    lo, ot = ob.last_times(); loops += lo; ortho += ot
+    ob.nuclear()
+    lo, ot = ob.last_times(); loops += lo; ortho += ot
+    # EP term by term: accumulate the per-term times
+    for t in range(ob.pot_dim):
+        ob.elec_pot(t, t + 1)
+        lo, ot = ob.last_times(); loops += lo; ortho += ot
+    ob.close()
+    return loops * pair_stride + ortho, loops, ortho
+
+
+def k_subset(system, k_stride):
+    import copy
+    s = copy.copy(system)
+    s.kpoints_abc = system.kpoints_abc[::k_stride].copy()
+    return s
+
+
+def cpu_baseline(system, nthreads, budget_s=20.0):
+    """Bounded CPU sample: every 4th atom pair and every 16th k-point (the
+    per-k work scales linearly in nk), extrapolated to the full build."""
+    pair_stride, k_stride = 4, 16
+    sub = k_subset(system, k_stride)
+    t0 = time.perf_counter()
+    est, loops, ortho = cpu_sample_build(sub, pair_stride, k_stride, nthreads)
+    wall = time.perf_counter() - t0
+    # loops scale with pairs and (through the phase application) with k;
+    # the orthogonalisation with k only.
+    value = loops * pair_stride * k_stride + ortho * k_stride
+    return value, wall, pair_stride, k_stride
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle  # noqa: F401
+    system = system_for_rank(0)
+    nthreads = os.cpu_count() or 1
+    times, walls = [], []
+    for i in range(args.warmup + args.steps):
+        v, wall, ps, ks = cpu_baseline(system, nthreads)
+        if i >= args.warmup:
+            times.append(v)
+            walls.append(wall)
+    value = float(np.mean(times))
+    sample = (f"CPU restatement of the reference path (oracle/, C, OpenMP over "
+              f"atom pairs) on every {ps}th atom pair and every {ks}th k-point, "
+              f"scaled to one full build; {np.mean(walls):.1f} s of CPU work per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- our arm --
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from imago_b200 import intg
+
+    system = system_for_rank(rank)
+    stream = torch.cuda.current_stream()
+    g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
+                           stream=stream.cuda_stream)
+    nk, npk, V, C, P = g.nk, g.npacked, g.vale_dim, g.core_dim, g.pot_dim
+    dev = torch.device("cuda", local)
+    bufs = {
+        "ol_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
+        "ol_cv_re": torch.empty((nk, V, max(C, 1)), dtype=torch.float64, device=dev),
+        "ol_cv_im": torch.empty((nk, V, max(C, 1)), dtype=torch.float64, device=dev),
+        "ke_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
+        "np_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
+        "ep_packed": torch.empty((P, nk, npk, 2), dtype=torch.float64, device=dev),
+    }
+    flush = torch.empty(512 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+
+    def one_build():
+        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
+
+    for _ in range(args.warmup):
+        one_build()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_s = []
+    kms = np.zeros(4)
+    launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # write 512 MiB > L2 between timed steps
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            one_build()
+            e.record(stream)
+            e.synchronize()
+            step_s.append(s.elapsed_time(e) / 1e3)
+            ms, n = g.kernel_stats()
+            kms += ms
+            launches += n
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    total = float(np.sum(step_s))
+    if world > 1:
+        t = torch.tensor([total], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+    value = total / args.steps
+    kms /= args.steps
+
+    # end to end through the C ABI with host buffers: create (stages the
+    # system on the device) + all builds + copies into pinned host memory
+    pinned = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+              for k, v in bufs.items()}
+    e2e_s = []
+    h2d = _system_bytes(system)
+    d2h = sum(v.numel() * 8 for v in pinned.values())
+    e2e_steps = max(2, min(args.steps, 3))
+    for i in range(e2e_steps + 1):
+        torch.cuda.synchronize()
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        g2 = intg.IntegralSetup(system, device=local, outputs_on_device=False,
+                                stream=stream.cuda_stream)
+        g2.build(out={k: v.data_ptr() for k, v in pinned.items()})
+        e.record(stream)
+        e.synchronize()
+        g2.close()
+        if i > 0:  # first is a warm-up
+            e2e_s.append(s.elapsed_time(e) / 1e3)
+    e2e = float(np.mean(e2e_s))
+
+    flops = algorithmic_flops(g)
+    fp64 = fp64_peak_tflops(torch) if rank == 0 else None
+    stage_names = ["prim", "contract", "bloch", "ortho"]
+    top = int(np.argmax(kms))
+    top_name = stage_names[top]
+    roofline = None
+    if top_name in flops and fp64:
+        achieved = flops[top_name] / (kms[top] / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64,
+                    "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": None,
+                    "kernel": top_name,
+                    "peak_source": "measured cuBLAS DGEMM 8192^3 in this run "
+                                   "(MEASURED_PEAKS.json has no FP64 figure)"}
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.skip_cpu:
+            v, wall, ps, ks = cpu_baseline(system, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
+                   "kind": "port",
+                   "sample": (f"oracle (CPU restatement, OpenMP) on every {ps}th "
+                              f"atom pair and every {ks}th k-point, scaled to one "
+                              f"build; {wall:.1f} s wall")}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jitter, synthesised contraction coefficients)",
+            "config": {"workload": WORKLOAD, "l2": "512 MiB flush between steps",
+                       "vale_dim": V, "core_dim": C, "kpoints": nk, "pot_terms": P,
+                       "pair_images": g.num_pair_images,
+                       "shell_pairs": g.num_shell_pairs},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "stage_ms": dict(zip(stage_names, [float(x) for x in kms])),
+            "shell_pairs_per_s": g.num_shell_pairs * (3 + P) / value,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def _system_bytes(system):
+    s, keep = system.to_c()
+    return int(sum(a.nbytes for a in keep)) + 9 * 8
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -258,3 +258,18 @@ def small_test_system(seed=7, kmesh=(2, 2, 1)):
                        title="small two-element test cell", kmesh=km)
     sys_.validate()
     return sys_
+
+
+def f_test_system(kmesh=(2, 1, 1)):
+    """Two atoms of one element with s, p, d and f functions, so every class
+    up to f-f appears; small enough for the CPU oracle."""
+    a = 7.0
+    rv = np.array([[a, 0.0, 0.0], [0.5, a, 0.0], [0.0, 0.3, a]])
+    pos = np.array([[0.1, 0.2, 0.3], [2.1, 1.7, 2.6]])
+    alphas = even_tempered(6, 0.3, 3.0e2)
+    t = _make_type(1, "x1_1", alphas, (6, 6, 5, 4), [(1, 0, 6.0)],
+                   [(2, 0, 1.6), (2, 1, 1.5), (3, 2, 1.2), (4, 3, 1.0)])
+    p = _pot(1, "x1_1", 10, 3, 0.3, 1.0e3)
+    k, km = _mesh(kmesh, (0.5, 0.0, 0.0))
+    return _system(rv, [t], [1, 1], pos, [p], [1, 1], k,
+                   title="f-class test pair", kmesh=km)

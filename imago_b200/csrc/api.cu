@@ -1,0 +1,1029 @@
+// api.cu -- the C ABI of include/imago_intg.h: system set-up on the host,
+// device staging, and the four integral builds.
+//
+// Host set-up restates what setupSCF does before the integral calls:
+//   setCutoffThresh            lattice.f90:239-308
+//   initializeLattice          lattice.f90:310-444 (cutoff sphere)
+//   getNumCells/makeLattice    lattice.f90:469-690, cellBorderCheck 698-782
+//   getRecipCellVectors        lattice.f90:182-233
+//   convertKPointsToXYZ        kpoints.f90:543-576
+//   renormalizeBasis           basis.f90:55-243
+// and builds the work lists that the reference's loop nests walk
+// (integrals.F90:323-569): atom pairs i <= j with their nearest-image
+// lattice vector, the lattice images within each pair's cutoff, and the
+// screened alpha pairs of each image in the reference's staircase order.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "intg.cuh"
+
+using namespace imago;
+
+namespace {
+
+// basis.f90:91-106
+const double kAngNorm[16] = {
+    0.2820947917738782, 0.4886025119029199, 0.4886025119029199,
+    0.4886025119029199, 1.0925484305920790, 1.0925484305920790,
+    1.0925484305920790, 0.5462742152960396, 0.3153915652525200,
+    2.8906114426405543, 1.4453057213202771, 0.5900435899266435,
+    0.5900435899266435, 0.3731763325901154, 0.4570457994644657,
+    0.4570457994644657};
+
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (count <= n && p) return IMAGO_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (count == 0) return IMAGO_OK;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_NOMEM;
+    }
+    n = count;
+    return IMAGO_OK;
+  }
+  int upload(const std::vector<T> &v, cudaStream_t st) {
+    int rc = alloc(v.empty() ? 1 : v.size());
+    if (rc) return rc;
+    if (!v.empty())
+      IMAGO_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T),
+                                 cudaMemcpyHostToDevice, st));
+    return IMAGO_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct HType {
+  int element;
+  int norb[4];
+  int nalpha, ncore, nvale, nstates;
+  std::vector<double> alphas;
+  std::vector<int> cls, lm;
+  std::vector<double> basis;  // [a * nstates + m]
+};
+
+struct HPType {
+  int element;
+  double z, nucalpha;
+  std::vector<double> alphas;
+  int first_site = -1, mult = 0, cumul = 0;
+};
+
+}  // namespace
+
+struct imago_ctx {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  int outputs_on_device = 0;
+  size_t scratch_bytes = 0;
+
+  // host description
+  std::vector<HType> types;
+  std::vector<HPType> ptypes;
+  std::vector<int> type_screen, ptype_screen;
+  int nt = 0, ns = 0, npt = 0, nps = 0, nk = 0, ncell = 0;
+  int vale_dim = 0, core_dim = 0, pot_dim = 0;
+  double T = 0.0;
+  double rv[9], recip[9], inv[9];
+  std::vector<double> site_pos, psite_pos, cells, csize, kxyz;
+  std::vector<int> site_type, psite_ptype, cum_vale, cum_core;
+
+  // work lists
+  std::vector<DPair> pairs;
+  std::vector<DUnit> units;
+  std::vector<DSp> sps;
+  std::vector<int> sp_by_cls;
+  int cls_beg[17];
+  long long blk_total = 0, m_total = 0;
+  std::vector<Term3c> ep_terms;
+
+  // device copies
+  DBuf<int> d_type_nalpha, d_type_alpha_off, d_type_nstates, d_type_nvale,
+      d_type_state_off, d_type_basis_off, d_type_screen, d_alpha_cls,
+      d_state_lm, d_site_type, d_site_cum_vale, d_site_cum_core,
+      d_ptype_alpha_off, d_ptype_nalpha, d_ptype_first_site, d_ptype_mult,
+      d_ptype_screen, d_psite_ptype, d_sp_by_cls;
+  DBuf<double> d_alpha, d_basis, d_site_pos, d_ptype_z, d_ptype_nucalpha,
+      d_palpha, d_psite_pos, d_cell, d_csize, d_kxyz;
+  DBuf<double2> d_phase;
+  DBuf<DPair> d_pairs;
+  DBuf<DUnit> d_units;
+  DBuf<DSp> d_sps;
+  DBuf<Term3c> d_terms;
+
+  // scratch
+  DBuf<double> blk, M, packed_stage;
+  DBuf<double2> vv, cv, cc, y, s_cv;
+  bool have_ol = false;
+
+  DevSys sys;
+  DevWork work;
+  float stage_ms[4] = {0, 0, 0, 0};
+  cudaEvent_t ev[8];
+  bool events = false;
+  // per-kernel-stage timing of the current build call: 5 events per
+  // run_build (start, after prim, contract, bloch, ortho)
+  std::vector<cudaEvent_t> kev;
+  int kev_used = 0;
+  long long launches = 0;
+  double kernel_ms[4] = {0, 0, 0, 0};
+
+  ~imago_ctx() {
+    d_type_nalpha.release(); d_type_alpha_off.release(); d_type_nstates.release();
+    d_type_nvale.release(); d_type_state_off.release(); d_type_basis_off.release();
+    d_type_screen.release(); d_alpha_cls.release(); d_state_lm.release();
+    d_site_type.release(); d_site_cum_vale.release(); d_site_cum_core.release();
+    d_ptype_alpha_off.release(); d_ptype_nalpha.release();
+    d_ptype_first_site.release(); d_ptype_mult.release(); d_ptype_screen.release();
+    d_psite_ptype.release(); d_sp_by_cls.release(); d_alpha.release();
+    d_basis.release(); d_site_pos.release(); d_ptype_z.release();
+    d_ptype_nucalpha.release(); d_palpha.release(); d_psite_pos.release();
+    d_cell.release(); d_csize.release(); d_kxyz.release(); d_phase.release();
+    d_pairs.release(); d_units.release(); d_sps.release(); d_terms.release();
+    blk.release(); M.release(); packed_stage.release(); vv.release();
+    cv.release(); cc.release(); y.release(); s_cv.release();
+    if (events)
+      for (auto &e : ev) cudaEventDestroy(e);
+    for (auto &e : kev) cudaEventDestroy(e);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// ------------------------------------------------------------ lattice --
+void recip_vectors(imago_ctx *c) {
+  for (int i = 0; i < 3; ++i) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+    double vol = 0.0;
+    double r[3];
+    for (int j = 0; j < 3; ++j) {
+      const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+      r[j] = c->rv[3 * i1 + j1] * c->rv[3 * i2 + j2] -
+             c->rv[3 * i1 + j2] * c->rv[3 * i2 + j1];
+      vol += r[j] * c->rv[3 * i + j];
+    }
+    for (int j = 0; j < 3; ++j) c->recip[3 * i + j] = 2.0 * kPi * r[j] / vol;
+  }
+  for (int i = 0; i < 9; ++i) c->inv[i] = c->recip[i] / (2.0 * kPi);
+}
+
+bool border_within(const double *rv, const double *t, double lim) {
+  double sh[3] = {0, 0, 0}, cur[3] = {t[0], t[1], t[2]};
+  for (int i = 0; i < 3; ++i)
+    for (int x = 0; x < 3; ++x) sh[x] += rv[3 * i + x];
+  // The seven other corners, walked as cellBorderCheck walks them.
+  const int ax[7] = {0, 1, 0, 2, 0, 1, 0};
+  const int sg[7] = {1, 1, -1, 1, 1, -1, -1};
+  for (int s = 0; s < 7; ++s) {
+    cur[ax[s]] += sg[s] * sh[ax[s]];
+    if (cur[0] * cur[0] + cur[1] * cur[1] + cur[2] * cur[2] < lim) return true;
+  }
+  return false;
+}
+
+int make_cells(imago_ctx *c, double min_atom_alpha, double min_pot_alpha) {
+  double lim = c->T * std::max(2.0 / min_atom_alpha,
+                               1.0 / min_pot_alpha + 0.5 / min_atom_alpha);
+  double maxsq = 0.0, len2[3];
+  for (int i = 0; i < 3; ++i) {
+    len2[i] = 0.0;
+    for (int x = 0; x < 3; ++x) len2[i] += c->rv[3 * i + x] * c->rv[3 * i + x];
+    maxsq = std::max(len2[i], maxsq);
+  }
+  lim = lim + 0.75 * maxsq + std::sqrt(3.0 * maxsq * lim);
+  lim = std::max(lim, 2.0 * c->T / min_atom_alpha);
+  int reps[3];
+  for (int i = 0; i < 3; ++i)
+    reps[i] = 2 * (int)std::ceil(std::sqrt(lim) / std::sqrt(len2[i])) + 1;
+  struct Cell {
+    double size, d[3];
+    int idx;
+  };
+  std::vector<Cell> list;
+  for (int i = 1; i <= reps[0]; ++i)
+    for (int j = 1; j <= reps[1]; ++j)
+      for (int k = 1; k <= reps[2]; ++k) {
+        const int rep[3] = {i - (1 + reps[0]) / 2, j - (1 + reps[1]) / 2,
+                            k - (1 + reps[2]) / 2};
+        double t[3] = {0, 0, 0};
+        for (int l = 0; l < 3; ++l)
+          for (int m = 0; m < 3; ++m) t[m] = t[m] + c->rv[3 * l + m] * rep[l];
+        const double s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+        if (s > lim && !border_within(c->rv, t, lim)) continue;
+        list.push_back({s, {t[0], t[1], t[2]}, (int)list.size()});
+      }
+  std::stable_sort(list.begin(), list.end(),
+                   [](const Cell &a, const Cell &b) { return a.size < b.size; });
+  c->ncell = (int)list.size();
+  c->cells.resize(3 * list.size());
+  c->csize.resize(list.size());
+  for (size_t i = 0; i < list.size(); ++i) {
+    std::memcpy(&c->cells[3 * i], list[i].d, sizeof(double) * 3);
+    c->csize[i] = list[i].size;
+  }
+  return IMAGO_OK;
+}
+
+void nearest_lattice_host(const imago_ctx *c, const double *v, double *out) {
+  double base[3] = {0, 0, 0};
+  for (int i = 0; i < 3; ++i) {
+    const double f = v[0] * c->inv[3 * i] + v[1] * c->inv[3 * i + 1] +
+                     v[2] * c->inv[3 * i + 2];
+    double r = (double)(long long)(std::fabs(f) + 0.5);
+    if (f < 0.0) r = -r;
+    for (int x = 0; x < 3; ++x) base[x] += c->rv[3 * i + x] * r;
+  }
+  double best[3] = {base[0], base[1], base[2]};
+  double bd = 0.0;
+  for (int x = 0; x < 3; ++x) bd += (v[x] - base[x]) * (v[x] - base[x]);
+  for (int i = -1; i <= 1; ++i)
+    for (int j = -1; j <= 1; ++j)
+      for (int k = -1; k <= 1; ++k) {
+        if (!i && !j && !k) continue;
+        double cand[3], d = 0.0;
+        for (int x = 0; x < 3; ++x) {
+          cand[x] = base[x] + i * c->rv[x] + j * c->rv[3 + x] + k * c->rv[6 + x];
+          d += (v[x] - cand[x]) * (v[x] - cand[x]);
+        }
+        if (d < bd * (1.0 - 1e-12)) {
+          bd = d;
+          std::memcpy(best, cand, sizeof best);
+        }
+      }
+  std::memcpy(out, best, sizeof best);
+}
+
+// ------------------------------------------------------------ set-up --
+int read_system(imago_ctx *c, const imago_system *s) {
+  if (!s || s->num_atom_types <= 0 || s->num_atom_sites <= 0 ||
+      s->num_pot_types <= 0 || s->num_pot_sites <= 0 || s->num_kpoints <= 0)
+    return IMAGO_ERR_INVALID;
+  if (!(s->basis_fn_convg > 0.0 && s->basis_fn_convg <= 1.0))
+    return IMAGO_ERR_INVALID;
+  c->nt = s->num_atom_types;
+  c->ns = s->num_atom_sites;
+  c->npt = s->num_pot_types;
+  c->nps = s->num_pot_sites;
+  c->nk = s->num_kpoints;
+  std::memcpy(c->rv, s->real_vectors, sizeof c->rv);
+  c->T = -std::log(s->basis_fn_convg);
+  recip_vectors(c);
+  double min_atom_alpha = 100.0, min_pot_alpha = 10000.0;
+  int aoff = 0, foff = 0, coff = 0;
+  c->types.resize(c->nt);
+  for (int t = 0; t < c->nt; ++t) {
+    HType &ty = c->types[t];
+    ty.element = s->type_element[t] - 1;
+    if (ty.element < 0) return IMAGO_ERR_INVALID;
+    for (int l = 0; l < 4; ++l) ty.norb[l] = s->type_num_orb_alphas[4 * t + l];
+    for (int l = 0; l < 3; ++l)
+      if (ty.norb[l] < ty.norb[l + 1] || ty.norb[l + 1] < 0)
+        return IMAGO_ERR_INVALID;
+    ty.nalpha = ty.norb[0];
+    if (ty.nalpha <= 0 || ty.nalpha > 32767) return IMAGO_ERR_INVALID;
+    ty.alphas.assign(s->type_alphas + aoff, s->type_alphas + aoff + ty.nalpha);
+    aoff += ty.nalpha;
+    for (double a : ty.alphas)
+      if (!(a > 0.0)) return IMAGO_ERR_INVALID;
+    min_atom_alpha = std::min(min_atom_alpha, ty.alphas[0]);
+    ty.cls.resize(ty.nalpha);
+    for (int j = 0; j < ty.nalpha; ++j)
+      ty.cls[j] = j < ty.norb[3] ? 3 : j < ty.norb[2] ? 2 : j < ty.norb[1] ? 1 : 0;
+    const int ncf = s->type_num_core_fns[t], nvf = s->type_num_vale_fns[t];
+    if (ncf < 0 || nvf < 0) return IMAGO_ERR_INVALID;
+    const int *fl = s->fn_l + foff;
+    std::vector<int> fco(ncf + nvf);
+    ty.ncore = ty.nvale = 0;
+    for (int f = 0; f < ncf + nvf; ++f) {
+      if (fl[f] < 0 || fl[f] > 3 || ty.norb[fl[f]] <= 0) return IMAGO_ERR_INVALID;
+      fco[f] = coff;
+      coff += ty.norb[fl[f]];
+      (f < ncf ? ty.ncore : ty.nvale) += 2 * fl[f] + 1;
+    }
+    ty.nstates = ty.ncore + ty.nvale;
+    ty.lm.resize(ty.nstates);
+    ty.basis.assign((size_t)ty.nalpha * ty.nstates, 0.0);
+    // renormalizeBasis: valence functions first, then core; each l repeated
+    // 2l+1 times with lm = l^2 + k and the angular norm folded in.
+    int m = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      const int f0 = pass == 0 ? ncf : 0, f1 = pass == 0 ? ncf + nvf : ncf;
+      for (int f = f0; f < f1; ++f) {
+        const int l = fl[f], na = ty.norb[l];
+        for (int k = 1; k <= 2 * l + 1; ++k) {
+          ty.lm[m] = l * l + k - 1;
+          for (int a = 0; a < na; ++a)
+            ty.basis[(size_t)a * ty.nstates + m] =
+                s->fn_coeffs[fco[f] + a] * kAngNorm[ty.lm[m]];
+          ++m;
+        }
+      }
+    }
+    foff += ncf + nvf;
+  }
+  c->site_type.resize(c->ns);
+  c->site_pos.assign(s->site_pos, s->site_pos + 3 * c->ns);
+  c->cum_vale.resize(c->ns);
+  c->cum_core.resize(c->ns);
+  for (int i = 0; i < c->ns; ++i) {
+    const int t = s->site_type[i] - 1;
+    if (t < 0 || t >= c->nt) return IMAGO_ERR_INVALID;
+    c->site_type[i] = t;
+    c->cum_vale[i] = c->vale_dim;
+    c->cum_core[i] = c->core_dim;
+    c->vale_dim += c->types[t].nvale;
+    c->core_dim += c->types[t].ncore;
+  }
+  c->ptypes.resize(c->npt);
+  int poff = 0;
+  for (int t = 0; t < c->npt; ++t) {
+    HPType &p = c->ptypes[t];
+    p.element = s->pot_type_element[t] - 1;
+    if (p.element < 0) return IMAGO_ERR_INVALID;
+    p.z = s->pot_type_nuc_charge[t];
+    p.nucalpha = s->pot_type_nuc_alpha[t];
+    const int n = s->pot_type_num_alphas[t];
+    if (n <= 0 || !(p.nucalpha > 0.0)) return IMAGO_ERR_INVALID;
+    p.alphas.assign(s->pot_type_alphas + poff, s->pot_type_alphas + poff + n);
+    poff += n;
+    p.cumul = c->pot_dim;
+    c->pot_dim += n;
+    min_pot_alpha = std::min(min_pot_alpha, p.alphas[0]);
+  }
+  c->psite_ptype.resize(c->nps);
+  c->psite_pos.assign(s->pot_site_pos, s->pot_site_pos + 3 * c->nps);
+  for (int i = 0; i < c->nps; ++i) {
+    const int t = s->pot_site_type[i] - 1;
+    if (t < 0 || t >= c->npt) return IMAGO_ERR_INVALID;
+    if (i > 0 && t < c->psite_ptype[i - 1]) return IMAGO_ERR_INVALID;
+    c->psite_ptype[i] = t;
+    if (c->ptypes[t].first_site < 0) c->ptypes[t].first_site = i;
+    c->ptypes[t].mult += 1;
+  }
+  // Screening tables are built per element from the first type (and first
+  // potential type) of that element (gaussRelations.f90:85-100,158-173).
+  c->type_screen.resize(c->nt);
+  for (int t = 0; t < c->nt; ++t) {
+    int f = t;
+    for (int u = 0; u < t; ++u)
+      if (c->types[u].element == c->types[t].element) { f = u; break; }
+    c->type_screen[t] = f;
+    if (c->types[f].nalpha < c->types[t].nalpha) return IMAGO_ERR_INVALID;
+  }
+  c->ptype_screen.resize(c->npt);
+  for (int t = 0; t < c->npt; ++t) {
+    int f = t;
+    for (int u = 0; u < t; ++u)
+      if (c->ptypes[u].element == c->ptypes[t].element) { f = u; break; }
+    c->ptype_screen[t] = f;
+    if (c->ptypes[f].alphas.size() < c->ptypes[t].alphas.size())
+      return IMAGO_ERR_INVALID;
+  }
+  int rc = make_cells(c, min_atom_alpha, min_pot_alpha);
+  if (rc) return rc;
+  c->kxyz.resize(3 * c->nk);
+  for (int k = 0; k < c->nk; ++k) {
+    const double *f = s->kpoints_abc + 3 * k;
+    for (int x = 0; x < 3; ++x)
+      c->kxyz[3 * k + x] = f[0] * c->recip[x] + f[1] * c->recip[3 + x] +
+                           f[2] * c->recip[6 + x];
+  }
+  return IMAGO_OK;
+}
+
+// The pair / image / alpha-pair screens of integrals.F90:323-569.
+int build_work(imago_ctx *c) {
+  c->pairs.clear();
+  c->units.clear();
+  c->sps.clear();
+  long long moff = 0, boff = 0;
+  for (int i = 0; i < c->ns; ++i)
+    for (int j = i; j < c->ns; ++j) {
+      DPair p{};
+      p.i = i;
+      p.j = j;
+      p.ti = c->site_type[i];
+      p.tj = c->site_type[j];
+      const HType &t1 = c->types[p.ti], &t2 = c->types[p.tj];
+      const HType &s1 = c->types[c->type_screen[p.ti]];
+      const HType &s2 = c->types[c->type_screen[p.tj]];
+      p.ni = t1.nstates;
+      p.nj = t2.nstates;
+      const double *A = &c->site_pos[3 * i], *B = &c->site_pos[3 * j];
+      double dv[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+      nearest_lattice_host(c, dv, p.L0);
+      double r02 = 0.0;
+      for (int x = 0; x < 3; ++x)
+        r02 += (A[x] - B[x] - p.L0[x]) * (A[x] - B[x] - p.L0[x]);
+      auto adist = [&](int a, int b) {
+        const double x1 = s1.alphas[a], x2 = s2.alphas[b];
+        return c->T / x2 / (x1 / (x1 + x2));
+      };
+      const double lim = adist(0, 0);
+      p.ubeg = (int)c->units.size();
+      p.moff = moff;
+      if (r02 <= lim) {
+        const double maxr = r02 + lim + 2.0 * std::sqrt(r02 * lim);
+        if (maxr > c->csize[c->ncell - 1]) return IMAGO_ERR_CELL_LIST;
+        for (int k = 0; k < c->ncell; ++k) {
+          if (c->csize[k] > maxr) break;
+          double r2 = 0.0;
+          for (int x = 0; x < 3; ++x) {
+            const double bp = B[x] + p.L0[x] + c->cells[3 * k + x];
+            r2 += (A[x] - bp) * (A[x] - bp);
+          }
+          if (r2 > lim) continue;
+          DUnit u{};
+          u.pair = (int)c->pairs.size();
+          u.cell = k;
+          u.r2 = r2;
+          u.spbeg = (int)c->sps.size();
+          const int nmin = std::min(t1.nalpha, t2.nalpha);
+          for (int l = 0; l < nmin; ++l) {
+            int mode = 0, a = l, b = l;
+            if (adist(l, l) < r2) break;
+            for (;;) {
+              if (mode == 1) {
+                ++a;
+                if (a >= t1.nalpha) { mode = 2; a = l; continue; }
+              } else if (mode == 2) {
+                ++b;
+                if (b >= t2.nalpha) break;
+              }
+              if (adist(a, b) < r2) {
+                if (mode == 1) { mode = 2; a = l; continue; }
+                break;
+              }
+              if (mode == 0) mode = 1;
+              DSp sp{};
+              sp.unit = (int)c->units.size();
+              sp.a = (short)a;
+              sp.b = (short)b;
+              sp.la = (short)t1.cls[a];
+              sp.lb = (short)t2.cls[b];
+              sp.boff = boff;
+              boff += nsh(sp.la) * nsh(sp.lb);
+              c->sps.push_back(sp);
+            }
+          }
+          u.spend = (int)c->sps.size();
+          c->units.push_back(u);
+        }
+      }
+      p.uend = (int)c->units.size();
+      moff += (long long)(p.uend - p.ubeg) * p.ni * p.nj;
+      c->pairs.push_back(p);
+    }
+  c->blk_total = boff;
+  c->m_total = moff;
+  // shell pairs by class, stable in unit order
+  std::vector<int> idx(c->sps.size());
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+    return c->sps[x].la * 4 + c->sps[x].lb < c->sps[y].la * 4 + c->sps[y].lb;
+  });
+  c->sp_by_cls = idx;
+  for (int k = 0; k <= 16; ++k) c->cls_beg[k] = 0;
+  for (const DSp &sp : c->sps) c->cls_beg[sp.la * 4 + sp.lb + 1] += 1;
+  for (int k = 0; k < 16; ++k) c->cls_beg[k + 1] += c->cls_beg[k];
+  // EP terms in the reference's order (cumulAlphaSum + alpha index)
+  c->ep_terms.clear();
+  for (int t = 0; t < c->npt; ++t)
+    for (int j = 0; j < (int)c->ptypes[t].alphas.size(); ++j)
+      c->ep_terms.push_back({0, t, j});
+  return IMAGO_OK;
+}
+
+int upload(imago_ctx *c) {
+  cudaStream_t st = c->stream;
+  std::vector<int> nalpha, aoff, nstates, nvale, soff, boff, cls, lm;
+  std::vector<double> alpha, basis;
+  for (const HType &t : c->types) {
+    nalpha.push_back(t.nalpha);
+    aoff.push_back((int)alpha.size());
+    nstates.push_back(t.nstates);
+    nvale.push_back(t.nvale);
+    soff.push_back((int)lm.size());
+    boff.push_back((int)basis.size());
+    alpha.insert(alpha.end(), t.alphas.begin(), t.alphas.end());
+    cls.insert(cls.end(), t.cls.begin(), t.cls.end());
+    lm.insert(lm.end(), t.lm.begin(), t.lm.end());
+    basis.insert(basis.end(), t.basis.begin(), t.basis.end());
+  }
+  std::vector<int> paoff, pn, pfirst, pmult;
+  std::vector<double> pz, pnuc, palpha;
+  for (const HPType &p : c->ptypes) {
+    paoff.push_back((int)palpha.size());
+    pn.push_back((int)p.alphas.size());
+    pfirst.push_back(p.first_site < 0 ? 0 : p.first_site);
+    pmult.push_back(p.mult);
+    pz.push_back(p.z);
+    pnuc.push_back(p.nucalpha);
+    palpha.insert(palpha.end(), p.alphas.begin(), p.alphas.end());
+  }
+  int rc = 0;
+#define UP(buf, vec) \
+  if ((rc = c->buf.upload(vec, st))) return rc;
+  UP(d_type_nalpha, nalpha) UP(d_type_alpha_off, aoff) UP(d_type_nstates, nstates)
+  UP(d_type_nvale, nvale) UP(d_type_state_off, soff) UP(d_type_basis_off, boff)
+  UP(d_type_screen, c->type_screen) UP(d_alpha_cls, cls) UP(d_state_lm, lm)
+  UP(d_alpha, alpha) UP(d_basis, basis) UP(d_site_pos, c->site_pos)
+  UP(d_site_type, c->site_type) UP(d_site_cum_vale, c->cum_vale)
+  UP(d_site_cum_core, c->cum_core) UP(d_ptype_z, pz) UP(d_ptype_nucalpha, pnuc)
+  UP(d_palpha, palpha) UP(d_ptype_alpha_off, paoff) UP(d_ptype_nalpha, pn)
+  UP(d_ptype_first_site, pfirst) UP(d_ptype_mult, pmult)
+  UP(d_ptype_screen, c->ptype_screen) UP(d_psite_pos, c->psite_pos)
+  UP(d_psite_ptype, c->psite_ptype) UP(d_cell, c->cells) UP(d_csize, c->csize)
+  UP(d_kxyz, c->kxyz) UP(d_pairs, c->pairs) UP(d_units, c->units)
+  UP(d_sps, c->sps) UP(d_sp_by_cls, c->sp_by_cls) UP(d_terms, c->ep_terms)
+#undef UP
+  if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk))) return rc;
+
+  DevSys &s = c->sys;
+  s.nt = c->nt; s.ns = c->ns; s.npt = c->npt; s.nps = c->nps; s.nk = c->nk;
+  s.ncell = c->ncell; s.vale_dim = c->vale_dim; s.core_dim = c->core_dim;
+  s.T = c->T;
+  std::memcpy(s.rv, c->rv, sizeof s.rv);
+  std::memcpy(s.inv, c->inv, sizeof s.inv);
+  s.type_nalpha = c->d_type_nalpha.p; s.type_alpha_off = c->d_type_alpha_off.p;
+  s.type_nstates = c->d_type_nstates.p; s.type_nvale = c->d_type_nvale.p;
+  s.type_state_off = c->d_type_state_off.p; s.type_basis_off = c->d_type_basis_off.p;
+  s.type_screen = c->d_type_screen.p; s.alpha = c->d_alpha.p;
+  s.alpha_cls = c->d_alpha_cls.p; s.state_lm = c->d_state_lm.p; s.basis = c->d_basis.p;
+  s.site_pos = c->d_site_pos.p; s.site_type = c->d_site_type.p;
+  s.site_cum_vale = c->d_site_cum_vale.p; s.site_cum_core = c->d_site_cum_core.p;
+  s.ptype_z = c->d_ptype_z.p; s.ptype_nucalpha = c->d_ptype_nucalpha.p;
+  s.palpha = c->d_palpha.p; s.ptype_alpha_off = c->d_ptype_alpha_off.p;
+  s.ptype_nalpha = c->d_ptype_nalpha.p; s.ptype_first_site = c->d_ptype_first_site.p;
+  s.ptype_mult = c->d_ptype_mult.p; s.ptype_screen = c->d_ptype_screen.p;
+  s.psite_pos = c->d_psite_pos.p; s.psite_ptype = c->d_psite_ptype.p;
+  s.cell = c->d_cell.p; s.csize = c->d_csize.p; s.kxyz = c->d_kxyz.p;
+  s.phase = c->d_phase.p;
+  DevWork &w = c->work;
+  w.npairs = (int)c->pairs.size();
+  w.nunits = (int)c->units.size();
+  w.nsp = (int)c->sps.size();
+  w.pairs = c->d_pairs.p; w.units = c->d_units.p; w.sps = c->d_sps.p;
+  w.sp_by_cls = c->d_sp_by_cls.p;
+  w.blk_total = c->blk_total;
+  w.m_total = c->m_total;
+  return launch_phase(s, c->d_phase.p, st);
+}
+
+// Device bytes one term of a build needs between its stages.
+size_t term_bytes(const imago_ctx *c) {
+  const size_t V = c->vale_dim, C = c->core_dim, nk = c->nk;
+  return sizeof(double) * (size_t)(c->blk_total + c->m_total) +
+         sizeof(double2) * nk * (V * V + 2 * V * C + C * C) +
+         sizeof(double2) * nk * (V * (V + 1) / 2);
+}
+
+int ensure_scratch(imago_ctx *c, int nterm) {
+  const size_t V = c->vale_dim, C = c->core_dim, nk = c->nk;
+  int rc;
+  if ((rc = c->blk.alloc((size_t)c->blk_total * nterm + 1))) return rc;
+  if ((rc = c->M.alloc((size_t)c->m_total * nterm + 1))) return rc;
+  if ((rc = c->vv.alloc(nk * V * V * nterm + 1))) return rc;
+  if ((rc = c->cv.alloc(nk * V * C * nterm + 1))) return rc;
+  if ((rc = c->cc.alloc(nk * C * C * nterm + 1))) return rc;
+  if ((rc = c->y.alloc(nk * V * C * nterm + 1))) return rc;
+  return IMAGO_OK;
+}
+
+enum Kind { KIND_OL = 0, KIND_KE = 1, KIND_NP = 2, KIND_EP = 3 };
+
+// One build of `nterm` matrices of one kind, writing packed output to
+// `packed_dev` (device) [nterm][nk][np][2].
+cudaEvent_t next_event(imago_ctx *c) {
+  if (c->kev_used == (int)c->kev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    c->kev.push_back(e);
+  }
+  return c->kev[c->kev_used++];
+}
+
+void mark(imago_ctx *c) {
+  cudaEvent_t e = next_event(c);
+  if (e) cudaEventRecord(e, c->stream);
+}
+
+int class_launches(const imago_ctx *c) {
+  int n = 0;
+  for (int k = 0; k < 16; ++k) n += c->cls_beg[k + 1] > c->cls_beg[k];
+  return n;
+}
+
+int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
+              double *packed_dev) {
+  cudaStream_t st = c->stream;
+  int rc = ensure_scratch(c, nterm);
+  if (rc) return rc;
+  const DevSys &s = c->sys;
+  const DevWork &w = c->work;
+  c->launches += class_launches(c) + 2 + (c->core_dim > 0 ? 2 : 1);
+  mark(c);
+  if (kind == KIND_OL || kind == KIND_KE) {
+    rc = launch_prim2c(s, w, c->cls_beg, kind == KIND_KE, c->blk.p, st);
+  } else if (kind == KIND_NP) {
+    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, c->blk.p, st);
+  } else {
+    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + term0, nterm, false,
+                       c->blk.p, st);
+  }
+  if (rc) return rc;
+  mark(c);
+  if ((rc = launch_contract(s, w, nterm, c->blk.p, c->M.p, st))) return rc;
+  mark(c);
+  if ((rc = launch_bloch(s, w, nterm, c->M.p, c->vv.p, c->cv.p, c->cc.p, st)))
+    return rc;
+  mark(c);
+  if (kind == KIND_OL && c->core_dim > 0) {
+    const size_t n = (size_t)c->nk * c->vale_dim * c->core_dim;
+    if ((rc = c->s_cv.alloc(n))) return rc;
+    IMAGO_CUDA(cudaMemcpyAsync(c->s_cv.p, c->cv.p, n * sizeof(double2),
+                               cudaMemcpyDeviceToDevice, st));
+  }
+  rc = launch_ortho(s, nterm, c->vv.p, c->cv.p, c->cc.p, c->s_cv.p, c->y.p,
+                    packed_dev, st);
+  mark(c);
+  return rc;
+}
+
+int copy_out(imago_ctx *c, double *dst, const double *src, size_t n) {
+  if (!dst) return IMAGO_OK;
+  IMAGO_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                             c->outputs_on_device ? cudaMemcpyDeviceToDevice
+                                                  : cudaMemcpyDeviceToHost,
+                             c->stream));
+  return IMAGO_OK;
+}
+
+size_t packed_doubles(const imago_ctx *c) {
+  return (size_t)2 * c->nk * ((size_t)c->vale_dim * (c->vale_dim + 1) / 2);
+}
+
+// Destination for a build's packed output: the caller's device buffer
+// directly, or a device staging buffer copied out afterwards.
+double *packed_target(imago_ctx *c, double *user, int nterm, int *rc) {
+  if (c->outputs_on_device && user) return user;
+  *rc = c->packed_stage.alloc(packed_doubles(c) * nterm);
+  return c->packed_stage.p;
+}
+
+int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
+  int rc = IMAGO_OK;
+  double *tgt = packed_target(c, packed, 1, &rc);
+  if (rc) return rc;
+  if ((rc = run_build(c, KIND_OL, 0, 1, tgt))) return rc;
+  c->have_ol = true;
+  if (tgt != packed && (rc = copy_out(c, packed, tgt, packed_doubles(c)))) return rc;
+  const size_t ncv = (size_t)c->nk * c->vale_dim * c->core_dim;
+  if (ncv && (cv_re || cv_im)) {
+    double *re = cv_re, *im = cv_im;
+    if (!c->outputs_on_device) {
+      // stage the split through the y buffer
+      re = reinterpret_cast<double *>(c->y.p);
+      im = re + ncv;
+    }
+    if ((rc = launch_split_cv(c->sys, c->s_cv.p, re, im, c->stream))) return rc;
+    c->launches += 1;
+    if (!c->outputs_on_device) {
+      if ((rc = copy_out(c, cv_re, re, ncv))) return rc;
+      if ((rc = copy_out(c, cv_im, im, ncv))) return rc;
+    }
+  }
+  return IMAGO_OK;
+}
+
+int do_simple(imago_ctx *c, Kind kind, double *packed) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  int rc = IMAGO_OK;
+  double *tgt = packed_target(c, packed, 1, &rc);
+  if (rc) return rc;
+  if ((rc = run_build(c, kind, 0, 1, tgt))) return rc;
+  if (tgt != packed) rc = copy_out(c, packed, tgt, packed_doubles(c));
+  return rc;
+}
+
+int do_ep(imago_ctx *c, double *packed) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  const int nterm = c->pot_dim;
+  size_t budget = c->scratch_bytes;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    budget = fr / 4;
+  }
+  const size_t per = term_bytes(c);
+  int chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
+  chunk = std::min(chunk, nterm);
+  const size_t npd = packed_doubles(c);
+  for (int t0 = 0; t0 < nterm; t0 += chunk) {
+    const int n = std::min(chunk, nterm - t0);
+    int rc = IMAGO_OK;
+    double *user = packed ? packed + npd * t0 : nullptr;
+    double *tgt = packed_target(c, user, n, &rc);
+    if (rc) return rc;
+    if ((rc = run_build(c, KIND_EP, t0, n, tgt))) return rc;
+    if (tgt != user && (rc = copy_out(c, user, tgt, npd * n))) return rc;
+  }
+  return IMAGO_OK;
+}
+
+void begin_call(imago_ctx *c) {
+  c->kev_used = 0;
+  c->launches = 0;
+}
+
+int finish(imago_ctx *c, int rc) {
+  if (rc != IMAGO_OK) {
+    cudaStreamSynchronize(c->stream);
+    cudaGetLastError();
+    return rc;
+  }
+  IMAGO_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 4; ++k) c->kernel_ms[k] = 0.0;
+  for (int b = 0; b + 4 < c->kev_used; b += 5)
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->kev[b + k], c->kev[b + k + 1]) == cudaSuccess)
+        c->kernel_ms[k] += ms;
+      else
+        cudaGetLastError();
+    }
+  return IMAGO_OK;
+}
+
+int set_device(imago_ctx *c) {
+  IMAGO_CUDA(cudaSetDevice(c->device));
+  return IMAGO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int imago_intg_create(const imago_system *sys, const imago_opts *opts,
+                      imago_ctx **out_ctx) {
+  if (!out_ctx) return IMAGO_ERR_INVALID;
+  *out_ctx = nullptr;
+  imago_ctx *c = new (std::nothrow) imago_ctx();
+  if (!c) return IMAGO_ERR_NOMEM;
+  if (opts) {
+    c->device = opts->device;
+    c->outputs_on_device = opts->outputs_on_device;
+    c->scratch_bytes = opts->scratch_bytes;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c->device) {
+    cudaGetLastError();
+    delete c;
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess ||
+      prop.major != 10) {
+    cudaGetLastError();
+    delete c;
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  int rc = set_device(c);
+  if (!rc) rc = read_system(c, sys);
+  if (!rc) rc = build_work(c);
+  if (!rc) {
+    if (opts && opts->stream) {
+      c->stream = (cudaStream_t)opts->stream;
+    } else {
+      if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) !=
+          cudaSuccess)
+        rc = IMAGO_ERR_CUDA;
+      c->own_stream = true;
+    }
+  }
+  if (!rc) {
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    c->events = true;
+    rc = upload(c);
+  }
+  if (!rc) rc = finish(c, rc);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out_ctx = c;
+  return IMAGO_OK;
+}
+
+int imago_intg_dims(const imago_ctx *c, imago_dims *d) {
+  if (!c || !d) return IMAGO_ERR_INVALID;
+  d->vale_dim = c->vale_dim;
+  d->core_dim = c->core_dim;
+  d->num_kpoints = c->nk;
+  d->pot_dim = c->pot_dim;
+  d->num_cells = c->ncell;
+  d->packed = (long long)c->vale_dim * (c->vale_dim + 1) / 2;
+  d->num_pair_images = (long long)c->units.size();
+  d->num_shell_pairs = (long long)c->sps.size();
+  d->block_elements = c->m_total;
+  return IMAGO_OK;
+}
+
+int imago_gauss_overlap_ol(imago_ctx *c, double *packed, double *cv_re,
+                           double *cv_im) {
+  if (!c) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  begin_call(c);
+  cudaEventRecord(c->ev[0], c->stream);
+  rc = do_ol(c, packed, cv_re, cv_im);
+  cudaEventRecord(c->ev[1], c->stream);
+  rc = finish(c, rc);
+  if (!rc) cudaEventElapsedTime(&c->stage_ms[0], c->ev[0], c->ev[1]);
+  return rc;
+}
+
+int imago_gauss_overlap_ke(imago_ctx *c, double *packed) {
+  if (!c) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  begin_call(c);
+  cudaEventRecord(c->ev[2], c->stream);
+  rc = do_simple(c, KIND_KE, packed);
+  cudaEventRecord(c->ev[3], c->stream);
+  rc = finish(c, rc);
+  if (!rc) cudaEventElapsedTime(&c->stage_ms[1], c->ev[2], c->ev[3]);
+  return rc;
+}
+
+int imago_gauss_overlap_np(imago_ctx *c, double *packed) {
+  if (!c) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  begin_call(c);
+  cudaEventRecord(c->ev[4], c->stream);
+  rc = do_simple(c, KIND_NP, packed);
+  cudaEventRecord(c->ev[5], c->stream);
+  rc = finish(c, rc);
+  if (!rc) cudaEventElapsedTime(&c->stage_ms[2], c->ev[4], c->ev[5]);
+  return rc;
+}
+
+int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
+  if (!c) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  begin_call(c);
+  cudaEventRecord(c->ev[6], c->stream);
+  rc = do_ep(c, packed);
+  cudaEventRecord(c->ev[7], c->stream);
+  rc = finish(c, rc);
+  if (!rc) cudaEventElapsedTime(&c->stage_ms[3], c->ev[6], c->ev[7]);
+  return rc;
+}
+
+int imago_intg_build(imago_ctx *c, unsigned which, const imago_out *out) {
+  if (!c || !out) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  begin_call(c);
+  if (which & IMAGO_OL) {
+    cudaEventRecord(c->ev[0], c->stream);
+    rc = do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im);
+    cudaEventRecord(c->ev[1], c->stream);
+  }
+  if (!rc && (which & IMAGO_KE)) {
+    cudaEventRecord(c->ev[2], c->stream);
+    rc = do_simple(c, KIND_KE, out->ke_packed);
+    cudaEventRecord(c->ev[3], c->stream);
+  }
+  if (!rc && (which & IMAGO_NP)) {
+    cudaEventRecord(c->ev[4], c->stream);
+    rc = do_simple(c, KIND_NP, out->np_packed);
+    cudaEventRecord(c->ev[5], c->stream);
+  }
+  if (!rc && (which & IMAGO_EP)) {
+    cudaEventRecord(c->ev[6], c->stream);
+    rc = do_ep(c, out->ep_packed);
+    cudaEventRecord(c->ev[7], c->stream);
+  }
+  rc = finish(c, rc);
+  if (!rc)
+    for (int s = 0; s < 4; ++s)
+      if (which & (1u << s))
+        cudaEventElapsedTime(&c->stage_ms[s], c->ev[2 * s], c->ev[2 * s + 1]);
+  return rc;
+}
+
+int imago_intg_stage_ms(const imago_ctx *c, double ms[4]) {
+  if (!c || !ms) return IMAGO_ERR_INVALID;
+  for (int s = 0; s < 4; ++s) ms[s] = c->stage_ms[s];
+  return IMAGO_OK;
+}
+
+int imago_intg_kernel_stats(const imago_ctx *c, double ms[4],
+                            long long *launches) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (ms)
+    for (int k = 0; k < 4; ++k) ms[k] = c->kernel_ms[k];
+  if (launches) *launches = c->launches;
+  return IMAGO_OK;
+}
+
+void imago_intg_destroy(imago_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+const char *imago_strerror(int status) {
+  switch (status) {
+    case IMAGO_OK: return "success";
+    case IMAGO_ERR_INVALID: return "invalid system description or argument";
+    case IMAGO_ERR_CELL_LIST:
+      return "More lattice points needed for this atom overlap pair";
+    case IMAGO_ERR_NEED_OVERLAP:
+      return "the overlap (OL) build must run before KE/NP/EP when coreDim > 0";
+    case IMAGO_ERR_NOMEM: return "out of memory";
+    case IMAGO_ERR_CUDA: return "CUDA error";
+    case IMAGO_ERR_TIMEOUT: return "a bounded device wait gave up";
+    case IMAGO_ERR_NO_DEVICE: return "no CUDA device of compute capability 10.x";
+    case IMAGO_ERR_RANGE: return "argument out of range";
+    default: return "unknown status";
+  }
+}
+
+int imago_kpoint_mesh(const int n[3], const double shift[3],
+                      double *kpoints_abc) {
+  if (!n || !shift || !kpoints_abc) return IMAGO_ERR_INVALID;
+  if (n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return IMAGO_ERR_RANGE;
+  const double delta[3] = {1.0 / n[0], 1.0 / n[1], 1.0 / n[2]};
+  long long m = 0;
+  for (int i = 1; i <= n[0]; ++i)
+    for (int j = 1; j <= n[1]; ++j)
+      for (int k = 1; k <= n[2]; ++k, ++m) {
+        const int idx[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a)
+          kpoints_abc[3 * m + a] = -0.5 + (idx[a] - 1.0 + shift[a]) * delta[a];
+      }
+  return IMAGO_OK;
+}
+
+int imago_prim_eval(int kind, int n, const double *params, const int *cls,
+                    double *sh) {
+  if (kind < 0 || kind > 4 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
+  if (kind < 4 && !cls) return IMAGO_ERR_INVALID;
+  if (n == 0) return IMAGO_OK;
+  for (int r = 0; kind < 4 && r < n; ++r)
+    if (cls[2 * r] < 0 || cls[2 * r] > 3 || cls[2 * r + 1] < 0 || cls[2 * r + 1] > 3)
+      return IMAGO_ERR_RANGE;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  double *dp = nullptr, *ds = nullptr;
+  int *dc = nullptr;
+  int rc = IMAGO_OK;
+  if (cudaMalloc(&dp, sizeof(double) * 12 * n) != cudaSuccess ||
+      cudaMalloc(&ds, sizeof(double) * 256 * n) != cudaSuccess ||
+      cudaMalloc(&dc, sizeof(int) * 2 * n) != cudaSuccess) {
+    rc = IMAGO_ERR_NOMEM;
+  }
+  if (!rc && cudaMemcpy(dp, params, sizeof(double) * 12 * n,
+                        cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  if (!rc && kind < 4 &&
+      cudaMemcpy(dc, cls, sizeof(int) * 2 * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  if (!rc && kind == 4) cudaMemset(dc, 0, sizeof(int) * 2 * n);
+  if (!rc) rc = launch_prim_eval(kind, n, dp, dc, ds, 0);
+  if (!rc && cudaMemcpy(sh, ds, sizeof(double) * 256 * n,
+                        cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  cudaFree(dp);
+  cudaFree(ds);
+  cudaFree(dc);
+  cudaGetLastError();
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+// intg.cuh -- device-side system description, work lists and kernel
+// launchers of the B200 integral setup.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace imago {
+
+// Everything the kernels read about the system, as device pointers.
+struct DevSys {
+  int nt, ns, npt, nps, nk, ncell;
+  int vale_dim, core_dim;
+  double T;            // logBasisFnThresh = -ln(basisFnConvg)
+  double rv[9];        // realVectors [abc*3 + xyz]
+  double inv[9];       // invRealVectors [abc*3 + xyz]
+  // atom types
+  const int *type_nalpha, *type_alpha_off, *type_nstates, *type_nvale,
+      *type_state_off, *type_basis_off, *type_screen;
+  const double *alpha;
+  const int *alpha_cls;   // 0..3
+  const int *state_lm;    // 0-based lm per state
+  const double *basis;    // [basis_off + a * nstates + m]
+  // atom sites
+  const double *site_pos;
+  const int *site_type, *site_cum_vale, *site_cum_core;
+  // potential types and sites
+  const double *ptype_z, *ptype_nucalpha, *palpha;
+  const int *ptype_alpha_off, *ptype_nalpha, *ptype_first_site, *ptype_mult,
+      *ptype_screen;
+  const double *psite_pos;
+  const int *psite_ptype;
+  // lattice cells sorted by |R|^2, k-points, phase table
+  const double *cell;     // [n*3]
+  const double *csize;    // [n]
+  const double *kxyz;     // [nk*3]
+  const double2 *phase;   // [cell * nk + k]  exp(i k.R)
+};
+
+// Atom pair (i <= j) that passes the nearest-image screen.
+struct DPair {
+  int i, j, ti, tj;
+  int ni, nj;             // total states of the two atoms
+  int ubeg, uend;         // units [ubeg, uend)
+  double L0[3];           // nearest lattice vector to pos_i - pos_j
+  long long moff;         // first element of the pair's unit blocks
+};
+
+// (pair, lattice image) within the pair cutoff.
+struct DUnit {
+  int pair, cell;
+  int spbeg, spend;       // shell pairs [spbeg, spend), staircase order
+  double r2;              // |A - B'|^2
+};
+
+// Screened primitive pair of one unit.
+struct DSp {
+  int unit;
+  short a, b;             // alpha indices (0-based)
+  short la, lb;           // classes
+  long long boff;         // offset of its sh block in a term's block buffer
+};
+
+struct DevWork {
+  int npairs, nunits, nsp;
+  const DPair *pairs;
+  const DUnit *units;
+  const DSp *sps;
+  const int *sp_by_cls;   // shell pairs sorted by class (la*4+lb), then unit
+  long long blk_total;    // doubles of sh blocks per term
+  long long m_total;      // doubles of unit blocks per term
+};
+
+// Term of a three-centre build: NP is one term over all sites; EP term j of
+// potential type t has alpha index j.
+struct Term3c {
+  int nuclear;            // 1: NP
+  int ptype, j;           // EP only
+};
+
+// Launchers (kernels.cu).  All take the stream to run on.
+int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
+                  bool kinetic, double *blk, cudaStream_t st);
+int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
+                  const Term3c *terms_dev, int nterm, bool nuclear,
+                  double *blk, cudaStream_t st);
+int launch_contract(const DevSys &s, const DevWork &w, int nterm,
+                    const double *blk, double *M, cudaStream_t st);
+int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
+                 double2 *vv, double2 *cv, double2 *cc, cudaStream_t st);
+int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
+                 const double2 *cv, const double2 *cc, const double2 *s_cv,
+                 double2 *y, double *packed, cudaStream_t st);
+int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
+                    cudaStream_t st);
+int launch_phase(const DevSys &s, double2 *phase, cudaStream_t st);
+int launch_prim_eval(int kind, int n, const double *params, const int *cls,
+                     double *sh, cudaStream_t st);
+
+}  // namespace imago

@@ -1,0 +1,289 @@
+// k_prim.cu -- primitive shell-pair blocks per class.
+//
+// Shell pairs are sorted by class; each s/p/d class runs a fully unrolled
+// kernel, the f classes share runtime-class kernels.
+#include "geom.cuh"
+#include "prim.cuh"
+
+namespace imago {
+
+// ------------------------------------------------------------ prim2c --
+template <int LA, int LB, bool KIN>
+__global__ void __launch_bounds__(128)
+    k_prim2c(DevSys s, DevWork w, int beg, int end, double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  prim2c<LA, LB, KIN>(q.a1, q.a2, q.A, q.B, blk + sp.boff);
+}
+
+// ------------------------------------------------------------ prim3c --
+// One thread per (shell pair, term).  The site and lattice-image loops are
+// those of nuclearPE (integrals.F90:2533-2698) and electronicPE
+// (2700-2858): a closest-image screen per site, then the images of that
+// site within threeAlphaDist of the overlap centre, in |R| order.
+template <int LA, int LB, bool NUC>
+__global__ void __launch_bounds__(128)
+    k_prim3c(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
+             int nterm, double *blk) {
+  constexpr int L = LA + LB;
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * nterm) return;
+  const int tl = (int)(g / n);
+  const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
+  const SpGeom q = sp_geom(s, w, sp);
+  const Term3c tm = terms[tl];
+
+  // alphaDist / alphaCenter (gaussRelations.f90:112-131) from the element's
+  // first-type exponents, as the reference tables are built.
+  const double cen = q.a1s / (q.a1s + q.a2s);
+  const double adist = s.T / q.a2s / cen;
+  const double frac = 1 - q.r2 / adist;
+  double Ps[3], Pt[3];
+  const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
+    Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+  }
+  double Q[nherm(L)];
+#pragma unroll
+  for (int i = 0; i < nherm(L); ++i) Q[i] = 0.0;
+
+  int s0, s1;
+  double tcut = 0.0, a3 = 0.0;
+  if (NUC) {
+    s0 = 0;
+    s1 = s.nps;
+  } else {
+    const int pt = tm.ptype;
+    s0 = s.ptype_first_site[pt];
+    s1 = s0 + s.ptype_mult[pt];
+    a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
+    const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
+    // alphaPotDist (gaussRelations.f90:187-196)
+    tcut = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
+  }
+  const double z3e = zeta + a3, mue = zeta * a3 / z3e;
+
+  for (int site = s0; site < s1; ++site) {
+    double w0 = 1.0, mu = mue, nu = 0.0, t = tcut;
+    if (NUC) {
+      const int pt = s.psite_ptype[site];
+      const double Z = s.ptype_z[pt];
+      if (Z < kSmallThresh) continue;
+      const double an = s.ptype_nucalpha[pt];
+      const double ans = s.ptype_nucalpha[s.ptype_screen[pt]];
+      // alphaNucDist (gaussRelations.f90:262-270)
+      t = frac * (s.T * (q.a1s + q.a2s + ans) / (q.a1s + q.a2s) / ans);
+      const double z3 = zeta + an;
+      mu = zeta * an / z3;
+      nu = zeta * zeta / z3;
+      w0 = -Z * (2.0 * kPi / z3);
+    }
+    const double *C = s.psite_pos + 3 * site;
+    double d[3], L2[3], v[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) d[x] = Ps[x] - C[x];
+    nearest_lattice(s, d, L2);
+    double c0 = 0.0;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      v[x] = Ps[x] - C[x] - L2[x];
+      c0 += v[x] * v[x];
+    }
+    if (c0 > t) continue;
+    const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+    for (int nc = 0; nc < s.ncell; ++nc) {
+      if (s.csize[nc] > maxr) break;
+      const double *R = s.cell + 3 * nc;
+      const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+      if (dx * dx + dy * dy + dz * dz > t) continue;
+      double X[3];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+      if (NUC)
+        accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
+      else
+        accumulate_overlap_q<L>(X, mu, 1.0, Q);
+    }
+  }
+  const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
+  hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q,
+                        blk + (long long)tl * w.blk_total + sp.boff);
+}
+
+// f classes: one runtime-class kernel each for 2C and 3C.
+template <bool KIN>
+__global__ void __launch_bounds__(128)
+    k_prim2c_rt(DevSys s, DevWork w, int beg, int end, int la, int lb,
+                double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  prim2c_rt(la, lb, KIN, q.a1, q.a2, q.A, q.B, blk + sp.boff);
+}
+
+template <bool NUC>
+__global__ void __launch_bounds__(128)
+    k_prim3c_rt(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
+                int nterm, int la, int lb, double *blk) {
+  const int L = la + lb;
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * nterm) return;
+  const int tl = (int)(g / n);
+  const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
+  const SpGeom q = sp_geom(s, w, sp);
+  const Term3c tm = terms[tl];
+  const double cen = q.a1s / (q.a1s + q.a2s);
+  const double adist = s.T / q.a2s / cen;
+  const double frac = 1 - q.r2 / adist;
+  double Ps[3], Pt[3];
+  const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
+  for (int x = 0; x < 3; ++x) {
+    Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
+    Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+  }
+  double Q[kMaxHerm];
+  for (int i = 0; i < kMaxHerm; ++i) Q[i] = 0.0;
+  int s0, s1;
+  double tcut = 0.0, a3 = 0.0;
+  if (NUC) {
+    s0 = 0;
+    s1 = s.nps;
+  } else {
+    const int pt = tm.ptype;
+    s0 = s.ptype_first_site[pt];
+    s1 = s0 + s.ptype_mult[pt];
+    a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
+    const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
+    tcut = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
+  }
+  const double z3e = zeta + a3, mue = zeta * a3 / z3e;
+  for (int site = s0; site < s1; ++site) {
+    double w0 = 1.0, mu = mue, nu = 0.0, t = tcut;
+    if (NUC) {
+      const int pt = s.psite_ptype[site];
+      const double Z = s.ptype_z[pt];
+      if (Z < kSmallThresh) continue;
+      const double an = s.ptype_nucalpha[pt];
+      const double ans = s.ptype_nucalpha[s.ptype_screen[pt]];
+      t = frac * (s.T * (q.a1s + q.a2s + ans) / (q.a1s + q.a2s) / ans);
+      const double z3 = zeta + an;
+      mu = zeta * an / z3;
+      nu = zeta * zeta / z3;
+      w0 = -Z * (2.0 * kPi / z3);
+    }
+    const double *C = s.psite_pos + 3 * site;
+    double d[3], L2[3], v[3];
+    for (int x = 0; x < 3; ++x) d[x] = Ps[x] - C[x];
+    nearest_lattice(s, d, L2);
+    double c0 = 0.0;
+    for (int x = 0; x < 3; ++x) {
+      v[x] = Ps[x] - C[x] - L2[x];
+      c0 += v[x] * v[x];
+    }
+    if (c0 > t) continue;
+    const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+    for (int nc = 0; nc < s.ncell; ++nc) {
+      if (s.csize[nc] > maxr) break;
+      const double *R = s.cell + 3 * nc;
+      const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+      if (dx * dx + dy * dy + dz * dz > t) continue;
+      double X[3];
+      for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+      if (NUC)
+        accumulate_nuclear_q_rt(L, X, mu, nu, w0, Q);
+      else
+        accumulate_overlap_q_rt(L, X, mu, 1.0, Q);
+    }
+  }
+  const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
+  hermite_to_sh_rt(la, lb, q.A, q.B, q.a1, q.a2, pref, Q,
+                   blk + (long long)tl * w.blk_total + sp.boff);
+}
+
+template <int LA, int LB>
+static int prim2c_one(const DevSys &s, const DevWork &w, int beg, int end,
+                      bool kin, double *blk, cudaStream_t st) {
+  const int n = end - beg, tb = 128;
+  if (n <= 0) return IMAGO_OK;
+  if (kin)
+    k_prim2c<LA, LB, true><<<(n + tb - 1) / tb, tb, 0, st>>>(s, w, beg, end, blk);
+  else
+    k_prim2c<LA, LB, false><<<(n + tb - 1) / tb, tb, 0, st>>>(s, w, beg, end, blk);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+template <int LA, int LB>
+static int prim3c_one(const DevSys &s, const DevWork &w, int beg, int end,
+                      const Term3c *terms, int nterm, bool nuc, double *blk,
+                      cudaStream_t st) {
+  const int n = end - beg, tb = 128;
+  if (n <= 0 || nterm <= 0) return IMAGO_OK;
+  const long long tot = (long long)n * nterm;
+  const unsigned grid = (unsigned)((tot + tb - 1) / tb);
+  if (nuc)
+    k_prim3c<LA, LB, true><<<grid, tb, 0, st>>>(s, w, beg, n, terms, nterm, blk);
+  else
+    k_prim3c<LA, LB, false><<<grid, tb, 0, st>>>(s, w, beg, n, terms, nterm, blk);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+#define IMAGO_FOR_SPD_CLASSES(M) \
+  M(0, 0) M(0, 1) M(0, 2) M(1, 0) M(1, 1) M(1, 2) M(2, 0) M(2, 1) M(2, 2)
+
+int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
+                  bool kinetic, double *blk, cudaStream_t st) {
+  int rc = IMAGO_OK;
+#define IMAGO_P2(a, b)                                                       \
+  if (rc == IMAGO_OK)                                                       \
+    rc = prim2c_one<a, b>(s, w, cls_beg[a * 4 + b], cls_beg[a * 4 + b + 1], \
+                          kinetic, blk, st);
+  IMAGO_FOR_SPD_CLASSES(IMAGO_P2)
+#undef IMAGO_P2
+  for (int c = 0; c < 16 && rc == IMAGO_OK; ++c) {
+    const int la = c / 4, lb = c % 4;
+    if (la < 3 && lb < 3) continue;
+    const int beg = cls_beg[c], end = cls_beg[c + 1], n = end - beg;
+    if (n <= 0) continue;
+    if (kinetic)
+      k_prim2c_rt<true><<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, end, la, lb, blk);
+    else
+      k_prim2c_rt<false><<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, end, la, lb, blk);
+    IMAGO_CUDA(cudaGetLastError());
+  }
+  return rc;
+}
+
+int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
+                  const Term3c *terms_dev, int nterm, bool nuclear,
+                  double *blk, cudaStream_t st) {
+  int rc = IMAGO_OK;
+#define IMAGO_P3(a, b)                                                        \
+  if (rc == IMAGO_OK)                                                        \
+    rc = prim3c_one<a, b>(s, w, cls_beg[a * 4 + b], cls_beg[a * 4 + b + 1],  \
+                          terms_dev, nterm, nuclear, blk, st);
+  IMAGO_FOR_SPD_CLASSES(IMAGO_P3)
+#undef IMAGO_P3
+  for (int c = 0; c < 16 && rc == IMAGO_OK; ++c) {
+    const int la = c / 4, lb = c % 4;
+    if (la < 3 && lb < 3) continue;
+    const int beg = cls_beg[c], end = cls_beg[c + 1], n = end - beg;
+    if (n <= 0 || nterm <= 0) continue;
+    const long long tot = (long long)n * nterm;
+    const unsigned grid = (unsigned)((tot + 127) / 128);
+    if (nuclear)
+      k_prim3c_rt<true><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev, nterm, la, lb, blk);
+    else
+      k_prim3c_rt<false><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev, nterm, la, lb, blk);
+    IMAGO_CUDA(cudaGetLastError());
+  }
+  return rc;
+}
+
+}  // namespace imago

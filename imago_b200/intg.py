@@ -1,0 +1,266 @@
+"""Python mirror of the integral-setup calls in Imago's setupSCF.
+
+The four builds keep the reference's names and meaning
+(src/imago/imago.F90:262-293):
+
+    gauss_overlap_ol()       -> gaussOverlapOL       (integrals.F90:151)
+    gauss_overlap_ke()       -> gaussOverlapKE       (integrals.F90:656)
+    gauss_overlap_np()       -> gaussOverlapNP       (integrals.F90:1531)
+    elec_pot_gauss_overlap() -> elecPotGaussOverlap  (integrals.F90:2357)
+
+Each returns the packed valence-valence matrices exactly as the reference
+writes them to HDF5: an array [nk, valeDim*(valeDim+1)/2, 2] of (re, im)
+per packed upper-triangle element (EP: one such array per potential term).
+The overlap also returns coreValeOL as (re, im) arrays [nk, valeDim,
+coreDim].  Where the reference would `stop`, these raise ImagoError with
+the reference's message.
+
+All work runs in libimago_b200.so on a compute-capability 10.0 GPU; there
+is no CPU path.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from .system import ImagoDimsC
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libimago_b200.so")
+
+IMAGO_OL, IMAGO_KE, IMAGO_NP, IMAGO_EP = 1, 2, 4, 8
+IMAGO_ERR_NO_DEVICE = 7
+
+_LIB = None
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+class ImagoError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = lib().imago_strerror(status).decode()
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+class ImagoOptsC(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("stream", ctypes.c_void_p),
+                ("outputs_on_device", ctypes.c_int),
+                ("scratch_bytes", ctypes.c_size_t)]
+
+
+class ImagoOutC(ctypes.Structure):
+    _fields_ = [("ol_packed", _D), ("ol_cv_re", _D), ("ol_cv_im", _D),
+                ("ke_packed", _D), ("np_packed", _D), ("ep_packed", _D)]
+
+
+def lib():
+    """Load libimago_b200.so; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m imago_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.imago_intg_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(ImagoOptsC),
+                                        ctypes.POINTER(ctypes.c_void_p)]
+        L.imago_intg_create.restype = ctypes.c_int
+        L.imago_intg_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ImagoDimsC)]
+        L.imago_intg_dims.restype = ctypes.c_int
+        L.imago_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
+        L.imago_gauss_overlap_ol.restype = ctypes.c_int
+        for n in ("imago_gauss_overlap_ke", "imago_gauss_overlap_np",
+                  "imago_elec_pot_gauss_overlap"):
+            getattr(L, n).argtypes = [ctypes.c_void_p, _D]
+            getattr(L, n).restype = ctypes.c_int
+        L.imago_intg_build.argtypes = [ctypes.c_void_p, ctypes.c_uint,
+                                       ctypes.POINTER(ImagoOutC)]
+        L.imago_intg_build.restype = ctypes.c_int
+        L.imago_intg_stage_ms.argtypes = [ctypes.c_void_p, _D]
+        L.imago_intg_stage_ms.restype = ctypes.c_int
+        L.imago_intg_kernel_stats.argtypes = [ctypes.c_void_p, _D,
+                                              ctypes.POINTER(ctypes.c_longlong)]
+        L.imago_intg_kernel_stats.restype = ctypes.c_int
+        L.imago_intg_destroy.argtypes = [ctypes.c_void_p]
+        L.imago_intg_destroy.restype = None
+        L.imago_strerror.argtypes = [ctypes.c_int]
+        L.imago_strerror.restype = ctypes.c_char_p
+        L.imago_kpoint_mesh.argtypes = [ctypes.POINTER(ctypes.c_int), _D, _D]
+        L.imago_kpoint_mesh.restype = ctypes.c_int
+        L.imago_prim_eval.argtypes = [ctypes.c_int, ctypes.c_int, _D,
+                                      ctypes.POINTER(ctypes.c_int), _D]
+        L.imago_prim_eval.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def _check(st, what):
+    if st != 0:
+        raise ImagoError(st, what)
+
+
+def kpoint_mesh(n, shift=(0.0, 0.0, 0.0)):
+    """k-point mesh made by the library (kpoints.f90:896-899, no folding)."""
+    n3 = (ctypes.c_int * 3)(*[int(x) for x in n])
+    sh = np.ascontiguousarray(shift, dtype=np.float64)
+    out = np.zeros((int(np.prod(n)), 3))
+    _check(lib().imago_kpoint_mesh(n3, _p(sh), _p(out)), "imago_kpoint_mesh")
+    return out
+
+
+PRIM_KINDS = {"overlap": 0, "kinetic": 1, "electron3c": 2, "nuclear3c": 3,
+              "boys": 4}
+
+
+def prim_eval(kind, params, cls=None):
+    """Evaluate primitive integrals on the GPU.  params: [n, 12] rows
+    (a1, a2, a3, A, B, C); cls: [n, 2] (l of atom 1, l of atom 2).
+    Returns [n, 16, 16] in the reference's sh layout."""
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, 12)
+    n = len(params)
+    c = (np.ascontiguousarray(cls, dtype=np.int32).reshape(-1, 2) if cls is not None
+         else np.zeros((n, 2), np.int32))
+    out = np.zeros((n, 256))
+    st = lib().imago_prim_eval(PRIM_KINDS[kind], n, _p(params),
+                               c.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                               _p(out))
+    _check(st, "imago_prim_eval")
+    return out.reshape(n, 16, 16)
+
+
+class IntegralSetup:
+    """One system staged on the GPU: imago_intg_create .. imago_intg_destroy.
+
+    outputs_on_device=True makes the build methods take torch CUDA tensors
+    (or raw device pointers) instead of returning numpy arrays."""
+
+    def __init__(self, system, device=0, outputs_on_device=False,
+                 scratch_bytes=0, stream=None):
+        self.system = system
+        self._cs, self._keep = system.to_c()
+        opts = ImagoOptsC(device, stream, 1 if outputs_on_device else 0,
+                          scratch_bytes)
+        self._ctx = ctypes.c_void_p()
+        st = lib().imago_intg_create(ctypes.byref(self._cs), ctypes.byref(opts),
+                                     ctypes.byref(self._ctx))
+        _check(st, "imago_intg_create")
+        d = ImagoDimsC()
+        lib().imago_intg_dims(self._ctx, ctypes.byref(d))
+        self.vale_dim, self.core_dim = d.vale_dim, d.core_dim
+        self.nk, self.pot_dim, self.num_cells = d.num_kpoints, d.pot_dim, d.num_cells
+        self.npacked = int(d.packed)
+        self.num_pair_images = int(d.num_pair_images)
+        self.num_shell_pairs = int(d.num_shell_pairs)
+        self.block_elements = int(d.block_elements)
+        self.outputs_on_device = outputs_on_device
+
+    def close(self):
+        if self._ctx:
+            lib().imago_intg_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- host-output builds (reference layout, numpy) --
+    def _packed(self, n=None):
+        shape = (self.nk, self.npacked, 2) if n is None else (n, self.nk, self.npacked, 2)
+        return np.zeros(shape)
+
+    def gauss_overlap_ol(self):
+        out = self._packed()
+        c = max(self.core_dim, 1)
+        re = np.zeros((self.nk, self.vale_dim, c))
+        im = np.zeros_like(re)
+        _check(lib().imago_gauss_overlap_ol(self._ctx, _p(out), _p(re), _p(im)),
+               "gaussOverlapOL")
+        return out, re[:, :, :self.core_dim], im[:, :, :self.core_dim]
+
+    def gauss_overlap_ke(self):
+        out = self._packed()
+        _check(lib().imago_gauss_overlap_ke(self._ctx, _p(out)), "gaussOverlapKE")
+        return out
+
+    def gauss_overlap_np(self):
+        out = self._packed()
+        _check(lib().imago_gauss_overlap_np(self._ctx, _p(out)), "gaussOverlapNP")
+        return out
+
+    def elec_pot_gauss_overlap(self):
+        out = self._packed(self.pot_dim)
+        _check(lib().imago_elec_pot_gauss_overlap(self._ctx, _p(out)),
+               "elecPotGaussOverlap")
+        return out
+
+    # -- all matrices in one call --
+    def build(self, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP, out=None):
+        """Run the selected builds.  `out` maps ol_packed, ol_cv_re, ol_cv_im,
+        ke_packed, np_packed, ep_packed to numpy arrays (host outputs) or
+        integer device pointers (outputs_on_device).  Returns `out`."""
+        if out is None:
+            out = {}
+            if which & IMAGO_OL:
+                out["ol_packed"] = self._packed()
+                c = max(self.core_dim, 1)
+                out["ol_cv_re"] = np.zeros((self.nk, self.vale_dim, c))
+                out["ol_cv_im"] = np.zeros((self.nk, self.vale_dim, c))
+            if which & IMAGO_KE:
+                out["ke_packed"] = self._packed()
+            if which & IMAGO_NP:
+                out["np_packed"] = self._packed()
+            if which & IMAGO_EP:
+                out["ep_packed"] = self._packed(self.pot_dim)
+        s = ImagoOutC()
+        for name in ("ol_packed", "ol_cv_re", "ol_cv_im", "ke_packed",
+                     "np_packed", "ep_packed"):
+            v = out.get(name)
+            if v is None:
+                setattr(s, name, _D())
+            elif isinstance(v, int):
+                setattr(s, name, ctypes.cast(ctypes.c_void_p(v), _D))
+            elif hasattr(v, "data_ptr"):
+                setattr(s, name, ctypes.cast(ctypes.c_void_p(v.data_ptr()), _D))
+            else:
+                setattr(s, name, _p(v))
+        _check(lib().imago_intg_build(self._ctx, which, ctypes.byref(s)),
+               "imago_intg_build")
+        return out
+
+    def stage_ms(self):
+        ms = np.zeros(4)
+        lib().imago_intg_stage_ms(self._ctx, _p(ms))
+        return ms
+
+    def kernel_stats(self):
+        """(ms by stage [prim, contract, bloch, ortho], kernel launches) of
+        the last build call."""
+        ms = np.zeros(4)
+        n = ctypes.c_longlong()
+        lib().imago_intg_kernel_stats(self._ctx, _p(ms), ctypes.byref(n))
+        return ms, n.value
+
+    def output_bytes(self, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP):
+        per = 16 * self.nk * self.npacked
+        n = 0
+        if which & IMAGO_OL:
+            n += per + 16 * self.nk * self.vale_dim * self.core_dim
+        if which & IMAGO_KE:
+            n += per
+        if which & IMAGO_NP:
+            n += per
+        if which & IMAGO_EP:
+            n += per * self.pot_dim
+        return n

@@ -194,6 +194,7 @@ class ImagoDimsC(ctypes.Structure):
         ("packed", ctypes.c_longlong),
         ("num_pair_images", ctypes.c_longlong),
         ("num_shell_pairs", ctypes.c_longlong),
+        ("block_elements", ctypes.c_longlong),
     ]
 
 

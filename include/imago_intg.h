@@ -36,6 +36,12 @@
 
 #include <stddef.h>
 
+#if defined(__GNUC__)
+#define IMAGO_API __attribute__((visibility("default")))
+#else
+#define IMAGO_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -137,6 +143,8 @@ typedef struct imago_dims {
   long long packed;  /* valeDim*(valeDim+1)/2 */
   long long num_pair_images;  /* (atom pair, lattice image) units within cutoffs */
   long long num_shell_pairs;  /* screened primitive (pair, image, alpha1, alpha2) */
+  long long block_elements;   /* sum over units of n_i * n_j (states of the two
+                                 atoms): the real blocks one build phases */
 } imago_dims;
 
 typedef struct imago_ctx imago_ctx;
@@ -147,47 +155,54 @@ typedef struct imago_ctx imago_ctx;
  * (imago.F90:185-258: initializeLattice, initializeFindVec,
  * initializeKPoints, renormalizeBasis, makeAlphaDist, makeAlphaNucDist,
  * makeAlphaPotDist). */
-int imago_intg_create(const imago_system *sys, const imago_opts *opts,
+IMAGO_API int imago_intg_create(const imago_system *sys, const imago_opts *opts,
                       imago_ctx **out_ctx);
 
 /* Fill *dims for a created context. */
-int imago_intg_dims(const imago_ctx *ctx, imago_dims *dims);
+IMAGO_API int imago_intg_dims(const imago_ctx *ctx, imago_dims *dims);
 
 /* Overlap: replaces gaussOverlapOL + orthoOL (integrals.F90:151-652,
  * 3608-3745).  Must run first when coreDim > 0: the context keeps
  * coreValeOL on the device for the other builds' orthogonalisation. */
-int imago_gauss_overlap_ol(imago_ctx *ctx, double *packed, double *cv_re,
+IMAGO_API int imago_gauss_overlap_ol(imago_ctx *ctx, double *packed, double *cv_re,
                            double *cv_im);
 
 /* Kinetic energy: replaces gaussOverlapKE + ortho(2)
  * (integrals.F90:656-1090). */
-int imago_gauss_overlap_ke(imago_ctx *ctx, double *packed);
+IMAGO_API int imago_gauss_overlap_ke(imago_ctx *ctx, double *packed);
 
 /* Nuclear potential: replaces gaussOverlapNP + nuclearPE + ortho(3)
  * (integrals.F90:1531-1942, 2533-2698). */
-int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
+IMAGO_API int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
 
 /* Every electronic potential term: replaces elecPotGaussOverlap,
  * gaussOverlapEP, electronicPE and ortho(4) for all potDim terms
  * (integrals.F90:1946-2531, 2700-2858). */
-int imago_elec_pot_gauss_overlap(imago_ctx *ctx, double *packed);
+IMAGO_API int imago_elec_pot_gauss_overlap(imago_ctx *ctx, double *packed);
 
 /* All matrices selected by `which` (IMAGO_OL|IMAGO_KE|IMAGO_NP|IMAGO_EP)
  * in one call; OL runs first. */
-int imago_intg_build(imago_ctx *ctx, unsigned which, const imago_out *out);
+IMAGO_API int imago_intg_build(imago_ctx *ctx, unsigned which, const imago_out *out);
 
 /* Device time in milliseconds of the stages of the last build:
  * ms[0..3] = OL, KE, NP, EP (timeStamps.f90:45-48 labels 8-11). */
-int imago_intg_stage_ms(const imago_ctx *ctx, double ms[4]);
+IMAGO_API int imago_intg_stage_ms(const imago_ctx *ctx, double ms[4]);
 
-void imago_intg_destroy(imago_ctx *ctx);
+/* Device milliseconds of the last build call by kernel stage, summed over
+ * matrices: ms[0] primitive integrals, ms[1] basis contraction, ms[2]
+ * lattice-to-k phase sums with the scatter into the global blocks, ms[3]
+ * core orthogonalisation and packing.  *launches = kernels launched. */
+IMAGO_API int imago_intg_kernel_stats(const imago_ctx *ctx, double ms[4],
+                                      long long *launches);
 
-const char *imago_strerror(int status);
+IMAGO_API void imago_intg_destroy(imago_ctx *ctx);
+
+IMAGO_API const char *imago_strerror(int status);
 
 /* Monkhorst-Pack style mesh of kpoints.f90:837-899 without symmetry
  * folding (the P1 case): k_abc = -1/2 + (i - 1 + shift)/n for each axis,
  * a-major.  Writes n[0]*n[1]*n[2] points to kpoints_abc[3*k + abc]. */
-int imago_kpoint_mesh(const int n[3], const double shift[3],
+IMAGO_API int imago_kpoint_mesh(const int n[3], const double shift[3],
                       double *kpoints_abc);
 
 /*
@@ -200,7 +215,7 @@ int imago_kpoint_mesh(const int n[3], const double shift[3],
  * and cls[2*r + 0..1] = l of atom 1 and atom 2 (0..3); it writes
  * sh[r*256 + i*16 + j] = reference sh(i+1, j+1).  Host pointers.
  */
-int imago_prim_eval(int kind, int n, const double *params, const int *cls,
+IMAGO_API int imago_prim_eval(int kind, int n, const double *params, const int *cls,
                     double *sh);
 
 #ifdef __cplusplus

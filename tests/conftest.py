@@ -1,6 +1,7 @@
 import os
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -18,3 +19,40 @@ def golden():
     import json
     with open(os.path.join(ROOT, "tests", "golden", "primitives.json")) as fh:
         return json.load(fh)
+
+
+@pytest.fixture(scope="session")
+def imago_lib():
+    """The product library, built in-tree when missing."""
+    from imago_b200 import build, intg
+    if not os.path.exists(intg.LIB_PATH):
+        build.build()
+    return intg.lib()
+
+
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+# Matrix elements must agree within 1e-10 absolute.  The reference zeroes
+# packed elements with |x| < 1e-10 when coreDim > 0 (intgOrtho.F90:185-190),
+# so a value that sits on that threshold may be zeroed on one side only; such
+# a pair differs by at most the threshold plus the tolerance.
+ATOL = 1e-10
+ZERO_THRESH = 1e-10
+
+
+def packed_mismatch(got, ref, atol=ATOL):
+    """Largest |got - ref| that is not explained by the 1e-10 zeroing, and
+    the count of elements beyond atol."""
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    d = np.abs(got - ref)
+    flip = ((got == 0.0) & (np.abs(ref) < ZERO_THRESH + atol)) | \
+           ((ref == 0.0) & (np.abs(got) < ZERO_THRESH + atol))
+    d = np.where(flip, 0.0, d)
+    return float(d.max()) if d.size else 0.0, int((d > atol).sum())

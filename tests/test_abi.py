@@ -1,0 +1,81 @@
+"""The C ABI library: it loads, exports what include/imago_intg.h
+declares, and its host-only entry points behave (no GPU needed)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+from imago_b200 import configs, intg
+from imago_b200.system import kpoint_mesh, pot_alphas
+
+
+def declared_symbols():
+    names = []
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            txt = open(os.path.join(inc, f)).read()
+            names += re.findall(r"IMAGO_API\s+[\w\s\*]*?\b(imago_\w+)\s*\(", txt)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(imago_lib):
+    names = declared_symbols()
+    assert len(names) >= 12
+    out = subprocess.run(["nm", "-D", "--defined-only", intg.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (imago_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        assert hasattr(imago_lib, n)
+
+
+def test_strerror_messages(imago_lib):
+    assert imago_lib.imago_strerror(0) == b"success"
+    assert b"More lattice points" in imago_lib.imago_strerror(2)
+    assert imago_lib.imago_strerror(12345) == b"unknown status"
+
+
+def test_kpoint_mesh_matches_reference_formula(imago_lib):
+    for n, sh in [((4, 4, 4), (0.5, 0.5, 0.5)), ((3, 2, 5), (0.0, 0.5, 0.25)),
+                  ((1, 1, 1), (0.0, 0.0, 0.0))]:
+        got = intg.kpoint_mesh(n, sh)
+        assert np.array_equal(got, kpoint_mesh(n, sh))
+        # kpoints.f90:896-899 : -1/2 + (i - 1 + shift) / n, a-major
+        i = np.arange(n[0])
+        assert np.allclose(np.unique(got[:, 0]), -0.5 + (i + sh[0]) / n[0])
+
+
+def test_kpoint_mesh_rejects_bad_sizes(imago_lib):
+    n3 = (ctypes.c_int * 3)(0, 2, 2)
+    sh = np.zeros(3)
+    out = np.zeros(3)
+    st = imago_lib.imago_kpoint_mesh(n3, sh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert st == 8
+
+
+def test_pot_alphas_geometric_series():
+    a = pot_alphas(16, 0.12, 1.0e5)
+    assert a[0] == 0.12
+    assert abs(a[-1] - 1.0e5) < 1e-8 * 1.0e5
+    assert np.allclose(a[1:] / a[:-1], (1.0e5 / 0.12) ** (1 / 15), rtol=1e-12)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_create_without_device_fails_loudly(imago_lib):
+    with pytest.raises(intg.ImagoError) as e:
+        intg.IntegralSetup(configs.diamond_primitive())
+    assert e.value.status == intg.IMAGO_ERR_NO_DEVICE
+
+
+def test_system_validation():
+    s = configs.diamond_primitive()
+    s.atom_types[0].num_orb_alphas = [16, 8, 12, 0]
+    with pytest.raises(ValueError):
+        s.validate()
