@@ -142,26 +142,24 @@ def fp64_peak_tflops(torch):
 
 
 # ------------------------------------------------------------- CPU legs --
-def cpu_sample_build(system, pair_stride, k_stride, nthreads):
-    """Time the oracle on 1/pair_stride of the atom pairs and 1/k_stride of
-    the k-points in the orthogonalisation, scaled to one full build."""
+def oracle_build_time(system, nthreads, pair_stride=1):
+    """Seconds the oracle takes for the pair loops and the
+    orthogonalisation of OL, KE, NP and every EP term."""
     import oracle
-    from imago_b200.system import ImagoSystem  # noqa: F401
-    sub = system
-    ob = oracle.OracleBuild(sub, stride=pair_stride, nthreads=nthreads)
+    ob = oracle.OracleBuild(system, stride=pair_stride, nthreads=nthreads)
     loops = ortho = 0.0
-    ob.overlap()
-    lo, ot = ob.last_times(); loops += lo; ortho += ot
-    ob.kinetic()
-    lo, ot = ob.last_times(); loops += lo; ortho += ot
-    ob.nuclear()
-    lo, ot = ob.last_times(); loops += lo; ortho += ot
-    # EP term by term: accumulate the per-term times
+    for call in (ob.overlap, ob.kinetic, ob.nuclear):
+        call()
+        lo, ot = ob.last_times()
+        loops += lo
+        ortho += ot
     for t in range(ob.pot_dim):
         ob.elec_pot(t, t + 1)
-        lo, ot = ob.last_times(); loops += lo; ortho += ot
+        lo, ot = ob.last_times()
+        loops += lo
+        ortho += ot
     ob.close()
-    return loops * pair_stride + ortho, loops, ortho
+    return loops, ortho
 
 
 def k_subset(system, k_stride):
@@ -171,18 +169,22 @@ def k_subset(system, k_stride):
     return s
 
 
-def cpu_baseline(system, nthreads, budget_s=20.0):
-    """Bounded CPU sample: every 4th atom pair and every 16th k-point (the
-    per-k work scales linearly in nk), extrapolated to the full build."""
-    pair_stride, k_stride = 4, 16
-    sub = k_subset(system, k_stride)
+def cpu_baseline(system, nthreads, limit_s=40.0):
+    """The oracle on the host cores.  A quick probe (every 8th atom pair,
+    every 16th k-point) estimates the full build; when that is within
+    limit_s the full build is timed, otherwise every 4th atom pair at every
+    k-point is timed and the pair loops are scaled by 4."""
+    lo, ot = oracle_build_time(k_subset(system, 16), nthreads, pair_stride=8)
+    estimate = 16 * (8 * lo + ot)
     t0 = time.perf_counter()
-    est, loops, ortho = cpu_sample_build(sub, pair_stride, k_stride, nthreads)
-    wall = time.perf_counter() - t0
-    # loops scale with pairs and (through the phase application) with k;
-    # the orthogonalisation with k only.
-    value = loops * pair_stride * k_stride + ortho * k_stride
-    return value, wall, pair_stride, k_stride
+    if estimate <= limit_s:
+        lo, ot = oracle_build_time(system, nthreads)
+        value, sample = lo + ot, "the full build"
+    else:
+        lo, ot = oracle_build_time(system, nthreads, pair_stride=4)
+        value = 4 * lo + ot
+        sample = "every 4th atom pair at all k-points, pair loops scaled by 4"
+    return value, time.perf_counter() - t0, sample
 
 
 def run_reference(args):
@@ -193,15 +195,16 @@ def run_reference(args):
     system = system_for_rank(0)
     nthreads = os.cpu_count() or 1
     times, walls = [], []
-    for i in range(args.warmup + args.steps):
-        v, wall, ps, ks = cpu_baseline(system, nthreads)
-        if i >= args.warmup:
-            times.append(v)
-            walls.append(wall)
+    for _ in range(args.warmup):  # warm caches and pages on a small probe
+        oracle_build_time(k_subset(system, 16), nthreads, pair_stride=8)
+    for _ in range(args.steps):
+        v, wall, what = cpu_baseline(system, nthreads, limit_s=30.0)
+        times.append(v)
+        walls.append(wall)
     value = float(np.mean(times))
     sample = (f"CPU restatement of the reference path (oracle/, C, OpenMP over "
-              f"atom pairs) on every {ps}th atom pair and every {ks}th k-point, "
-              f"scaled to one full build; {np.mean(walls):.1f} s of CPU work per step")
+              f"atom pairs, {nthreads} threads): {what}; "
+              f"{np.mean(walls):.1f} s of CPU work per step")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -319,12 +322,11 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.skip_cpu:
-            v, wall, ps, ks = cpu_baseline(system, os.cpu_count() or 1)
-            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1,
-                   "kind": "port",
-                   "sample": (f"oracle (CPU restatement, OpenMP) on every {ps}th "
-                              f"atom pair and every {ks}th k-point, scaled to one "
-                              f"build; {wall:.1f} s wall")}
+            ncores = os.cpu_count() or 1
+            v, wall, what = cpu_baseline(system, ncores)
+            cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+                   "sample": (f"oracle (CPU restatement, OpenMP over atom "
+                              f"pairs): {what}; {wall:.1f} s wall")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -358,7 +360,7 @@ def _system_bytes(system):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")

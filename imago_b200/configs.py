@@ -56,10 +56,13 @@ def _radial_overlap(alphas, l, c1, c2):
 
 
 def _make_type(element, label, alphas, norb, core, vale):
-    """core/vale: lists of (n, l, zeta)."""
-    fns = {}
+    """core/vale: lists of (n, l, zeta).  Functions are stored l-major, n
+    within l, the order the reference's contracted basis files use
+    (src/contract/printResults.f90:71-115)."""
     t = AtomType(element=element, label=label, num_orb_alphas=list(norb),
                  alphas=np.asarray(alphas, float))
+    core = sorted(core, key=lambda f: (f[1], f[0]))
+    vale = sorted(vale, key=lambda f: (f[1], f[0]))
     done = []
     for kind, lst in (("core", core), ("vale", vale)):
         for (n, l, zeta) in lst:
@@ -78,7 +81,6 @@ def _make_type(element, label, alphas, norb, core, vale):
                 t.vale_l.append(l)
                 t.vale_n.append(n)
                 t.vale_coeffs.append(c)
-    del fns
     return t
 
 

@@ -106,6 +106,7 @@ struct imago_ctx {
   std::vector<DUnit> units;
   std::vector<DSp> sps;
   std::vector<int> sp_by_cls;
+  std::vector<int2> btile;
   int cls_beg[17];
   long long blk_total = 0, m_total = 0;
   std::vector<Term3c> ep_terms;
@@ -123,6 +124,7 @@ struct imago_ctx {
   DBuf<DUnit> d_units;
   DBuf<DSp> d_sps;
   DBuf<Term3c> d_terms;
+  DBuf<int2> d_btile;
 
   // scratch
   DBuf<double> blk, M, packed_stage;
@@ -153,6 +155,7 @@ struct imago_ctx {
     d_ptype_nucalpha.release(); d_palpha.release(); d_psite_pos.release();
     d_cell.release(); d_csize.release(); d_kxyz.release(); d_phase.release();
     d_pairs.release(); d_units.release(); d_sps.release(); d_terms.release();
+    d_btile.release();
     blk.release(); M.release(); packed_stage.release(); vv.release();
     cv.release(); cc.release(); y.release(); s_cv.release();
     if (events)
@@ -500,6 +503,13 @@ int build_work(imago_ctx *c) {
   for (int k = 0; k <= 16; ++k) c->cls_beg[k] = 0;
   for (const DSp &sp : c->sps) c->cls_beg[sp.la * 4 + sp.lb + 1] += 1;
   for (int k = 0; k < 16; ++k) c->cls_beg[k + 1] += c->cls_beg[k];
+  // phase-sum tiles: every pair (also those with no image, whose blocks
+  // are written as zeros) in column tiles of kBlochCols block elements
+  c->btile.clear();
+  for (int p = 0; p < (int)c->pairs.size(); ++p) {
+    const int ne = c->pairs[p].ni * c->pairs[p].nj;
+    for (int t = 0; t * kBlochCols < ne; ++t) c->btile.push_back(make_int2(p, t));
+  }
   // EP terms in the reference's order (cumulAlphaSum + alpha index)
   c->ep_terms.clear();
   for (int t = 0; t < c->npt; ++t)
@@ -550,6 +560,7 @@ int upload(imago_ctx *c) {
   UP(d_psite_ptype, c->psite_ptype) UP(d_cell, c->cells) UP(d_csize, c->csize)
   UP(d_kxyz, c->kxyz) UP(d_pairs, c->pairs) UP(d_units, c->units)
   UP(d_sps, c->sps) UP(d_sp_by_cls, c->sp_by_cls) UP(d_terms, c->ep_terms)
+  UP(d_btile, c->btile)
 #undef UP
   if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk))) return rc;
 
@@ -581,6 +592,8 @@ int upload(imago_ctx *c) {
   w.sp_by_cls = c->d_sp_by_cls.p;
   w.blk_total = c->blk_total;
   w.m_total = c->m_total;
+  w.nbtile = (int)c->btile.size();
+  w.btile = c->d_btile.p;
   return launch_phase(s, c->d_phase.p, st);
 }
 

@@ -70,7 +70,12 @@ struct DevWork {
   const int *sp_by_cls;   // shell pairs sorted by class (la*4+lb), then unit
   long long blk_total;    // doubles of sh blocks per term
   long long m_total;      // doubles of unit blocks per term
+  int nbtile;             // phase-sum column tiles: (pair, tile)
+  const int2 *btile;
 };
+
+// Columns (block elements) per phase-sum CTA.
+constexpr int kBlochCols = 64;
 
 // Term of a three-centre build: NP is one term over all sites; EP term j of
 // potential type t has alpha index j.

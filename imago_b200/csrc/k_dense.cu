@@ -1,71 +1,99 @@
 // k_dense.cu -- contraction, lattice-to-k phase sums, scatter and core
 // orthogonalisation of one integral build.
+//
+// The phase sums and the orthogonalisation are dense complex contractions
+// and run on the FP64 tensor cores (mma.sync m8n8k4 f64), tiled through
+// shared memory.
+#include <algorithm>
+
 #include "intg.cuh"
 
 namespace imago {
 
+// D += A * B for one 8x8x4 FP64 tile.  Fragments (PTX ISA, mma.m8n8k4 .f64):
+// a = A(row = lane/4, k = lane%4), b = B(k = lane%4, col = lane/4),
+// d[i] = D(row = lane/4, col = 2*(lane%4) + i).
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a,
+                                     double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, "
+      "{%0,%1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
 // ---------------------------------------------------------- contract --
-// One warp per (unit, term):
-//   M(m1, m2) = sum_{(a,b) in unit} C1(a, m1) C2(b, m2) sh_ab(lm1, lm2),
+// One CTA per (unit, group of terms), threads over the block elements:
+//   M_t(m1, m2) = sum_{(a,b) in unit} C1(a, m1) C2(b, m2) sh_t,ab(lm1, lm2),
 // the pairXBasisFn2 / multWithBasisFn1 contraction (integrals.F90:555-563,
-// intgSaving.F90:56-89).  Terms with lm beyond a primitive's class carry a
-// zero coefficient in the reference and are skipped here.
-__global__ void __launch_bounds__(256)
+// intgSaving.F90:56-89).  Entries whose lm lies beyond a primitive's class
+// carry a zero coefficient in the reference and are skipped.  Blocks are
+// stored column-major, e = m2 * ni + m1.  The coefficient product of an
+// (element, shell pair) is shared by the terms of the group.
+constexpr int kTermsPerCta = 4;
+
+__global__ void __launch_bounds__(128)
     k_contract(DevSys s, DevWork w, int nterm, const double *blk, double *M) {
-  const long long wid =
-      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (wid >= (long long)w.nunits * nterm) return;
-  const int term = (int)(wid / w.nunits);
-  const int ui = (int)(wid % w.nunits);
+  const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
+  const int ui = blockIdx.x / ntg;
+  const int t0 = (blockIdx.x % ntg) * kTermsPerCta;
+  const int tn = min(kTermsPerCta, nterm - t0);
   const DUnit u = w.units[ui];
   const DPair p = w.pairs[u.pair];
   const int ni = p.ni, nj = p.nj, ne = ni * nj;
-  const double *bk = blk + (long long)term * w.blk_total;
-  double *out = M + (long long)term * w.m_total + p.moff +
-                (long long)(ui - p.ubeg) * ne;
+  const long long base = p.moff + (long long)(ui - p.ubeg) * ne;
   const int so1 = s.type_state_off[p.ti], so2 = s.type_state_off[p.tj];
   const double *c1 = s.basis + s.type_basis_off[p.ti];
   const double *c2 = s.basis + s.type_basis_off[p.tj];
-  for (int e = lane; e < ne; e += 32) {
-    const int m1 = e / nj, m2 = e - m1 * nj;
+  const double *bt = blk + (long long)t0 * w.blk_total;
+  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+    const int m2 = e / ni, m1 = e - m2 * ni;
     const int lm1 = s.state_lm[so1 + m1], lm2 = s.state_lm[so2 + m2];
-    double acc = 0.0;
+    double acc[kTermsPerCta];
+#pragma unroll
+    for (int t = 0; t < kTermsPerCta; ++t) acc[t] = 0.0;
     for (int q = u.spbeg; q < u.spend; ++q) {
       const DSp sp = w.sps[q];
       const int na = nsh(sp.la), nb = nsh(sp.lb);
       if (lm1 >= na || lm2 >= nb) continue;
-      acc += c1[sp.a * ni + m1] * c2[sp.b * nj + m2] *
-             bk[sp.boff + lm1 * nb + lm2];
+      const double cw = c1[sp.a * ni + m1] * c2[sp.b * nj + m2];
+      const double *b = bt + sp.boff + lm1 * nb + lm2;
+#pragma unroll
+      for (int t = 0; t < kTermsPerCta; ++t)
+        if (t < tn) acc[t] += cw * b[(long long)t * w.blk_total];
     }
-    out[e] = acc;
+#pragma unroll
+    for (int t = 0; t < kTermsPerCta; ++t)
+      if (t < tn) M[(long long)(t0 + t) * w.m_total + base + e] = acc[t];
   }
 }
 
 int launch_contract(const DevSys &s, const DevWork &w, int nterm,
                     const double *blk, double *M, cudaStream_t st) {
-  const long long warps = (long long)w.nunits * nterm;
-  if (warps == 0) return IMAGO_OK;
-  const int tb = 256;
-  const long long grid = (warps * 32 + tb - 1) / tb;
-  k_contract<<<(unsigned)grid, tb, 0, st>>>(s, w, nterm, blk, M);
+  if (w.nunits == 0 || nterm == 0) return IMAGO_OK;
+  const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
+  const long long grid = (long long)w.nunits * ntg;
+  k_contract<<<(unsigned)grid, 128, 0, st>>>(s, w, nterm, blk, M);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
 
 // ------------------------------------------------------------- bloch --
-// P_pair(k) = exp(i k.L0) sum_{images} exp(i k.R) M(R), then the block is
-// scattered as saveCurrentPair does (valence first, core after, dagger for
-// the transposed core blocks, the last write winning for i == j).
-constexpr int kBlochK = 16;
+// For each atom pair, P(k) = exp(i k.L0) sum_{images u} exp(i k.R_u) M_u:
+// a GEMM of the complex phase table [k x u] with the real image blocks
+// [u x e], per term.  The result is scattered as saveCurrentPair does
+// (valence first, core after, dagger for the transposed core blocks, the
+// last write winning for i == j), intgSaving.F90:132-702.
+constexpr int kBK = 32;   // k-points per CTA
+constexpr int kBC = kBlochCols;  // block elements per CTA
+constexpr int kBU = 16;   // images per shared-memory stage
 
 __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
-                                        int term, int k, int m1, int m2,
+                                        long long tk, int m1, int m2,
                                         double re, double im, double2 *vv,
                                         double2 *cv, double2 *cc) {
   const int V = s.vale_dim, C = s.core_dim;
   const int v1 = s.type_nvale[p.ti], v2 = s.type_nvale[p.tj];
-  const long long tk = (long long)term * s.nk + k;
   if (m1 < v1 && m2 < v2) {
     if (p.i == p.j && m1 > m2) return;  // lower triangle: never read
     const int row = s.site_cum_vale[p.i] + m1, col = s.site_cum_vale[p.j] + m2;
@@ -94,56 +122,83 @@ __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
 __global__ void __launch_bounds__(128)
     k_bloch(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
             double2 *cc) {
-  const int pi = blockIdx.x, term = blockIdx.y, k0 = blockIdx.z * kBlochK;
-  const DPair p = w.pairs[pi];
-  const int ne = p.ni * p.nj;
+  __shared__ double2 ph_s[kBU][kBK];
+  __shared__ double m_s[kBU][kBC];
+  const int2 bt = w.btile[blockIdx.x];
+  const DPair p = w.pairs[bt.x];
+  const int ne = p.ni * p.nj, c0 = bt.y * kBC;
+  const int k0 = blockIdx.y * kBK, term = blockIdx.z, nk = s.nk;
+  const int nu = p.uend - p.ubeg;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double *Mt = M + (long long)term * w.m_total + p.moff;
-  const int nk = s.nk;
-  double cs[kBlochK], sn[kBlochK];
+  double ar[4][2][2], ai[4][2][2];
 #pragma unroll
-  for (int kk = 0; kk < kBlochK; ++kk) {
-    cs[kk] = 1.0;
-    sn[kk] = 0.0;
-    const int k = k0 + kk;
-    if (k < nk) {
-      const double *kv = s.kxyz + 3 * k;
-      const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
-      // kPointLatticeOriginShift (intgSaving.F90:241-292) skips the shift
-      // when |k.L0| < smallThresh.
-      if (fabs(dot) >= kSmallThresh) sincos(dot, &sn[kk], &cs[kk]);
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) ar[a][b][0] = ar[a][b][1] = ai[a][b][0] = ai[a][b][1] = 0.0;
+
+  for (int u0 = 0; u0 < nu; u0 += kBU) {
+    for (int i = tid; i < kBU * kBK; i += 128) {
+      const int uu = i / kBK, kk = i % kBK;
+      double2 v = make_double2(0.0, 0.0);
+      if (u0 + uu < nu && k0 + kk < nk)
+        v = s.phase[(long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk];
+      ph_s[uu][kk] = v;
     }
-  }
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-    double re[kBlochK], im[kBlochK];
+    for (int i = tid; i < kBU * kBC; i += 128) {
+      const int uu = i / kBC, cc2 = i % kBC;
+      double v = 0.0;
+      if (u0 + uu < nu && c0 + cc2 < ne)
+        v = Mt[(long long)(u0 + uu) * ne + c0 + cc2];
+      m_s[uu][cc2] = v;
+    }
+    __syncthreads();
 #pragma unroll
-    for (int kk = 0; kk < kBlochK; ++kk) re[kk] = im[kk] = 0.0;
-    for (int u = p.ubeg; u < p.uend; ++u) {
-      const double x = Mt[(long long)(u - p.ubeg) * ne + e];
-      const double2 *ph = s.phase + (long long)w.units[u].cell * nk + k0;
+    for (int ks = 0; ks < kBU; ks += 4) {
+      const int ku = ks + (lane & 3);
+      double b[2];
 #pragma unroll
-      for (int kk = 0; kk < kBlochK; ++kk)
-        if (k0 + kk < nk) {
-          const double2 f = ph[kk];
-          re[kk] += f.x * x;
-          im[kk] += f.y * x;
+      for (int nt = 0; nt < 2; ++nt) b[nt] = m_s[ku][warp * 16 + nt * 8 + (lane >> 2)];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const double2 a = ph_s[ku][mt * 8 + (lane >> 2)];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          dmma(ar[mt][nt][0], ar[mt][nt][1], a.x, b[nt]);
+          dmma(ai[mt][nt][0], ai[mt][nt][1], a.y, b[nt]);
         }
+      }
     }
-    const int m1 = e / p.nj, m2 = e - m1 * p.nj;
+    __syncthreads();
+  }
+  // epilogue: origin shift (kPointLatticeOriginShift, intgSaving.F90:241-292,
+  // skipped when |k.L0| < smallThresh) and the scatter
 #pragma unroll
-    for (int kk = 0; kk < kBlochK; ++kk) {
-      const int k = k0 + kk;
-      if (k >= nk) break;
-      const double r = cs[kk] * re[kk] - sn[kk] * im[kk];
-      const double i = cs[kk] * im[kk] + sn[kk] * re[kk];
-      scatter(s, p, term, k, m1, m2, r, i, vv, cv, cc);
-    }
+  for (int mt = 0; mt < 4; ++mt) {
+    const int k = k0 + mt * 8 + (lane >> 2);
+    if (k >= nk) continue;
+    const double *kv = s.kxyz + 3 * k;
+    const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
+    double sn = 0.0, cs = 1.0;
+    if (fabs(dot) >= kSmallThresh) sincos(dot, &sn, &cs);
+    const long long tk = (long long)term * nk + k;
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int e = c0 + warp * 16 + nt * 8 + 2 * (lane & 3) + i;
+        if (e >= ne) continue;
+        const double re = ar[mt][nt][i], im = ai[mt][nt][i];
+        const int m2 = e / p.ni, m1 = e - m2 * p.ni;
+        scatter(s, p, tk, m1, m2, cs * re - sn * im, cs * im + sn * re, vv, cv, cc);
+      }
   }
 }
 
 int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
                  double2 *vv, double2 *cv, double2 *cc, cudaStream_t st) {
-  if (w.npairs == 0 || nterm == 0) return IMAGO_OK;
-  dim3 grid(w.npairs, nterm, (s.nk + kBlochK - 1) / kBlochK);
+  if (w.nbtile == 0 || nterm == 0) return IMAGO_OK;
+  dim3 grid(w.nbtile, (s.nk + kBK - 1) / kBK, nterm);
   k_bloch<<<grid, 128, 0, st>>>(s, w, M, vv, cv, cc);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
@@ -154,45 +209,171 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
 // computes (zherk or zher2k on the upper triangle, then coreValeCoreCore
 // and makeValeVale):
 //   VV' = VV - S^H X_cv - X_cv^H S + S^H X_cc S.
-// Here the same is formed as VV' = VV - (S^H Y + Y^H S) with
-// Y = X_cv - X_cc S / 2, which needs one product less (X_cc is Hermitian).
-// For the overlap itself X = S and this is VV - 2 S^H S + S^H S_cc S.
-__global__ void __launch_bounds__(256)
-    k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
-              const double2 *s_cv, double2 *y) {
-  const int k = blockIdx.y, term = blockIdx.z;
-  const int V = s.vale_dim, C = s.core_dim;
-  const long long tk = (long long)term * s.nk + k;
-  const double2 *X = cv + tk * V * C;
-  const double2 *XC = cc + tk * C * C;
-  const double2 *S = s_cv + (long long)k * V * C;
-  double2 *Y = y + tk * V * C;
-  const long long n = (long long)V * C;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-       idx < n; idx += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(idx % C), v = (int)(idx / C);
-    double ar = 0.0, ai = 0.0;
-    for (int l = 0; l < C; ++l) {
-      const double2 a = XC[(long long)l * C + c];  // X_cc(c, l)
-      const double2 b = S[(long long)v * C + l];   // S(l, v)
-      ar += a.x * b.x - a.y * b.y;
-      ai += a.x * b.y + a.y * b.x;
+// Here it is formed as VV' = VV - (S^H Y + Y^H S) with Y = X_cv - X_cc S/2
+// (X_cc is Hermitian), two complex GEMMs on 32x32 output tiles:
+//   k_ortho_y: Y (C x V),  k_ortho_w: the upper tiles of S^H Y + Y^H S,
+// then the packing of the upper triangle with the 1e-10 zeroing.
+// For the overlap itself X = S: VV - 2 S^H S + S^H S_cc S.
+constexpr int kOT = 32;  // output tile
+constexpr int kOK = 8;   // complex K per shared-memory stage
+
+// 32x32 complex tile accumulate from shared operands:
+// A_s[re/im][k][r], B_s[re/im][k][c]; acc (+)= op(A)^T B with op = conj when
+// CONJ.  Warp w owns rows 16*(w/2).., cols 16*(w%2)..
+template <bool CONJ>
+__device__ __forceinline__ void ctile_mma(const double (*A)[kOK][kOT],
+                                          const double (*B)[kOK][kOT],
+                                          double wr[2][2][2], double wi[2][2][2],
+                                          int lane, int warp) {
+  const int r0 = (warp >> 1) * 16, cb = (warp & 1) * 16;
+#pragma unroll
+  for (int ks = 0; ks < kOK; ks += 4) {
+    const int kk = ks + (lane & 3);
+    double a_r[2], a_i[2], b_r[2], b_i[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      a_r[t] = A[0][kk][r0 + 8 * t + (lane >> 2)];
+      a_i[t] = A[1][kk][r0 + 8 * t + (lane >> 2)];
+      b_r[t] = B[0][kk][cb + 8 * t + (lane >> 2)];
+      b_i[t] = B[1][kk][cb + 8 * t + (lane >> 2)];
     }
-    const double2 x = X[idx];
-    Y[idx] = make_double2(x.x - 0.5 * ar, x.y - 0.5 * ai);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        // conj(a) b = (ar br + ai bi) + i (ar bi - ai br)
+        //      a b  = (ar br - ai bi) + i (ar bi + ai br)
+        dmma(wr[mt][nt][0], wr[mt][nt][1], a_r[mt], b_r[nt]);
+        dmma(wr[mt][nt][0], wr[mt][nt][1], CONJ ? a_i[mt] : -a_i[mt], b_i[nt]);
+        dmma(wi[mt][nt][0], wi[mt][nt][1], a_r[mt], b_i[nt]);
+        dmma(wi[mt][nt][0], wi[mt][nt][1], CONJ ? -a_i[mt] : a_i[mt], b_r[nt]);
+      }
   }
 }
 
-__global__ void __launch_bounds__(256)
-    k_ortho_pack(DevSys s, const double2 *vv, const double2 *y,
-                 const double2 *s_cv, double *packed) {
-  const int k = blockIdx.y, term = blockIdx.z;
+// Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v)
+__global__ void __launch_bounds__(128)
+    k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
+              const double2 *s_cv, double2 *y) {
+  __shared__ double A_s[2][kOK][kOT];
+  __shared__ double B_s[2][kOK][kOT];
   const int V = s.vale_dim, C = s.core_dim;
+  const int ntc = (C + kOT - 1) / kOT;
+  const int tr = blockIdx.x % ntc, tc = blockIdx.x / ntc;  // c tile, v tile
+  const int k = blockIdx.y, term = blockIdx.z;
+  const long long tk = (long long)term * s.nk + k;
+  const double2 *XC = cc + tk * C * C;
+  const double2 *S = s_cv + (long long)k * V * C;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double wr[2][2][2] = {}, wi[2][2][2] = {};
+  for (int l0 = 0; l0 < C; l0 += kOK) {
+    for (int i = tid; i < kOK * kOT; i += 128) {
+      const int kk = i / kOT, r = i % kOT;
+      const int l = l0 + kk, c = tr * kOT + r, v = tc * kOT + r;
+      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+      if (l < C && c < C) a = XC[(long long)l * C + c];  // X_cc(c, l)
+      if (l < C && v < V) b = S[(long long)v * C + l];   // S(l, v)
+      A_s[0][kk][r] = a.x;
+      A_s[1][kk][r] = a.y;
+      B_s[0][kk][r] = b.x;
+      B_s[1][kk][r] = b.y;
+    }
+    __syncthreads();
+    ctile_mma<false>(A_s, B_s, wr, wi, lane, warp);
+    __syncthreads();
+  }
+  const double2 *X = cv + tk * V * C;
+  double2 *Y = y + tk * V * C;
+  const int r0 = (warp >> 1) * 16, cb = (warp & 1) * 16;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int c = tr * kOT + r0 + 8 * mt + (lane >> 2);
+        const int v = tc * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
+        if (c >= C || v >= V) continue;
+        const double2 x = X[(long long)v * C + c];
+        Y[(long long)v * C + c] =
+            make_double2(x.x - 0.5 * wr[mt][nt][i], x.y - 0.5 * wi[mt][nt][i]);
+      }
+}
+
+// Upper tiles (J <= I) of W = S^H Y + Y^H S, then
+// VV'(j, i) = VV(j, i) - W(j, i) packed at i(i+1)/2 + j.
+__global__ void __launch_bounds__(128)
+    k_ortho_w(DevSys s, const double2 *vv, const double2 *y,
+              const double2 *s_cv, double *packed) {
+  __shared__ double A_s[2][kOK][kOT];
+  __shared__ double B_s[2][kOK][kOT];
+  const int V = s.vale_dim, C = s.core_dim;
+  // upper-triangular tile index -> (J, I), J <= I
+  int t = blockIdx.x, I = 0;
+  while (t > I) {
+    t -= I + 1;
+    ++I;
+  }
+  const int J = t;
+  const int k = blockIdx.y, term = blockIdx.z;
+  const long long tk = (long long)term * s.nk + k;
+  const double2 *S = s_cv + (long long)k * V * C;
+  const double2 *Y = y + tk * V * C;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double wr[2][2][2] = {}, wi[2][2][2] = {};
+  for (int pass = 0; pass < 2; ++pass) {
+    const double2 *Aop = pass == 0 ? S : Y;  // conj(A)^T
+    const double2 *Bop = pass == 0 ? Y : S;
+    for (int l0 = 0; l0 < C; l0 += kOK) {
+      for (int i = tid; i < kOK * kOT; i += 128) {
+        const int kk = i % kOK, r = i / kOK;  // l fastest: contiguous loads
+        const int l = l0 + kk, j = J * kOT + r, ii = I * kOT + r;
+        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        if (l < C && j < V) a = Aop[(long long)j * C + l];
+        if (l < C && ii < V) b = Bop[(long long)ii * C + l];
+        A_s[0][kk][r] = a.x;
+        A_s[1][kk][r] = a.y;
+        B_s[0][kk][r] = b.x;
+        B_s[1][kk][r] = b.y;
+      }
+      __syncthreads();
+      ctile_mma<true>(A_s, B_s, wr, wi, lane, warp);
+      __syncthreads();
+    }
+  }
+  const double2 *VVt = vv + tk * V * V;
+  const long long np = (long long)V * (V + 1) / 2;
+  double *out = packed + 2 * tk * np;
+  const int r0 = (warp >> 1) * 16, cb = (warp & 1) * 16;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int row = J * kOT + r0 + 8 * mt + (lane >> 2);
+        const int col = I * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
+        if (row >= V || col >= V || row > col) continue;
+        double2 v = VVt[(long long)col * V + row];
+        v.x -= wr[mt][nt][i];
+        v.y -= wi[mt][nt][i];
+        if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
+        if (fabs(v.x) < kPackThresh) v.x = 0.0;
+        if (fabs(v.y) < kPackThresh) v.y = 0.0;
+        const long long idx = (long long)col * (col + 1) / 2 + row;
+        out[2 * idx] = v.x;
+        out[2 * idx + 1] = v.y;
+      }
+}
+
+// coreDim == 0: the reference packs valeVale as it is (integrals.F90:3657-3676).
+__global__ void __launch_bounds__(256)
+    k_pack_plain(DevSys s, const double2 *vv, double *packed) {
+  const int k = blockIdx.y, term = blockIdx.z;
+  const int V = s.vale_dim;
   const long long np = (long long)V * (V + 1) / 2;
   const long long tk = (long long)term * s.nk + k;
   const double2 *VVt = vv + tk * V * V;
-  const double2 *Y = y + tk * V * C;
-  const double2 *S = s_cv + (long long)k * V * C;
   double *out = packed + 2 * tk * np;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
        idx < np; idx += (long long)gridDim.x * blockDim.x) {
@@ -200,23 +381,7 @@ __global__ void __launch_bounds__(256)
     while ((long long)col * (col + 1) / 2 > idx) --col;
     while ((long long)(col + 1) * (col + 2) / 2 <= idx) ++col;
     const int row = (int)(idx - (long long)col * (col + 1) / 2);
-    double2 v = VVt[(long long)col * V + row];
-    if (C > 0) {
-      double sr = 0.0, si = 0.0;
-      const double2 *Sr = S + (long long)row * C, *Sc = S + (long long)col * C;
-      const double2 *Yr = Y + (long long)row * C, *Yc = Y + (long long)col * C;
-      for (int l = 0; l < C; ++l) {
-        const double2 a = Sr[l], b = Yc[l], c = Yr[l], d = Sc[l];
-        // conj(a) b + conj(c) d
-        sr += a.x * b.x + a.y * b.y + c.x * d.x + c.y * d.y;
-        si += a.x * b.y - a.y * b.x + c.x * d.y - c.y * d.x;
-      }
-      v.x -= sr;
-      v.y -= si;
-      if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
-      if (fabs(v.x) < kPackThresh) v.x = 0.0;
-      if (fabs(v.y) < kPackThresh) v.y = 0.0;
-    }
+    const double2 v = VVt[(long long)col * V + row];
     out[2 * idx] = v.x;
     out[2 * idx + 1] = v.y;
   }
@@ -227,15 +392,19 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  double2 *y, double *packed, cudaStream_t st) {
   const int V = s.vale_dim, C = s.core_dim;
   if (nterm == 0) return IMAGO_OK;
-  if (C > 0) {
-    const long long n = (long long)V * C;
-    dim3 g((unsigned)((n + 255) / 256 > 64 ? 64 : (n + 255) / 256), s.nk, nterm);
-    k_ortho_y<<<g, 256, 0, st>>>(s, cv, cc, s_cv, y);
+  if (C == 0) {
+    const long long np = (long long)V * (V + 1) / 2;
+    dim3 g((unsigned)std::min<long long>((np + 255) / 256, 128), s.nk, nterm);
+    k_pack_plain<<<g, 256, 0, st>>>(s, vv, packed);
     IMAGO_CUDA(cudaGetLastError());
+    return IMAGO_OK;
   }
-  const long long np = (long long)V * (V + 1) / 2;
-  dim3 g2((unsigned)((np + 255) / 256 > 128 ? 128 : (np + 255) / 256), s.nk, nterm);
-  k_ortho_pack<<<g2, 256, 0, st>>>(s, vv, y, s_cv, packed);
+  const int tcv = (C + kOT - 1) / kOT, tvv = (V + kOT - 1) / kOT;
+  dim3 gy(tcv * tvv, s.nk, nterm);
+  k_ortho_y<<<gy, 128, 0, st>>>(s, cv, cc, s_cv, y);
+  IMAGO_CUDA(cudaGetLastError());
+  dim3 gw(tvv * (tvv + 1) / 2, s.nk, nterm);
+  k_ortho_w<<<gw, 128, 0, st>>>(s, vv, y, s_cv, packed);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
@@ -256,7 +425,7 @@ int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
                     cudaStream_t st) {
   const long long n = (long long)s.nk * s.vale_dim * s.core_dim;
   if (n == 0) return IMAGO_OK;
-  k_split_cv<<<(unsigned)((n + 255) / 256 > 4096 ? 4096 : (n + 255) / 256), 256, 0, st>>>(
+  k_split_cv<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
       n, cv, re, im);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
@@ -279,7 +448,7 @@ __global__ void k_phase(DevSys s, double2 *phase) {
 
 int launch_phase(const DevSys &s, double2 *phase, cudaStream_t st) {
   const long long n = (long long)s.ncell * s.nk;
-  k_phase<<<(unsigned)((n + 255) / 256 > 4096 ? 4096 : (n + 255) / 256), 256, 0, st>>>(s, phase);
+  k_phase<<<(unsigned)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(s, phase);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
