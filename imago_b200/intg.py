@@ -90,6 +90,9 @@ def lib():
         L.imago_prim_eval.argtypes = [ctypes.c_int, ctypes.c_int, _D,
                                       ctypes.POINTER(ctypes.c_int), _D]
         L.imago_prim_eval.restype = ctypes.c_int
+        L.imago_prim_eval_static.argtypes = [ctypes.c_int, ctypes.c_int, _D,
+                                             ctypes.POINTER(ctypes.c_int), _D]
+        L.imago_prim_eval_static.restype = ctypes.c_int
         _LIB = L
     return _LIB
 
@@ -129,6 +132,29 @@ def prim_eval(kind, params, cls=None):
                                c.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
                                _p(out))
     _check(st, "imago_prim_eval")
+    return out.reshape(n, 16, 16)
+
+
+PRIM_STATIC_MAX_RECORDS = 512
+
+
+def prim_eval_static(kind, params, cls=None):
+    """prim_eval through imago_prim_eval_static, which stages the records in
+    a fixed device array instead of allocating: for callers that must not
+    call cudaMalloc (a GPU shared under a fixed memory budget, device memory
+    owned by a pool allocator, or a loop that cannot afford the
+    synchronisation of cudaMalloc/cudaFree).  At most
+    PRIM_STATIC_MAX_RECORDS records per call; calls must not overlap on the
+    GPU, since they share the array."""
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, 12)
+    n = len(params)
+    c = (np.ascontiguousarray(cls, dtype=np.int32).reshape(-1, 2) if cls is not None
+         else np.zeros((n, 2), np.int32))
+    out = np.zeros((n, 256))
+    st = lib().imago_prim_eval_static(PRIM_KINDS[kind], n, _p(params),
+                                      c.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                      _p(out))
+    _check(st, "imago_prim_eval_static")
     return out.reshape(n, 16, 16)
 
 

@@ -218,6 +218,28 @@ IMAGO_API int imago_kpoint_mesh(const int n[3], const double shift[3],
 IMAGO_API int imago_prim_eval(int kind, int n, const double *params, const int *cls,
                     double *sh);
 
+/* Records one imago_prim_eval_static call accepts, and the device memory
+ * its fixed scratch array occupies on every GPU that loads this library,
+ * for as long as the library stays loaded (1,101,824 bytes). */
+#define IMAGO_PRIM_STATIC_MAX_RECORDS 512
+#define IMAGO_PRIM_STATIC_BYTES 1101824
+
+/*
+ * imago_prim_eval without any device allocation; no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: a process sharing a
+ * GPU under a fixed memory budget or whose device memory already belongs to
+ * a pool allocator, or a loop that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Same arguments, layout and
+ * results as imago_prim_eval; the records are staged in one fixed
+ * module-scope device array instead of per-call buffers.  n above
+ * IMAGO_PRIM_STATIC_MAX_RECORDS returns IMAGO_ERR_RANGE.  The first call on
+ * a device looks up the array's device address (with that device current)
+ * and should precede any stream capture on that device.  Calls share the
+ * array: calls that overlap on the GPU race and must not be issued.
+ */
+IMAGO_API int imago_prim_eval_static(int kind, int n, const double *params,
+                                     const int *cls, double *sh);
+
 #ifdef __cplusplus
 }
 #endif
