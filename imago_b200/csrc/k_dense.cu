@@ -28,12 +28,22 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a,
 // the pairXBasisFn2 / multWithBasisFn1 contraction (integrals.F90:555-563,
 // intgSaving.F90:56-89).  Entries whose lm lies beyond a primitive's class
 // carry a zero coefficient in the reference and are skipped.  Blocks are
-// stored column-major, e = m2 * ni + m1.  The coefficient product of an
-// (element, shell pair) is shared by the terms of the group.
+// stored column-major, e = m2 * ni + m1.  The unit's shell-pair list and
+// both atoms' coefficient tables are staged in shared memory; the
+// coefficient product of an (element, shell pair) serves every term of the
+// group.
 constexpr int kTermsPerCta = 4;
+constexpr int kContractThreads = 128;
+constexpr int kElemsPerThread = 3;          // n_i n_j <= 384 per pass
+constexpr int kSpStage = 256;               // shell pairs staged at a time
+constexpr int kCoefMax = 1024;              // alphas x states per atom
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kContractThreads, 6)
     k_contract(DevSys s, DevWork w, int nterm, const double *blk, double *M) {
+  __shared__ int sp_ab[kSpStage];            // a | b << 16
+  __shared__ int sp_cls[kSpStage];           // nsh(la) | nsh(lb) << 8
+  __shared__ long long sp_off[kSpStage];
+  __shared__ double c1s[kCoefMax], c2s[kCoefMax];
   const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
   const int ui = blockIdx.x / ntg;
   const int t0 = (blockIdx.x % ntg) * kTermsPerCta;
@@ -41,30 +51,66 @@ __global__ void __launch_bounds__(128)
   const DUnit u = w.units[ui];
   const DPair p = w.pairs[u.pair];
   const int ni = p.ni, nj = p.nj, ne = ni * nj;
+  const int na1 = s.type_nalpha[p.ti], na2 = s.type_nalpha[p.tj];
   const long long base = p.moff + (long long)(ui - p.ubeg) * ne;
   const int so1 = s.type_state_off[p.ti], so2 = s.type_state_off[p.tj];
   const double *c1 = s.basis + s.type_basis_off[p.ti];
   const double *c2 = s.basis + s.type_basis_off[p.tj];
+  const bool stage_coef = na1 * ni <= kCoefMax && na2 * nj <= kCoefMax;
+  if (stage_coef) {
+    for (int i = threadIdx.x; i < na1 * ni; i += kContractThreads) c1s[i] = c1[i];
+    for (int i = threadIdx.x; i < na2 * nj; i += kContractThreads) c2s[i] = c2[i];
+  }
+  const double *cf1 = stage_coef ? c1s : c1;
+  const double *cf2 = stage_coef ? c2s : c2;
   const double *bt = blk + (long long)t0 * w.blk_total;
-  for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-    const int m2 = e / ni, m1 = e - m2 * ni;
-    const int lm1 = s.state_lm[so1 + m1], lm2 = s.state_lm[so2 + m2];
-    double acc[kTermsPerCta];
+  for (int e0 = 0; e0 < ne; e0 += kContractThreads * kElemsPerThread) {
+    int lm1[kElemsPerThread], lm2[kElemsPerThread], m1[kElemsPerThread],
+        m2[kElemsPerThread];
+    double acc[kElemsPerThread][kTermsPerCta];
 #pragma unroll
-    for (int t = 0; t < kTermsPerCta; ++t) acc[t] = 0.0;
-    for (int q = u.spbeg; q < u.spend; ++q) {
-      const DSp sp = w.sps[q];
-      const int na = nsh(sp.la), nb = nsh(sp.lb);
-      if (lm1 >= na || lm2 >= nb) continue;
-      const double cw = c1[sp.a * ni + m1] * c2[sp.b * nj + m2];
-      const double *b = bt + sp.boff + lm1 * nb + lm2;
+    for (int j = 0; j < kElemsPerThread; ++j) {
+      const int e = e0 + threadIdx.x + j * kContractThreads;
+      m2[j] = e < ne ? e / ni : 0;
+      m1[j] = e < ne ? e - m2[j] * ni : 0;
+      lm1[j] = e < ne ? s.state_lm[so1 + m1[j]] : 1 << 20;
+      lm2[j] = e < ne ? s.state_lm[so2 + m2[j]] : 1 << 20;
 #pragma unroll
-      for (int t = 0; t < kTermsPerCta; ++t)
-        if (t < tn) acc[t] += cw * b[(long long)t * w.blk_total];
+      for (int t = 0; t < kTermsPerCta; ++t) acc[j][t] = 0.0;
+    }
+    for (int q0 = u.spbeg; q0 < u.spend; q0 += kSpStage) {
+      const int nq = min(kSpStage, u.spend - q0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < nq; i += kContractThreads) {
+        const DSp sp = w.sps[q0 + i];
+        sp_ab[i] = sp.a | (sp.b << 16);
+        sp_cls[i] = nsh(sp.la) | (nsh(sp.lb) << 8);
+        sp_off[i] = sp.boff;
+      }
+      __syncthreads();
+      for (int q = 0; q < nq; ++q) {
+        const int ab = sp_ab[q], cl = sp_cls[q];
+        const int a = ab & 0xffff, b = ab >> 16, na = cl & 0xff, nb = cl >> 8;
+        const double *bq = bt + sp_off[q];
+#pragma unroll
+        for (int j = 0; j < kElemsPerThread; ++j) {
+          if (lm1[j] >= na || lm2[j] >= nb) continue;
+          const double cw = cf1[a * ni + m1[j]] * cf2[b * nj + m2[j]];
+          const double *bb = bq + lm1[j] * nb + lm2[j];
+#pragma unroll
+          for (int t = 0; t < kTermsPerCta; ++t)
+            if (t < tn) acc[j][t] += cw * bb[(long long)t * w.blk_total];
+        }
+      }
     }
 #pragma unroll
-    for (int t = 0; t < kTermsPerCta; ++t)
-      if (t < tn) M[(long long)(t0 + t) * w.m_total + base + e] = acc[t];
+    for (int j = 0; j < kElemsPerThread; ++j) {
+      const int e = e0 + threadIdx.x + j * kContractThreads;
+      if (e >= ne) continue;
+#pragma unroll
+      for (int t = 0; t < kTermsPerCta; ++t)
+        if (t < tn) M[(long long)(t0 + t) * w.m_total + base + e] = acc[j][t];
+    }
   }
 }
 
@@ -73,7 +119,7 @@ int launch_contract(const DevSys &s, const DevWork &w, int nterm,
   if (w.nunits == 0 || nterm == 0) return IMAGO_OK;
   const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
   const long long grid = (long long)w.nunits * ntg;
-  k_contract<<<(unsigned)grid, 128, 0, st>>>(s, w, nterm, blk, M);
+  k_contract<<<(unsigned)grid, kContractThreads, 0, st>>>(s, w, nterm, blk, M);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
@@ -119,63 +165,84 @@ __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
   }
 }
 
-__global__ void __launch_bounds__(128)
+constexpr int kBThreads = 256;              // 8 warps: 2 (k) x 4 (columns)
+// Padded rows: a fragment read (4 k rows x 8 columns) then covers all 32
+// banks in each of its wavefronts.
+constexpr int kBMP = kBC + 4;
+constexpr int kBKP = kBK + 4;
+constexpr int kBPhLoads = kBU * kBK / kBThreads;
+constexpr int kBMLoads = kBU * kBC / kBThreads;
+
+__global__ void __launch_bounds__(kBThreads)
     k_bloch(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
             double2 *cc) {
-  __shared__ double2 ph_s[kBU][kBK];
-  __shared__ double m_s[kBU][kBC];
+  __shared__ double2 ph_s[kBU][kBKP];
+  __shared__ double m_s[kBU][kBMP];
   const int2 bt = w.btile[blockIdx.x];
   const DPair p = w.pairs[bt.x];
   const int ne = p.ni * p.nj, c0 = bt.y * kBC;
   const int k0 = blockIdx.y * kBK, term = blockIdx.z, nk = s.nk;
   const int nu = p.uend - p.ubeg;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wk = (warp >> 2) * 16, wc = (warp & 3) * 16;  // warp tile origin
   const double *Mt = M + (long long)term * w.m_total + p.moff;
-  double ar[4][2][2], ai[4][2][2];
+  double ar[2][2][2] = {}, ai[2][2][2] = {};
+  double2 rph[kBPhLoads];
+  double rm[kBMLoads];
+  auto fetch = [&](int u0) {
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 2; ++b) ar[a][b][0] = ar[a][b][1] = ai[a][b][0] = ai[a][b][1] = 0.0;
-
-  for (int u0 = 0; u0 < nu; u0 += kBU) {
-    for (int i = tid; i < kBU * kBK; i += 128) {
-      const int uu = i / kBK, kk = i % kBK;
-      double2 v = make_double2(0.0, 0.0);
-      if (u0 + uu < nu && k0 + kk < nk)
-        v = s.phase[(long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk];
-      ph_s[uu][kk] = v;
+    for (int q = 0; q < kBPhLoads; ++q) {
+      const int i = tid + q * kBThreads, uu = i / kBK, kk = i % kBK;
+      rph[q] = (u0 + uu < nu && k0 + kk < nk)
+                   ? s.phase[(long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk]
+                   : make_double2(0.0, 0.0);
     }
-    for (int i = tid; i < kBU * kBC; i += 128) {
-      const int uu = i / kBC, cc2 = i % kBC;
-      double v = 0.0;
-      if (u0 + uu < nu && c0 + cc2 < ne)
-        v = Mt[(long long)(u0 + uu) * ne + c0 + cc2];
-      m_s[uu][cc2] = v;
+#pragma unroll
+    for (int q = 0; q < kBMLoads; ++q) {
+      const int i = tid + q * kBThreads, uu = i / kBC, cc2 = i % kBC;
+      rm[q] = (u0 + uu < nu && c0 + cc2 < ne) ? Mt[(long long)(u0 + uu) * ne + c0 + cc2]
+                                              : 0.0;
+    }
+  };
+  if (nu > 0) fetch(0);
+  for (int u0 = 0; u0 < nu; u0 += kBU) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kBPhLoads; ++q) {
+      const int i = tid + q * kBThreads;
+      ph_s[i / kBK][i % kBK] = rph[q];
+    }
+#pragma unroll
+    for (int q = 0; q < kBMLoads; ++q) {
+      const int i = tid + q * kBThreads;
+      m_s[i / kBC][i % kBC] = rm[q];
     }
     __syncthreads();
+    if (u0 + kBU < nu) fetch(u0 + kBU);
 #pragma unroll
     for (int ks = 0; ks < kBU; ks += 4) {
       const int ku = ks + (lane & 3);
       double b[2];
+      double2 a[2];
 #pragma unroll
-      for (int nt = 0; nt < 2; ++nt) b[nt] = m_s[ku][warp * 16 + nt * 8 + (lane >> 2)];
+      for (int t = 0; t < 2; ++t) {
+        b[t] = m_s[ku][wc + t * 8 + (lane >> 2)];
+        a[t] = ph_s[ku][wk + t * 8 + (lane >> 2)];
+      }
 #pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const double2 a = ph_s[ku][mt * 8 + (lane >> 2)];
+      for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
-          dmma(ar[mt][nt][0], ar[mt][nt][1], a.x, b[nt]);
-          dmma(ai[mt][nt][0], ai[mt][nt][1], a.y, b[nt]);
+          dmma(ar[mt][nt][0], ar[mt][nt][1], a[mt].x, b[nt]);
+          dmma(ai[mt][nt][0], ai[mt][nt][1], a[mt].y, b[nt]);
         }
-      }
     }
-    __syncthreads();
   }
   // epilogue: origin shift (kPointLatticeOriginShift, intgSaving.F90:241-292,
   // skipped when |k.L0| < smallThresh) and the scatter
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int k = k0 + mt * 8 + (lane >> 2);
+  for (int mt = 0; mt < 2; ++mt) {
+    const int k = k0 + wk + mt * 8 + (lane >> 2);
     if (k >= nk) continue;
     const double *kv = s.kxyz + 3 * k;
     const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
@@ -186,7 +253,7 @@ __global__ void __launch_bounds__(128)
     for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
-        const int e = c0 + warp * 16 + nt * 8 + 2 * (lane & 3) + i;
+        const int e = c0 + wc + nt * 8 + 2 * (lane & 3) + i;
         if (e >= ne) continue;
         const double re = ar[mt][nt][i], im = ai[mt][nt][i];
         const int m2 = e / p.ni, m1 = e - m2 * p.ni;
@@ -199,7 +266,7 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
                  double2 *vv, double2 *cv, double2 *cc, cudaStream_t st) {
   if (w.nbtile == 0 || nterm == 0) return IMAGO_OK;
   dim3 grid(w.nbtile, (s.nk + kBK - 1) / kBK, nterm);
-  k_bloch<<<grid, 128, 0, st>>>(s, w, M, vv, cv, cc);
+  k_bloch<<<grid, kBThreads, 0, st>>>(s, w, M, vv, cv, cc);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
@@ -214,28 +281,34 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
 //   k_ortho_y: Y (C x V),  k_ortho_w: the upper tiles of S^H Y + Y^H S,
 // then the packing of the upper triangle with the 1e-10 zeroing.
 // For the overlap itself X = S: VV - 2 S^H S + S^H S_cc S.
-constexpr int kOT = 32;  // output tile
-constexpr int kOK = 8;   // complex K per shared-memory stage
+constexpr int kOT = 32;   // output tile
+constexpr int kOK = 16;   // complex K per shared-memory stage
+constexpr int kOP = kOT + 4;  // padded row: fragment reads are conflict-free
+constexpr int kOThreads = 128;
+constexpr int kOLoads = kOK * kOT / kOThreads;  // double2 per thread per operand
 
-// 32x32 complex tile accumulate from shared operands:
-// A_s[re/im][k][r], B_s[re/im][k][c]; acc (+)= op(A)^T B with op = conj when
-// CONJ.  Warp w owns rows 16*(w/2).., cols 16*(w%2)..
+// Shared operands of one stage: A(k, r) and B(k, c), complex, interleaved.
+struct OStage {
+  double2 a[kOK][kOP];
+  double2 b[kOK][kOP];
+};
+
+// Accumulate the stage into the warp's 16x16 complex tile:
+// acc (+)= op(A)^T B, op = conj when CONJ.  Warp w owns rows 16*(w/2).. and
+// columns 16*(w%2)..
 template <bool CONJ>
-__device__ __forceinline__ void ctile_mma(const double (*A)[kOK][kOT],
-                                          const double (*B)[kOK][kOT],
-                                          double wr[2][2][2], double wi[2][2][2],
-                                          int lane, int warp) {
+__device__ __forceinline__ void ostage_mma(const OStage &st, double wr[2][2][2],
+                                           double wi[2][2][2], int lane,
+                                           int warp) {
   const int r0 = (warp >> 1) * 16, cb = (warp & 1) * 16;
 #pragma unroll
   for (int ks = 0; ks < kOK; ks += 4) {
     const int kk = ks + (lane & 3);
-    double a_r[2], a_i[2], b_r[2], b_i[2];
+    double2 a[2], b[2];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      a_r[t] = A[0][kk][r0 + 8 * t + (lane >> 2)];
-      a_i[t] = A[1][kk][r0 + 8 * t + (lane >> 2)];
-      b_r[t] = B[0][kk][cb + 8 * t + (lane >> 2)];
-      b_i[t] = B[1][kk][cb + 8 * t + (lane >> 2)];
+      a[t] = st.a[kk][r0 + 8 * t + (lane >> 2)];
+      b[t] = st.b[kk][cb + 8 * t + (lane >> 2)];
     }
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
@@ -243,20 +316,20 @@ __device__ __forceinline__ void ctile_mma(const double (*A)[kOK][kOT],
       for (int nt = 0; nt < 2; ++nt) {
         // conj(a) b = (ar br + ai bi) + i (ar bi - ai br)
         //      a b  = (ar br - ai bi) + i (ar bi + ai br)
-        dmma(wr[mt][nt][0], wr[mt][nt][1], a_r[mt], b_r[nt]);
-        dmma(wr[mt][nt][0], wr[mt][nt][1], CONJ ? a_i[mt] : -a_i[mt], b_i[nt]);
-        dmma(wi[mt][nt][0], wi[mt][nt][1], a_r[mt], b_i[nt]);
-        dmma(wi[mt][nt][0], wi[mt][nt][1], CONJ ? -a_i[mt] : a_i[mt], b_r[nt]);
+        dmma(wr[mt][nt][0], wr[mt][nt][1], a[mt].x, b[nt].x);
+        dmma(wr[mt][nt][0], wr[mt][nt][1], CONJ ? a[mt].y : -a[mt].y, b[nt].y);
+        dmma(wi[mt][nt][0], wi[mt][nt][1], a[mt].x, b[nt].y);
+        dmma(wi[mt][nt][0], wi[mt][nt][1], CONJ ? -a[mt].y : a[mt].y, b[nt].x);
       }
   }
 }
 
-// Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v)
-__global__ void __launch_bounds__(128)
+// Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v).  Operands are staged
+// through registers one K stage ahead of the MMAs.
+__global__ void __launch_bounds__(kOThreads)
     k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
               const double2 *s_cv, double2 *y) {
-  __shared__ double A_s[2][kOK][kOT];
-  __shared__ double B_s[2][kOK][kOT];
+  __shared__ OStage st;
   const int V = s.vale_dim, C = s.core_dim;
   const int ntc = (C + kOT - 1) / kOT;
   const int tr = blockIdx.x % ntc, tc = blockIdx.x / ntc;  // c tile, v tile
@@ -266,21 +339,36 @@ __global__ void __launch_bounds__(128)
   const double2 *S = s_cv + (long long)k * V * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double wr[2][2][2] = {}, wi[2][2][2] = {};
-  for (int l0 = 0; l0 < C; l0 += kOK) {
-    for (int i = tid; i < kOK * kOT; i += 128) {
-      const int kk = i / kOT, r = i % kOT;
-      const int l = l0 + kk, c = tr * kOT + r, v = tc * kOT + r;
-      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-      if (l < C && c < C) a = XC[(long long)l * C + c];  // X_cc(c, l)
-      if (l < C && v < V) b = S[(long long)v * C + l];   // S(l, v)
-      A_s[0][kk][r] = a.x;
-      A_s[1][kk][r] = a.y;
-      B_s[0][kk][r] = b.x;
-      B_s[1][kk][r] = b.y;
+  double2 ra[kOLoads], rb[kOLoads];
+  auto fetch = [&](int l0) {
+#pragma unroll
+    for (int q = 0; q < kOLoads; ++q) {
+      const int i = tid + q * kOThreads;
+      // A: X_cc(c, l), c fastest in memory
+      const int ar = i % kOT, ak = i / kOT;
+      const int l = l0 + ak, c = tr * kOT + ar;
+      ra[q] = (l < C && c < C) ? XC[(long long)l * C + c] : make_double2(0.0, 0.0);
+      // B: S(l, v), l fastest in memory
+      const int bk = i % kOK, br = i / kOK;
+      const int lb = l0 + bk, v = tc * kOT + br;
+      rb[q] = (lb < C && v < V) ? S[(long long)v * C + lb] : make_double2(0.0, 0.0);
     }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int q = 0; q < kOLoads; ++q) {
+      const int i = tid + q * kOThreads;
+      st.a[i / kOT][i % kOT] = ra[q];
+      st.b[i % kOK][i / kOK] = rb[q];
+    }
+  };
+  fetch(0);
+  for (int l0 = 0; l0 < C; l0 += kOK) {
     __syncthreads();
-    ctile_mma<false>(A_s, B_s, wr, wi, lane, warp);
+    store();
     __syncthreads();
+    if (l0 + kOK < C) fetch(l0 + kOK);
+    ostage_mma<false>(st, wr, wi, lane, warp);
   }
   const double2 *X = cv + tk * V * C;
   double2 *Y = y + tk * V * C;
@@ -300,13 +388,13 @@ __global__ void __launch_bounds__(128)
       }
 }
 
-// Upper tiles (J <= I) of W = S^H Y + Y^H S, then
-// VV'(j, i) = VV(j, i) - W(j, i) packed at i(i+1)/2 + j.
-__global__ void __launch_bounds__(128)
+// Upper tiles (J <= I) of W = S^H Y + Y^H S as one K loop over the stacked
+// core index (S;Y)^H (Y;S), then VV'(j, i) = VV(j, i) - W(j, i) packed at
+// i(i+1)/2 + j.
+__global__ void __launch_bounds__(kOThreads)
     k_ortho_w(DevSys s, const double2 *vv, const double2 *y,
               const double2 *s_cv, double *packed) {
-  __shared__ double A_s[2][kOK][kOT];
-  __shared__ double B_s[2][kOK][kOT];
+  __shared__ OStage st;
   const int V = s.vale_dim, C = s.core_dim;
   // upper-triangular tile index -> (J, I), J <= I
   int t = blockIdx.x, I = 0;
@@ -320,26 +408,43 @@ __global__ void __launch_bounds__(128)
   const double2 *S = s_cv + (long long)k * V * C;
   const double2 *Y = y + tk * V * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int K2 = 2 * C;
   double wr[2][2][2] = {}, wi[2][2][2] = {};
-  for (int pass = 0; pass < 2; ++pass) {
-    const double2 *Aop = pass == 0 ? S : Y;  // conj(A)^T
-    const double2 *Bop = pass == 0 ? Y : S;
-    for (int l0 = 0; l0 < C; l0 += kOK) {
-      for (int i = tid; i < kOK * kOT; i += 128) {
-        const int kk = i % kOK, r = i / kOK;  // l fastest: contiguous loads
-        const int l = l0 + kk, j = J * kOT + r, ii = I * kOT + r;
-        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
-        if (l < C && j < V) a = Aop[(long long)j * C + l];
-        if (l < C && ii < V) b = Bop[(long long)ii * C + l];
-        A_s[0][kk][r] = a.x;
-        A_s[1][kk][r] = a.y;
-        B_s[0][kk][r] = b.x;
-        B_s[1][kk][r] = b.y;
+  double2 ra[kOLoads], rb[kOLoads];
+  auto fetch = [&](int l0) {
+#pragma unroll
+    for (int q = 0; q < kOLoads; ++q) {
+      const int i = tid + q * kOThreads;
+      const int kk = i % kOK, r = i / kOK;
+      const int l = l0 + kk;
+      const int j = J * kOT + r, ii = I * kOT + r;
+      double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+      if (l < K2) {
+        const double2 *Aop = l < C ? S : Y;   // (S; Y), conjugated in the MMA
+        const double2 *Bop = l < C ? Y : S;   // (Y; S)
+        const int lc = l < C ? l : l - C;
+        if (j < V) a = Aop[(long long)j * C + lc];
+        if (ii < V) b = Bop[(long long)ii * C + lc];
       }
-      __syncthreads();
-      ctile_mma<true>(A_s, B_s, wr, wi, lane, warp);
-      __syncthreads();
+      ra[q] = a;
+      rb[q] = b;
     }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int q = 0; q < kOLoads; ++q) {
+      const int i = tid + q * kOThreads;
+      st.a[i % kOK][i / kOK] = ra[q];
+      st.b[i % kOK][i / kOK] = rb[q];
+    }
+  };
+  fetch(0);
+  for (int l0 = 0; l0 < K2; l0 += kOK) {
+    __syncthreads();
+    store();
+    __syncthreads();
+    if (l0 + kOK < K2) fetch(l0 + kOK);
+    ostage_mma<true>(st, wr, wi, lane, warp);
   }
   const double2 *VVt = vv + tk * V * V;
   const long long np = (long long)V * (V + 1) / 2;
@@ -401,10 +506,10 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
   }
   const int tcv = (C + kOT - 1) / kOT, tvv = (V + kOT - 1) / kOT;
   dim3 gy(tcv * tvv, s.nk, nterm);
-  k_ortho_y<<<gy, 128, 0, st>>>(s, cv, cc, s_cv, y);
+  k_ortho_y<<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
   IMAGO_CUDA(cudaGetLastError());
   dim3 gw(tvv * (tvv + 1) / 2, s.nk, nterm);
-  k_ortho_w<<<gw, 128, 0, st>>>(s, vv, y, s_cv, packed);
+  k_ortho_w<<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }

@@ -137,3 +137,24 @@ def test_hermitian_diagonal_and_gamma(imago_lib):
         ke = g.gauss_overlap_ke()
     assert np.abs(ol[..., 1]).max() < 1e-12
     assert np.abs(ke[..., 1]).max() < 1e-12
+
+
+def test_quartz_162_atoms_gamma(imago_lib):
+    # alpha-quartz 3x3x2 supercell (162 atoms, Si s,p,d and O s,p) at Gamma:
+    # OL, KE, NP and the most diffuse EP term of each element against the
+    # oracle.
+    s = configs.quartz_supercell(gamma=True)
+    ob = oracle.OracleBuild(s)
+    ref_ol = ob.overlap()[0]
+    ref_ke = ob.kinetic()
+    ref_np = ob.nuclear()
+    ref_ep_si = ob.elec_pot(0, 1)[0]
+    ref_ep_o = ob.elec_pot(20, 21)[0]
+    with intg.IntegralSetup(s) as g:
+        out = g.build()
+    res = {"OL": packed_mismatch(out["ol_packed"], ref_ol),
+           "KE": packed_mismatch(out["ke_packed"], ref_ke),
+           "NP": packed_mismatch(out["np_packed"], ref_np),
+           "EP0": packed_mismatch(out["ep_packed"][0], ref_ep_si),
+           "EP20": packed_mismatch(out["ep_packed"][20], ref_ep_o)}
+    _assert_all(res)
