@@ -1,21 +1,25 @@
 """Integral-build benchmark: Imago's SCF integral setup on B200.
 
-Workload (one "step"): the full integral setup of the jittered 8-atom
-silicon conventional cell with an s,p,d basis of 20 even-tempered
-primitives, 20 potential terms and an 8x8x8 k-mesh: the overlap, kinetic,
-nuclear and all 20 electronic-potential matrices, lattice-summed,
-Bloch-phased onto 512 k-points, core-orthogonalised and packed as the
-reference hands them to SCF.  Inputs are synthetic (seeded positions and
-synthesised contraction coefficients; the reference's basis database is not
-available).
+Workload (one "step", default --workload si8): the full integral setup of
+the jittered 8-atom silicon conventional cell with an s,p,d basis of 20
+even-tempered primitives, 20 potential terms and an 8x8x8 k-mesh: the
+overlap, kinetic, nuclear and all 20 electronic-potential matrices,
+lattice-summed, Bloch-phased onto 512 k-points, core-orthogonalised and
+packed as the reference hands them to SCF.  Inputs are synthetic (seeded
+positions and synthesised contraction coefficients; the reference's basis
+database is not available).  --workload quartz-gamma / quartz-222 runs the
+162-atom alpha-quartz supercell instead (Gamma only, or a 2x2x2 mesh); the
+default run also reports the quartz Gamma build as "silica_162".
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--workload si8|quartz-gamma|quartz-222]
 
 Our arm times K builds on the device (CUDA events on the library's stream,
 L2 flushed between steps, outputs resident in HBM), then the same build end
-to end through the C ABI with host buffers.  The reference arm times the
-CPU restatement of the reference's algorithm (oracle/, all host threads) on
-a bounded sample of the same workload and scales it to one build.
+to end through the C ABI with host buffers (create + build + copies into
+pinned host memory, wall clock).  The reference arm times the CPU
+restatement of the reference's algorithm (oracle/, all host threads) on a
+bounded sample of the same workload and scales it to one build.
 Under torchrun each rank builds its own independently jittered cell (weak
 scaling, no collective on the data path).
 """
@@ -33,15 +37,39 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "integral build time (OL+KE+NP+20 EP, 512 k-points)"
 UNIT = "s"
-WORKLOAD = ("Si8 conventional cell, jitter N(0,0.02 A), s,p,d basis 20 "
-            "primitives (20/20/14/0), 20 potential terms, 8x8x8 k")
+WORKLOADS = {
+    "si8": {
+        "metric": "integral build time (OL+KE+NP+20 EP, 512 k-points)",
+        "desc": ("Si8 conventional cell, jitter N(0,0.02 A), s,p,d basis 20 "
+                 "primitives (20/20/14/0), 20 potential terms, 8x8x8 k"),
+        # the oracle runs the whole build when it is this cheap
+        "cpu_stride": 1,
+    },
+    "quartz-gamma": {
+        "metric": "integral build time (OL+KE+NP+40 EP, Gamma)",
+        "desc": ("alpha-quartz SiO2 3x3x2 supercell, 162 atoms, jitter "
+                 "N(0,0.03 A), Si s,p,d (20/20/14) and O s,p (18/18) "
+                 "primitives, 20+20 potential terms, Gamma"),
+        "cpu_stride": 8,
+    },
+    "quartz-222": {
+        "metric": "integral build time (OL+KE+NP+40 EP, 8 k-points)",
+        "desc": ("alpha-quartz SiO2 3x3x2 supercell, 162 atoms, jitter "
+                 "N(0,0.03 A), Si s,p,d (20/20/14) and O s,p (18/18) "
+                 "primitives, 20+20 potential terms, 2x2x2 k (shift 1/2)"),
+        "cpu_stride": 8,
+    },
+}
 
 
-def system_for_rank(rank, kmesh=(8, 8, 8)):
+def system_for(workload, rank=0, kmesh=(8, 8, 8)):
     from imago_b200 import configs
-    return configs.silicon_cubic8(seed=2 + rank, kmesh=tuple(kmesh))
+    if workload == "si8":
+        return configs.silicon_cubic8(seed=2 + rank, kmesh=tuple(kmesh))
+    if workload == "quartz-gamma":
+        return configs.quartz_supercell(seed=3 + rank, gamma=True)
+    return configs.quartz_supercell(seed=3 + rank, kmesh=(2, 2, 2))
 
 
 def dist_env():
@@ -142,24 +170,32 @@ def fp64_peak_tflops(torch):
 
 
 # ------------------------------------------------------------- CPU legs --
-def oracle_build_time(system, nthreads, pair_stride=1):
+def oracle_build_time(system, nthreads, pair_stride=1, ep_ortho_sampled=False):
     """Seconds the oracle takes for the pair loops and the
-    orthogonalisation of OL, KE, NP and every EP term."""
+    orthogonalisation of OL, KE, NP and every EP term.  With pair_stride > 1
+    every pair_stride-th atom pair runs and the pair loops are scaled up.
+    With ep_ortho_sampled the EP terms run their pair loops only and their
+    orthogonalisation (the same Hermitian rank-2k update for every term) is
+    the mean of the KE and NP ones."""
     import oracle
     ob = oracle.OracleBuild(system, stride=pair_stride, nthreads=nthreads)
     loops = ortho = 0.0
+    zher2k = []
     for call in (ob.overlap, ob.kinetic, ob.nuclear):
         call()
         lo, ot = ob.last_times()
         loops += lo
         ortho += ot
+        if call != ob.overlap:
+            zher2k.append(ot)
+    ob.set_skip_ortho(ep_ortho_sampled)
     for t in range(ob.pot_dim):
         ob.elec_pot(t, t + 1)
         lo, ot = ob.last_times()
         loops += lo
-        ortho += ot
+        ortho += float(np.mean(zher2k)) if ep_ortho_sampled else ot
     ob.close()
-    return loops, ortho
+    return pair_stride * loops + ortho
 
 
 def k_subset(system, k_stride):
@@ -169,20 +205,25 @@ def k_subset(system, k_stride):
     return s
 
 
-def cpu_baseline(system, nthreads, limit_s=40.0):
-    """The oracle on the host cores.  A quick probe (every 8th atom pair,
-    every 16th k-point) estimates the full build; when that is within
-    limit_s the full build is timed, otherwise every 4th atom pair at every
-    k-point is timed and the pair loops are scaled by 4."""
-    lo, ot = oracle_build_time(k_subset(system, 16), nthreads, pair_stride=8)
-    estimate = 16 * (8 * lo + ot)
+def cpu_baseline(system, nthreads, workload, limit_s=40.0):
+    """The oracle on the host cores, scaled to one build of the workload.
+    Si8: a quick probe (every 8th atom pair, every 16th k-point) estimates
+    the full build; when that is within limit_s the full build is timed,
+    otherwise every 4th atom pair.  Quartz: every cpu_stride-th atom pair,
+    the EP orthogonalisations sampled."""
     t0 = time.perf_counter()
-    if estimate <= limit_s:
-        lo, ot = oracle_build_time(system, nthreads)
-        value, sample = lo + ot, "the full build"
+    stride = WORKLOADS[workload]["cpu_stride"]
+    if stride > 1:
+        value = oracle_build_time(system, nthreads, pair_stride=stride,
+                                  ep_ortho_sampled=True)
+        sample = (f"every {stride}th atom pair (pair loops scaled by {stride}), "
+                  f"EP orthogonalisation timed on KE and NP")
+        return value, time.perf_counter() - t0, sample
+    est = 16 * oracle_build_time(k_subset(system, 16), nthreads, pair_stride=8)
+    if est <= limit_s:
+        value, sample = oracle_build_time(system, nthreads), "the full build"
     else:
-        lo, ot = oracle_build_time(system, nthreads, pair_stride=4)
-        value = 4 * lo + ot
+        value = oracle_build_time(system, nthreads, pair_stride=4)
         sample = "every 4th atom pair at all k-points, pair loops scaled by 4"
     return value, time.perf_counter() - t0, sample
 
@@ -192,13 +233,16 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle  # noqa: F401
-    system = system_for_rank(0, args.kmesh)
+    wl = WORKLOADS[args.workload]
+    system = system_for(args.workload, 0, args.kmesh)
     nthreads = os.cpu_count() or 1
     times, walls = [], []
     for _ in range(args.warmup):  # warm caches and pages on a small probe
-        oracle_build_time(k_subset(system, 16), nthreads, pair_stride=8)
+        oracle_build_time(k_subset(system, 16), nthreads, pair_stride=16,
+                          ep_ortho_sampled=True)
+    what = ""
     for _ in range(args.steps):
-        v, wall, what = cpu_baseline(system, nthreads, limit_s=30.0)
+        v, wall, what = cpu_baseline(system, nthreads, args.workload, limit_s=30.0)
         times.append(v)
         walls.append(wall)
     value = float(np.mean(times))
@@ -206,11 +250,11 @@ def run_reference(args):
               f"atom pairs, {nthreads} threads): {what}; "
               f"{np.mean(walls):.1f} s of CPU work per step")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "impl": "reference", "metric": wl["metric"], "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD},
+        "data": "synthetic", "config": {"workload": wl["desc"]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -220,6 +264,105 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------- our arm --
+def device_outputs(g, torch, dev):
+    nk, npk, V, C, P = g.nk, g.npacked, g.vale_dim, g.core_dim, g.pot_dim
+    f64 = torch.float64
+    return {
+        "ol_packed": torch.empty((nk, npk, 2), dtype=f64, device=dev),
+        "ol_cv_re": torch.empty((nk, V, max(C, 1)), dtype=f64, device=dev),
+        "ol_cv_im": torch.empty((nk, V, max(C, 1)), dtype=f64, device=dev),
+        "ke_packed": torch.empty((nk, npk, 2), dtype=f64, device=dev),
+        "np_packed": torch.empty((nk, npk, 2), dtype=f64, device=dev),
+        "ep_packed": torch.empty((P, nk, npk, 2), dtype=f64, device=dev),
+    }
+
+
+def time_device_builds(g, bufs, stream, steps, flush, torch):
+    """Device seconds of each build (outputs in HBM), with 512 MiB written
+    between builds to flush L2; kernel-stage milliseconds summed."""
+    step_s, kms, launches = [], np.zeros(4), 0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
+        e.record(stream)
+        e.synchronize()
+        step_s.append(s.elapsed_time(e) / 1e3)
+        ms, n = g.kernel_stats()
+        kms += ms
+        launches += n
+    return step_s, kms, launches
+
+
+def time_e2e(system, local, stream, bufs, steps, torch):
+    """End to end through the C ABI with host buffers, wall clock: create
+    (host set-up, H2D of the system, device tables) + one build of every
+    matrix into pinned host memory (the call returns once the copies have
+    landed).  The first of steps + 1 runs is a warm-up."""
+    from imago_b200 import intg
+    pinned = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+              for k, v in bufs.items()}
+    tot, cre = [], []
+    for i in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g2 = intg.IntegralSetup(system, device=local, outputs_on_device=False,
+                                stream=stream.cuda_stream)
+        t1 = time.perf_counter()
+        g2.build(out={k: v.data_ptr() for k, v in pinned.items()})
+        t2 = time.perf_counter()
+        g2.close()
+        if i > 0:
+            tot.append(t2 - t0)
+            cre.append(t1 - t0)
+    d2h = sum(v.numel() * 8 for v in pinned.values())
+    return {"value": float(np.mean(tot)), "unit": UNIT,
+            "h2d_bytes_per_step": _system_bytes(system), "d2h_bytes_per_step": d2h,
+            "create_s": float(np.mean(cre)),
+            "build_and_copy_s": float(np.mean(tot) - np.mean(cre))}
+
+
+def silica_headline(args, local, stream, torch):
+    """The 162-atom alpha-quartz build at Gamma (device time, end to end
+    and the oracle on the host cores), reported beside the main line."""
+    from imago_b200 import intg
+    wl = "quartz-gamma"
+    system = system_for(wl)
+    dev = torch.device("cuda", local)
+    g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
+                           stream=stream.cuda_stream)
+    bufs = device_outputs(g, torch, dev)
+    flush = torch.empty(512 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        step_s, kms, launches = time_device_builds(g, bufs, stream, 5, flush, torch)
+    out = {"workload": WORKLOADS[wl]["desc"], "metric": WORKLOADS[wl]["metric"],
+           "value": float(np.mean(step_s)), "unit": UNIT,
+           "stage_ms": dict(zip(STAGES, [float(x) / 5 for x in kms])),
+           "vale_dim": g.vale_dim, "core_dim": g.core_dim, "pot_terms": g.pot_dim,
+           "pair_images": g.num_pair_images, "shell_pairs": g.num_shell_pairs,
+           "gpu_launches": int(launches), "clocks": clk.summary()}
+    g.close()
+    out["e2e"] = time_e2e(system, local, stream, bufs, 2, torch)
+    del bufs, flush
+    torch.cuda.empty_cache()
+    if not args.skip_cpu:
+        ncores = os.cpu_count() or 1
+        v, wall, what = cpu_baseline(system, ncores, wl)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": ncores,
+                               "kind": "port",
+                               "sample": (f"oracle (CPU restatement, OpenMP over "
+                                          f"atom pairs): {what}; {wall:.1f} s wall")}
+    return out
+
+
+STAGES = ["prim", "contract", "bloch", "ortho"]
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -230,47 +373,26 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from imago_b200 import intg
 
-    system = system_for_rank(rank, args.kmesh)
+    wl = WORKLOADS[args.workload]
+    system = system_for(args.workload, rank, args.kmesh)
     stream = torch.cuda.current_stream()
     g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
-                           stream=stream.cuda_stream)
-    nk, npk, V, C, P = g.nk, g.npacked, g.vale_dim, g.core_dim, g.pot_dim
+                           stream=stream.cuda_stream,
+                           scratch_bytes=args.scratch_mb << 20)
+    nk, V, C, P = g.nk, g.vale_dim, g.core_dim, g.pot_dim
     dev = torch.device("cuda", local)
-    bufs = {
-        "ol_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
-        "ol_cv_re": torch.empty((nk, V, max(C, 1)), dtype=torch.float64, device=dev),
-        "ol_cv_im": torch.empty((nk, V, max(C, 1)), dtype=torch.float64, device=dev),
-        "ke_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
-        "np_packed": torch.empty((nk, npk, 2), dtype=torch.float64, device=dev),
-        "ep_packed": torch.empty((P, nk, npk, 2), dtype=torch.float64, device=dev),
-    }
+    bufs = device_outputs(g, torch, dev)
     flush = torch.empty(512 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
 
-    def one_build():
-        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
-
     for _ in range(args.warmup):
-        one_build()
+        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    step_s = []
-    kms = np.zeros(4)
-    launches = 0
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1.0)  # write 512 MiB > L2 between timed steps
-            s = torch.cuda.Event(enable_timing=True)
-            e = torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            one_build()
-            e.record(stream)
-            e.synchronize()
-            step_s.append(s.elapsed_time(e) / 1e3)
-            ms, n = g.kernel_stats()
-            kms += ms
-            launches += n
+        step_s, kms, launches = time_device_builds(g, bufs, stream, args.steps,
+                                                   flush, torch)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -282,34 +404,12 @@ def run_ours(args):
     value = total / args.steps
     kms /= args.steps
 
-    # end to end through the C ABI with host buffers: create (stages the
-    # system on the device) + all builds + copies into pinned host memory
-    pinned = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
-              for k, v in bufs.items()}
-    e2e_s = []
-    h2d = _system_bytes(system)
-    d2h = sum(v.numel() * 8 for v in pinned.values())
-    e2e_steps = max(2, min(args.steps, 3))
-    for i in range(e2e_steps + 1):
-        torch.cuda.synchronize()
-        s = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        g2 = intg.IntegralSetup(system, device=local, outputs_on_device=False,
-                                stream=stream.cuda_stream)
-        g2.build(out={k: v.data_ptr() for k, v in pinned.items()})
-        e.record(stream)
-        e.synchronize()
-        g2.close()
-        if i > 0:  # first is a warm-up
-            e2e_s.append(s.elapsed_time(e) / 1e3)
-    e2e = float(np.mean(e2e_s))
+    e2e = time_e2e(system, local, stream, bufs, max(2, min(args.steps, 3)), torch)
 
     flops = algorithmic_flops(g)
     fp64 = fp64_peak_tflops(torch) if rank == 0 else None
-    stage_names = ["prim", "contract", "bloch", "ortho"]
     top = int(np.argmax(kms))
-    top_name = stage_names[top]
+    top_name = STAGES[top]
     roofline = None
     if top_name in flops and fp64:
         achieved = flops[top_name] / (kms[top] / 1e3) / 1e12
@@ -318,40 +418,40 @@ def run_ours(args):
                     "kernel": top_name,
                     "peak_source": "measured cuBLAS DGEMM 8192^3 in this run "
                                    "(MEASURED_PEAKS.json has no FP64 figure)"}
-    line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.skip_cpu:
             ncores = os.cpu_count() or 1
-            v, wall, what = cpu_baseline(system, ncores)
+            v, wall, what = cpu_baseline(system, ncores, args.workload)
             cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
                    "sample": (f"oracle (CPU restatement, OpenMP over atom "
                               f"pairs): {what}; {wall:.1f} s wall")}
-        if list(args.kmesh) != [8, 8, 8]:
-            line_note = f"k-mesh {args.kmesh} (profiling case, not the measured workload)"
-        else:
-            line_note = None
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": wl["metric"], "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded jitter, synthesised contraction coefficients)",
-            "config": {"workload": WORKLOAD, "l2": "512 MiB flush between steps",
+            "config": {"workload": wl["desc"], "l2": "512 MiB flush between steps",
                        "vale_dim": V, "core_dim": C, "kpoints": nk, "pot_terms": P,
                        "pair_images": g.num_pair_images,
                        "shell_pairs": g.num_shell_pairs},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": e2e,
             "gpu_launches": int(launches),
-            "stage_ms": dict(zip(stage_names, [float(x) for x in kms])),
+            "stage_ms": dict(zip(STAGES, [float(x) for x in kms])),
             "shell_pairs_per_s": g.num_shell_pairs * (3 + P) / value,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
-        if line_note:
-            line["note"] = line_note
+        if args.workload == "si8" and list(args.kmesh) != [8, 8, 8]:
+            line["note"] = (f"k-mesh {args.kmesh} (profiling case, not the "
+                            f"measured workload)")
+        g.close()
+        del bufs, flush
+        torch.cuda.empty_cache()
+        if world == 1 and args.workload == "si8" and not args.no_silica:
+            line["silica_162"] = silica_headline(args, local, stream, torch)
         print(json.dumps(line), flush=True)
     g.close()
     if world > 1:
@@ -370,9 +470,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--workload", default="si8", choices=sorted(WORKLOADS))
     ap.add_argument("--kmesh", type=int, nargs=3, default=[8, 8, 8],
                     help="k-mesh of the Si8 cell; the measured workload is 8 8 8, "
                          "smaller meshes are for profiling captures")
+    ap.add_argument("--scratch-mb", type=int, default=0,
+                    help="device scratch budget of the EP chunks (0: a quarter "
+                         "of free memory); small budgets are for profiling")
+    ap.add_argument("--no-silica", action="store_true",
+                    help="skip the 162-atom quartz report of the default run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -33,33 +34,68 @@ const double kAngNorm[16] = {
     0.5900435899266435, 0.3731763325901154, 0.4570457994644657,
     0.4570457994644657};
 
+// Device scratch comes from one library-owned stream-ordered memory pool
+// per device (cudaMallocFromPoolAsync / cudaFreeAsync on the context's
+// stream).  Freed memory stays in the pool, so a context created after
+// another reuses it without cudaMalloc/cudaFree and their device-wide
+// synchronisation; imago_trim_memory hands it back to the driver.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_lock;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+
+cudaMemPool_t scratch_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxPoolDevices) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> guard(g_pool_lock);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
 template <class T>
 struct DBuf {
   T *p = nullptr;
   size_t n = 0;
-  int alloc(size_t count) {
+  int alloc(size_t count, cudaStream_t st) {
     if (count <= n && p) return IMAGO_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
+    release(st);
     if (count == 0) return IMAGO_OK;
-    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+    cudaMemPool_t pool = scratch_pool();
+    void *q = nullptr;
+    if (!pool || cudaMallocFromPoolAsync(&q, count * sizeof(T), pool, st) !=
+                     cudaSuccess) {
       cudaGetLastError();
       return IMAGO_ERR_NOMEM;
     }
+    p = static_cast<T *>(q);
     n = count;
     return IMAGO_OK;
   }
   int upload(const std::vector<T> &v, cudaStream_t st) {
-    int rc = alloc(v.empty() ? 1 : v.size());
+    int rc = alloc(v.empty() ? 1 : v.size(), st);
     if (rc) return rc;
     if (!v.empty())
       IMAGO_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T),
                                  cudaMemcpyHostToDevice, st));
     return IMAGO_OK;
   }
-  void release() {
-    if (p) cudaFree(p);
+  void release(cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     n = 0;
   }
@@ -125,9 +161,16 @@ struct imago_ctx {
   DBuf<DSp> d_sps;
   DBuf<Term3c> d_terms;
   DBuf<int2> d_btile;
+  DBuf<SiteImage> d_simg;
 
   // scratch
-  DBuf<double> blk, M, packed_stage;
+  DBuf<double> blk, M;
+  // host-output staging: one region per output matrix, so that each can be
+  // copied out on copy_stream while the next build runs
+  DBuf<double> out_stage;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> cev;
+  int cev_used = 0;
   DBuf<double2> vv, cv, cc, y, s_cv;
   bool have_ol = false;
 
@@ -144,23 +187,27 @@ struct imago_ctx {
   double kernel_ms[4] = {0, 0, 0, 0};
 
   ~imago_ctx() {
-    d_type_nalpha.release(); d_type_alpha_off.release(); d_type_nstates.release();
-    d_type_nvale.release(); d_type_state_off.release(); d_type_basis_off.release();
-    d_type_screen.release(); d_alpha_cls.release(); d_state_lm.release();
-    d_site_type.release(); d_site_cum_vale.release(); d_site_cum_core.release();
-    d_ptype_alpha_off.release(); d_ptype_nalpha.release();
-    d_ptype_first_site.release(); d_ptype_mult.release(); d_ptype_screen.release();
-    d_psite_ptype.release(); d_sp_by_cls.release(); d_alpha.release();
-    d_basis.release(); d_site_pos.release(); d_ptype_z.release();
-    d_ptype_nucalpha.release(); d_palpha.release(); d_psite_pos.release();
-    d_cell.release(); d_csize.release(); d_kxyz.release(); d_phase.release();
-    d_pairs.release(); d_units.release(); d_sps.release(); d_terms.release();
-    d_btile.release();
-    blk.release(); M.release(); packed_stage.release(); vv.release();
-    cv.release(); cc.release(); y.release(); s_cv.release();
+    cudaStream_t st = stream;
+    for (auto *b : {&d_type_nalpha, &d_type_alpha_off, &d_type_nstates,
+                    &d_type_nvale, &d_type_state_off, &d_type_basis_off,
+                    &d_type_screen, &d_alpha_cls, &d_state_lm, &d_site_type,
+                    &d_site_cum_vale, &d_site_cum_core, &d_ptype_alpha_off,
+                    &d_ptype_nalpha, &d_ptype_first_site, &d_ptype_mult,
+                    &d_ptype_screen, &d_psite_ptype, &d_sp_by_cls})
+      b->release(st);
+    for (auto *b : {&d_alpha, &d_basis, &d_site_pos, &d_ptype_z,
+                    &d_ptype_nucalpha, &d_palpha, &d_psite_pos, &d_cell,
+                    &d_csize, &d_kxyz, &blk, &M, &out_stage})
+      b->release(st);
+    for (auto *b : {&d_phase, &vv, &cv, &cc, &y, &s_cv}) b->release(st);
+    d_pairs.release(st); d_units.release(st); d_sps.release(st);
+    d_terms.release(st); d_btile.release(st); d_simg.release(st);
+    if (st) cudaStreamSynchronize(st);
     if (events)
       for (auto &e : ev) cudaEventDestroy(e);
     for (auto &e : kev) cudaEventDestroy(e);
+    for (auto &e : cev) cudaEventDestroy(e);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 };
@@ -182,6 +229,40 @@ void recip_vectors(imago_ctx *c) {
     for (int j = 0; j < 3; ++j) c->recip[3 * i + j] = 2.0 * kPi * r[j] / vol;
   }
   for (int i = 0; i < 9; ++i) c->inv[i] = c->recip[i] / (2.0 * kPi);
+}
+
+// Smallest singular value of realVectors: the square root of the smallest
+// eigenvalue of the Gram matrix G = R R^T, by cyclic Jacobi rotations.
+double smallest_singular(const double *rv) {
+  double g[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      g[i][j] = 0.0;
+      for (int x = 0; x < 3; ++x) g[i][j] += rv[3 * i + x] * rv[3 * j + x];
+    }
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    const double off = g[0][1] * g[0][1] + g[0][2] * g[0][2] + g[1][2] * g[1][2];
+    const double dia = g[0][0] * g[0][0] + g[1][1] * g[1][1] + g[2][2] * g[2][2];
+    if (off <= 1e-30 * dia) break;
+    for (int p = 0; p < 2; ++p)
+      for (int q = p + 1; q < 3; ++q) {
+        if (g[p][q] == 0.0) continue;
+        const double th = 0.5 * std::atan2(2.0 * g[p][q], g[q][q] - g[p][p]);
+        const double c = std::cos(th), sn = std::sin(th);
+        for (int k = 0; k < 3; ++k) {  // G <- G J
+          const double a = g[k][p], b = g[k][q];
+          g[k][p] = c * a - sn * b;
+          g[k][q] = sn * a + c * b;
+        }
+        for (int k = 0; k < 3; ++k) {  // G <- J^T G
+          const double a = g[p][k], b = g[q][k];
+          g[p][k] = c * a - sn * b;
+          g[q][k] = sn * a + c * b;
+        }
+      }
+  }
+  const double lmin = std::min(g[0][0], std::min(g[1][1], g[2][2]));
+  return std::sqrt(std::max(lmin, 0.0));
 }
 
 bool border_within(const double *rv, const double *t, double lim) {
@@ -518,6 +599,8 @@ int build_work(imago_ctx *c) {
   return IMAGO_OK;
 }
 
+constexpr size_t kMaxSiteImageBytes = size_t(4) << 30;
+
 int upload(imago_ctx *c) {
   cudaStream_t st = c->stream;
   std::vector<int> nalpha, aoff, nstates, nvale, soff, boff, cls, lm;
@@ -562,7 +645,7 @@ int upload(imago_ctx *c) {
   UP(d_sps, c->sps) UP(d_sp_by_cls, c->sp_by_cls) UP(d_terms, c->ep_terms)
   UP(d_btile, c->btile)
 #undef UP
-  if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk))) return rc;
+  if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk, st))) return rc;
 
   DevSys &s = c->sys;
   s.nt = c->nt; s.ns = c->ns; s.npt = c->npt; s.nps = c->nps; s.nk = c->nk;
@@ -570,6 +653,7 @@ int upload(imago_ctx *c) {
   s.T = c->T;
   std::memcpy(s.rv, c->rv, sizeof s.rv);
   std::memcpy(s.inv, c->inv, sizeof s.inv);
+  s.far_lattice = 1.5 * smallest_singular(c->rv) * (1.0 - 1e-6);
   s.type_nalpha = c->d_type_nalpha.p; s.type_alpha_off = c->d_type_alpha_off.p;
   s.type_nstates = c->d_type_nstates.p; s.type_nvale = c->d_type_nvale.p;
   s.type_state_off = c->d_type_state_off.p; s.type_basis_off = c->d_type_basis_off.p;
@@ -594,7 +678,18 @@ int upload(imago_ctx *c) {
   w.m_total = c->m_total;
   w.nbtile = (int)c->btile.size();
   w.btile = c->d_btile.p;
-  return launch_phase(s, c->d_phase.p, st);
+  w.simg = nullptr;
+  if ((rc = launch_phase(s, c->d_phase.p, st))) return rc;
+  // midpoint images of the potential sites for the three-centre screens,
+  // when the table fits in kMaxSiteImageBytes; without it every site is
+  // searched in full
+  const size_t nb = (size_t)w.nunits * c->nps;
+  if (nb > 0 && nb * sizeof(SiteImage) <= kMaxSiteImageBytes &&
+      c->d_simg.alloc(nb, st) == IMAGO_OK) {
+    w.simg = c->d_simg.p;
+    rc = launch_site_images(s, w, c->d_simg.p, st);
+  }
+  return rc;
 }
 
 // Device bytes one term of a build needs between its stages.
@@ -608,12 +703,12 @@ size_t term_bytes(const imago_ctx *c) {
 int ensure_scratch(imago_ctx *c, int nterm) {
   const size_t V = c->vale_dim, C = c->core_dim, nk = c->nk;
   int rc;
-  if ((rc = c->blk.alloc((size_t)c->blk_total * nterm + 1))) return rc;
-  if ((rc = c->M.alloc((size_t)c->m_total * nterm + 1))) return rc;
-  if ((rc = c->vv.alloc(nk * V * V * nterm + 1))) return rc;
-  if ((rc = c->cv.alloc(nk * V * C * nterm + 1))) return rc;
-  if ((rc = c->cc.alloc(nk * C * C * nterm + 1))) return rc;
-  if ((rc = c->y.alloc(nk * V * C * nterm + 1))) return rc;
+  if ((rc = c->blk.alloc((size_t)c->blk_total * nterm + 1, c->stream))) return rc;
+  if ((rc = c->M.alloc((size_t)c->m_total * nterm + 1, c->stream))) return rc;
+  if ((rc = c->vv.alloc(nk * V * V * nterm + 1, c->stream))) return rc;
+  if ((rc = c->cv.alloc(nk * V * C * nterm + 1, c->stream))) return rc;
+  if ((rc = c->cc.alloc(nk * C * C * nterm + 1, c->stream))) return rc;
+  if ((rc = c->y.alloc(nk * V * C * nterm + 1, c->stream))) return rc;
   return IMAGO_OK;
 }
 
@@ -670,7 +765,7 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   mark(c);
   if (kind == KIND_OL && c->core_dim > 0) {
     const size_t n = (size_t)c->nk * c->vale_dim * c->core_dim;
-    if ((rc = c->s_cv.alloc(n))) return rc;
+    if ((rc = c->s_cv.alloc(n, st))) return rc;
     IMAGO_CUDA(cudaMemcpyAsync(c->s_cv.p, c->cv.p, n * sizeof(double2),
                                cudaMemcpyDeviceToDevice, st));
   }
@@ -680,12 +775,34 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   return rc;
 }
 
+cudaEvent_t next_copy_event(imago_ctx *c) {
+  if (c->cev_used == (int)c->cev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    c->cev.push_back(e);
+  }
+  return c->cev[c->cev_used++];
+}
+
+// Copy a finished output to the caller.  Device outputs: on the build
+// stream.  Host outputs: on copy_stream once the build stream has produced
+// it, so the transfer overlaps the builds that follow.
 int copy_out(imago_ctx *c, double *dst, const double *src, size_t n) {
-  if (!dst) return IMAGO_OK;
+  if (!dst || n == 0) return IMAGO_OK;
+  if (c->outputs_on_device) {
+    IMAGO_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+    return IMAGO_OK;
+  }
+  cudaEvent_t e = next_copy_event(c);
+  if (!e) return IMAGO_ERR_CUDA;
+  IMAGO_CUDA(cudaEventRecord(e, c->stream));
+  IMAGO_CUDA(cudaStreamWaitEvent(c->copy_stream, e, 0));
   IMAGO_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
-                             c->outputs_on_device ? cudaMemcpyDeviceToDevice
-                                                  : cudaMemcpyDeviceToHost,
-                             c->stream));
+                             cudaMemcpyDeviceToHost, c->copy_stream));
   return IMAGO_OK;
 }
 
@@ -693,28 +810,52 @@ size_t packed_doubles(const imago_ctx *c) {
   return (size_t)2 * c->nk * ((size_t)c->vale_dim * (c->vale_dim + 1) / 2);
 }
 
-// Destination for a build's packed output: the caller's device buffer
-// directly, or a device staging buffer copied out afterwards.
-double *packed_target(imago_ctx *c, double *user, int nterm, int *rc) {
+size_t cv_doubles(const imago_ctx *c) {
+  return (size_t)c->nk * c->vale_dim * c->core_dim;
+}
+
+// Host-output staging layout: packed OL, KE, NP, then one region per EP
+// term, then coreValeOL (re, im).  Allocated whole before a call's first
+// build, so no region moves while a copy out of it is pending.
+enum Slot { SLOT_OL = 0, SLOT_KE = 1, SLOT_NP = 2, SLOT_EP = 3 };
+
+int ensure_out_stage(imago_ctx *c) {
+  if (c->outputs_on_device) return IMAGO_OK;
+  if (!c->copy_stream &&
+      cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    c->copy_stream = nullptr;
+    return IMAGO_ERR_CUDA;
+  }
+  const size_t n = packed_doubles(c) * (3 + (size_t)c->pot_dim) + 2 * cv_doubles(c);
+  return c->out_stage.alloc(n, c->stream);
+}
+
+// Destination of a build's packed output: the caller's device buffer
+// directly, or the output's staging region.
+double *packed_target(imago_ctx *c, double *user, int slot) {
   if (c->outputs_on_device && user) return user;
-  *rc = c->packed_stage.alloc(packed_doubles(c) * nterm);
-  return c->packed_stage.p;
+  return c->out_stage.p + packed_doubles(c) * slot;
 }
 
 int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
   int rc = IMAGO_OK;
-  double *tgt = packed_target(c, packed, 1, &rc);
-  if (rc) return rc;
+  double *tgt = packed_target(c, packed, SLOT_OL);
   if ((rc = run_build(c, KIND_OL, 0, 1, tgt))) return rc;
   c->have_ol = true;
   if (tgt != packed && (rc = copy_out(c, packed, tgt, packed_doubles(c)))) return rc;
-  const size_t ncv = (size_t)c->nk * c->vale_dim * c->core_dim;
+  const size_t ncv = cv_doubles(c);
   if (ncv && (cv_re || cv_im)) {
     double *re = cv_re, *im = cv_im;
     if (!c->outputs_on_device) {
-      // stage the split through the y buffer
-      re = reinterpret_cast<double *>(c->y.p);
+      re = c->out_stage.p + packed_doubles(c) * (3 + (size_t)c->pot_dim);
       im = re + ncv;
+    } else if (!re || !im) {
+      // one of the two requested on the device: split through y
+      double *scratch = reinterpret_cast<double *>(c->y.p);
+      if (!re) re = scratch;
+      if (!im) im = scratch + ncv;
     }
     if ((rc = launch_split_cv(c->sys, c->s_cv.p, re, im, c->stream))) return rc;
     c->launches += 1;
@@ -729,12 +870,15 @@ int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
 int do_simple(imago_ctx *c, Kind kind, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
   int rc = IMAGO_OK;
-  double *tgt = packed_target(c, packed, 1, &rc);
-  if (rc) return rc;
+  double *tgt = packed_target(c, packed, kind == KIND_KE ? SLOT_KE : SLOT_NP);
   if ((rc = run_build(c, kind, 0, 1, tgt))) return rc;
   if (tgt != packed) rc = copy_out(c, packed, tgt, packed_doubles(c));
   return rc;
 }
+
+// Host outputs: EP runs in at least kEpCopyChunks chunks, so that copying
+// one chunk's matrices overlaps building the next.
+constexpr int kEpCopyChunks = 4;
 
 int do_ep(imago_ctx *c, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
@@ -748,31 +892,36 @@ int do_ep(imago_ctx *c, double *packed) {
   const size_t per = term_bytes(c);
   int chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
   chunk = std::min(chunk, nterm);
+  if (!c->outputs_on_device)
+    chunk = std::min(chunk, std::max(1, (nterm + kEpCopyChunks - 1) / kEpCopyChunks));
   const size_t npd = packed_doubles(c);
   for (int t0 = 0; t0 < nterm; t0 += chunk) {
     const int n = std::min(chunk, nterm - t0);
     int rc = IMAGO_OK;
     double *user = packed ? packed + npd * t0 : nullptr;
-    double *tgt = packed_target(c, user, n, &rc);
-    if (rc) return rc;
+    double *tgt = packed_target(c, user, SLOT_EP + t0);
     if ((rc = run_build(c, KIND_EP, t0, n, tgt))) return rc;
     if (tgt != user && (rc = copy_out(c, user, tgt, npd * n))) return rc;
   }
   return IMAGO_OK;
 }
 
-void begin_call(imago_ctx *c) {
+int begin_call(imago_ctx *c) {
   c->kev_used = 0;
+  c->cev_used = 0;
   c->launches = 0;
+  return ensure_out_stage(c);
 }
 
 int finish(imago_ctx *c, int rc) {
   if (rc != IMAGO_OK) {
     cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     cudaGetLastError();
     return rc;
   }
   IMAGO_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->copy_stream) IMAGO_CUDA(cudaStreamSynchronize(c->copy_stream));
   for (int k = 0; k < 4; ++k) c->kernel_ms[k] = 0.0;
   for (int b = 0; b + 4 < c->kev_used; b += 5)
     for (int k = 0; k < 4; ++k) {
@@ -864,7 +1013,7 @@ int imago_gauss_overlap_ol(imago_ctx *c, double *packed, double *cv_re,
   if (!c) return IMAGO_ERR_INVALID;
   int rc = set_device(c);
   if (rc) return rc;
-  begin_call(c);
+  if ((rc = begin_call(c))) return finish(c, rc);
   cudaEventRecord(c->ev[0], c->stream);
   rc = do_ol(c, packed, cv_re, cv_im);
   cudaEventRecord(c->ev[1], c->stream);
@@ -877,7 +1026,7 @@ int imago_gauss_overlap_ke(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
   int rc = set_device(c);
   if (rc) return rc;
-  begin_call(c);
+  if ((rc = begin_call(c))) return finish(c, rc);
   cudaEventRecord(c->ev[2], c->stream);
   rc = do_simple(c, KIND_KE, packed);
   cudaEventRecord(c->ev[3], c->stream);
@@ -890,7 +1039,7 @@ int imago_gauss_overlap_np(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
   int rc = set_device(c);
   if (rc) return rc;
-  begin_call(c);
+  if ((rc = begin_call(c))) return finish(c, rc);
   cudaEventRecord(c->ev[4], c->stream);
   rc = do_simple(c, KIND_NP, packed);
   cudaEventRecord(c->ev[5], c->stream);
@@ -903,7 +1052,7 @@ int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
   int rc = set_device(c);
   if (rc) return rc;
-  begin_call(c);
+  if ((rc = begin_call(c))) return finish(c, rc);
   cudaEventRecord(c->ev[6], c->stream);
   rc = do_ep(c, packed);
   cudaEventRecord(c->ev[7], c->stream);
@@ -916,7 +1065,7 @@ int imago_intg_build(imago_ctx *c, unsigned which, const imago_out *out) {
   if (!c || !out) return IMAGO_ERR_INVALID;
   int rc = set_device(c);
   if (rc) return rc;
-  begin_call(c);
+  if ((rc = begin_call(c))) return finish(c, rc);
   if (which & IMAGO_OL) {
     cudaEventRecord(c->ev[0], c->stream);
     rc = do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im);
@@ -964,7 +1113,20 @@ void imago_intg_destroy(imago_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   delete c;
+}
+
+int imago_trim_memory(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  if (device >= kMaxPoolDevices) return IMAGO_OK;
+  std::lock_guard<std::mutex> guard(g_pool_lock);
+  if (g_pools[device]) IMAGO_CUDA(cudaMemPoolTrimTo(g_pools[device], 0));
+  return IMAGO_OK;
 }
 
 const char *imago_strerror(int status) {

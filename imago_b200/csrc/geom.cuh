@@ -47,6 +47,109 @@ __device__ __forceinline__ void nearest_lattice(const DevSys &s,
   out[2] = best[2];
 }
 
+// Nearest image of potential site `site` to the midpoint of the unit's
+// segment, over the 27 lattice points around the rounded fractional
+// coordinates; every lattice point outside that block is at least
+// far_lattice away, which caps both bounds.  Bounds are shrunk by 1e-9
+// relative and 1e-9 bohr and rounded down to float, so that they stay
+// below the exact distances.
+__device__ __forceinline__ SiteImage site_image(const DevSys &s,
+                                                const DevWork &w, int unit,
+                                                int site) {
+  const DUnit u = w.units[unit];
+  const DPair p = w.pairs[u.pair];
+  double d[3], f[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double a = s.site_pos[3 * p.i + x];
+    const double b = s.site_pos[3 * p.j + x] + p.L0[x] + s.cell[3 * u.cell + x];
+    d[x] = 0.5 * (a + b) - s.psite_pos[3 * site + x];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    f[i] = rint(d[0] * s.inv[3 * i] + d[1] * s.inv[3 * i + 1] +
+                d[2] * s.inv[3 * i + 2]);
+  double b1 = 1e300, b2 = 1e300;
+  int n1[3] = {0, 0, 0};
+  for (int i = -1; i <= 1; ++i)
+    for (int j = -1; j <= 1; ++j)
+      for (int k = -1; k <= 1; ++k) {
+        const double c0 = f[0] + i, c1 = f[1] + j, c2 = f[2] + k;
+        double dd = 0.0;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+          const double e = d[x] - (c0 * s.rv[x] + c1 * s.rv[3 + x] + c2 * s.rv[6 + x]);
+          dd += e * e;
+        }
+        if (dd < b1) {
+          b2 = b1;
+          b1 = dd;
+          n1[0] = (int)c0;
+          n1[1] = (int)c1;
+          n1[2] = (int)c2;
+        } else if (dd < b2) {
+          b2 = dd;
+        }
+      }
+  SiteImage r;
+  const bool fits = abs(n1[0]) < 32000 && abs(n1[1]) < 32000 && abs(n1[2]) < 32000;
+  auto lower = [](double dist) {
+    return __double2float_rd(fmax(0.0, dist * (1.0 - 1e-9) - 1e-9));
+  };
+  r.n[0] = fits ? (short)n1[0] : 0;
+  r.n[1] = fits ? (short)n1[1] : 0;
+  r.n[2] = fits ? (short)n1[2] : 0;
+  r.pad = 0;
+  // without a representable image both bounds are 0: the kernels then fall
+  // back to the full search whenever the stored image is out of range
+  r.d1 = fits ? lower(fmin(sqrt(b1), s.far_lattice)) : 0.f;
+  r.d2 = fits ? lower(fmin(sqrt(b2), s.far_lattice)) : 0.f;
+  return r;
+}
+
+// Closest-image search of a three-centre screen (the findLatticeVector step
+// of nuclearPE/electronicPE, integrals.F90:2632,2791) for the point Ps with
+// |Ps - M| = pm, radius^2 t.  Returns false when no image of site C lies
+// within the radius; otherwise sets L2, the lattice vector from which the
+// images in range are enumerated, and v = Ps - C - L2 with |v|^2 <= t.  With
+// the stored midpoint image: no lattice point is nearer to Ps - C than
+// d1 - pm, none but the stored one nearer than d2 - pm.
+__device__ __forceinline__ bool site_search(const DevSys &s, const DevWork &w,
+                                            int unit, int site,
+                                            const double Ps[3], double pm,
+                                            double t, double L2[3],
+                                            double v[3], double &c0) {
+  const double *C = s.psite_pos + 3 * site;
+  if (w.simg) {
+    const SiteImage im = w.simg[(long long)unit * s.nps + site];
+    const double rt = sqrt(t);
+    if ((double)im.d1 - pm > rt) return false;
+    double c = 0.0;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      L2[x] = im.n[0] * s.rv[x] + im.n[1] * s.rv[3 + x] + im.n[2] * s.rv[6 + x];
+      v[x] = Ps[x] - C[x] - L2[x];
+      c += v[x] * v[x];
+    }
+    if (c <= t) {
+      c0 = c;
+      return true;
+    }
+    if ((double)im.d2 - pm > rt) return false;
+  }
+  double d[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) d[x] = Ps[x] - C[x];
+  nearest_lattice(s, d, L2);
+  c0 = 0.0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    v[x] = Ps[x] - C[x] - L2[x];
+    c0 += v[x] * v[x];
+  }
+  return c0 <= t;
+}
+
 struct SpGeom {
   double A[3], B[3];   // atom 1, shifted atom 2
   double a1, a2;       // primitive exponents

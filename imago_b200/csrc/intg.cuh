@@ -15,6 +15,9 @@ struct DevSys {
   double T;            // logBasisFnThresh = -ln(basisFnConvg)
   double rv[9];        // realVectors [abc*3 + xyz]
   double inv[9];       // invRealVectors [abc*3 + xyz]
+  // 1.5 x the smallest singular value of realVectors: every lattice point
+  // outside the 3x3x3 block around a rounded point is at least this far
+  double far_lattice;
   // atom types
   const int *type_nalpha, *type_alpha_off, *type_nstates, *type_nvale,
       *type_state_off, *type_basis_off, *type_screen;
@@ -72,6 +75,19 @@ struct DevWork {
   long long m_total;      // doubles of unit blocks per term
   int nbtile;             // phase-sum column tiles: (pair, tile)
   const int2 *btile;
+  // [unit * nps + site]: the potential site's nearest image to the midpoint
+  // of the unit's A-B segment (null: every site is searched in full)
+  const struct SiteImage *simg;
+};
+
+// Nearest image of a potential site C to the midpoint M of a unit's A-B
+// segment: M - C - (n0 a + n1 b + n2 c) is shortest for lattice coordinates
+// n; d1 and d2 are lower bounds of the distance from M - C to that lattice
+// point and to every other one.
+struct __align__(16) SiteImage {
+  short n[3];
+  short pad;
+  float d1, d2;
 };
 
 // Columns (block elements) per phase-sum CTA.
@@ -100,6 +116,8 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
 int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
                     cudaStream_t st);
 int launch_phase(const DevSys &s, double2 *phase, cudaStream_t st);
+int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
+                       cudaStream_t st);
 int launch_prim_eval(int kind, int n, const double *params, const int *cls,
                      double *sh, cudaStream_t st);
 

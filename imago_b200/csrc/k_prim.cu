@@ -2,6 +2,8 @@
 //
 // Shell pairs are sorted by class; each s/p/d class runs a fully unrolled
 // kernel, the f classes share runtime-class kernels.
+#include <algorithm>
+
 #include "geom.cuh"
 #include "prim.cuh"
 
@@ -42,11 +44,15 @@ __global__ void __launch_bounds__(128)
   const double frac = 1 - q.r2 / adist;
   double Ps[3], Pt[3];
   const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
+  double pm = 0.0;  // |Ps - M|, M the midpoint of A and B
 #pragma unroll
   for (int x = 0; x < 3; ++x) {
     Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
     Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+    const double e = Ps[x] - 0.5 * (q.A[x] + q.B[x]);
+    pm += e * e;
   }
+  pm = sqrt(pm);
   double Q[nherm(L)];
 #pragma unroll
   for (int i = 0; i < nherm(L); ++i) Q[i] = 0.0;
@@ -83,17 +89,8 @@ __global__ void __launch_bounds__(128)
       w0 = -Z * (2.0 * kPi / z3);
     }
     const double *C = s.psite_pos + 3 * site;
-    double d[3], L2[3], v[3];
-#pragma unroll
-    for (int x = 0; x < 3; ++x) d[x] = Ps[x] - C[x];
-    nearest_lattice(s, d, L2);
-    double c0 = 0.0;
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-      v[x] = Ps[x] - C[x] - L2[x];
-      c0 += v[x] * v[x];
-    }
-    if (c0 > t) continue;
+    double L2[3], v[3], c0;
+    if (!site_search(s, w, sp.unit, site, Ps, pm, t, L2, v, c0)) continue;
     const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
     for (int nc = 0; nc < s.ncell; ++nc) {
       if (s.csize[nc] > maxr) break;
@@ -142,10 +139,14 @@ __global__ void __launch_bounds__(128)
   const double frac = 1 - q.r2 / adist;
   double Ps[3], Pt[3];
   const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
+  double pm = 0.0;  // |Ps - M|, M the midpoint of A and B
   for (int x = 0; x < 3; ++x) {
     Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
     Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+    const double e = Ps[x] - 0.5 * (q.A[x] + q.B[x]);
+    pm += e * e;
   }
+  pm = sqrt(pm);
   double Q[kMaxHerm];
   for (int i = 0; i < kMaxHerm; ++i) Q[i] = 0.0;
   int s0, s1;
@@ -177,15 +178,8 @@ __global__ void __launch_bounds__(128)
       w0 = -Z * (2.0 * kPi / z3);
     }
     const double *C = s.psite_pos + 3 * site;
-    double d[3], L2[3], v[3];
-    for (int x = 0; x < 3; ++x) d[x] = Ps[x] - C[x];
-    nearest_lattice(s, d, L2);
-    double c0 = 0.0;
-    for (int x = 0; x < 3; ++x) {
-      v[x] = Ps[x] - C[x] - L2[x];
-      c0 += v[x] * v[x];
-    }
-    if (c0 > t) continue;
+    double L2[3], v[3], c0;
+    if (!site_search(s, w, sp.unit, site, Ps, pm, t, L2, v, c0)) continue;
     const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
     for (int nc = 0; nc < s.ncell; ++nc) {
       if (s.csize[nc] > maxr) break;
@@ -284,6 +278,24 @@ int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
     IMAGO_CUDA(cudaGetLastError());
   }
   return rc;
+}
+
+// ------------------------------------------------------- site images --
+__global__ void k_site_images(DevSys s, DevWork w, SiteImage *simg) {
+  const long long n = (long long)w.nunits * s.nps;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    simg[i] = site_image(s, w, (int)(i / s.nps), (int)(i % s.nps));
+}
+
+int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
+                       cudaStream_t st) {
+  const long long n = (long long)w.nunits * s.nps;
+  if (n == 0) return IMAGO_OK;
+  k_site_images<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256,
+                  0, st>>>(s, w, simg);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
 }
 
 }  // namespace imago

@@ -83,6 +83,8 @@ def lib():
         L.imago_intg_kernel_stats.restype = ctypes.c_int
         L.imago_intg_destroy.argtypes = [ctypes.c_void_p]
         L.imago_intg_destroy.restype = None
+        L.imago_trim_memory.argtypes = [ctypes.c_int]
+        L.imago_trim_memory.restype = ctypes.c_int
         L.imago_strerror.argtypes = [ctypes.c_int]
         L.imago_strerror.restype = ctypes.c_char_p
         L.imago_kpoint_mesh.argtypes = [ctypes.POINTER(ctypes.c_int), _D, _D]
@@ -104,6 +106,12 @@ def _p(a):
 def _check(st, what):
     if st != 0:
         raise ImagoError(st, what)
+
+
+def trim_memory(device=0):
+    """Hand the unused memory of the library's device pool back to the
+    driver (contexts keep taking scratch from the pool afterwards)."""
+    _check(lib().imago_trim_memory(device), "imago_trim_memory")
 
 
 def kpoint_mesh(n, shift=(0.0, 0.0, 0.0)):

@@ -197,6 +197,12 @@ IMAGO_API int imago_intg_kernel_stats(const imago_ctx *ctx, double ms[4],
 
 IMAGO_API void imago_intg_destroy(imago_ctx *ctx);
 
+/* No counterpart in the reference.  Device scratch of every context comes
+ * from one stream-ordered memory pool per device that keeps freed memory
+ * for the next context; this hands the pool's unused memory on `device`
+ * back to the driver (cudaMemPoolTrimTo). */
+IMAGO_API int imago_trim_memory(int device);
+
 IMAGO_API const char *imago_strerror(int status);
 
 /* Monkhorst-Pack style mesh of kpoints.f90:837-899 without symmetry

@@ -50,6 +50,8 @@ def lib():
         L.orc_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ImagoDimsC)]
         L.orc_set_sampling.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_set_sampling.restype = None
+        L.orc_set_skip_ortho.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_skip_ortho.restype = None
         L.orc_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
         L.orc_gauss_overlap_ke.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_np.argtypes = [ctypes.c_void_p, _D]
@@ -159,6 +161,11 @@ class OracleBuild:
         out = self._packed(hi - lo)
         self._check(lib().orc_elec_pot_gauss_overlap(self._ctx, lo, hi, _p(out)), "EP")
         return out
+
+    def set_skip_ortho(self, skip=True):
+        """Timing samples only: run the pair loops without the
+        orthogonalisation and packing (outputs are left unwritten)."""
+        lib().orc_set_skip_ortho(self._ctx, 1 if skip else 0)
 
     def last_times(self):
         a, b = ctypes.c_double(), ctypes.c_double()

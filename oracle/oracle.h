@@ -48,6 +48,8 @@ int orc_dims(const orc_ctx *c, imago_dims *d);
  * index (i-major over i <= j) is a multiple of `stride` are integrated.
  * stride 1 (the default) is the full build.  nthreads <= 0: all cores. */
 void orc_set_sampling(orc_ctx *c, int stride, int nthreads);
+/* Timing samples only: skip the orthogonalisation and packing. */
+void orc_set_skip_ortho(orc_ctx *c, int skip);
 
 int orc_gauss_overlap_ol(orc_ctx *c, double *packed, double *cv_re,
                          double *cv_im);

@@ -87,6 +87,7 @@ struct orc_ctx {
   double *s_cv;       /* [k][v][c] complex: ((k*V + v)*C + c)*2 */
   int have_ol;
   int stride, nthreads;
+  int skip_ortho; /* timing samples: pair loops only */
   double t_loops, t_ortho;
   long long n_pair_images, n_shell_pairs, n_triples;
 };
@@ -497,6 +498,10 @@ int orc_dims(const orc_ctx *c, imago_dims *d) {
   d->num_shell_pairs = c->n_shell_pairs;
   return IMAGO_OK;
 }
+
+/* Timing samples only: with skip != 0 the builds run their pair loops but
+ * not the orthogonalisation and packing, so their outputs stay unwritten. */
+void orc_set_skip_ortho(orc_ctx *c, int skip) { c->skip_ortho = skip; }
 
 void orc_set_sampling(orc_ctx *c, int stride, int nthreads) {
   c->stride = stride > 0 ? stride : 1;
@@ -987,7 +992,7 @@ static int build_one(orc_ctx *c, const buildspec *bs, double *packed,
         cv_im[q] = g.cv[2 * q + 1];
       }
   }
-  ortho_pack(c, &g, bs->kind == K_OL, packed);
+  if (!c->skip_ortho) ortho_pack(c, &g, bs->kind == K_OL, packed);
   c->t_ortho += now_s() - t1;
   free_gmats(&g);
   return IMAGO_OK;

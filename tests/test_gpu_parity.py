@@ -158,3 +158,37 @@ def test_quartz_162_atoms_gamma(imago_lib):
            "EP0": packed_mismatch(out["ep_packed"][0], ref_ep_si),
            "EP20": packed_mismatch(out["ep_packed"][20], ref_ep_o)}
     _assert_all(res)
+
+
+def test_host_outputs_equal_device_outputs(imago_lib):
+    # Host outputs go through per-matrix staging regions copied out on a
+    # second stream while later builds run; the numbers must be the ones
+    # the device-output path writes, bit for bit.
+    import torch
+    s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+    with intg.IntegralSetup(s) as g:
+        host = g.build()
+    dev = torch.device("cuda", 0)
+    with intg.IntegralSetup(s, outputs_on_device=True) as g:
+        nk, npk, V, C, P = g.nk, g.npacked, g.vale_dim, g.core_dim, g.pot_dim
+        bufs = {"ol_packed": (nk, npk, 2), "ol_cv_re": (nk, V, C),
+                "ol_cv_im": (nk, V, C), "ke_packed": (nk, npk, 2),
+                "np_packed": (nk, npk, 2), "ep_packed": (P, nk, npk, 2)}
+        bufs = {k: torch.full(v, np.nan, dtype=torch.float64, device=dev)
+                for k, v in bufs.items()}
+        g.build(out={k: v.data_ptr() for k, v in bufs.items()})
+        torch.cuda.synchronize()
+    for k, v in bufs.items():
+        assert np.array_equal(host[k], v.cpu().numpy().reshape(host[k].shape)), k
+
+
+def test_contexts_reuse_and_trim_the_memory_pool(imago_lib):
+    s = configs.small_test_system()
+    with intg.IntegralSetup(s) as g:
+        first = g.build()["np_packed"]
+    intg.trim_memory(0)
+    with intg.IntegralSetup(s) as g:
+        again = g.build()["np_packed"]
+    assert np.array_equal(first, again)
+    with pytest.raises(intg.ImagoError):
+        intg.trim_memory(-1)
