@@ -28,26 +28,32 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a,
 // the pairXBasisFn2 / multWithBasisFn1 contraction (integrals.F90:555-563,
 // intgSaving.F90:56-89).  Entries whose lm lies beyond a primitive's class
 // carry a zero coefficient in the reference and are skipped.  Blocks are
-// stored column-major, e = m2 * ni + m1.  The unit's shell-pair list and
-// both atoms' coefficient tables are staged in shared memory; the
-// coefficient product of an (element, shell pair) serves every term of the
-// group.
+// stored column-major, e = m2 * ni + m1.  A unit's primitive blocks of one
+// term are contiguous in `blk`: they are staged through shared memory in
+// chunks of whole shell pairs with coalesced loads, together with the
+// chunk's shell-pair list and both atoms' coefficient tables; the
+// coefficient product of an (element, shell pair) serves every term of
+// the group.
 constexpr int kTermsPerCta = 4;
 constexpr int kContractThreads = 128;
 constexpr int kElemsPerThread = 3;          // n_i n_j <= 384 per pass
 constexpr int kSpStage = 256;               // shell pairs staged at a time
+constexpr int kBlkStage = 768;              // block doubles per term staged
 constexpr int kCoefMax = 1024;              // alphas x states per atom
 
-__global__ void __launch_bounds__(kContractThreads, 6)
+__global__ void __launch_bounds__(kContractThreads, 4)
     k_contract(DevSys s, DevWork w, int nterm, const double *blk, double *M) {
   __shared__ int sp_ab[kSpStage];            // a | b << 16
   __shared__ int sp_cls[kSpStage];           // nsh(la) | nsh(lb) << 8
-  __shared__ long long sp_off[kSpStage];
+  __shared__ int sp_rel[kSpStage];           // block offset from the chunk's
   __shared__ double c1s[kCoefMax], c2s[kCoefMax];
+  __shared__ double bs[kTermsPerCta][kBlkStage];
+  __shared__ long long chunk_base;
   const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
   const int ui = blockIdx.x / ntg;
   const int t0 = (blockIdx.x % ntg) * kTermsPerCta;
   const int tn = min(kTermsPerCta, nterm - t0);
+  const int tid = threadIdx.x;
   const DUnit u = w.units[ui];
   const DPair p = w.pairs[u.pair];
   const int ni = p.ni, nj = p.nj, ne = ni * nj;
@@ -58,8 +64,8 @@ __global__ void __launch_bounds__(kContractThreads, 6)
   const double *c2 = s.basis + s.type_basis_off[p.tj];
   const bool stage_coef = na1 * ni <= kCoefMax && na2 * nj <= kCoefMax;
   if (stage_coef) {
-    for (int i = threadIdx.x; i < na1 * ni; i += kContractThreads) c1s[i] = c1[i];
-    for (int i = threadIdx.x; i < na2 * nj; i += kContractThreads) c2s[i] = c2[i];
+    for (int i = tid; i < na1 * ni; i += kContractThreads) c1s[i] = c1[i];
+    for (int i = tid; i < na2 * nj; i += kContractThreads) c2s[i] = c2[i];
   }
   const double *cf1 = stage_coef ? c1s : c1;
   const double *cf2 = stage_coef ? c2s : c2;
@@ -70,7 +76,7 @@ __global__ void __launch_bounds__(kContractThreads, 6)
     double acc[kElemsPerThread][kTermsPerCta];
 #pragma unroll
     for (int j = 0; j < kElemsPerThread; ++j) {
-      const int e = e0 + threadIdx.x + j * kContractThreads;
+      const int e = e0 + tid + j * kContractThreads;
       m2[j] = e < ne ? e / ni : 0;
       m1[j] = e < ne ? e - m2[j] * ni : 0;
       lm1[j] = e < ne ? s.state_lm[so1 + m1[j]] : 1 << 20;
@@ -78,34 +84,52 @@ __global__ void __launch_bounds__(kContractThreads, 6)
 #pragma unroll
       for (int t = 0; t < kTermsPerCta; ++t) acc[j][t] = 0.0;
     }
-    for (int q0 = u.spbeg; q0 < u.spend; q0 += kSpStage) {
+    for (int q0 = u.spbeg; q0 < u.spend;) {
       const int nq = min(kSpStage, u.spend - q0);
       __syncthreads();
-      for (int i = threadIdx.x; i < nq; i += kContractThreads) {
-        const DSp sp = w.sps[q0 + i];
-        sp_ab[i] = sp.a | (sp.b << 16);
-        sp_cls[i] = nsh(sp.la) | (nsh(sp.lb) << 8);
-        sp_off[i] = sp.boff;
+      // shell pairs of the chunk: those whose blocks end within kBlkStage
+      // doubles of the first one's start (at least one: a block has <= 256)
+      int fit = 0;
+      for (int i = tid; i < kSpStage; i += kContractThreads) {
+        if (i < nq) {
+          const DSp sp = w.sps[q0 + i];
+          const long long b0 = w.sps[q0].boff;
+          const int rel = (int)(sp.boff - b0);
+          sp_ab[i] = sp.a | (sp.b << 16);
+          sp_cls[i] = nsh(sp.la) | (nsh(sp.lb) << 8);
+          sp_rel[i] = rel;
+          fit += rel + nsh(sp.la) * nsh(sp.lb) <= kBlkStage;
+          if (i == 0) chunk_base = b0;
+        }
       }
+      const int cnt = max(1, __syncthreads_count(fit > 0 && tid < nq) +
+                                 __syncthreads_count(fit > 1));
+      const int last = cnt - 1;
+      const int len = sp_rel[last] + (sp_cls[last] & 0xff) * (sp_cls[last] >> 8);
+      const double *src = bt + chunk_base;
+      for (int t = 0; t < tn; ++t)
+        for (int i = tid; i < len; i += kContractThreads)
+          bs[t][i] = src[(long long)t * w.blk_total + i];
       __syncthreads();
-      for (int q = 0; q < nq; ++q) {
+      for (int q = 0; q < cnt; ++q) {
         const int ab = sp_ab[q], cl = sp_cls[q];
         const int a = ab & 0xffff, b = ab >> 16, na = cl & 0xff, nb = cl >> 8;
-        const double *bq = bt + sp_off[q];
+        const int rel = sp_rel[q];
 #pragma unroll
         for (int j = 0; j < kElemsPerThread; ++j) {
           if (lm1[j] >= na || lm2[j] >= nb) continue;
           const double cw = cf1[a * ni + m1[j]] * cf2[b * nj + m2[j]];
-          const double *bb = bq + lm1[j] * nb + lm2[j];
+          const int o = rel + lm1[j] * nb + lm2[j];
 #pragma unroll
           for (int t = 0; t < kTermsPerCta; ++t)
-            if (t < tn) acc[j][t] += cw * bb[(long long)t * w.blk_total];
+            if (t < tn) acc[j][t] += cw * bs[t][o];
         }
       }
+      q0 += cnt;
     }
 #pragma unroll
     for (int j = 0; j < kElemsPerThread; ++j) {
-      const int e = e0 + threadIdx.x + j * kContractThreads;
+      const int e = e0 + tid + j * kContractThreads;
       if (e >= ne) continue;
 #pragma unroll
       for (int t = 0; t < kTermsPerCta; ++t)
@@ -262,9 +286,62 @@ __global__ void __launch_bounds__(kBThreads)
   }
 }
 
+// Few k-points (Gamma, 2x2x2): the tensor-core tiles would idle on k, so
+// one thread per block column keeps the nk complex sums in registers and
+// reads each image block once.
+constexpr int kBlochSmallNk = 8;
+
+__global__ void __launch_bounds__(kBC)
+    k_bloch_small(DevSys s, DevWork w, const double *M, double2 *vv,
+                  double2 *cv, double2 *cc) {
+  __shared__ double2 shift[kBlochSmallNk];
+  const int2 bt = w.btile[blockIdx.x];
+  const DPair p = w.pairs[bt.x];
+  const int ne = p.ni * p.nj, e = bt.y * kBC + threadIdx.x;
+  const int term = blockIdx.y, nk = s.nk;
+  if (threadIdx.x < nk) {
+    // kPointLatticeOriginShift (intgSaving.F90:241-292)
+    const double *kv = s.kxyz + 3 * threadIdx.x;
+    const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
+    double sn = 0.0, cs = 1.0;
+    if (fabs(dot) >= kSmallThresh) sincos(dot, &sn, &cs);
+    shift[threadIdx.x] = make_double2(cs, sn);
+  }
+  __syncthreads();
+  if (e >= ne) return;
+  const double *Mt = M + (long long)term * w.m_total + p.moff + e;
+  double re[kBlochSmallNk], im[kBlochSmallNk];
+#pragma unroll
+  for (int k = 0; k < kBlochSmallNk; ++k) re[k] = im[k] = 0.0;
+  for (int u = p.ubeg; u < p.uend; ++u) {
+    const double m = Mt[(long long)(u - p.ubeg) * ne];
+    const double2 *ph = s.phase + (long long)w.units[u].cell * nk;
+#pragma unroll
+    for (int k = 0; k < kBlochSmallNk; ++k)
+      if (k < nk) {
+        const double2 f = ph[k];
+        re[k] += f.x * m;
+        im[k] += f.y * m;
+      }
+  }
+  const int m2 = e / p.ni, m1 = e - m2 * p.ni;
+#pragma unroll
+  for (int k = 0; k < kBlochSmallNk; ++k)
+    if (k < nk) {
+      const double2 f = shift[k];
+      scatter(s, p, (long long)term * nk + k, m1, m2, f.x * re[k] - f.y * im[k],
+              f.x * im[k] + f.y * re[k], vv, cv, cc);
+    }
+}
+
 int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
                  double2 *vv, double2 *cv, double2 *cc, cudaStream_t st) {
   if (w.nbtile == 0 || nterm == 0) return IMAGO_OK;
+  if (s.nk <= kBlochSmallNk) {
+    k_bloch_small<<<dim3(w.nbtile, nterm), kBC, 0, st>>>(s, w, M, vv, cv, cc);
+    IMAGO_CUDA(cudaGetLastError());
+    return IMAGO_OK;
+  }
   dim3 grid(w.nbtile, (s.nk + kBK - 1) / kBK, nterm);
   k_bloch<<<grid, kBThreads, 0, st>>>(s, w, M, vv, cv, cc);
   IMAGO_CUDA(cudaGetLastError());
