@@ -107,23 +107,31 @@ __device__ __forceinline__ SiteImage site_image(const DevSys &s,
   return r;
 }
 
+// True when a point at least d - pm from every lattice point of interest
+// is certainly outside the screening radius^2 t: the float lower bound of
+// d - pm (pmf >= pm, rounded down) squared, rounded down, exceeds tf >= t.
+__device__ __forceinline__ bool beyond(float d, float pmf, float tf) {
+  const float a = __fsub_rd(d, pmf);
+  return a > 0.f && __fmul_rd(a, a) > tf;
+}
+
 // Closest-image search of a three-centre screen (the findLatticeVector step
 // of nuclearPE/electronicPE, integrals.F90:2632,2791) for the point Ps with
 // |Ps - M| = pm, radius^2 t.  Returns false when no image of site C lies
 // within the radius; otherwise sets L2, the lattice vector from which the
 // images in range are enumerated, and v = Ps - C - L2 with |v|^2 <= t.  With
 // the stored midpoint image: no lattice point is nearer to Ps - C than
-// d1 - pm, none but the stored one nearer than d2 - pm.
+// d1 - pm, none but the stored one nearer than d2 - pm.  pmf and tf are
+// float upper bounds of pm and t for those tests.
 __device__ __forceinline__ bool site_search(const DevSys &s, const DevWork &w,
                                             int unit, int site,
-                                            const double Ps[3], double pm,
-                                            double t, double L2[3],
+                                            const double Ps[3], float pmf,
+                                            double t, float tf, double L2[3],
                                             double v[3], double &c0) {
   const double *C = s.psite_pos + 3 * site;
   if (w.simg) {
     const SiteImage im = w.simg[(long long)unit * s.nps + site];
-    const double rt = sqrt(t);
-    if ((double)im.d1 - pm > rt) return false;
+    if (beyond(im.d1, pmf, tf)) return false;
     double c = 0.0;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
@@ -135,7 +143,7 @@ __device__ __forceinline__ bool site_search(const DevSys &s, const DevWork &w,
       c0 = c;
       return true;
     }
-    if ((double)im.d2 - pm > rt) return false;
+    if (beyond(im.d2, pmf, tf)) return false;
   }
   double d[3];
 #pragma unroll

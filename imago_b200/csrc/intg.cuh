@@ -83,7 +83,8 @@ struct DevWork {
 // Nearest image of a potential site C to the midpoint M of a unit's A-B
 // segment: M - C - (n0 a + n1 b + n2 c) is shortest for lattice coordinates
 // n; d1 and d2 are lower bounds of the distance from M - C to that lattice
-// point and to every other one.
+// point and to every other one.  16 bytes, so that the table of a large
+// cell stays compact.
 struct __align__(16) SiteImage {
   short n[3];
   short pad;

@@ -57,26 +57,23 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
   for (int i = 0; i < nherm(L); ++i) Q[i] = 0.0;
 
-  int s0, s1;
+  // NP runs over every potential type, EP over the term's type; sites of a
+  // type are contiguous and types come in site order.
+  const int pt0 = NUC ? 0 : tm.ptype, pt1 = NUC ? s.npt : tm.ptype + 1;
   double tcut = 0.0, a3 = 0.0;
-  if (NUC) {
-    s0 = 0;
-    s1 = s.nps;
-  } else {
+  if (!NUC) {
     const int pt = tm.ptype;
-    s0 = s.ptype_first_site[pt];
-    s1 = s0 + s.ptype_mult[pt];
     a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
     const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
     // alphaPotDist (gaussRelations.f90:187-196)
     tcut = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
   }
   const double z3e = zeta + a3, mue = zeta * a3 / z3e;
+  const float pmf = __double2float_ru(pm);
 
-  for (int site = s0; site < s1; ++site) {
+  for (int pt = pt0; pt < pt1; ++pt) {
     double w0 = 1.0, mu = mue, nu = 0.0, t = tcut;
     if (NUC) {
-      const int pt = s.psite_ptype[site];
       const double Z = s.ptype_z[pt];
       if (Z < kSmallThresh) continue;
       const double an = s.ptype_nucalpha[pt];
@@ -88,22 +85,26 @@ __global__ void __launch_bounds__(128)
       nu = zeta * zeta / z3;
       w0 = -Z * (2.0 * kPi / z3);
     }
-    const double *C = s.psite_pos + 3 * site;
-    double L2[3], v[3], c0;
-    if (!site_search(s, w, sp.unit, site, Ps, pm, t, L2, v, c0)) continue;
-    const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-    for (int nc = 0; nc < s.ncell; ++nc) {
-      if (s.csize[nc] > maxr) break;
-      const double *R = s.cell + 3 * nc;
-      const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-      if (dx * dx + dy * dy + dz * dz > t) continue;
-      double X[3];
+    const float tf = __double2float_ru(t);
+    const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
+    for (int site = s0; site < s1; ++site) {
+      double L2[3], v[3], c0;
+      if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+      const double *C = s.psite_pos + 3 * site;
+      const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+      for (int nc = 0; nc < s.ncell; ++nc) {
+        if (s.csize[nc] > maxr) break;
+        const double *R = s.cell + 3 * nc;
+        const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+        if (dx * dx + dy * dy + dz * dz > t) continue;
+        double X[3];
 #pragma unroll
-      for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-      if (NUC)
-        accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
-      else
-        accumulate_overlap_q<L>(X, mu, 1.0, Q);
+        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+        if (NUC)
+          accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
+        else
+          accumulate_overlap_q<L>(X, mu, 1.0, Q);
+      }
     }
   }
   const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
@@ -149,49 +150,53 @@ __global__ void __launch_bounds__(128)
   pm = sqrt(pm);
   double Q[kMaxHerm];
   for (int i = 0; i < kMaxHerm; ++i) Q[i] = 0.0;
-  int s0, s1;
+  // NP runs over every potential type, EP over the term's type; sites of a
+  // type are contiguous and types come in site order.
+  const int pt0 = NUC ? 0 : tm.ptype, pt1 = NUC ? s.npt : tm.ptype + 1;
   double tcut = 0.0, a3 = 0.0;
-  if (NUC) {
-    s0 = 0;
-    s1 = s.nps;
-  } else {
+  if (!NUC) {
     const int pt = tm.ptype;
-    s0 = s.ptype_first_site[pt];
-    s1 = s0 + s.ptype_mult[pt];
     a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
     const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
+    // alphaPotDist (gaussRelations.f90:187-196)
     tcut = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
   }
   const double z3e = zeta + a3, mue = zeta * a3 / z3e;
-  for (int site = s0; site < s1; ++site) {
+  const float pmf = __double2float_ru(pm);
+
+  for (int pt = pt0; pt < pt1; ++pt) {
     double w0 = 1.0, mu = mue, nu = 0.0, t = tcut;
     if (NUC) {
-      const int pt = s.psite_ptype[site];
       const double Z = s.ptype_z[pt];
       if (Z < kSmallThresh) continue;
       const double an = s.ptype_nucalpha[pt];
       const double ans = s.ptype_nucalpha[s.ptype_screen[pt]];
+      // alphaNucDist (gaussRelations.f90:262-270)
       t = frac * (s.T * (q.a1s + q.a2s + ans) / (q.a1s + q.a2s) / ans);
       const double z3 = zeta + an;
       mu = zeta * an / z3;
       nu = zeta * zeta / z3;
       w0 = -Z * (2.0 * kPi / z3);
     }
-    const double *C = s.psite_pos + 3 * site;
-    double L2[3], v[3], c0;
-    if (!site_search(s, w, sp.unit, site, Ps, pm, t, L2, v, c0)) continue;
-    const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-    for (int nc = 0; nc < s.ncell; ++nc) {
-      if (s.csize[nc] > maxr) break;
-      const double *R = s.cell + 3 * nc;
-      const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-      if (dx * dx + dy * dy + dz * dz > t) continue;
-      double X[3];
-      for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-      if (NUC)
-        accumulate_nuclear_q_rt(L, X, mu, nu, w0, Q);
-      else
-        accumulate_overlap_q_rt(L, X, mu, 1.0, Q);
+    const float tf = __double2float_ru(t);
+    const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
+    for (int site = s0; site < s1; ++site) {
+      double L2[3], v[3], c0;
+      if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+      const double *C = s.psite_pos + 3 * site;
+      const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+      for (int nc = 0; nc < s.ncell; ++nc) {
+        if (s.csize[nc] > maxr) break;
+        const double *R = s.cell + 3 * nc;
+        const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+        if (dx * dx + dy * dy + dz * dz > t) continue;
+        double X[3];
+        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+        if (NUC)
+          accumulate_nuclear_q_rt(L, X, mu, nu, w0, Q);
+        else
+          accumulate_overlap_q_rt(L, X, mu, 1.0, Q);
+      }
     }
   }
   const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
