@@ -190,10 +190,11 @@ __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
 }
 
 constexpr int kBThreads = 256;              // 8 warps: 2 (k) x 4 (columns)
-// Padded rows: a fragment read (4 k rows x 8 columns) then covers all 32
-// banks in each of its wavefronts.
+// Padded rows: a row of m_s is 136 bank words and a row of ph_s 136 too
+// (34 double2), both 8 mod 32, so the 4 k rows of a fragment read fall on
+// distinct banks in each wavefront.
 constexpr int kBMP = kBC + 4;
-constexpr int kBKP = kBK + 4;
+constexpr int kBKP = kBK + 2;
 constexpr int kBPhLoads = kBU * kBK / kBThreads;
 constexpr int kBMLoads = kBU * kBC / kBThreads;
 
@@ -360,7 +361,7 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
 // For the overlap itself X = S: VV - 2 S^H S + S^H S_cc S.
 constexpr int kOT = 32;   // output tile
 constexpr int kOK = 16;   // complex K per shared-memory stage
-constexpr int kOP = kOT + 4;  // padded row: fragment reads are conflict-free
+constexpr int kOP = kOT + 2;  // 34 double2 = 136 bank words: conflict-free fragment reads
 constexpr int kOThreads = 128;
 constexpr int kOLoads = kOK * kOT / kOThreads;  // double2 per thread per operand
 
@@ -370,40 +371,50 @@ struct OStage {
   double2 b[kOK][kOP];
 };
 
-// Accumulate the stage into the warp's 16x16 complex tile:
-// acc (+)= op(A)^T B, op = conj when CONJ.  Warp w owns rows 16*(w/2).. and
-// columns 16*(w%2)..
+// Accumulate the stage into the warp's 16x16 complex tile, op(A)^T B with
+// op = conj when CONJ, by three real products per complex one (the 3M
+// form): t1 += ar br, t2 += ai bi, t3 += (ar -/+ ai)(br + bi).  Then
+//   CONJ:  re = t1 + t2, im = t3 - t1 + t2
+//   plain: re = t1 - t2, im = t3 - t1 - t2.
+// Warp w owns rows 16*(w/2).. and columns 16*(w%2)..
 template <bool CONJ>
-__device__ __forceinline__ void ostage_mma(const OStage &st, double wr[2][2][2],
-                                           double wi[2][2][2], int lane,
-                                           int warp) {
+__device__ __forceinline__ void ostage_mma(const OStage &st, double t1[2][2][2],
+                                           double t2[2][2][2], double t3[2][2][2],
+                                           int lane, int warp) {
   const int r0 = (warp >> 1) * 16, cb = (warp & 1) * 16;
 #pragma unroll
   for (int ks = 0; ks < kOK; ks += 4) {
     const int kk = ks + (lane & 3);
     double2 a[2], b[2];
+    double as[2], bs[2];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
       a[t] = st.a[kk][r0 + 8 * t + (lane >> 2)];
       b[t] = st.b[kk][cb + 8 * t + (lane >> 2)];
+      as[t] = CONJ ? a[t].x - a[t].y : a[t].x + a[t].y;
+      bs[t] = b[t].x + b[t].y;
     }
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
-        // conj(a) b = (ar br + ai bi) + i (ar bi - ai br)
-        //      a b  = (ar br - ai bi) + i (ar bi + ai br)
-        dmma(wr[mt][nt][0], wr[mt][nt][1], a[mt].x, b[nt].x);
-        dmma(wr[mt][nt][0], wr[mt][nt][1], CONJ ? a[mt].y : -a[mt].y, b[nt].y);
-        dmma(wi[mt][nt][0], wi[mt][nt][1], a[mt].x, b[nt].y);
-        dmma(wi[mt][nt][0], wi[mt][nt][1], CONJ ? -a[mt].y : a[mt].y, b[nt].x);
+        dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
+        dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
       }
   }
 }
 
+// Complex tile entry from the three 3M sums.
+template <bool CONJ>
+__device__ __forceinline__ double2 ocombine(double t1, double t2, double t3) {
+  return CONJ ? make_double2(t1 + t2, t3 - t1 + t2)
+              : make_double2(t1 - t2, t3 - t1 - t2);
+}
+
 // Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v).  Operands are staged
 // through registers one K stage ahead of the MMAs.
-__global__ void __launch_bounds__(kOThreads)
+__global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
               const double2 *s_cv, double2 *y) {
   __shared__ OStage st;
@@ -415,7 +426,7 @@ __global__ void __launch_bounds__(kOThreads)
   const double2 *XC = cc + tk * C * C;
   const double2 *S = s_cv + (long long)k * V * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double wr[2][2][2] = {}, wi[2][2][2] = {};
+  double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
   double2 ra[kOLoads], rb[kOLoads];
   auto fetch = [&](int l0) {
 #pragma unroll
@@ -445,7 +456,7 @@ __global__ void __launch_bounds__(kOThreads)
     store();
     __syncthreads();
     if (l0 + kOK < C) fetch(l0 + kOK);
-    ostage_mma<false>(st, wr, wi, lane, warp);
+    ostage_mma<false>(st, t1, t2, t3, lane, warp);
   }
   const double2 *X = cv + tk * V * C;
   double2 *Y = y + tk * V * C;
@@ -460,15 +471,15 @@ __global__ void __launch_bounds__(kOThreads)
         const int v = tc * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
         if (c >= C || v >= V) continue;
         const double2 x = X[(long long)v * C + c];
-        Y[(long long)v * C + c] =
-            make_double2(x.x - 0.5 * wr[mt][nt][i], x.y - 0.5 * wi[mt][nt][i]);
+        const double2 p = ocombine<false>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+        Y[(long long)v * C + c] = make_double2(x.x - 0.5 * p.x, x.y - 0.5 * p.y);
       }
 }
 
 // Upper tiles (J <= I) of W = S^H Y + Y^H S as one K loop over the stacked
 // core index (S;Y)^H (Y;S), then VV'(j, i) = VV(j, i) - W(j, i) packed at
 // i(i+1)/2 + j.
-__global__ void __launch_bounds__(kOThreads)
+__global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_w(DevSys s, const double2 *vv, const double2 *y,
               const double2 *s_cv, double *packed) {
   __shared__ OStage st;
@@ -486,7 +497,10 @@ __global__ void __launch_bounds__(kOThreads)
   const double2 *Y = y + tk * V * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K2 = 2 * C;
-  double wr[2][2][2] = {}, wi[2][2][2] = {};
+  double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
+  // on a diagonal tile the warp owning rows 16..31 x columns 0..15 lies
+  // wholly below the diagonal, which is never stored
+  const bool lower = J == I && (warp >> 1) > (warp & 1);
   double2 ra[kOLoads], rb[kOLoads];
   auto fetch = [&](int l0) {
 #pragma unroll
@@ -521,7 +535,7 @@ __global__ void __launch_bounds__(kOThreads)
     store();
     __syncthreads();
     if (l0 + kOK < K2) fetch(l0 + kOK);
-    ostage_mma<true>(st, wr, wi, lane, warp);
+    if (!lower) ostage_mma<true>(st, t1, t2, t3, lane, warp);
   }
   const double2 *VVt = vv + tk * V * V;
   const long long np = (long long)V * (V + 1) / 2;
@@ -537,8 +551,9 @@ __global__ void __launch_bounds__(kOThreads)
         const int col = I * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
         if (row >= V || col >= V || row > col) continue;
         double2 v = VVt[(long long)col * V + row];
-        v.x -= wr[mt][nt][i];
-        v.y -= wi[mt][nt][i];
+        const double2 p = ocombine<true>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+        v.x -= p.x;
+        v.y -= p.y;
         if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
         if (fabs(v.x) < kPackThresh) v.x = 0.0;
         if (fabs(v.y) < kPackThresh) v.y = 0.0;
