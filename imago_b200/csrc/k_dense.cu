@@ -198,7 +198,7 @@ constexpr int kBKP = kBK + 2;
 constexpr int kBPhLoads = kBU * kBK / kBThreads;
 constexpr int kBMLoads = kBU * kBC / kBThreads;
 
-__global__ void __launch_bounds__(kBThreads)
+__global__ void __launch_bounds__(kBThreads, 4)
     k_bloch(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
             double2 *cc) {
   __shared__ double2 ph_s[kBU][kBKP];

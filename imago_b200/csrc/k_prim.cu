@@ -25,8 +25,10 @@ __global__ void __launch_bounds__(128)
 // those of nuclearPE (integrals.F90:2533-2698) and electronicPE
 // (2700-2858): a closest-image screen per site, then the images of that
 // site within threeAlphaDist of the overlap centre, in |R| order.
+// Registers: four CTAs per SM up to d-p (a few bytes of spill for d-p),
+// three for d-d, whose Hermite accumulator alone holds 35 doubles.
 template <int LA, int LB, bool NUC>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
     k_prim3c(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
              int nterm, double *blk) {
   constexpr int L = LA + LB;
