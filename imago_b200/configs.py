@@ -22,6 +22,11 @@ Workloads (sizes are the ones the integral path is quoted on):
                      (18 18 0 0), 1s core + 2s 2p 3s 3p valence; 20 potential
                      terms per element; Gamma or 2x2x2 k.
   graphite_cell      AB graphite a=2.46 A, c=6.71 A.
+  batch_cells        64 independent cells of uneven size for the batched
+                     stream: Si (8..64 atoms), diamond and graphite (8..216
+                     atoms) supercells, each strained by a random symmetric
+                     strain with components in +-3% and jittered by
+                     N(0, 0.02 A), 2x2x2 k.
 """
 
 import math
@@ -232,6 +237,73 @@ def graphite_cell(reps=(1, 1, 1), kmesh=(2, 2, 2), shift=(0.5, 0.5, 0.5),
     n = len(frac)
     return _system(rv, [t], [1] * n, pos, [p], [1] * n, k,
                    title="AB graphite", kmesh=km)
+
+
+def cubic_supercell(element="si", reps=(1, 1, 1), kmesh=(2, 2, 2),
+                    shift=(0.5, 0.5, 0.5), seed=6, jitter=0.02, strain=None):
+    """Diamond-structure conventional cell (Si a=5.431 A with the s,p,d
+    basis and 20 potential terms, or C a=3.567 A with the 1s/2s2p basis and
+    16 terms) repeated reps times, optionally strained (rv <- rv (1 + e))
+    and jittered."""
+    si = element == "si"
+    a = (5.431 if si else 3.567) * ANGSTROM
+    rng = np.random.default_rng(seed)
+    rv = np.eye(3) * a * np.array(reps)[:, None]
+    if strain is not None:
+        rv = rv @ (np.eye(3) + np.asarray(strain))
+    frac = []
+    for i in range(reps[0]):
+        for j in range(reps[1]):
+            for k in range(reps[2]):
+                frac += [(np.array(f) + [i, j, k]) / reps for f in DIAMOND_FRAC]
+    pos = np.array(frac) @ rv
+    if jitter:
+        pos = pos + rng.normal(0.0, jitter * ANGSTROM, size=pos.shape)
+    if si:
+        t, p = silicon_type(), _pot(1, "si1_1", 14, 20, 0.10, 1.0e5)
+    else:
+        t, p = carbon_type(), _pot(1, "c1_1", 6, 16, 0.12, 1.0e5)
+    k, km = _mesh(kmesh, shift)
+    n = len(frac)
+    return _system(rv, [t], [1] * n, pos, [p], [1] * n, k,
+                   title=f"{'silicon' if si else 'diamond'} {tuple(reps)} supercell",
+                   kmesh=km)
+
+
+# Supercell repetitions of the batched workload by kind (atoms in brackets):
+# Si conventional 8 (8..64), diamond conventional 8 (8..216), graphite 4
+# (8..216).  Si stops at 64 atoms: its 13 valence and 5 core states per atom
+# make a 216-atom cell alone a second-long build.
+BATCH_REPS = {
+    "si": [(1, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2)],
+    "diamond": [(1, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2), (3, 2, 2),
+                (3, 3, 2), (3, 3, 3)],
+    "graphite": [(2, 1, 1), (2, 2, 1), (2, 2, 2), (3, 3, 1), (4, 4, 1),
+                 (3, 3, 2), (4, 4, 2), (6, 6, 1), (6, 3, 3)],
+}
+
+
+def batch_cells(n=64, seed=5, kmesh=(2, 2, 2), jitter=0.02, strain=0.03):
+    """The batched multi-cell workload: n cells drawn (seeded) over Si,
+    diamond and graphite supercells of BATCH_REPS, each with its own
+    symmetric strain (components uniform in +-strain, off-diagonal halved)
+    and jitter."""
+    rng = np.random.default_rng(seed)
+    kinds = ["si", "diamond", "graphite"]
+    cells = []
+    for i in range(n):
+        kind = kinds[int(rng.integers(3))]
+        reps = BATCH_REPS[kind][int(rng.integers(len(BATCH_REPS[kind])))]
+        e = rng.uniform(-strain, strain, size=(3, 3))
+        e = np.diag(np.diag(e)) + 0.25 * (np.triu(e, 1) + np.triu(e, 1).T)
+        cseed = int(rng.integers(1 << 30))
+        if kind == "graphite":
+            cells.append(graphite_cell(reps=reps, kmesh=kmesh, seed=cseed,
+                                       jitter=jitter, strain=e))
+        else:
+            cells.append(cubic_supercell(kind, reps=reps, kmesh=kmesh,
+                                         seed=cseed, jitter=jitter, strain=e))
+    return cells
 
 
 def small_test_system(seed=7, kmesh=(2, 2, 1)):

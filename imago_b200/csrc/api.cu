@@ -173,6 +173,14 @@ struct imago_ctx {
   int cev_used = 0;
   DBuf<double2> vv, cv, cc, y, s_cv;
   bool have_ol = false;
+  // CUDA-graph capture of the build: no timing events are recorded and EP
+  // keeps the chunk size of the last eager build (scratch already sized)
+  bool capturing = false;
+  int ep_chunk = 0;
+  cudaGraphExec_t gexec = nullptr;
+  unsigned gwhich = 0;
+  imago_out gout{};
+  long long glaunches = 0;   // kernels in the captured graph
 
   DevSys sys;
   DevWork work;
@@ -207,7 +215,35 @@ struct imago_ctx {
       for (auto &e : ev) cudaEventDestroy(e);
     for (auto &e : kev) cudaEventDestroy(e);
     for (auto &e : cev) cudaEventDestroy(e);
+    if (gexec) cudaGraphExecDestroy(gexec);
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+// Cells built together: each cell is a context of its own (own stream and
+// scratch); the first build of a given output set runs the cells eagerly
+// on their streams and captures the same launches, one fork/join branch
+// per cell, into a graph that later builds replay on `stream`.
+struct imago_batch {
+  int device = 0;
+  std::vector<imago_ctx *> cells;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t exec = nullptr;
+  unsigned which = 0;
+  std::vector<imago_out> outs;
+  long long glaunches = 0;
+
+  ~imago_batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (fork) cudaEventDestroy(fork);
+    for (auto e : join)
+      if (e) cudaEventDestroy(e);
+    for (auto *c : cells) imago_intg_destroy(c);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 };
@@ -729,6 +765,7 @@ cudaEvent_t next_event(imago_ctx *c) {
 }
 
 void mark(imago_ctx *c) {
+  if (c->capturing) return;
   cudaEvent_t e = next_event(c);
   if (e) cudaEventRecord(e, c->stream);
 }
@@ -883,17 +920,21 @@ constexpr int kEpCopyChunks = 4;
 int do_ep(imago_ctx *c, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
   const int nterm = c->pot_dim;
-  size_t budget = c->scratch_bytes;
-  if (budget == 0) {
-    size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
-    budget = fr / 4;
+  int chunk = c->ep_chunk;
+  if (!c->capturing || chunk <= 0) {
+    size_t budget = c->scratch_bytes;
+    if (budget == 0) {
+      size_t fr = 0, tot = 0;
+      cudaMemGetInfo(&fr, &tot);
+      budget = fr / 4;
+    }
+    const size_t per = term_bytes(c);
+    chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
+    chunk = std::min(chunk, nterm);
+    if (!c->outputs_on_device)
+      chunk = std::min(chunk, std::max(1, (nterm + kEpCopyChunks - 1) / kEpCopyChunks));
+    c->ep_chunk = chunk;
   }
-  const size_t per = term_bytes(c);
-  int chunk = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
-  chunk = std::min(chunk, nterm);
-  if (!c->outputs_on_device)
-    chunk = std::min(chunk, std::max(1, (nterm + kEpCopyChunks - 1) / kEpCopyChunks));
   const size_t npd = packed_doubles(c);
   for (int t0 = 0; t0 < nterm; t0 += chunk) {
     const int n = std::min(chunk, nterm - t0);
@@ -937,6 +978,42 @@ int finish(imago_ctx *c, int rc) {
 int set_device(imago_ctx *c) {
   IMAGO_CUDA(cudaSetDevice(c->device));
   return IMAGO_OK;
+}
+
+// Enqueue every build selected by `which` on the context's stream (and its
+// copy stream for host outputs) without waiting for them.
+int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out) {
+  int rc = IMAGO_OK;
+  auto rec = [&](int i) {
+    if (!c->capturing) cudaEventRecord(c->ev[i], c->stream);
+  };
+  if (which & IMAGO_OL) {
+    rec(0);
+    rc = do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im);
+    rec(1);
+  }
+  if (!rc && (which & IMAGO_KE)) {
+    rec(2);
+    rc = do_simple(c, KIND_KE, out->ke_packed);
+    rec(3);
+  }
+  if (!rc && (which & IMAGO_NP)) {
+    rec(4);
+    rc = do_simple(c, KIND_NP, out->np_packed);
+    rec(5);
+  }
+  if (!rc && (which & IMAGO_EP)) {
+    rec(6);
+    rc = do_ep(c, out->ep_packed);
+    rec(7);
+  }
+  return rc;
+}
+
+bool same_out(const imago_out &a, const imago_out &b) {
+  return a.ol_packed == b.ol_packed && a.ol_cv_re == b.ol_cv_re &&
+         a.ol_cv_im == b.ol_cv_im && a.ke_packed == b.ke_packed &&
+         a.np_packed == b.np_packed && a.ep_packed == b.ep_packed;
 }
 
 }  // namespace
@@ -1066,32 +1143,195 @@ int imago_intg_build(imago_ctx *c, unsigned which, const imago_out *out) {
   int rc = set_device(c);
   if (rc) return rc;
   if ((rc = begin_call(c))) return finish(c, rc);
-  if (which & IMAGO_OL) {
-    cudaEventRecord(c->ev[0], c->stream);
-    rc = do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im);
-    cudaEventRecord(c->ev[1], c->stream);
-  }
-  if (!rc && (which & IMAGO_KE)) {
-    cudaEventRecord(c->ev[2], c->stream);
-    rc = do_simple(c, KIND_KE, out->ke_packed);
-    cudaEventRecord(c->ev[3], c->stream);
-  }
-  if (!rc && (which & IMAGO_NP)) {
-    cudaEventRecord(c->ev[4], c->stream);
-    rc = do_simple(c, KIND_NP, out->np_packed);
-    cudaEventRecord(c->ev[5], c->stream);
-  }
-  if (!rc && (which & IMAGO_EP)) {
-    cudaEventRecord(c->ev[6], c->stream);
-    rc = do_ep(c, out->ep_packed);
-    cudaEventRecord(c->ev[7], c->stream);
-  }
-  rc = finish(c, rc);
+  rc = finish(c, enqueue_build(c, which, out));
   if (!rc)
     for (int s = 0; s < 4; ++s)
       if (which & (1u << s))
         cudaEventElapsedTime(&c->stage_ms[s], c->ev[2 * s], c->ev[2 * s + 1]);
   return rc;
+}
+
+int imago_intg_build_graph(imago_ctx *c, unsigned which, const imago_out *out) {
+  if (!c || !out || !c->outputs_on_device || !c->stream) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  if (c->gexec && c->gwhich == which && same_out(c->gout, *out)) {
+    begin_call(c);
+    c->launches = c->glaunches;
+    IMAGO_CUDA(cudaGraphLaunch(c->gexec, c->stream));
+    return finish(c, IMAGO_OK);
+  }
+  // first call for these outputs: an eager build (which also sizes every
+  // scratch buffer), then the same launch sequence captured for replay
+  if ((rc = imago_intg_build(c, which, out))) return rc;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  const long long l0 = c->launches;
+  IMAGO_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  c->capturing = true;
+  rc = enqueue_build(c, which, out);
+  c->capturing = false;
+  c->glaunches = c->launches - l0;
+  c->launches = l0;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (!rc && e != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  if (!rc && cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
+    c->gexec = nullptr;
+    rc = IMAGO_ERR_CUDA;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  if (rc) return rc;
+  c->gwhich = which;
+  c->gout = *out;
+  return IMAGO_OK;
+}
+
+int imago_batch_create(int n, const imago_system *systems,
+                       const imago_opts *opts, imago_batch **out) {
+  if (!out) return IMAGO_ERR_INVALID;
+  *out = nullptr;
+  if (n <= 0 || !systems) return IMAGO_ERR_INVALID;
+  imago_batch *b = new (std::nothrow) imago_batch();
+  if (!b) return IMAGO_ERR_NOMEM;
+  b->device = opts ? opts->device : 0;
+  if (cudaSetDevice(b->device) != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  imago_opts co{};
+  co.device = b->device;
+  co.outputs_on_device = 1;
+  co.scratch_bytes = opts ? opts->scratch_bytes : 0;
+  if (co.scratch_bytes == 0) {
+    // every cell keeps its scratch for the graph: a third of free memory
+    // shared out over the cells
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    co.scratch_bytes = std::max<size_t>(fr / 3 / (size_t)n, 1);
+  }
+  int rc = IMAGO_OK;
+  for (int i = 0; i < n && !rc; ++i) {
+    imago_ctx *c = nullptr;
+    rc = imago_intg_create(&systems[i], &co, &c);
+    if (!rc) b->cells.push_back(c);
+  }
+  if (!rc) {
+    if (opts && opts->stream) {
+      b->stream = (cudaStream_t)opts->stream;
+    } else if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) ==
+               cudaSuccess) {
+      b->own_stream = true;
+    } else {
+      b->stream = nullptr;
+      rc = IMAGO_ERR_CUDA;
+    }
+  }
+  if (!rc && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  b->join.assign(b->cells.size(), nullptr);
+  for (size_t i = 0; i < b->join.size() && !rc; ++i)
+    if (cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) != cudaSuccess)
+      rc = IMAGO_ERR_CUDA;
+  if (rc) {
+    cudaGetLastError();
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return IMAGO_OK;
+}
+
+int imago_batch_size(const imago_batch *b) {
+  return b ? (int)b->cells.size() : 0;
+}
+
+int imago_batch_dims(const imago_batch *b, int cell, imago_dims *dims) {
+  if (!b || cell < 0 || cell >= (int)b->cells.size()) return IMAGO_ERR_INVALID;
+  return imago_intg_dims(b->cells[cell], dims);
+}
+
+int imago_batch_build(imago_batch *b, unsigned which, const imago_out *outs) {
+  if (!b || !outs) return IMAGO_ERR_INVALID;
+  if (cudaSetDevice(b->device) != cudaSuccess) {
+    cudaGetLastError();
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  const int n = (int)b->cells.size();
+  bool same = b->exec && b->which == which && (int)b->outs.size() == n;
+  for (int i = 0; same && i < n; ++i) same = same_out(b->outs[i], outs[i]);
+  if (same) {
+    IMAGO_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    IMAGO_CUDA(cudaStreamSynchronize(b->stream));
+    return IMAGO_OK;
+  }
+  // eager: every cell on its own stream, all enqueued before any wait
+  int rc = IMAGO_OK;
+  std::vector<int> crc(n, IMAGO_OK);
+  for (int i = 0; i < n; ++i) {
+    imago_ctx *c = b->cells[i];
+    crc[i] = begin_call(c);
+    if (!crc[i]) crc[i] = enqueue_build(c, which, &outs[i]);
+  }
+  for (int i = 0; i < n; ++i) {
+    const int r = finish(b->cells[i], crc[i]);
+    if (!rc) rc = r;
+  }
+  if (rc) return rc;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  // capture: fork every cell's stream from `stream`, join them back
+  cudaGraph_t graph = nullptr;
+  IMAGO_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  if (cudaEventRecord(b->fork, b->stream) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  long long launches = 0;
+  for (int i = 0; i < n && !rc; ++i) {
+    imago_ctx *c = b->cells[i];
+    if (cudaStreamWaitEvent(c->stream, b->fork, 0) != cudaSuccess) {
+      rc = IMAGO_ERR_CUDA;
+      break;
+    }
+    const long long l0 = c->launches;
+    c->capturing = true;
+    rc = enqueue_build(c, which, &outs[i]);
+    c->capturing = false;
+    launches += c->launches - l0;
+    c->launches = l0;
+    if (cudaEventRecord(b->join[i], c->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(b->stream, b->join[i], 0) != cudaSuccess)
+      rc = rc ? rc : IMAGO_ERR_CUDA;
+  }
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+  if (!rc && e != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  if (!rc && cudaGraphInstantiate(&b->exec, graph, 0) != cudaSuccess) {
+    b->exec = nullptr;
+    rc = IMAGO_ERR_CUDA;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  if (rc) return rc;
+  b->which = which;
+  b->outs.assign(outs, outs + n);
+  b->glaunches = launches;
+  return IMAGO_OK;
+}
+
+int imago_batch_launches(const imago_batch *b, long long *launches) {
+  if (!b || !launches) return IMAGO_ERR_INVALID;
+  *launches = b->glaunches;
+  return IMAGO_OK;
+}
+
+void imago_batch_destroy(imago_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  delete b;
 }
 
 int imago_intg_stage_ms(const imago_ctx *c, double ms[4]) {

@@ -85,6 +85,25 @@ def lib():
         L.imago_intg_destroy.restype = None
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
+        L.imago_intg_build_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint,
+                                             ctypes.POINTER(ImagoOutC)]
+        L.imago_intg_build_graph.restype = ctypes.c_int
+        L.imago_batch_create.argtypes = [ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.POINTER(ImagoOptsC),
+                                         ctypes.POINTER(ctypes.c_void_p)]
+        L.imago_batch_create.restype = ctypes.c_int
+        L.imago_batch_size.argtypes = [ctypes.c_void_p]
+        L.imago_batch_size.restype = ctypes.c_int
+        L.imago_batch_dims.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.POINTER(ImagoDimsC)]
+        L.imago_batch_dims.restype = ctypes.c_int
+        L.imago_batch_build.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+        L.imago_batch_build.restype = ctypes.c_int
+        L.imago_batch_launches.argtypes = [ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        L.imago_batch_launches.restype = ctypes.c_int
+        L.imago_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.imago_batch_destroy.restype = None
         L.imago_strerror.argtypes = [ctypes.c_int]
         L.imago_strerror.restype = ctypes.c_char_p
         L.imago_kpoint_mesh.argtypes = [ctypes.POINTER(ctypes.c_int), _D, _D]
@@ -164,6 +183,25 @@ def prim_eval_static(kind, params, cls=None):
                                       _p(out))
     _check(st, "imago_prim_eval_static")
     return out.reshape(n, 16, 16)
+
+
+_OUT_NAMES = ("ol_packed", "ol_cv_re", "ol_cv_im", "ke_packed", "np_packed",
+              "ep_packed")
+
+
+def _out_struct(out):
+    s = ImagoOutC()
+    for name in _OUT_NAMES:
+        v = out.get(name)
+        if v is None:
+            setattr(s, name, _D())
+        elif isinstance(v, int):
+            setattr(s, name, ctypes.cast(ctypes.c_void_p(v), _D))
+        elif hasattr(v, "data_ptr"):
+            setattr(s, name, ctypes.cast(ctypes.c_void_p(v.data_ptr()), _D))
+        else:
+            setattr(s, name, _p(v))
+    return s
 
 
 class IntegralSetup:
@@ -257,20 +295,19 @@ class IntegralSetup:
                 out["np_packed"] = self._packed()
             if which & IMAGO_EP:
                 out["ep_packed"] = self._packed(self.pot_dim)
-        s = ImagoOutC()
-        for name in ("ol_packed", "ol_cv_re", "ol_cv_im", "ke_packed",
-                     "np_packed", "ep_packed"):
-            v = out.get(name)
-            if v is None:
-                setattr(s, name, _D())
-            elif isinstance(v, int):
-                setattr(s, name, ctypes.cast(ctypes.c_void_p(v), _D))
-            elif hasattr(v, "data_ptr"):
-                setattr(s, name, ctypes.cast(ctypes.c_void_p(v.data_ptr()), _D))
-            else:
-                setattr(s, name, _p(v))
+        s = _out_struct(out)
         _check(lib().imago_intg_build(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build")
+        return out
+
+    def build_graph(self, out, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP):
+        """imago_intg_build_graph: the same builds replayed from a CUDA
+        graph (outputs_on_device contexts; `out` maps names to device
+        pointers or CUDA tensors).  The first call for an output set builds
+        eagerly and captures, later calls replay."""
+        s = _out_struct(out)
+        _check(lib().imago_intg_build_graph(self._ctx, which, ctypes.byref(s)),
+               "imago_intg_build_graph")
         return out
 
     def stage_ms(self):
@@ -298,3 +335,70 @@ class IntegralSetup:
         if which & IMAGO_EP:
             n += per * self.pot_dim
         return n
+
+
+class IntegralBatch:
+    """Independent cells built together (imago_batch_*): one context per
+    cell, outputs on the device, the builds of all cells captured as one
+    CUDA graph on their first call and replayed afterwards."""
+
+    def __init__(self, systems, device=0, scratch_bytes=0, stream=None):
+        from .system import ImagoSystemC
+        self.systems = list(systems)
+        conv = [s.to_c() for s in self.systems]
+        self._keep = conv
+        arr = (ImagoSystemC * len(conv))(*[c for c, _ in conv])
+        self._arr = arr
+        opts = ImagoOptsC(device, stream, 1, scratch_bytes)
+        self._b = ctypes.c_void_p()
+        _check(lib().imago_batch_create(len(conv), ctypes.cast(arr, ctypes.c_void_p),
+                                        ctypes.byref(opts), ctypes.byref(self._b)),
+               "imago_batch_create")
+        self.dims = []
+        for i in range(len(conv)):
+            d = ImagoDimsC()
+            _check(lib().imago_batch_dims(self._b, i, ctypes.byref(d)), "imago_batch_dims")
+            self.dims.append(d)
+
+    def __len__(self):
+        return len(self.dims)
+
+    def output_shapes(self, i):
+        d = self.dims[i]
+        nk, npk, V, C, P = (d.num_kpoints, int(d.packed), d.vale_dim,
+                            max(d.core_dim, 1), d.pot_dim)
+        return {"ol_packed": (nk, npk, 2), "ol_cv_re": (nk, V, C),
+                "ol_cv_im": (nk, V, C), "ke_packed": (nk, npk, 2),
+                "np_packed": (nk, npk, 2), "ep_packed": (P, nk, npk, 2)}
+
+    def build(self, outs, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP):
+        """`outs[i]` maps output names of cell i to device pointers or CUDA
+        tensors."""
+        if len(outs) != len(self.dims):
+            raise ValueError("one output set per cell")
+        arr = (ImagoOutC * len(outs))(*[_out_struct(o) for o in outs])
+        _check(lib().imago_batch_build(self._b, which, ctypes.cast(arr, ctypes.c_void_p)),
+               "imago_batch_build")
+        return outs
+
+    def graph_launches(self):
+        n = ctypes.c_longlong()
+        _check(lib().imago_batch_launches(self._b, ctypes.byref(n)), "imago_batch_launches")
+        return n.value
+
+    def close(self):
+        if self._b:
+            lib().imago_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -197,6 +197,38 @@ IMAGO_API int imago_intg_kernel_stats(const imago_ctx *ctx, double ms[4],
 
 IMAGO_API void imago_intg_destroy(imago_ctx *ctx);
 
+/* No counterpart in the reference: the same builds as imago_intg_build,
+ * replayed from a CUDA graph.  Device outputs only (outputs_on_device), on
+ * the context's own stream or a non-default one.  The first call for a
+ * given `which` and output set runs an eager build (its results are
+ * valid) and captures the launch sequence; later calls with the same
+ * arguments replay it.  Kernel timings are not recorded for replays. */
+IMAGO_API int imago_intg_build_graph(imago_ctx *ctx, unsigned which,
+                                     const imago_out *out);
+
+/*
+ * Batched builds of independent cells (no counterpart in the reference):
+ * one context per cell, each with its own stream and scratch (by default a
+ * third of the free device memory shared out over the cells), all outputs
+ * on the device.  imago_batch_build takes one imago_out per cell.  Its
+ * first call for an output set runs every cell's builds concurrently on the
+ * cells' streams, then captures them as one CUDA graph with a branch per
+ * cell, which later calls with the same outputs replay on the batch's
+ * stream (opts->stream, or a stream of its own).  Returns when all cells are
+ * done.
+ */
+typedef struct imago_batch imago_batch;
+IMAGO_API int imago_batch_create(int n, const imago_system *systems,
+                                 const imago_opts *opts, imago_batch **out);
+IMAGO_API int imago_batch_size(const imago_batch *batch);
+IMAGO_API int imago_batch_dims(const imago_batch *batch, int cell,
+                               imago_dims *dims);
+IMAGO_API int imago_batch_build(imago_batch *batch, unsigned which,
+                                const imago_out *outs);
+/* Kernels in the captured graph (0 before the first build). */
+IMAGO_API int imago_batch_launches(const imago_batch *batch, long long *launches);
+IMAGO_API void imago_batch_destroy(imago_batch *batch);
+
 /* No counterpart in the reference.  Device scratch of every context comes
  * from one stream-ordered memory pool per device that keeps freed memory
  * for the next context; this hands the pool's unused memory on `device`

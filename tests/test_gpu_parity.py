@@ -192,3 +192,79 @@ def test_contexts_reuse_and_trim_the_memory_pool(imago_lib):
     assert np.array_equal(first, again)
     with pytest.raises(intg.ImagoError):
         intg.trim_memory(-1)
+
+
+def _device_outputs(torch, shapes):
+    dev = torch.device("cuda", 0)
+    return {k: torch.full(v, np.nan, dtype=torch.float64, device=dev)
+            for k, v in shapes.items()}
+
+
+def _same(a, b):
+    # bitwise-equal values; NaN where neither side writes (no core states)
+    return bool(((a == b) | (a.isnan() & b.isnan())).all())
+
+
+def _shapes(g):
+    C = max(g.core_dim, 1)
+    return {"ol_packed": (g.nk, g.npacked, 2), "ol_cv_re": (g.nk, g.vale_dim, C),
+            "ol_cv_im": (g.nk, g.vale_dim, C), "ke_packed": (g.nk, g.npacked, 2),
+            "np_packed": (g.nk, g.npacked, 2),
+            "ep_packed": (g.pot_dim, g.nk, g.npacked, 2)}
+
+
+def test_graph_replay_matches_eager_build(imago_lib):
+    # imago_intg_build_graph: the first call builds eagerly and captures,
+    # the second replays the captured graph; both must reproduce the eager
+    # build bit for bit.
+    import torch
+    s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+    with intg.IntegralSetup(s, outputs_on_device=True) as g:
+        ref = _device_outputs(torch, _shapes(g))
+        g.build(out=ref)
+        got = _device_outputs(torch, _shapes(g))
+        for _ in range(2):
+            for v in got.values():
+                v.fill_(np.nan)
+            g.build_graph(got)
+            torch.cuda.synchronize()
+            for k in ref:
+                assert _same(ref[k], got[k]), k
+
+
+def test_batch_matches_single_cells(imago_lib):
+    # Three independent cells of different kinds and sizes in one batch:
+    # the eager first build and the graph replay both equal the cells'
+    # own builds, and a strained, jittered graphite cell matches the oracle.
+    import torch
+    e = np.array([[0.02, 0.004, 0.0], [0.004, -0.015, 0.003], [0.0, 0.003, 0.01]])
+    cells = [configs.small_test_system(),
+             configs.graphite_cell(reps=(2, 1, 1), kmesh=(2, 2, 2), seed=11,
+                                   jitter=0.02, strain=e),
+             configs.cubic_supercell("si", reps=(1, 1, 1), kmesh=(2, 1, 1), seed=12,
+                                     strain=-e)]
+    refs = []
+    for s in cells:
+        with intg.IntegralSetup(s, outputs_on_device=True) as g:
+            r = _device_outputs(torch, _shapes(g))
+            g.build(out=r)
+            refs.append(r)
+    with intg.IntegralBatch(cells) as b:
+        outs = [_device_outputs(torch, b.output_shapes(i)) for i in range(len(b))]
+        for _ in range(2):
+            for o in outs:
+                for v in o.values():
+                    v.fill_(np.nan)
+            b.build(outs)
+            torch.cuda.synchronize()
+            for r, o in zip(refs, outs):
+                for k in r:
+                    assert _same(r[k], o[k]), k
+        assert b.graph_launches() > 0
+    ob = oracle.OracleBuild(cells[1])
+    res = {"OL": packed_mismatch(outs[1]["ol_packed"].cpu().numpy(), ob.overlap()[0]),
+           "KE": packed_mismatch(outs[1]["ke_packed"].cpu().numpy(), ob.kinetic()),
+           "NP": packed_mismatch(outs[1]["np_packed"].cpu().numpy(), ob.nuclear()),
+           "EP0": packed_mismatch(outs[1]["ep_packed"][0].cpu().numpy(),
+                                  ob.elec_pot(0, 1)[0])}
+    _assert_all(res)
