@@ -162,6 +162,7 @@ struct imago_ctx {
   DBuf<Term3c> d_terms;
   DBuf<int2> d_btile;
   DBuf<SiteImage> d_simg;
+  DBuf<float> d_cl_d1;
 
   // scratch
   DBuf<double> blk, M;
@@ -210,6 +211,7 @@ struct imago_ctx {
     for (auto *b : {&d_phase, &vv, &cv, &cc, &y, &s_cv}) b->release(st);
     d_pairs.release(st); d_units.release(st); d_sps.release(st);
     d_terms.release(st); d_btile.release(st); d_simg.release(st);
+    d_cl_d1.release(st);
     if (st) cudaStreamSynchronize(st);
     if (events)
       for (auto &e : ev) cudaEventDestroy(e);
@@ -610,12 +612,29 @@ int build_work(imago_ctx *c) {
     }
   c->blk_total = boff;
   c->m_total = moff;
-  // shell pairs by class, stable in unit order
+  // Shell pairs by class and, within a class, by the pair's own part of
+  // the three-centre screening radius^2, frac T / (a1 + a2) (gaussRelations
+  // alphaNucDist/alphaPotDist without the third exponent), in four buckets
+  // (above 64, 16, 4 bohr^2 and below), stable in unit order: a warp then
+  // holds shell pairs of similar reach, whose site screens agree.  The
+  // order only maps threads to shell pairs.
+  std::vector<int> key(c->sps.size());
+  for (size_t q = 0; q < c->sps.size(); ++q) {
+    const DSp &sp = c->sps[q];
+    const DUnit &u = c->units[sp.unit];
+    const DPair &p = c->pairs[u.pair];
+    const HType &s1 = c->types[c->type_screen[p.ti]];
+    const HType &s2 = c->types[c->type_screen[p.tj]];
+    const double x1 = s1.alphas[sp.a], x2 = s2.alphas[sp.b];
+    const double frac = 1.0 - u.r2 / (c->T / x2 / (x1 / (x1 + x2)));
+    const double reach = frac * c->T / (x1 + x2);
+    const int bucket = reach > 64.0 ? 0 : reach > 16.0 ? 1 : reach > 4.0 ? 2 : 3;
+    key[q] = (sp.la * 4 + sp.lb) * 4 + bucket;
+  }
   std::vector<int> idx(c->sps.size());
   std::iota(idx.begin(), idx.end(), 0);
-  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-    return c->sps[x].la * 4 + c->sps[x].lb < c->sps[y].la * 4 + c->sps[y].lb;
-  });
+  std::stable_sort(idx.begin(), idx.end(),
+                   [&](int x, int y) { return key[x] < key[y]; });
   c->sp_by_cls = idx;
   for (int k = 0; k <= 16; ++k) c->cls_beg[k] = 0;
   for (const DSp &sp : c->sps) c->cls_beg[sp.la * 4 + sp.lb + 1] += 1;
@@ -715,15 +734,19 @@ int upload(imago_ctx *c) {
   w.nbtile = (int)c->btile.size();
   w.btile = c->d_btile.p;
   w.simg = nullptr;
+  w.cl_d1 = nullptr;
+  w.ncl = (c->nps + kSiteCluster - 1) / kSiteCluster;
   if ((rc = launch_phase(s, c->d_phase.p, st))) return rc;
-  // midpoint images of the potential sites for the three-centre screens,
-  // when the table fits in kMaxSiteImageBytes; without it every site is
-  // searched in full
+  // midpoint images of the potential sites, and their cluster bounds, for
+  // the three-centre screens, when the table fits in kMaxSiteImageBytes;
+  // without it every site is searched in full
   const size_t nb = (size_t)w.nunits * c->nps;
   if (nb > 0 && nb * sizeof(SiteImage) <= kMaxSiteImageBytes &&
-      c->d_simg.alloc(nb, st) == IMAGO_OK) {
+      c->d_simg.alloc(nb, st) == IMAGO_OK &&
+      c->d_cl_d1.alloc((size_t)w.nunits * w.ncl, st) == IMAGO_OK) {
     w.simg = c->d_simg.p;
-    rc = launch_site_images(s, w, c->d_simg.p, st);
+    w.cl_d1 = c->d_cl_d1.p;
+    rc = launch_site_images(s, w, c->d_simg.p, c->d_cl_d1.p, st);
   }
   return rc;
 }

@@ -78,7 +78,14 @@ struct DevWork {
   // [unit * nps + site]: the potential site's nearest image to the midpoint
   // of the unit's A-B segment (null: every site is searched in full)
   const struct SiteImage *simg;
+  // [unit * ncl + c]: the smallest d1 of sites kSiteCluster*c .. +7 (null
+  // with simg)
+  const float *cl_d1;
+  int ncl;
 };
+
+// Consecutive potential sites screened together before their own tests.
+constexpr int kSiteCluster = 8;
 
 // Nearest image of a potential site C to the midpoint M of a unit's A-B
 // segment: M - C - (n0 a + n1 b + n2 c) is shortest for lattice coordinates
@@ -118,7 +125,7 @@ int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
                     cudaStream_t st);
 int launch_phase(const DevSys &s, double2 *phase, cudaStream_t st);
 int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
-                       cudaStream_t st);
+                       float *cl_d1, cudaStream_t st);
 int launch_prim_eval(int kind, int n, const double *params, const int *cls,
                      double *sh, cudaStream_t st);
 

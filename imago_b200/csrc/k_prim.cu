@@ -89,23 +89,30 @@ __global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
     }
     const float tf = __double2float_ru(t);
     const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
-    for (int site = s0; site < s1; ++site) {
-      double L2[3], v[3], c0;
-      if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
-      const double *C = s.psite_pos + 3 * site;
-      const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-      for (int nc = 0; nc < s.ncell; ++nc) {
-        if (s.csize[nc] > maxr) break;
-        const double *R = s.cell + 3 * nc;
-        const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-        if (dx * dx + dy * dy + dz * dz > t) continue;
-        double X[3];
+    // clusters of kSiteCluster sites first: one bound rules out all of them
+    for (int cb = s0 - s0 % kSiteCluster; cb < s1; cb += kSiteCluster) {
+      if (w.cl_d1 &&
+          beyond(w.cl_d1[(long long)sp.unit * w.ncl + cb / kSiteCluster], pmf, tf))
+        continue;
+      const int lo = max(cb, s0), hi = min(cb + kSiteCluster, s1);
+      for (int site = lo; site < hi; ++site) {
+        double L2[3], v[3], c0;
+        if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+        const double *C = s.psite_pos + 3 * site;
+        const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+        for (int nc = 0; nc < s.ncell; ++nc) {
+          if (s.csize[nc] > maxr) break;
+          const double *R = s.cell + 3 * nc;
+          const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+          if (dx * dx + dy * dy + dz * dz > t) continue;
+          double X[3];
 #pragma unroll
-        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-        if (NUC)
-          accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
-        else
-          accumulate_overlap_q<L>(X, mu, 1.0, Q);
+          for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+          if (NUC)
+            accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
+          else
+            accumulate_overlap_q<L>(X, mu, 1.0, Q);
+        }
       }
     }
   }
@@ -182,22 +189,29 @@ __global__ void __launch_bounds__(128)
     }
     const float tf = __double2float_ru(t);
     const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
-    for (int site = s0; site < s1; ++site) {
-      double L2[3], v[3], c0;
-      if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
-      const double *C = s.psite_pos + 3 * site;
-      const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-      for (int nc = 0; nc < s.ncell; ++nc) {
-        if (s.csize[nc] > maxr) break;
-        const double *R = s.cell + 3 * nc;
-        const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-        if (dx * dx + dy * dy + dz * dz > t) continue;
-        double X[3];
-        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-        if (NUC)
-          accumulate_nuclear_q_rt(L, X, mu, nu, w0, Q);
-        else
-          accumulate_overlap_q_rt(L, X, mu, 1.0, Q);
+    // clusters of kSiteCluster sites first: one bound rules out all of them
+    for (int cb = s0 - s0 % kSiteCluster; cb < s1; cb += kSiteCluster) {
+      if (w.cl_d1 &&
+          beyond(w.cl_d1[(long long)sp.unit * w.ncl + cb / kSiteCluster], pmf, tf))
+        continue;
+      const int lo = max(cb, s0), hi = min(cb + kSiteCluster, s1);
+      for (int site = lo; site < hi; ++site) {
+        double L2[3], v[3], c0;
+        if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+        const double *C = s.psite_pos + 3 * site;
+        const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+        for (int nc = 0; nc < s.ncell; ++nc) {
+          if (s.csize[nc] > maxr) break;
+          const double *R = s.cell + 3 * nc;
+          const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+          if (dx * dx + dy * dy + dz * dz > t) continue;
+          double X[3];
+          for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+          if (NUC)
+            accumulate_nuclear_q_rt(L, X, mu, nu, w0, Q);
+          else
+            accumulate_overlap_q_rt(L, X, mu, 1.0, Q);
+        }
       }
     }
   }
@@ -295,13 +309,33 @@ __global__ void k_site_images(DevSys s, DevWork w, SiteImage *simg) {
     simg[i] = site_image(s, w, (int)(i / s.nps), (int)(i % s.nps));
 }
 
+__global__ void k_cluster_bounds(DevSys s, DevWork w, const SiteImage *simg,
+                                 float *cl_d1) {
+  const long long n = (long long)w.nunits * w.ncl;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int unit = (int)(i / w.ncl), c = (int)(i % w.ncl);
+    const int hi = min((c + 1) * kSiteCluster, s.nps);
+    float d = 3.0e38f;
+    for (int site = c * kSiteCluster; site < hi; ++site)
+      d = fminf(d, simg[(long long)unit * s.nps + site].d1);
+    cl_d1[i] = d;
+  }
+}
+
 int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
-                       cudaStream_t st) {
+                       float *cl_d1, cudaStream_t st) {
   const long long n = (long long)w.nunits * s.nps;
   if (n == 0) return IMAGO_OK;
   k_site_images<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256,
                   0, st>>>(s, w, simg);
   IMAGO_CUDA(cudaGetLastError());
+  const long long nc = (long long)w.nunits * w.ncl;
+  if (cl_d1 && nc > 0) {
+    k_cluster_bounds<<<(unsigned)std::min<long long>((nc + 255) / 256, 148 * 16),
+                       256, 0, st>>>(s, w, simg, cl_d1);
+    IMAGO_CUDA(cudaGetLastError());
+  }
   return IMAGO_OK;
 }
 
