@@ -563,6 +563,155 @@ __global__ void __launch_bounds__(kOThreads, 4)
       }
 }
 
+// Small systems: the whole orthogonalisation of one (k, term) in one CTA.
+// S (C x V), X_cv (C x V) and X_cc (C x C) are read once into shared
+// memory (k-major rows, zero padded to multiples of 4 in k and 16 in the
+// output index, rows of 2 mod 8 complex values for conflict-free fragment
+// reads); Y = X_cv - X_cc S / 2 is formed in place of X_cv, then the upper
+// 16x16 subtiles of S^H Y + Y^H S are taken straight from shared memory and
+// subtracted from VV in the packing epilogue.  Used while the three arrays
+// fit in kFusedMaxSmem.
+constexpr int kFThreads = 512;
+constexpr int kFWarps = kFThreads / 32;
+constexpr size_t kFusedMaxSmem = 200 * 1024;
+
+struct FusedDims {
+  int C4, C16, V16, Vp, Cp;
+};
+
+__host__ __device__ inline FusedDims fused_dims(int C, int V) {
+  FusedDims d;
+  d.C4 = (C + 3) / 4 * 4;
+  d.C16 = (C + 15) / 16 * 16;
+  d.V16 = (V + 15) / 16 * 16;
+  d.Vp = d.V16 + 2;
+  d.Cp = d.C16 + 2;
+  return d;
+}
+
+inline size_t fused_smem(int C, int V) {
+  const FusedDims d = fused_dims(C, V);
+  return sizeof(double2) * ((size_t)2 * d.C4 * d.Vp + (size_t)d.C4 * d.Cp);
+}
+
+// One warp's 16x16 complex subtile of op(A)^T B over k in [k0, k0 + nk4)
+// from k-major shared arrays (row strides lda, ldb), 3M form.
+template <bool CONJ>
+__device__ __forceinline__ void fused_tile(const double2 *A, int lda, int r0,
+                                           const double2 *B, int ldb, int c0,
+                                           int nk4, bool skip_lower,
+                                           double t1[2][2][2], double t2[2][2][2],
+                                           double t3[2][2][2], int lane) {
+  for (int ks = 0; ks < nk4; ks += 4) {
+    const int kk = ks + (lane & 3);
+    double2 a[2], b[2];
+    double as[2], bs[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      a[t] = A[kk * lda + r0 + 8 * t + (lane >> 2)];
+      b[t] = B[kk * ldb + c0 + 8 * t + (lane >> 2)];
+      as[t] = CONJ ? a[t].x - a[t].y : a[t].x + a[t].y;
+      bs[t] = b[t].x + b[t].y;
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        if (skip_lower && mt > nt) continue;  // rows 8..15 x cols 0..7
+        dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
+        dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
+      }
+  }
+}
+
+__global__ void __launch_bounds__(kFThreads, 1)
+    k_ortho_fused(DevSys s, const double2 *vv, const double2 *cv,
+                  const double2 *cc, const double2 *s_cv, double *packed) {
+  extern __shared__ double2 fsm[];
+  const int V = s.vale_dim, C = s.core_dim;
+  const FusedDims d = fused_dims(C, V);
+  double2 *Ss = fsm, *Ys = fsm + d.C4 * d.Vp, *Xs = Ys + d.C4 * d.Vp;
+  const int k = blockIdx.x, term = blockIdx.y;
+  const long long tk = (long long)term * s.nk + k;
+  const double2 *S = s_cv + (long long)k * V * C;
+  const double2 *X = cv + tk * V * C;
+  const double2 *XC = cc + tk * C * C;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double2 zero = make_double2(0.0, 0.0);
+  // S(l, v) and X_cv(l, v), l fastest in memory, to [l][v]
+  for (int i = tid; i < d.C4 * d.V16; i += kFThreads) {
+    const int l = i % d.C4, v = i / d.C4;
+    const bool in = l < C && v < V;
+    Ss[l * d.Vp + v] = in ? S[(long long)v * C + l] : zero;
+    Ys[l * d.Vp + v] = in ? X[(long long)v * C + l] : zero;
+  }
+  // X_cc(c, l), c fastest in memory, to [l][c]
+  for (int i = tid; i < d.C4 * d.C16; i += kFThreads) {
+    const int c = i % d.C16, l = i / d.C16;
+    Xs[l * d.Cp + c] = (l < C && c < C) ? XC[(long long)l * C + c] : zero;
+  }
+  __syncthreads();
+  // Y = X_cv - X_cc S / 2, subtiles of 16 core x 16 valence indices
+  const int yr = d.C16 / 16, ny = yr * (d.V16 / 16);
+  for (int tile = warp; tile < ny; tile += kFWarps) {
+    const int r0 = (tile % yr) * 16, c0 = (tile / yr) * 16;
+    double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
+    fused_tile<false>(Xs, d.Cp, r0, Ss, d.Vp, c0, d.C4, false, t1, t2, t3, lane);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int c = r0 + 8 * mt + (lane >> 2);
+          const int v = c0 + 8 * nt + 2 * (lane & 3) + i;
+          if (c >= C || v >= V) continue;
+          const double2 p = ocombine<false>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+          double2 &y = Ys[c * d.Vp + v];
+          y.x -= 0.5 * p.x;
+          y.y -= 0.5 * p.y;
+        }
+  }
+  __syncthreads();
+  // upper subtiles (J <= I) of S^H Y + Y^H S over the stacked k = 2 C4
+  const double2 *VVt = vv + tk * V * V;
+  const long long np = (long long)V * (V + 1) / 2;
+  double *out = packed + 2 * tk * np;
+  const int nt16 = d.V16 / 16, nup = nt16 * (nt16 + 1) / 2;
+  for (int tile = warp; tile < nup; tile += kFWarps) {
+    int t = tile, I = 0;
+    while (t > I) {
+      t -= I + 1;
+      ++I;
+    }
+    const int J = t, r0 = J * 16, c0 = I * 16;
+    double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
+    fused_tile<true>(Ss, d.Vp, r0, Ys, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
+    fused_tile<true>(Ys, d.Vp, r0, Ss, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int row = r0 + 8 * mt + (lane >> 2);
+          const int col = c0 + 8 * nt + 2 * (lane & 3) + i;
+          if (row >= V || col >= V || row > col) continue;
+          double2 v = VVt[(long long)col * V + row];
+          const double2 p = ocombine<true>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+          v.x -= p.x;
+          v.y -= p.y;
+          if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
+          if (fabs(v.x) < kPackThresh) v.x = 0.0;
+          if (fabs(v.y) < kPackThresh) v.y = 0.0;
+          const long long idx = (long long)col * (col + 1) / 2 + row;
+          out[2 * idx] = v.x;
+          out[2 * idx + 1] = v.y;
+        }
+  }
+}
+
 // coreDim == 0: the reference packs valeVale as it is (integrals.F90:3657-3676).
 __global__ void __launch_bounds__(256)
     k_pack_plain(DevSys s, const double2 *vv, double *packed) {
@@ -593,6 +742,22 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
     const long long np = (long long)V * (V + 1) / 2;
     dim3 g((unsigned)std::min<long long>((np + 255) / 256, 128), s.nk, nterm);
     k_pack_plain<<<g, 256, 0, st>>>(s, vv, packed);
+    IMAGO_CUDA(cudaGetLastError());
+    return IMAGO_OK;
+  }
+  const size_t smem = fused_smem(C, V);
+  if (smem <= kFusedMaxSmem) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+      IMAGO_CUDA(cudaFuncSetAttribute(k_ortho_fused,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kFusedMaxSmem));
+      attr_set[dev] = true;
+    }
+    k_ortho_fused<<<dim3(s.nk, nterm), kFThreads, smem, st>>>(s, vv, cv, cc, s_cv,
+                                                              packed);
     IMAGO_CUDA(cudaGetLastError());
     return IMAGO_OK;
   }
