@@ -22,6 +22,17 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a,
       : "d"(a), "d"(b));
 }
 
+// 16-byte global-to-shared copy that does not pass through registers;
+// with `valid` false nothing is read and the destination is zero-filled.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem,
+                                           bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst),
+               "l"(gmem), "r"(n)
+               : "memory");
+}
+
 // ---------------------------------------------------------- contract --
 // One CTA per (unit, group of terms), threads over the block elements:
 //   M_t(m1, m2) = sum_{(a,b) in unit} C1(a, m1) C2(b, m2) sh_t,ab(lm1, lm2),
@@ -638,19 +649,23 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const double2 *X = cv + tk * V * C;
   const double2 *XC = cc + tk * C * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const double2 zero = make_double2(0.0, 0.0);
-  // S(l, v) and X_cv(l, v), l fastest in memory, to [l][v]
+  // S(l, v) and X_cv(l, v), l fastest in memory, to [l][v]; X_cc(c, l), c
+  // fastest, to [l][c]: asynchronous 16-byte copies, all in flight at once,
+  // the padding zero-filled
   for (int i = tid; i < d.C4 * d.V16; i += kFThreads) {
     const int l = i % d.C4, v = i / d.C4;
     const bool in = l < C && v < V;
-    Ss[l * d.Vp + v] = in ? S[(long long)v * C + l] : zero;
-    Ys[l * d.Vp + v] = in ? X[(long long)v * C + l] : zero;
+    const long long g = in ? (long long)v * C + l : 0;
+    cp_async16(&Ss[l * d.Vp + v], S + g, in);
+    cp_async16(&Ys[l * d.Vp + v], X + g, in);
   }
-  // X_cc(c, l), c fastest in memory, to [l][c]
   for (int i = tid; i < d.C4 * d.C16; i += kFThreads) {
     const int c = i % d.C16, l = i / d.C16;
-    Xs[l * d.Cp + c] = (l < C && c < C) ? XC[(long long)l * C + c] : zero;
+    const bool in = l < C && c < C;
+    cp_async16(&Xs[l * d.Cp + c], XC + (in ? (long long)l * C + c : 0), in);
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   // Y = X_cv - X_cc S / 2, subtiles of 16 core x 16 valence indices
   const int yr = d.C16 / 16, ny = yr * (d.V16 / 16);
@@ -686,6 +701,20 @@ __global__ void __launch_bounds__(kFThreads, 1)
       ++I;
     }
     const int J = t, r0 = J * 16, c0 = I * 16;
+    // the tile's VV entries, loaded before the MMAs so they arrive meanwhile
+    double2 vvp[2][2][2];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int row = r0 + 8 * mt + (lane >> 2);
+          const int col = c0 + 8 * nt + 2 * (lane & 3) + i;
+          vvp[mt][nt][i] = (row < V && col < V && row <= col)
+                               ? VVt[(long long)col * V + row]
+                               : make_double2(0.0, 0.0);
+        }
     double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
     fused_tile<true>(Ss, d.Vp, r0, Ys, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
     fused_tile<true>(Ys, d.Vp, r0, Ss, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
@@ -698,7 +727,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
           const int row = r0 + 8 * mt + (lane >> 2);
           const int col = c0 + 8 * nt + 2 * (lane & 3) + i;
           if (row >= V || col >= V || row > col) continue;
-          double2 v = VVt[(long long)col * V + row];
+          double2 v = vvp[mt][nt][i];
           const double2 p = ocombine<true>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
           v.x -= p.x;
           v.y -= p.y;
