@@ -302,7 +302,8 @@ def time_device_builds(g, bufs, stream, steps, flush, torch):
     between builds to flush L2; kernel-stage milliseconds summed."""
     step_s, kms, launches = [], np.zeros(4), 0
     for _ in range(steps):
-        flush.fill_(1.0)
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
         s.record(stream)
@@ -351,6 +352,7 @@ def silica_headline(args, local, stream, torch):
     wl = "quartz-gamma"
     system = system_for(wl)
     dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=local)
     g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
                            stream=stream.cuda_stream)
     bufs = device_outputs(g, torch, dev)
@@ -501,7 +503,9 @@ def run_ours(args):
 
     wl = WORKLOADS[args.workload]
     system = system_for(args.workload, rank, args.kmesh)
-    stream = torch.cuda.current_stream()
+    # the library runs on this stream, and the timing events are recorded on
+    # it, so they bracket exactly the build's work
+    stream = torch.cuda.Stream(device=local)
     g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
                            stream=stream.cuda_stream,
                            scratch_bytes=args.scratch_mb << 20)
@@ -530,6 +534,7 @@ def run_ours(args):
     value = total / args.steps
     kms /= args.steps
 
+    tuning = g.tuning()
     e2e = time_e2e(system, local, stream, bufs, max(2, min(args.steps, 3)), torch)
 
     flops = algorithmic_flops(g)
@@ -569,6 +574,7 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
+            "tuning": tuning,
         }
         if args.workload == "si8" and list(args.kmesh) != [8, 8, 8]:
             line["note"] = (f"k-mesh {args.kmesh} (profiling case, not the "

@@ -143,6 +143,12 @@ struct imago_ctx {
   std::vector<DSp> sps;
   std::vector<int> sp_by_cls;
   std::vector<int2> btile;
+  // tensor-core phase-sum tiles for each tuned width, concatenated, and
+  // where each width's list starts
+  std::vector<int2> btile_w;
+  int btile_off[kNumBlochWidths + 1] = {};
+  bool bloch_tuned = false;
+  float bloch_ms[kNumBlochWidths] = {};
   int cls_beg[17];
   long long blk_total = 0, m_total = 0;
   std::vector<Term3c> ep_terms;
@@ -160,7 +166,7 @@ struct imago_ctx {
   DBuf<DUnit> d_units;
   DBuf<DSp> d_sps;
   DBuf<Term3c> d_terms;
-  DBuf<int2> d_btile;
+  DBuf<int2> d_btile, d_btile_w;
   DBuf<SiteImage> d_simg;
   DBuf<float> d_cl_d1;
 
@@ -211,6 +217,7 @@ struct imago_ctx {
     for (auto *b : {&d_phase, &vv, &cv, &cc, &y, &s_cv}) b->release(st);
     d_pairs.release(st); d_units.release(st); d_sps.release(st);
     d_terms.release(st); d_btile.release(st); d_simg.release(st);
+    d_btile_w.release(st);
     d_cl_d1.release(st);
     if (st) cudaStreamSynchronize(st);
     if (events)
@@ -646,6 +653,16 @@ int build_work(imago_ctx *c) {
     const int ne = c->pairs[p].ni * c->pairs[p].nj;
     for (int t = 0; t * kBlochCols < ne; ++t) c->btile.push_back(make_int2(p, t));
   }
+  c->btile_w.clear();
+  for (int wi = 0; wi < kNumBlochWidths; ++wi) {
+    c->btile_off[wi] = (int)c->btile_w.size();
+    const int bw = bloch_width(wi);
+    for (int p = 0; p < (int)c->pairs.size(); ++p) {
+      const int ne = c->pairs[p].ni * c->pairs[p].nj;
+      for (int t = 0; t * bw < ne; ++t) c->btile_w.push_back(make_int2(p, t));
+    }
+  }
+  c->btile_off[kNumBlochWidths] = (int)c->btile_w.size();
   // EP terms in the reference's order (cumulAlphaSum + alpha index)
   c->ep_terms.clear();
   for (int t = 0; t < c->npt; ++t)
@@ -655,6 +672,12 @@ int build_work(imago_ctx *c) {
 }
 
 constexpr size_t kMaxSiteImageBytes = size_t(4) << 30;
+
+void set_bloch_width(imago_ctx *c, int wi) {
+  c->work.bw = bloch_width(wi);
+  c->work.btile_w = c->d_btile_w.p + c->btile_off[wi];
+  c->work.nbtile_w = c->btile_off[wi + 1] - c->btile_off[wi];
+}
 
 int upload(imago_ctx *c) {
   cudaStream_t st = c->stream;
@@ -698,7 +721,7 @@ int upload(imago_ctx *c) {
   UP(d_psite_ptype, c->psite_ptype) UP(d_cell, c->cells) UP(d_csize, c->csize)
   UP(d_kxyz, c->kxyz) UP(d_pairs, c->pairs) UP(d_units, c->units)
   UP(d_sps, c->sps) UP(d_sp_by_cls, c->sp_by_cls) UP(d_terms, c->ep_terms)
-  UP(d_btile, c->btile)
+  UP(d_btile, c->btile) UP(d_btile_w, c->btile_w)
 #undef UP
   if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk, st))) return rc;
 
@@ -733,6 +756,7 @@ int upload(imago_ctx *c) {
   w.m_total = c->m_total;
   w.nbtile = (int)c->btile.size();
   w.btile = c->d_btile.p;
+  set_bloch_width(c, kNumBlochWidths - 1);
   w.simg = nullptr;
   w.cl_d1 = nullptr;
   w.ncl = (c->nps + kSiteCluster - 1) / kSiteCluster;
@@ -799,6 +823,40 @@ int class_launches(const imago_ctx *c) {
   return n;
 }
 
+// The tensor-core phase sum's column-tile width is picked by measurement:
+// on the context's first phase sum each width runs once on the real blocks
+// (every run writes the same values) and the fastest is kept.  Narrower
+// tiles waste less on block widths that are not multiples of 64, wider
+// ones reuse each phase fragment more.
+int tune_bloch(imago_ctx *c, int nterm) {
+  cudaEvent_t e[kNumBlochWidths + 1];
+  for (auto &x : e)
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_CUDA;
+    }
+  int rc = IMAGO_OK;
+  cudaEventRecord(e[0], c->stream);
+  for (int wi = 0; wi < kNumBlochWidths && !rc; ++wi) {
+    set_bloch_width(c, wi);
+    rc = launch_bloch(c->sys, c->work, nterm, c->M.p, c->vv.p, c->cv.p, c->cc.p,
+                      c->stream);
+    cudaEventRecord(e[wi + 1], c->stream);
+  }
+  if (!rc && cudaEventSynchronize(e[kNumBlochWidths]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  int best = kNumBlochWidths - 1;
+  for (int wi = 0; wi < kNumBlochWidths && !rc; ++wi)
+    cudaEventElapsedTime(&c->bloch_ms[wi], e[wi], e[wi + 1]);
+  for (int wi = 0; wi < kNumBlochWidths && !rc; ++wi)
+    if (c->bloch_ms[wi] < c->bloch_ms[best]) best = wi;
+  for (auto &x : e) cudaEventDestroy(x);
+  cudaGetLastError();
+  set_bloch_width(c, best);
+  c->launches += kNumBlochWidths;
+  c->bloch_tuned = !rc;
+  return rc;
+}
+
 int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
               double *packed_dev) {
   cudaStream_t st = c->stream;
@@ -820,6 +878,9 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   mark(c);
   if ((rc = launch_contract(s, w, nterm, c->blk.p, c->M.p, st))) return rc;
   mark(c);
+  if (!c->bloch_tuned && !c->capturing && s.nk > kBlochSmallNk &&
+      (rc = tune_bloch(c, nterm)))
+    return rc;
   if ((rc = launch_bloch(s, w, nterm, c->M.p, c->vv.p, c->cv.p, c->cc.p, st)))
     return rc;
   mark(c);
@@ -1378,6 +1439,14 @@ void imago_intg_destroy(imago_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   delete c;
+}
+
+int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (bloch_width) *bloch_width = c->work.bw;
+  if (trial_ms)
+    for (int i = 0; i < kNumBlochWidths; ++i) trial_ms[i] = c->bloch_ms[i];
+  return IMAGO_OK;
 }
 
 int imago_trim_memory(int device) {

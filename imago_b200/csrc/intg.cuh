@@ -73,8 +73,11 @@ struct DevWork {
   const int *sp_by_cls;   // shell pairs sorted by class (la*4+lb), then unit
   long long blk_total;    // doubles of sh blocks per term
   long long m_total;      // doubles of unit blocks per term
-  int nbtile;             // phase-sum column tiles: (pair, tile)
+  int nbtile;             // phase-sum column tiles of kBlochCols: (pair, tile)
   const int2 *btile;
+  int bw;                 // column width of the tensor-core phase sum
+  int nbtile_w;           // its tiles: (pair, tile of bw columns)
+  const int2 *btile_w;
   // [unit * nps + site]: the potential site's nearest image to the midpoint
   // of the unit's A-B segment (null: every site is searched in full)
   const struct SiteImage *simg;
@@ -98,8 +101,13 @@ struct __align__(16) SiteImage {
   float d1, d2;
 };
 
-// Columns (block elements) per phase-sum CTA.
+// Columns (block elements) per CTA of the register phase sum, and the
+// column widths the tensor-core phase sum is tuned over (32, 48, 64).
 constexpr int kBlochCols = 64;
+constexpr int kNumBlochWidths = 3;
+__host__ __device__ constexpr int bloch_width(int i) { return 32 + 16 * i; }
+// Up to this many k-points the phase sum keeps its sums in registers.
+constexpr int kBlochSmallNk = 8;
 
 // Term of a three-centre build: NP is one term over all sites; EP term j of
 // potential type t has alpha index j.

@@ -200,42 +200,42 @@ __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
   }
 }
 
-constexpr int kBThreads = 256;              // 8 warps: 2 (k) x 4 (columns)
-// Padded rows: a row of m_s is 136 bank words and a row of ph_s 136 too
-// (34 double2), both 8 mod 32, so the 4 k rows of a fragment read fall on
-// distinct banks in each wavefront.
-constexpr int kBMP = kBC + 4;
+// Tensor-core phase sum over a (pair, BC-column tile, 32 k-points, term):
+// 2 x BC/16 warps, each a 16 k x 16 column tile.  Rows of m_s are BC + 4
+// doubles and rows of ph_s 34 complex values, both 8 mod 32 bank words, so
+// the 4 k rows of a fragment read fall on distinct banks in each wavefront.
 constexpr int kBKP = kBK + 2;
-constexpr int kBPhLoads = kBU * kBK / kBThreads;
-constexpr int kBMLoads = kBU * kBC / kBThreads;
 
-__global__ void __launch_bounds__(kBThreads, 4)
+template <int BC>
+__global__ void __launch_bounds__(4 * BC, 256 / BC)
     k_bloch(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
             double2 *cc) {
+  constexpr int T = 4 * BC, NWC = BC / 16;
+  constexpr int PH = (kBU * kBK + T - 1) / T, ML = kBU * BC / T;
   __shared__ double2 ph_s[kBU][kBKP];
-  __shared__ double m_s[kBU][kBMP];
-  const int2 bt = w.btile[blockIdx.x];
+  __shared__ double m_s[kBU][BC + 4];
+  const int2 bt = w.btile_w[blockIdx.x];
   const DPair p = w.pairs[bt.x];
-  const int ne = p.ni * p.nj, c0 = bt.y * kBC;
+  const int ne = p.ni * p.nj, c0 = bt.y * BC;
   const int k0 = blockIdx.y * kBK, term = blockIdx.z, nk = s.nk;
   const int nu = p.uend - p.ubeg;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wk = (warp >> 2) * 16, wc = (warp & 3) * 16;  // warp tile origin
+  const int wk = (warp / NWC) * 16, wc = (warp % NWC) * 16;  // warp tile origin
   const double *Mt = M + (long long)term * w.m_total + p.moff;
   double ar[2][2][2] = {}, ai[2][2][2] = {};
-  double2 rph[kBPhLoads];
-  double rm[kBMLoads];
+  double2 rph[PH];
+  double rm[ML];
   auto fetch = [&](int u0) {
 #pragma unroll
-    for (int q = 0; q < kBPhLoads; ++q) {
-      const int i = tid + q * kBThreads, uu = i / kBK, kk = i % kBK;
-      rph[q] = (u0 + uu < nu && k0 + kk < nk)
+    for (int q = 0; q < PH; ++q) {
+      const int i = tid + q * T, uu = i / kBK, kk = i % kBK;
+      rph[q] = (i < kBU * kBK && u0 + uu < nu && k0 + kk < nk)
                    ? s.phase[(long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk]
                    : make_double2(0.0, 0.0);
     }
 #pragma unroll
-    for (int q = 0; q < kBMLoads; ++q) {
-      const int i = tid + q * kBThreads, uu = i / kBC, cc2 = i % kBC;
+    for (int q = 0; q < ML; ++q) {
+      const int i = tid + q * T, uu = i / BC, cc2 = i % BC;
       rm[q] = (u0 + uu < nu && c0 + cc2 < ne) ? Mt[(long long)(u0 + uu) * ne + c0 + cc2]
                                               : 0.0;
     }
@@ -244,14 +244,14 @@ __global__ void __launch_bounds__(kBThreads, 4)
   for (int u0 = 0; u0 < nu; u0 += kBU) {
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < kBPhLoads; ++q) {
-      const int i = tid + q * kBThreads;
-      ph_s[i / kBK][i % kBK] = rph[q];
+    for (int q = 0; q < PH; ++q) {
+      const int i = tid + q * T;
+      if (i < kBU * kBK) ph_s[i / kBK][i % kBK] = rph[q];
     }
 #pragma unroll
-    for (int q = 0; q < kBMLoads; ++q) {
-      const int i = tid + q * kBThreads;
-      m_s[i / kBC][i % kBC] = rm[q];
+    for (int q = 0; q < ML; ++q) {
+      const int i = tid + q * T;
+      m_s[i / BC][i % BC] = rm[q];
     }
     __syncthreads();
     if (u0 + kBU < nu) fetch(u0 + kBU);
@@ -301,7 +301,6 @@ __global__ void __launch_bounds__(kBThreads, 4)
 // Few k-points (Gamma, 2x2x2): the tensor-core tiles would idle on k, so
 // one thread per block column keeps the nk complex sums in registers and
 // reads each image block once.
-constexpr int kBlochSmallNk = 8;
 
 __global__ void __launch_bounds__(kBC)
     k_bloch_small(DevSys s, DevWork w, const double *M, double2 *vv,
@@ -354,8 +353,21 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
     IMAGO_CUDA(cudaGetLastError());
     return IMAGO_OK;
   }
-  dim3 grid(w.nbtile, (s.nk + kBK - 1) / kBK, nterm);
-  k_bloch<<<grid, kBThreads, 0, st>>>(s, w, M, vv, cv, cc);
+  dim3 grid(w.nbtile_w, (s.nk + kBK - 1) / kBK, nterm);
+  if (w.nbtile_w == 0) return IMAGO_OK;
+  switch (w.bw) {
+    case bloch_width(0):
+      k_bloch<bloch_width(0)><<<grid, 4 * bloch_width(0), 0, st>>>(s, w, M, vv, cv, cc);
+      break;
+    case bloch_width(1):
+      k_bloch<bloch_width(1)><<<grid, 4 * bloch_width(1), 0, st>>>(s, w, M, vv, cv, cc);
+      break;
+    case bloch_width(2):
+      k_bloch<bloch_width(2)><<<grid, 4 * bloch_width(2), 0, st>>>(s, w, M, vv, cv, cc);
+      break;
+    default:
+      return IMAGO_ERR_INVALID;
+  }
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }

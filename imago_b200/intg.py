@@ -83,6 +83,8 @@ def lib():
         L.imago_intg_kernel_stats.restype = ctypes.c_int
         L.imago_intg_destroy.argtypes = [ctypes.c_void_p]
         L.imago_intg_destroy.restype = None
+        L.imago_intg_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
+        L.imago_intg_tuning.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
         L.imago_intg_build_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint,
@@ -309,6 +311,15 @@ class IntegralSetup:
         _check(lib().imago_intg_build_graph(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build_graph")
         return out
+
+    def tuning(self):
+        """The phase-sum column width the context measured fastest and the
+        trial milliseconds of widths 32, 48, 64 (imago_intg_tuning)."""
+        w = ctypes.c_int()
+        ms = np.zeros(3)
+        _check(lib().imago_intg_tuning(self._ctx, ctypes.byref(w), _p(ms)),
+               "imago_intg_tuning")
+        return {"bloch_width": w.value, "trial_ms": [float(x) for x in ms]}
 
     def stage_ms(self):
         ms = np.zeros(4)

@@ -197,6 +197,13 @@ IMAGO_API int imago_intg_kernel_stats(const imago_ctx *ctx, double ms[4],
 
 IMAGO_API void imago_intg_destroy(imago_ctx *ctx);
 
+/* No counterpart in the reference.  The column-tile width (32, 48 or 64
+ * block elements) that the tensor-core phase sum measured fastest on the
+ * context's first build with more than 8 k-points, and the milliseconds of
+ * that trial per width (zeros and width 64 before it has run). */
+IMAGO_API int imago_intg_tuning(const imago_ctx *ctx, int *bloch_width,
+                                double trial_ms[3]);
+
 /* No counterpart in the reference: the same builds as imago_intg_build,
  * replayed from a CUDA graph.  Device outputs only (outputs_on_device), on
  * the context's own stream or a non-default one.  The first call for a

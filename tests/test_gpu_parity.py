@@ -99,6 +99,23 @@ def test_silicon8_2x2x2(imago_lib):
     _assert_all(_compare_builds(configs.silicon_cubic8(kmesh=(2, 2, 2))))
 
 
+def test_silicon8_tensor_phase_sum_all_widths(imago_lib):
+    # 12 k-points: the tensor-core phase sum, whose column width (32, 48 or
+    # 64 of the 324 block elements) is tuned on the first build.  The
+    # tuning trial runs every width and the kept result must match the
+    # oracle; a second context repeats it bit for bit.
+    s = configs.silicon_cubic8(kmesh=(2, 2, 3))
+    _assert_all(_compare_builds(s))
+    with intg.IntegralSetup(s) as g:
+        a = g.build()
+        t = g.tuning()
+    assert t["bloch_width"] in (32, 48, 64) and min(t["trial_ms"]) > 0.0
+    with intg.IntegralSetup(s) as g:
+        b = g.build()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
 def test_overlap_required_first(imago_lib):
     with intg.IntegralSetup(configs.small_test_system()) as g:
         with pytest.raises(intg.ImagoError) as e:
