@@ -33,6 +33,13 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem,
                : "memory");
 }
 
+// 8-byte global-to-shared copy that does not pass through registers.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem)
+               : "memory");
+}
+
 // ---------------------------------------------------------- contract --
 // One CTA per (unit, group of terms), threads over the block elements:
 //   M_t(m1, m2) = sum_{(a,b) in unit} C1(a, m1) C2(b, m2) sh_t,ab(lm1, lm2),
@@ -120,7 +127,9 @@ __global__ void __launch_bounds__(kContractThreads, 4)
       const double *src = bt + chunk_base;
       for (int t = 0; t < tn; ++t)
         for (int i = tid; i < len; i += kContractThreads)
-          bs[t][i] = src[(long long)t * w.blk_total + i];
+          cp_async8(&bs[t][i], src + (long long)t * w.blk_total + i);
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       __syncthreads();
       for (int q = 0; q < cnt; ++q) {
         const int ab = sp_ab[q], cl = sp_cls[q];
