@@ -1004,8 +1004,10 @@ constexpr int kEpCopyChunks = 4;
 int do_ep(imago_ctx *c, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
   const int nterm = c->pot_dim;
+  // the chunk is fixed on a context's first EP build: its scratch is sized
+  // for it, so later builds (and graph captures) reuse it
   int chunk = c->ep_chunk;
-  if (!c->capturing || chunk <= 0) {
+  if (chunk <= 0) {
     size_t budget = c->scratch_bytes;
     if (budget == 0) {
       size_t fr = 0, tot = 0;
