@@ -638,10 +638,12 @@ int build_work(imago_ctx *c) {
     const int bucket = reach > 64.0 ? 0 : reach > 16.0 ? 1 : reach > 4.0 ? 2 : 3;
     key[q] = (sp.la * 4 + sp.lb) * 4 + bucket;
   }
-  std::vector<int> idx(c->sps.size());
-  std::iota(idx.begin(), idx.end(), 0);
-  std::stable_sort(idx.begin(), idx.end(),
-                   [&](int x, int y) { return key[x] < key[y]; });
+  // stable counting sort over the 16 x 4 keys
+  constexpr int kKeys = 16 * 4;
+  std::vector<int> start(kKeys + 1, 0), idx(c->sps.size());
+  for (int k : key) ++start[k + 1];
+  for (int k = 0; k < kKeys; ++k) start[k + 1] += start[k];
+  for (size_t q = 0; q < key.size(); ++q) idx[start[key[q]]++] = (int)q;
   c->sp_by_cls = idx;
   for (int k = 0; k <= 16; ++k) c->cls_beg[k] = 0;
   for (const DSp &sp : c->sps) c->cls_beg[sp.la * 4 + sp.lb + 1] += 1;

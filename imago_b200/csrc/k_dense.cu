@@ -33,6 +33,16 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem,
                : "memory");
 }
 
+// 8-byte copy with zero fill when `valid` is false (nothing is read).
+__device__ __forceinline__ void cp_async8z(void *smem, const void *gmem,
+                                           bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst),
+               "l"(gmem), "r"(n)
+               : "memory");
+}
+
 // 8-byte global-to-shared copy that does not pass through registers.
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
@@ -221,8 +231,9 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
             double2 *cc) {
   constexpr int T = 4 * BC, NWC = BC / 16;
   constexpr int PH = (kBU * kBK + T - 1) / T, ML = kBU * BC / T;
-  __shared__ double2 ph_s[kBU][kBKP];
-  __shared__ double m_s[kBU][BC + 4];
+  // two stages: the next 16 images load (cp.async) during this stage's MMAs
+  __shared__ double2 ph_s[2][kBU][kBKP];
+  __shared__ double m_s[2][kBU][BC + 4];
   const int2 bt = w.btile_w[blockIdx.x];
   const DPair p = w.pairs[bt.x];
   const int ne = p.ni * p.nj, c0 = bt.y * BC;
@@ -232,38 +243,36 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
   const int wk = (warp / NWC) * 16, wc = (warp % NWC) * 16;  // warp tile origin
   const double *Mt = M + (long long)term * w.m_total + p.moff;
   double ar[2][2][2] = {}, ai[2][2][2] = {};
-  double2 rph[PH];
-  double rm[ML];
-  auto fetch = [&](int u0) {
+  auto issue = [&](int u0, int buf) {
 #pragma unroll
     for (int q = 0; q < PH; ++q) {
       const int i = tid + q * T, uu = i / kBK, kk = i % kBK;
-      rph[q] = (i < kBU * kBK && u0 + uu < nu && k0 + kk < nk)
-                   ? s.phase[(long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk]
-                   : make_double2(0.0, 0.0);
+      if (i < kBU * kBK) {
+        const bool in = u0 + uu < nu && k0 + kk < nk;
+        const double2 *src =
+            in ? s.phase + (long long)w.units[p.ubeg + u0 + uu].cell * nk + k0 + kk
+               : s.phase;
+        cp_async16(&ph_s[buf][uu][kk], src, in);
+      }
     }
 #pragma unroll
     for (int q = 0; q < ML; ++q) {
       const int i = tid + q * T, uu = i / BC, cc2 = i % BC;
-      rm[q] = (u0 + uu < nu && c0 + cc2 < ne) ? Mt[(long long)(u0 + uu) * ne + c0 + cc2]
-                                              : 0.0;
+      const bool in = u0 + uu < nu && c0 + cc2 < ne;
+      cp_async8z(&m_s[buf][uu][cc2], in ? Mt + (long long)(u0 + uu) * ne + c0 + cc2 : Mt,
+                 in);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  if (nu > 0) fetch(0);
-  for (int u0 = 0; u0 < nu; u0 += kBU) {
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PH; ++q) {
-      const int i = tid + q * T;
-      if (i < kBU * kBK) ph_s[i / kBK][i % kBK] = rph[q];
-    }
-#pragma unroll
-    for (int q = 0; q < ML; ++q) {
-      const int i = tid + q * T;
-      m_s[i / BC][i % BC] = rm[q];
+  if (nu > 0) issue(0, 0);
+  for (int u0 = 0, buf = 0; u0 < nu; u0 += kBU, buf ^= 1) {
+    if (u0 + kBU < nu) {
+      issue(u0 + kBU, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
     __syncthreads();
-    if (u0 + kBU < nu) fetch(u0 + kBU);
 #pragma unroll
     for (int ks = 0; ks < kBU; ks += 4) {
       const int ku = ks + (lane & 3);
@@ -271,8 +280,8 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
       double2 a[2];
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
-        b[t] = m_s[ku][wc + t * 8 + (lane >> 2)];
-        a[t] = ph_s[ku][wk + t * 8 + (lane >> 2)];
+        b[t] = m_s[buf][ku][wc + t * 8 + (lane >> 2)];
+        a[t] = ph_s[buf][ku][wk + t * 8 + (lane >> 2)];
       }
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
@@ -282,6 +291,7 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
           dmma(ai[mt][nt][0], ai[mt][nt][1], a[mt].y, b[nt]);
         }
     }
+    __syncthreads();  // this stage's buffer is refilled two stages on
   }
   // epilogue: origin shift (kPointLatticeOriginShift, intgSaving.F90:241-292,
   // skipped when |k.L0| < smallThresh) and the scatter
