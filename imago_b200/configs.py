@@ -334,6 +334,22 @@ def small_test_system(seed=7, kmesh=(2, 2, 1)):
     return sys_
 
 
+def no_core_test_system(kmesh=(2, 2, 2)):
+    """Three atoms of a valence-only element (coreDim = 0): the reference
+    packs valeVale without orthogonalisation and without the 1e-10 zeroing
+    (integrals.F90:3657-3676)."""
+    a = 6.5
+    rv = np.array([[a, 0.0, 0.2], [0.4, a * 1.1, 0.0], [0.0, 0.3, a * 0.9]])
+    pos = np.array([[0.2, 0.1, 0.0], [2.3, 1.9, 1.1], [4.4, 0.5, 3.9]])
+    alphas = even_tempered(8, 0.2, 5.0e2)
+    t = _make_type(1, "v1_1", alphas, (8, 8, 5, 0), [],
+                   [(1, 0, 1.3), (2, 1, 1.1), (3, 2, 0.9)])
+    p = _pot(1, "v1_1", 3, 4, 0.2, 1.0e3)
+    k, km = _mesh(kmesh, (0.5, 0.5, 0.5))
+    return _system(rv, [t], [1, 1, 1], pos, [p], [1, 1, 1], k,
+                   title="valence-only test cell", kmesh=km)
+
+
 def f_test_system(kmesh=(2, 1, 1)):
     """Two atoms of one element with s, p, d and f functions, so every class
     up to f-f appears; small enough for the CPU oracle."""

@@ -87,6 +87,12 @@ def test_small_two_element_cell(imago_lib):
     _assert_all(_compare_builds(configs.small_test_system()))
 
 
+def test_no_core_states_packs_plain(imago_lib):
+    s = configs.no_core_test_system()
+    assert s.core_dim == 0
+    _assert_all(_compare_builds(s))
+
+
 def test_f_classes(imago_lib):
     _assert_all(_compare_builds(configs.f_test_system()))
 
