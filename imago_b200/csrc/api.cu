@@ -734,6 +734,8 @@ int upload(imago_ctx *c) {
   std::memcpy(s.rv, c->rv, sizeof s.rv);
   std::memcpy(s.inv, c->inv, sizeof s.inv);
   s.far_lattice = 1.5 * smallest_singular(c->rv) * (1.0 - 1e-6);
+  s.real_k = 1;
+  for (double x : c->kxyz) s.real_k &= x == 0.0;
   s.type_nalpha = c->d_type_nalpha.p; s.type_alpha_off = c->d_type_alpha_off.p;
   s.type_nstates = c->d_type_nstates.p; s.type_nvale = c->d_type_nvale.p;
   s.type_state_off = c->d_type_state_off.p; s.type_basis_off = c->d_type_basis_off.p;

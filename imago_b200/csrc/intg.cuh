@@ -18,6 +18,9 @@ struct DevSys {
   // 1.5 x the smallest singular value of realVectors: every lattice point
   // outside the 3x3x3 block around a rounded point is at least this far
   double far_lattice;
+  // every k-point is Gamma: all phases are exactly 1, every matrix is real,
+  // and the orthogonalisation runs on the real parts only
+  int real_k;
   // atom types
   const int *type_nalpha, *type_alpha_off, *type_nstates, *type_nvale,
       *type_state_off, *type_basis_off, *type_screen;

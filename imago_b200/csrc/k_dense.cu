@@ -419,7 +419,7 @@ struct OStage {
 //   CONJ:  re = t1 + t2, im = t3 - t1 + t2
 //   plain: re = t1 - t2, im = t3 - t1 - t2.
 // Warp w owns rows 16*(w/2).. and columns 16*(w%2)..
-template <bool CONJ>
+template <bool CONJ, bool REAL>
 __device__ __forceinline__ void ostage_mma(const OStage &st, double t1[2][2][2],
                                            double t2[2][2][2], double t3[2][2][2],
                                            int lane, int warp) {
@@ -441,6 +441,7 @@ __device__ __forceinline__ void ostage_mma(const OStage &st, double t1[2][2][2],
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
         dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        if (REAL) continue;  // imaginary parts are zero: t2 = 0, t3 = t1
         dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
         dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
       }
@@ -448,14 +449,16 @@ __device__ __forceinline__ void ostage_mma(const OStage &st, double t1[2][2][2],
 }
 
 // Complex tile entry from the three 3M sums.
-template <bool CONJ>
+template <bool CONJ, bool REAL>
 __device__ __forceinline__ double2 ocombine(double t1, double t2, double t3) {
+  if (REAL) return make_double2(t1, 0.0);
   return CONJ ? make_double2(t1 + t2, t3 - t1 + t2)
               : make_double2(t1 - t2, t3 - t1 - t2);
 }
 
 // Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v).  Operands are staged
 // through registers one K stage ahead of the MMAs.
+template <bool REAL>
 __global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
               const double2 *s_cv, double2 *y) {
@@ -498,7 +501,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
     store();
     __syncthreads();
     if (l0 + kOK < C) fetch(l0 + kOK);
-    ostage_mma<false>(st, t1, t2, t3, lane, warp);
+    ostage_mma<false, REAL>(st, t1, t2, t3, lane, warp);
   }
   const double2 *X = cv + tk * V * C;
   double2 *Y = y + tk * V * C;
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
         const int v = tc * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
         if (c >= C || v >= V) continue;
         const double2 x = X[(long long)v * C + c];
-        const double2 p = ocombine<false>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+        const double2 p = ocombine<false, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
         Y[(long long)v * C + c] = make_double2(x.x - 0.5 * p.x, x.y - 0.5 * p.y);
       }
 }
@@ -521,6 +524,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
 // Upper tiles (J <= I) of W = S^H Y + Y^H S as one K loop over the stacked
 // core index (S;Y)^H (Y;S), then VV'(j, i) = VV(j, i) - W(j, i) packed at
 // i(i+1)/2 + j.
+template <bool REAL>
 __global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_w(DevSys s, const double2 *vv, const double2 *y,
               const double2 *s_cv, double *packed) {
@@ -577,7 +581,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
     store();
     __syncthreads();
     if (l0 + kOK < K2) fetch(l0 + kOK);
-    if (!lower) ostage_mma<true>(st, t1, t2, t3, lane, warp);
+    if (!lower) ostage_mma<true, REAL>(st, t1, t2, t3, lane, warp);
   }
   const double2 *VVt = vv + tk * V * V;
   const long long np = (long long)V * (V + 1) / 2;
@@ -593,7 +597,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
         const int col = I * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
         if (row >= V || col >= V || row > col) continue;
         double2 v = VVt[(long long)col * V + row];
-        const double2 p = ocombine<true>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+        const double2 p = ocombine<true, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
         v.x -= p.x;
         v.y -= p.y;
         if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
@@ -638,7 +642,7 @@ inline size_t fused_smem(int C, int V) {
 
 // One warp's 16x16 complex subtile of op(A)^T B over k in [k0, k0 + nk4)
 // from k-major shared arrays (row strides lda, ldb), 3M form.
-template <bool CONJ>
+template <bool CONJ, bool REAL>
 __device__ __forceinline__ void fused_tile(const double2 *A, int lda, int r0,
                                            const double2 *B, int ldb, int c0,
                                            int nk4, bool skip_lower,
@@ -661,12 +665,14 @@ __device__ __forceinline__ void fused_tile(const double2 *A, int lda, int r0,
       for (int nt = 0; nt < 2; ++nt) {
         if (skip_lower && mt > nt) continue;  // rows 8..15 x cols 0..7
         dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        if (REAL) continue;  // imaginary parts are zero: t2 = 0, t3 = t1
         dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
         dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
       }
   }
 }
 
+template <bool REAL>
 __global__ void __launch_bounds__(kFThreads, 1)
     k_ortho_fused(DevSys s, const double2 *vv, const double2 *cv,
                   const double2 *cc, const double2 *s_cv, double *packed) {
@@ -703,7 +709,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
   for (int tile = warp; tile < ny; tile += kFWarps) {
     const int r0 = (tile % yr) * 16, c0 = (tile / yr) * 16;
     double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
-    fused_tile<false>(Xs, d.Cp, r0, Ss, d.Vp, c0, d.C4, false, t1, t2, t3, lane);
+    fused_tile<false, REAL>(Xs, d.Cp, r0, Ss, d.Vp, c0, d.C4, false, t1, t2, t3, lane);
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -713,7 +719,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
           const int c = r0 + 8 * mt + (lane >> 2);
           const int v = c0 + 8 * nt + 2 * (lane & 3) + i;
           if (c >= C || v >= V) continue;
-          const double2 p = ocombine<false>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+          const double2 p = ocombine<false, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
           double2 &y = Ys[c * d.Vp + v];
           y.x -= 0.5 * p.x;
           y.y -= 0.5 * p.y;
@@ -747,8 +753,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
                                : make_double2(0.0, 0.0);
         }
     double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
-    fused_tile<true>(Ss, d.Vp, r0, Ys, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
-    fused_tile<true>(Ys, d.Vp, r0, Ss, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
+    fused_tile<true, REAL>(Ss, d.Vp, r0, Ys, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
+    fused_tile<true, REAL>(Ys, d.Vp, r0, Ss, d.Vp, c0, d.C4, J == I, t1, t2, t3, lane);
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -759,7 +765,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
           const int col = c0 + 8 * nt + 2 * (lane & 3) + i;
           if (row >= V || col >= V || row > col) continue;
           double2 v = vvp[mt][nt][i];
-          const double2 p = ocombine<true>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
+          const double2 p = ocombine<true, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
           v.x -= p.x;
           v.y -= p.y;
           if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
@@ -807,26 +813,34 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
   }
   const size_t smem = fused_smem(C, V);
   if (smem <= kFusedMaxSmem) {
-    static bool attr_set[64] = {};
+    static bool attr_set[2][64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-      IMAGO_CUDA(cudaFuncSetAttribute(k_ortho_fused,
+    if (dev >= 0 && dev < 64 && !attr_set[s.real_k][dev]) {
+      IMAGO_CUDA(cudaFuncSetAttribute(s.real_k ? k_ortho_fused<true> : k_ortho_fused<false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kFusedMaxSmem));
-      attr_set[dev] = true;
+      attr_set[s.real_k][dev] = true;
     }
-    k_ortho_fused<<<dim3(s.nk, nterm), kFThreads, smem, st>>>(s, vv, cv, cc, s_cv,
-                                                              packed);
+    if (s.real_k)
+      k_ortho_fused<true><<<dim3(s.nk, nterm), kFThreads, smem, st>>>(s, vv, cv, cc,
+                                                                     s_cv, packed);
+    else
+      k_ortho_fused<false><<<dim3(s.nk, nterm), kFThreads, smem, st>>>(s, vv, cv, cc,
+                                                                      s_cv, packed);
     IMAGO_CUDA(cudaGetLastError());
     return IMAGO_OK;
   }
   const int tcv = (C + kOT - 1) / kOT, tvv = (V + kOT - 1) / kOT;
   dim3 gy(tcv * tvv, s.nk, nterm);
-  k_ortho_y<<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
-  IMAGO_CUDA(cudaGetLastError());
   dim3 gw(tvv * (tvv + 1) / 2, s.nk, nterm);
-  k_ortho_w<<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
+  if (s.real_k) {
+    k_ortho_y<true><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
+    k_ortho_w<true><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
+  } else {
+    k_ortho_y<false><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
+    k_ortho_w<false><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
+  }
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
