@@ -1005,8 +1005,10 @@ int do_simple(imago_ctx *c, Kind kind, double *packed) {
 // one chunk's matrices overlaps building the next.
 constexpr int kEpCopyChunks = 4;
 
-int do_ep(imago_ctx *c, double *packed) {
+// EP terms [first, first + count); `packed` holds their matrices in order.
+int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  if (count < 0) count = c->pot_dim - first;
   const int nterm = c->pot_dim;
   // the chunk is fixed on a context's first EP build: its scratch is sized
   // for it, so later builds (and graph captures) reuse it
@@ -1026,10 +1028,10 @@ int do_ep(imago_ctx *c, double *packed) {
     c->ep_chunk = chunk;
   }
   const size_t npd = packed_doubles(c);
-  for (int t0 = 0; t0 < nterm; t0 += chunk) {
-    const int n = std::min(chunk, nterm - t0);
+  for (int t0 = first; t0 < first + count; t0 += chunk) {
+    const int n = std::min(chunk, first + count - t0);
     int rc = IMAGO_OK;
-    double *user = packed ? packed + npd * t0 : nullptr;
+    double *user = packed ? packed + npd * (t0 - first) : nullptr;
     double *tgt = packed_target(c, user, SLOT_EP + t0);
     if ((rc = run_build(c, KIND_EP, t0, n, tgt))) return rc;
     if (tgt != user && (rc = copy_out(c, user, tgt, npd * n))) return rc;
@@ -1222,6 +1224,21 @@ int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
   if ((rc = begin_call(c))) return finish(c, rc);
   cudaEventRecord(c->ev[6], c->stream);
   rc = do_ep(c, packed);
+  cudaEventRecord(c->ev[7], c->stream);
+  rc = finish(c, rc);
+  if (!rc) cudaEventElapsedTime(&c->stage_ms[3], c->ev[6], c->ev[7]);
+  return rc;
+}
+
+int imago_elec_pot_gauss_overlap_range(imago_ctx *c, int first, int count,
+                                       double *packed) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (first < 0 || count < 0 || first + count > c->pot_dim) return IMAGO_ERR_RANGE;
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = begin_call(c))) return finish(c, rc);
+  cudaEventRecord(c->ev[6], c->stream);
+  if (count > 0) rc = do_ep(c, packed, first, count);
   cudaEventRecord(c->ev[7], c->stream);
   rc = finish(c, rc);
   if (!rc) cudaEventElapsedTime(&c->stage_ms[3], c->ev[6], c->ev[7]);

@@ -73,6 +73,9 @@ def lib():
                   "imago_elec_pot_gauss_overlap"):
             getattr(L, n).argtypes = [ctypes.c_void_p, _D]
             getattr(L, n).restype = ctypes.c_int
+        L.imago_elec_pot_gauss_overlap_range.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                                         ctypes.c_int, _D]
+        L.imago_elec_pot_gauss_overlap_range.restype = ctypes.c_int
         L.imago_intg_build.argtypes = [ctypes.c_void_p, ctypes.c_uint,
                                        ctypes.POINTER(ImagoOutC)]
         L.imago_intg_build.restype = ctypes.c_int
@@ -277,6 +280,18 @@ class IntegralSetup:
         out = self._packed(self.pot_dim)
         _check(lib().imago_elec_pot_gauss_overlap(self._ctx, _p(out)),
                "elecPotGaussOverlap")
+        return out
+
+    def elec_pot_gauss_overlap_range(self, first, count, out=None):
+        """EP terms first .. first+count-1 (imago_elec_pot_gauss_overlap_range);
+        `out` a device pointer/tensor for outputs_on_device contexts."""
+        if out is None:
+            out = self._packed(count)
+        ptr = (ctypes.cast(ctypes.c_void_p(out), _D) if isinstance(out, int) else
+               ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D) if hasattr(out, "data_ptr")
+               else _p(out))
+        _check(lib().imago_elec_pot_gauss_overlap_range(self._ctx, first, count, ptr),
+               "elecPotGaussOverlap terms")
         return out
 
     # -- all matrices in one call --

@@ -180,6 +180,13 @@ IMAGO_API int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
  * (integrals.F90:1946-2531, 2700-2858). */
 IMAGO_API int imago_elec_pot_gauss_overlap(imago_ctx *ctx, double *packed);
 
+/* EP terms first .. first + count - 1 only (same order and layout, `packed`
+ * holding `count` matrices): the elecPotGaussOverlap loop over a sub-range
+ * of its terms, for spreading the terms over several GPUs or calls.  No
+ * separate counterpart in the reference. */
+IMAGO_API int imago_elec_pot_gauss_overlap_range(imago_ctx *ctx, int first,
+                                                 int count, double *packed);
+
 /* All matrices selected by `which` (IMAGO_OL|IMAGO_KE|IMAGO_NP|IMAGO_EP)
  * in one call; OL runs first. */
 IMAGO_API int imago_intg_build(imago_ctx *ctx, unsigned which, const imago_out *out);

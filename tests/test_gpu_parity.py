@@ -291,3 +291,44 @@ def test_batch_matches_single_cells(imago_lib):
            "EP0": packed_mismatch(outs[1]["ep_packed"][0].cpu().numpy(),
                                   ob.elec_pot(0, 1)[0])}
     _assert_all(res)
+
+
+def test_ep_term_range_matches_full_build(imago_lib):
+    s = configs.small_test_system()
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        full = g.elec_pot_gauss_overlap()
+        part = g.elec_pot_gauss_overlap_range(2, 3)
+        assert np.array_equal(full[2:5], part)
+        with pytest.raises(intg.ImagoError) as e:
+            g.elec_pot_gauss_overlap_range(g.pot_dim - 1, 2)
+        assert e.value.status == 8
+
+
+def test_sharded_build_on_one_rank_matches_plain_build(imago_lib):
+    # imago_b200.shard with a single rank: the overlap, then KE, NP and the
+    # EP terms through their own calls, gathered in the reference's order.
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    from imago_b200 import shard
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+        with intg.IntegralSetup(s, outputs_on_device=True) as g:
+            ref = _device_outputs(torch, _shapes(g))
+            g.build(out=ref)
+            got = shard.ShardedBuild.from_setup(g).build()
+            torch.cuda.synchronize()
+        assert _same(ref["ol_packed"], got["ol"]["ol_packed"])
+        assert _same(ref["ke_packed"], got["ke"])
+        assert _same(ref["np_packed"], got["np"])
+        assert _same(ref["ep_packed"], got["ep"])
+    finally:
+        dist.destroy_process_group()
