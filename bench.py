@@ -500,6 +500,66 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
+def run_sharded(args):
+    """--shard terms: one system's build spread over the ranks
+    (imago_b200.shard): every rank builds the overlap and its block of the
+    KE, NP and EP matrices, then one gather brings all of them to rank 0.
+    Strong scaling: the work of the whole job is fixed."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from imago_b200 import intg, shard
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29517")
+    dist.init_process_group("nccl" if world > 1 else "gloo",
+                            timeout=datetime.timedelta(seconds=120))
+    wl = WORKLOADS[args.workload]
+    system = system_for(args.workload, 0, args.kmesh)  # the same cell everywhere
+    stream = torch.cuda.Stream(device=local)
+    g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
+                           stream=stream.cuda_stream)
+    sb = shard.ShardedBuild.from_setup(g)
+    for _ in range(args.warmup):
+        sb.build()
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    step_s = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            with torch.cuda.stream(stream):
+                sb.build()
+            e.record(stream)
+            e.synchronize()
+            step_s.append(s.elapsed_time(e) / 1e3)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([float(np.sum(step_s))], dtype=torch.float64,
+                     device=torch.device("cuda", local) if world > 1 else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = float(t.item()) / args.steps
+    if rank == 0:
+        line = {
+            "metric": wl["metric"], "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded jitter, synthesised contraction coefficients)",
+            "config": {"workload": wl["desc"], "parallelism": f"terms{world}",
+                       "shard": "overlap on every rank, KE/NP/EP matrices in "
+                                "contiguous blocks per rank, one gather to rank 0",
+                       "parts": shard.partition(g.pot_dim, world)},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    dist.destroy_process_group()
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -619,6 +679,10 @@ def main():
     ap.add_argument("--scratch-mb", type=int, default=0,
                     help="device scratch budget of the EP chunks (0: a quarter "
                          "of free memory); small budgets are for profiling")
+    ap.add_argument("--shard", default="none", choices=["none", "terms"],
+                    help="under torchrun: 'none' builds an independent cell per "
+                         "rank (weak scaling); 'terms' spreads one cell's "
+                         "matrices over the ranks (strong scaling)")
     ap.add_argument("--no-silica", action="store_true",
                     help="skip the 162-atom quartz report of the default run")
     args = ap.parse_args()
@@ -626,6 +690,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch64":
         run_batch(args)
+    elif args.shard == "terms":
+        run_sharded(args)
     else:
         run_ours(args)
 
