@@ -513,7 +513,8 @@ def run_sharded(args):
     torch.cuda.set_device(local)
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
     os.environ.setdefault("MASTER_PORT", "29517")
-    dist.init_process_group("nccl" if world > 1 else "gloo",
+    dist.init_process_group("nccl" if world > 1 else "gloo", rank=rank,
+                            world_size=world,
                             timeout=datetime.timedelta(seconds=120))
     wl = WORKLOADS[args.workload]
     system = system_for(args.workload, 0, args.kmesh)  # the same cell everywhere
