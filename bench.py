@@ -160,6 +160,14 @@ def algorithmic_flops(g):
     return {"bloch": bloch, "ortho": ortho}
 
 
+# DRAM bytes (read + write) per (k-point, matrix) of the fused
+# orthogonalisation, from one ncu capture of its Si8 4x4x4 EP launch: 243.66 MB
+# read and 83.76 MB written for 64 k x 20 terms.  The kernel's traffic grows
+# in proportion to the (k, matrix) pairs, so the build's figure is this times
+# nk x (3 + potDim).
+ORTHO_FUSED_BYTES_PER_KMAT = (243.658496e6 + 83.760128e6) / 1280
+
+
 def fp64_peak_tflops(torch):
     """Measured FP64 dense throughput of this GPU (cuBLAS DGEMM 8192^3)."""
     n = 8192
@@ -614,8 +622,12 @@ def run_ours(args):
     roofline = None
     if top_name in flops and fp64:
         achieved = flops[top_name] / (kms[top] / 1e3) / 1e12
+        traffic = None
+        if top_name == "ortho" and args.workload == "si8":
+            traffic = ORTHO_FUSED_BYTES_PER_KMAT * nk * (3 + P)
         roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64,
-                    "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": traffic,
+                    "traffic_unit": "bytes per build (ncu, scaled by (k, matrix) pairs)",
                     "kernel": top_name,
                     "peak_source": "measured cuBLAS DGEMM 8192^3 in this run "
                                    "(MEASURED_PEAKS.json has no FP64 figure)"}

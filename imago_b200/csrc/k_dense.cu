@@ -22,6 +22,17 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a,
       : "d"(a), "d"(b));
 }
 
+// One packed (re, im) element: a single 16-byte store when the caller's
+// buffer allows it (device allocations do), two 8-byte stores otherwise.
+__device__ __forceinline__ void store_packed(double *out, long long idx, double2 v) {
+  if (((size_t)out & 15) == 0)
+    reinterpret_cast<double2 *>(out)[idx] = v;
+  else {
+    out[2 * idx] = v.x;
+    out[2 * idx + 1] = v.y;
+  }
+}
+
 // 16-byte global-to-shared copy that does not pass through registers;
 // with `valid` false nothing is read and the destination is zero-filled.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem,
@@ -604,8 +615,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
         if (fabs(v.x) < kPackThresh) v.x = 0.0;
         if (fabs(v.y) < kPackThresh) v.y = 0.0;
         const long long idx = (long long)col * (col + 1) / 2 + row;
-        out[2 * idx] = v.x;
-        out[2 * idx + 1] = v.y;
+        store_packed(out, idx, v);
       }
 }
 
@@ -772,8 +782,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
           if (fabs(v.x) < kPackThresh) v.x = 0.0;
           if (fabs(v.y) < kPackThresh) v.y = 0.0;
           const long long idx = (long long)col * (col + 1) / 2 + row;
-          out[2 * idx] = v.x;
-          out[2 * idx + 1] = v.y;
+          store_packed(out, idx, v);
         }
   }
 }
@@ -794,8 +803,7 @@ __global__ void __launch_bounds__(256)
     while ((long long)(col + 1) * (col + 2) / 2 <= idx) ++col;
     const int row = (int)(idx - (long long)col * (col + 1) / 2);
     const double2 v = VVt[(long long)col * V + row];
-    out[2 * idx] = v.x;
-    out[2 * idx + 1] = v.y;
+    store_packed(out, idx, v);
   }
 }
 
