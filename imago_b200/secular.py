@@ -1,0 +1,59 @@
+"""The secular equation of one SCF step, on the GPU, from the integral
+builds (secularEqnSCF, src/imago/secularEqn.F90:37-330).
+
+    eigenvalues = secular_eigenvalues(out, pot_coeffs)
+
+`out` holds the device-resident packed matrices of an IntegralSetup build
+(np_packed, ke_packed, ep_packed, ol_packed as CUDA tensors); pot_coeffs are
+the potDim coefficients of the current SCF potential (potCoeffs in the
+reference).  H and S are assembled and unpacked on the device by
+imago_secular_matrices, then the generalised Hermitian problem
+H c = E S c, which the reference hands to LAPACK zhegv(1, 'V', 'U')
+(interfaces.F90:73-120), is reduced by the Cholesky factor of S and solved
+by cuSOLVER through torch.linalg.  Eigenvalues come back ascending per
+k-point, in Hartree.
+"""
+
+import ctypes
+
+import torch
+
+from . import intg
+
+
+def secular_matrices(out, pot_coeffs, stream=None):
+    """Full Hermitian H and S [nk, V, V] (complex128, CUDA) for every k."""
+    npk = out["np_packed"]
+    nk, npacked = npk.shape[0], npk.shape[1]
+    V = int((int((8 * npacked + 1) ** 0.5) - 1) // 2)
+    if V * (V + 1) // 2 != npacked:
+        raise ValueError("packed length is not V(V+1)/2")
+    ep = out.get("ep_packed")
+    P = 0 if ep is None else ep.shape[0]
+    w = torch.as_tensor(pot_coeffs, dtype=torch.float64, device=npk.device).contiguous()
+    if w.numel() != P:
+        raise ValueError(f"{w.numel()} coefficients for {P} potential terms")
+    h = torch.empty((nk, V, V), dtype=torch.complex128, device=npk.device)
+    s = torch.empty_like(h)
+    L = intg.lib()
+    L.imago_secular_matrices.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 8
+    L.imago_secular_matrices.restype = ctypes.c_int
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    rc = L.imago_secular_matrices(
+        V, nk, P, npk.data_ptr(), out["ke_packed"].data_ptr(),
+        ep.data_ptr() if P else None, w.data_ptr() if P else None,
+        out["ol_packed"].data_ptr(), h.data_ptr(), s.data_ptr(), st)
+    if rc:
+        raise intg.ImagoError(rc, "imago_secular_matrices")
+    # stored [k][col][row]: the matrix is the transpose of each slice
+    return h.transpose(-2, -1), s.transpose(-2, -1)
+
+
+def secular_eigenvalues(out, pot_coeffs, num_states=None):
+    """Eigenvalues of H c = E S c per k-point, ascending, [nk, num_states]."""
+    h, s = secular_matrices(out, pot_coeffs)
+    lo = torch.linalg.cholesky(s)
+    y = torch.linalg.solve_triangular(lo, h, upper=False)          # L^-1 H
+    a = torch.linalg.solve_triangular(lo, y.mH, upper=False)       # L^-1 H L^-H
+    ev = torch.linalg.eigvalsh(a)
+    return ev if num_states is None else ev[:, :num_states]

@@ -243,6 +243,24 @@ IMAGO_API int imago_batch_build(imago_batch *batch, unsigned which,
 IMAGO_API int imago_batch_launches(const imago_batch *batch, long long *launches);
 IMAGO_API void imago_batch_destroy(imago_batch *batch);
 
+/*
+ * The matrices of the secular equation of one SCF step (secularEqnSCF,
+ * secularEqn.F90:135-186), from device-resident packed builds: for every
+ * k-point H = NP + KE + sum_j w_j EP_j accumulated in that order with the
+ * reference's factor rule (readPackedMatrixAccum, matrixSubs.F90:339-375: a
+ * factor of exactly 0.0 adds the matrix unscaled), and S = OL, unpacked as
+ * unpackMatrix does (matrixSubs.F90:405-433) into full Hermitian matrices
+ * h_full, s_full [k][col][row] of (re, im) (both triangles written).  All
+ * pointers are device memory; pot_coeffs holds pot_dim factors.
+ */
+IMAGO_API int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
+                                     const double *np_packed,
+                                     const double *ke_packed,
+                                     const double *ep_packed,
+                                     const double *pot_coeffs,
+                                     const double *ol_packed, double *h_full,
+                                     double *s_full, void *stream);
+
 /* No counterpart in the reference.  Device scratch of every context comes
  * from one stream-ordered memory pool per device that keeps freed memory
  * for the next context; this hands the pool's unused memory on `device`

@@ -193,3 +193,33 @@ class OracleBuild:
         o = np.zeros(3)
         lib().orc_find_lattice_vector(self._ctx, _p(v), _p(o))
         return o
+
+
+def secular_eigenvalues(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed):
+    """The secular equation of one SCF step on the CPU, as secularEqnSCF
+    (secularEqn.F90:135-186) does it: H = NP + KE + sum_j w_j EP_j in that
+    order with readPackedMatrixAccum's rule (a factor of exactly 0.0 adds
+    the matrix unscaled, matrixSubs.F90:369-373), upper triangles unpacked
+    (matrixSubs.F90:405-433), then LAPACK's generalised Hermitian solver
+    (scipy.linalg.eigh(H, S), the problem of zhegv(1, 'V', 'U')).
+    Returns [nk, V] eigenvalues, ascending."""
+    import scipy.linalg
+    nk, npk = np_packed.shape[0], np_packed.shape[1]
+    V = int((int((8 * npk + 1) ** 0.5) - 1) // 2)
+    iu = np.triu_indices(V)
+    # packed index of (row, col), row <= col: col (col + 1) / 2 + row
+    pidx = iu[1] * (iu[1] + 1) // 2 + iu[0]
+    out = np.zeros((nk, V))
+    for k in range(nk):
+        hp = np_packed[k, :, 0] + 1j * np_packed[k, :, 1]
+        hp = hp + (ke_packed[k, :, 0] + 1j * ke_packed[k, :, 1])
+        for j, w in enumerate(pot_coeffs):
+            f = 1.0 if w == 0.0 else w
+            hp = hp + (ep_packed[j, k, :, 0] + 1j * ep_packed[j, k, :, 1]) * f
+        sp = ol_packed[k, :, 0] + 1j * ol_packed[k, :, 1]
+        H = np.zeros((V, V), complex)
+        S = np.zeros((V, V), complex)
+        H[iu] = hp[pidx]
+        S[iu] = sp[pidx]
+        out[k] = scipy.linalg.eigh(H, S, lower=False, eigvals_only=True)
+    return out
