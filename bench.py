@@ -362,6 +362,27 @@ def time_e2e(system, local, stream, bufs, steps, torch):
             "stat": f"median of {len(tot)} runs (mean {np.mean(tot):.4f} s)"}
 
 
+def time_secular(bufs, pot_dim, stream, torch, steps=3):
+    """Device seconds of one SCF step's secular equation from the resident
+    builds: H and S assembled for every k and the generalised eigenvalues
+    (imago_b200.secular), with synthetic potential coefficients."""
+    from imago_b200 import secular
+    w = -0.5 * np.ones(pot_dim)
+    out = {k: bufs[k] for k in ("np_packed", "ke_packed", "ep_packed", "ol_packed")}
+    with torch.cuda.stream(stream):
+        secular.secular_eigenvalues(out, w)
+        ts = []
+        for _ in range(steps):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            secular.secular_eigenvalues(out, w)
+            e.record(stream)
+            e.synchronize()
+            ts.append(s.elapsed_time(e) / 1e3)
+    return float(np.median(ts))
+
+
 def silica_headline(args, local, stream, torch):
     """The 162-atom alpha-quartz build at Gamma (device time, end to end
     and the oracle on the host cores), reported beside the main line."""
@@ -613,6 +634,7 @@ def run_ours(args):
     kms /= args.steps
 
     tuning = g.tuning()
+    secular_s = time_secular(bufs, P, stream, torch)
     e2e = time_e2e(system, local, stream, bufs, 5, torch)
 
     flops = algorithmic_flops(g)
@@ -658,6 +680,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "tuning": tuning,
+            "secular_step_s": secular_s,
         }
         if args.workload == "si8" and list(args.kmesh) != [8, 8, 8]:
             line["note"] = (f"k-mesh {args.kmesh} (profiling case, not the "
