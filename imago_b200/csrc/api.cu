@@ -15,7 +15,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <numeric>
 #include <vector>
 
@@ -535,88 +537,167 @@ int read_system(imago_ctx *c, const imago_system *s) {
 }
 
 // The pair / image / alpha-pair screens of integrals.F90:323-569.
+// Work lists of a contiguous range of atom pairs, with indices and offsets
+// local to the range; build_work joins the ranges in order.
+struct PairWork {
+  std::vector<DPair> pairs;
+  std::vector<DUnit> units;
+  std::vector<DSp> sps;
+  long long moff = 0, boff = 0;
+  int rc = IMAGO_OK;
+};
+
+void build_pairs(const imago_ctx *c, const std::vector<int2> &ij, size_t lo,
+                 size_t hi, PairWork &w) {
+  for (size_t q = lo; q < hi && w.rc == IMAGO_OK; ++q) {
+    const int i = ij[q].x, j = ij[q].y;
+    DPair p{};
+    p.i = i;
+    p.j = j;
+    p.ti = c->site_type[i];
+    p.tj = c->site_type[j];
+    const HType &t1 = c->types[p.ti], &t2 = c->types[p.tj];
+    const HType &s1 = c->types[c->type_screen[p.ti]];
+    const HType &s2 = c->types[c->type_screen[p.tj]];
+    p.ni = t1.nstates;
+    p.nj = t2.nstates;
+    const double *A = &c->site_pos[3 * i], *B = &c->site_pos[3 * j];
+    double dv[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
+    nearest_lattice_host(c, dv, p.L0);
+    double r02 = 0.0;
+    for (int x = 0; x < 3; ++x)
+      r02 += (A[x] - B[x] - p.L0[x]) * (A[x] - B[x] - p.L0[x]);
+    auto adist = [&](int a, int b) {
+      const double x1 = s1.alphas[a], x2 = s2.alphas[b];
+      return c->T / x2 / (x1 / (x1 + x2));
+    };
+    const double lim = adist(0, 0);
+    p.ubeg = (int)w.units.size();
+    p.moff = w.moff;
+    if (r02 <= lim) {
+      const double maxr = r02 + lim + 2.0 * std::sqrt(r02 * lim);
+      if (maxr > c->csize[c->ncell - 1]) {
+        w.rc = IMAGO_ERR_CELL_LIST;
+        return;
+      }
+      for (int k = 0; k < c->ncell; ++k) {
+        if (c->csize[k] > maxr) break;
+        double r2 = 0.0;
+        for (int x = 0; x < 3; ++x) {
+          const double bp = B[x] + p.L0[x] + c->cells[3 * k + x];
+          r2 += (A[x] - bp) * (A[x] - bp);
+        }
+        if (r2 > lim) continue;
+        DUnit u{};
+        u.pair = (int)w.pairs.size();
+        u.cell = k;
+        u.r2 = r2;
+        u.spbeg = (int)w.sps.size();
+        const int nmin = std::min(t1.nalpha, t2.nalpha);
+        for (int l = 0; l < nmin; ++l) {
+          int mode = 0, a = l, b = l;
+          if (adist(l, l) < r2) break;
+          for (;;) {
+            if (mode == 1) {
+              ++a;
+              if (a >= t1.nalpha) { mode = 2; a = l; continue; }
+            } else if (mode == 2) {
+              ++b;
+              if (b >= t2.nalpha) break;
+            }
+            if (adist(a, b) < r2) {
+              if (mode == 1) { mode = 2; a = l; continue; }
+              break;
+            }
+            if (mode == 0) mode = 1;
+            DSp sp{};
+            sp.unit = (int)w.units.size();
+            sp.a = (short)a;
+            sp.b = (short)b;
+            sp.la = (short)t1.cls[a];
+            sp.lb = (short)t2.cls[b];
+            sp.boff = w.boff;
+            w.boff += nsh(sp.la) * nsh(sp.lb);
+            w.sps.push_back(sp);
+          }
+        }
+        u.spend = (int)w.sps.size();
+        w.units.push_back(u);
+      }
+    }
+    p.uend = (int)w.units.size();
+    w.moff += (long long)(p.uend - p.ubeg) * p.ni * p.nj;
+    w.pairs.push_back(p);
+  }
+}
+
+// Runs f(lo, hi) over [0, n) in chunks on up to hardware_concurrency
+// threads (one thread for small n).
+template <class F>
+void parallel_ranges(size_t n, size_t nchunk, F f) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (n < 512 || hw == 1) {
+    for (size_t c = 0; c < nchunk; ++c) f(c, n * c / nchunk, n * (c + 1) / nchunk);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < hw; ++t)
+    th.emplace_back([&] {
+      for (size_t c; (c = next.fetch_add(1)) < nchunk;)
+        f(c, n * c / nchunk, n * (c + 1) / nchunk);
+    });
+  for (auto &x : th) x.join();
+}
+
 int build_work(imago_ctx *c) {
   c->pairs.clear();
   c->units.clear();
   c->sps.clear();
-  long long moff = 0, boff = 0;
+  // atom pairs i <= j, i-major as the reference loops them
+  std::vector<int2> ij;
+  ij.reserve((size_t)c->ns * (c->ns + 1) / 2);
   for (int i = 0; i < c->ns; ++i)
-    for (int j = i; j < c->ns; ++j) {
-      DPair p{};
-      p.i = i;
-      p.j = j;
-      p.ti = c->site_type[i];
-      p.tj = c->site_type[j];
-      const HType &t1 = c->types[p.ti], &t2 = c->types[p.tj];
-      const HType &s1 = c->types[c->type_screen[p.ti]];
-      const HType &s2 = c->types[c->type_screen[p.tj]];
-      p.ni = t1.nstates;
-      p.nj = t2.nstates;
-      const double *A = &c->site_pos[3 * i], *B = &c->site_pos[3 * j];
-      double dv[3] = {A[0] - B[0], A[1] - B[1], A[2] - B[2]};
-      nearest_lattice_host(c, dv, p.L0);
-      double r02 = 0.0;
-      for (int x = 0; x < 3; ++x)
-        r02 += (A[x] - B[x] - p.L0[x]) * (A[x] - B[x] - p.L0[x]);
-      auto adist = [&](int a, int b) {
-        const double x1 = s1.alphas[a], x2 = s2.alphas[b];
-        return c->T / x2 / (x1 / (x1 + x2));
-      };
-      const double lim = adist(0, 0);
-      p.ubeg = (int)c->units.size();
-      p.moff = moff;
-      if (r02 <= lim) {
-        const double maxr = r02 + lim + 2.0 * std::sqrt(r02 * lim);
-        if (maxr > c->csize[c->ncell - 1]) return IMAGO_ERR_CELL_LIST;
-        for (int k = 0; k < c->ncell; ++k) {
-          if (c->csize[k] > maxr) break;
-          double r2 = 0.0;
-          for (int x = 0; x < 3; ++x) {
-            const double bp = B[x] + p.L0[x] + c->cells[3 * k + x];
-            r2 += (A[x] - bp) * (A[x] - bp);
-          }
-          if (r2 > lim) continue;
-          DUnit u{};
-          u.pair = (int)c->pairs.size();
-          u.cell = k;
-          u.r2 = r2;
-          u.spbeg = (int)c->sps.size();
-          const int nmin = std::min(t1.nalpha, t2.nalpha);
-          for (int l = 0; l < nmin; ++l) {
-            int mode = 0, a = l, b = l;
-            if (adist(l, l) < r2) break;
-            for (;;) {
-              if (mode == 1) {
-                ++a;
-                if (a >= t1.nalpha) { mode = 2; a = l; continue; }
-              } else if (mode == 2) {
-                ++b;
-                if (b >= t2.nalpha) break;
-              }
-              if (adist(a, b) < r2) {
-                if (mode == 1) { mode = 2; a = l; continue; }
-                break;
-              }
-              if (mode == 0) mode = 1;
-              DSp sp{};
-              sp.unit = (int)c->units.size();
-              sp.a = (short)a;
-              sp.b = (short)b;
-              sp.la = (short)t1.cls[a];
-              sp.lb = (short)t2.cls[b];
-              sp.boff = boff;
-              boff += nsh(sp.la) * nsh(sp.lb);
-              c->sps.push_back(sp);
-            }
-          }
-          u.spend = (int)c->sps.size();
-          c->units.push_back(u);
-        }
-      }
-      p.uend = (int)c->units.size();
-      moff += (long long)(p.uend - p.ubeg) * p.ni * p.nj;
+    for (int j = i; j < c->ns; ++j) ij.push_back(make_int2(i, j));
+  const size_t nchunk = std::max<size_t>(1, std::min<size_t>(256, ij.size() / 8));
+  std::vector<PairWork> part(nchunk);
+  parallel_ranges(ij.size(), nchunk, [&](size_t k, size_t lo, size_t hi) {
+    build_pairs(c, ij, lo, hi, part[k]);
+  });
+  long long moff = 0, boff = 0;
+  size_t np = 0, nu = 0, ns = 0;
+  for (const PairWork &w : part) {
+    if (w.rc) return w.rc;
+    np += w.pairs.size();
+    nu += w.units.size();
+    ns += w.sps.size();
+  }
+  c->pairs.reserve(np);
+  c->units.reserve(nu);
+  c->sps.reserve(ns);
+  for (const PairWork &w : part) {
+    const int pb = (int)c->pairs.size(), ub = (int)c->units.size();
+    const int sb = (int)c->sps.size();
+    for (DPair p : w.pairs) {
+      p.ubeg += ub;
+      p.uend += ub;
+      p.moff += moff;
       c->pairs.push_back(p);
     }
+    for (DUnit u : w.units) {
+      u.pair += pb;
+      u.spbeg += sb;
+      u.spend += sb;
+      c->units.push_back(u);
+    }
+    for (DSp sp : w.sps) {
+      sp.unit += ub;
+      sp.boff += boff;
+      c->sps.push_back(sp);
+    }
+    moff += w.moff;
+    boff += w.boff;
+  }
   c->blk_total = boff;
   c->m_total = moff;
   // Shell pairs by class and, within a class, by the pair's own part of
