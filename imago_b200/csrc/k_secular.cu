@@ -17,6 +17,8 @@
 #include "intg.cuh"
 
 namespace imago {
+// dynamic shared memory the Jacobi kernel may take: matrices up to n = 112
+constexpr size_t kJacobiMaxSmem = 216 * 1024;
 namespace {
 
 __global__ void k_secular(int V, long long np, int nk, int pot_dim,
@@ -49,8 +51,173 @@ __global__ void k_secular(int V, long long np, int nk, int pot_dim,
   }
 }
 
+// Eigenvalues of a batch of Hermitian matrices by the cyclic two-sided
+// Jacobi method, one CTA per matrix held in shared memory.  Each step
+// zeroes the off-diagonal entries of m/2 disjoint index pairs at once (the
+// circle-method round robin over m = n rounded up to even indices, m - 1
+// steps per sweep): for a_pq = |a_pq| e^{i phi},
+//   tau = (a_qq - a_pp) / (2 |a_pq|),  t = sign(tau) / (|tau| + sqrt(1 + tau^2)),
+//   c = 1 / sqrt(1 + t^2),  s = t c,
+// and A <- J^H A J with J_pp = J_qq = c, J_pq = s e^{i phi},
+// J_qp = -s e^{-i phi} (columns first, then rows).  Sweeps stop when the
+// off-diagonal Frobenius norm is below 1e-14 of the whole, at most
+// kJacobiMaxSweeps; the diagonal is then returned in ascending order.
+constexpr int kJacobiThreads = 512;
+constexpr int kJacobiMaxSweeps = 30;
+
+__global__ void __launch_bounds__(kJacobiThreads, 1)
+    k_jacobi_eigvals(int n, const double2 *a, double *w) {
+  extern __shared__ double2 jsm[];
+  const int ld = n + 1, m = n + (n & 1), npair = m / 2;
+  double2 *A = jsm;
+  double *rc = reinterpret_cast<double *>(A + (size_t)n * ld);  // c, s per pair
+  double2 *re = reinterpret_cast<double2 *>(rc + 2 * npair);    // e^{i phi}
+  int2 *pq = reinterpret_cast<int2 *>(re + npair);
+  __shared__ double red[2][kJacobiThreads / 32];
+  const int tid = threadIdx.x;
+  const double2 *src = a + (size_t)blockIdx.x * n * n;
+  for (int i = tid; i < n * n; i += kJacobiThreads)
+    A[(i / n) * ld + i % n] = src[i];
+  __syncthreads();
+  for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
+    // convergence: off-diagonal part of the Frobenius norm
+    double off = 0.0, all = 0.0;
+    for (int i = tid; i < n * n; i += kJacobiThreads) {
+      const int r = i / n, c = i % n;
+      const double2 v = A[r * ld + c];
+      const double q = v.x * v.x + v.y * v.y;
+      all += q;
+      if (r != c) off += q;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      all += __shfl_xor_sync(0xffffffffu, all, o);
+    }
+    if ((tid & 31) == 0) {
+      red[0][tid >> 5] = off;
+      red[1][tid >> 5] = all;
+    }
+    __syncthreads();
+    off = all = 0.0;
+    for (int i = 0; i < kJacobiThreads / 32; ++i) {
+      off += red[0][i];
+      all += red[1][i];
+    }
+    __syncthreads();
+    if (off <= 1e-28 * all) break;
+    for (int r = 0; r < m - 1; ++r) {
+      if (tid < npair) {
+        // circle method: index 0 stays, the others turn
+        int p = 0, q = r % (m - 1) + 1;
+        if (tid > 0) {
+          p = (r + tid) % (m - 1) + 1;
+          q = (r - tid + m - 1) % (m - 1) + 1;
+        }
+        if (p > q) {
+          const int x = p;
+          p = q;
+          q = x;
+        }
+        double c = 1.0, sn = 0.0;
+        double2 e = make_double2(1.0, 0.0);
+        if (q < n) {
+          const double2 apq = A[p * ld + q];
+          const double mag = sqrt(apq.x * apq.x + apq.y * apq.y);
+          if (mag > 1e-300) {
+            e = make_double2(apq.x / mag, apq.y / mag);
+            const double tau = (A[q * ld + q].x - A[p * ld + p].x) / (2.0 * mag);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            sn = t * c;
+          }
+        }
+        pq[tid] = make_int2(p, q);
+        rc[2 * tid] = c;
+        rc[2 * tid + 1] = sn;
+        re[tid] = e;
+      }
+      __syncthreads();
+      // columns p, q of every row: A <- A J
+      for (int i = tid; i < npair * n; i += kJacobiThreads) {
+        const int k = i / n, row = i % n;
+        const int2 x = pq[k];
+        if (x.y >= n) continue;
+        const double c = rc[2 * k], sn = rc[2 * k + 1];
+        const double2 e = re[k];
+        const double2 ap = A[row * ld + x.x], aq = A[row * ld + x.y];
+        // conj(e) aq and e ap
+        const double2 ceq = make_double2(e.x * aq.x + e.y * aq.y, e.x * aq.y - e.y * aq.x);
+        const double2 eap = make_double2(e.x * ap.x - e.y * ap.y, e.x * ap.y + e.y * ap.x);
+        A[row * ld + x.x] = make_double2(c * ap.x - sn * ceq.x, c * ap.y - sn * ceq.y);
+        A[row * ld + x.y] = make_double2(sn * eap.x + c * aq.x, sn * eap.y + c * aq.y);
+      }
+      __syncthreads();
+      // rows p, q of every column: A <- J^H A
+      for (int i = tid; i < npair * n; i += kJacobiThreads) {
+        const int k = i / n, col = i % n;
+        const int2 x = pq[k];
+        if (x.y >= n) continue;
+        const double c = rc[2 * k], sn = rc[2 * k + 1];
+        const double2 e = re[k];
+        const double2 ap = A[x.x * ld + col], aq = A[x.y * ld + col];
+        // e aq and conj(e) ap
+        const double2 eaq = make_double2(e.x * aq.x - e.y * aq.y, e.x * aq.y + e.y * aq.x);
+        const double2 cep = make_double2(e.x * ap.x + e.y * ap.y, e.x * ap.y - e.y * ap.x);
+        A[x.x * ld + col] = make_double2(c * ap.x - sn * eaq.x, c * ap.y - sn * eaq.y);
+        A[x.y * ld + col] = make_double2(sn * cep.x + c * aq.x, sn * cep.y + c * aq.y);
+      }
+      __syncthreads();
+    }
+  }
+  // ascending order by rank (ties by index)
+  double *out = w + (size_t)blockIdx.x * n;
+  for (int i = tid; i < n; i += kJacobiThreads) {
+    const double d = A[i * ld + i].x;
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double dj = A[j * ld + j].x;
+      rank += dj < d || (dj == d && j < i);
+    }
+    out[rank] = d;
+  }
+}
+
 }  // namespace
+
+size_t jacobi_smem(int n) {
+  const int m = n + (n & 1);
+  return sizeof(double2) * (size_t)n * (n + 1) + sizeof(double) * m +
+         sizeof(double2) * (m / 2) + sizeof(int2) * (m / 2);
+}
+
 }  // namespace imago
+
+extern "C" int imago_hermitian_eigvals(int n, int batch, const double *a,
+                                       double *w, void *stream) {
+  if (n <= 0 || batch < 0 || !a || !w) return IMAGO_ERR_INVALID;
+  if (batch == 0) return IMAGO_OK;
+  const size_t smem = imago::jacobi_smem(n);
+  if (smem > imago::kJacobiMaxSmem) return IMAGO_ERR_RANGE;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return IMAGO_ERR_NO_DEVICE;
+  }
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (cudaFuncSetAttribute(imago::k_jacobi_eigvals,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)imago::kJacobiMaxSmem) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_CUDA;
+    }
+    attr_set[dev] = true;
+  }
+  imago::k_jacobi_eigvals<<<batch, imago::kJacobiThreads, smem, (cudaStream_t)stream>>>(
+      n, reinterpret_cast<const double2 *>(a), w);
+  if (cudaGetLastError() != cudaSuccess) return IMAGO_ERR_CUDA;
+  return IMAGO_OK;
+}
 
 extern "C" int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
                                       const double *np_packed,

@@ -9,8 +9,9 @@ the potDim coefficients of the current SCF potential (potCoeffs in the
 reference).  H and S are assembled and unpacked on the device by
 imago_secular_matrices, then the generalised Hermitian problem
 H c = E S c, which the reference hands to LAPACK zhegv(1, 'V', 'U')
-(interfaces.F90:73-120), is reduced by the Cholesky factor of S and solved
-by cuSOLVER through torch.linalg.  Eigenvalues come back ascending per
+(interfaces.F90:73-120), is reduced by the Cholesky factor of S (cuSOLVER
+through torch.linalg) and the eigenvalues of the reduced matrices come
+from the library's batched Jacobi kernel.  Eigenvalues come back ascending per
 k-point, in Hartree.
 """
 
@@ -49,11 +50,36 @@ def secular_matrices(out, pot_coeffs, stream=None):
     return h.transpose(-2, -1), s.transpose(-2, -1)
 
 
+JACOBI_MAX_N = 112
+
+
+def hermitian_eigvals(a):
+    """Ascending eigenvalues of a batch of Hermitian matrices [b, n, n]
+    (complex128, CUDA): imago_hermitian_eigvals (one CTA per matrix, cyclic
+    Jacobi in shared memory) up to n = 112, cuSOLVER through torch beyond."""
+    b, n = a.shape[0], a.shape[-1]
+    if n > JACOBI_MAX_N:
+        return torch.linalg.eigvalsh(a)
+    a = a.contiguous()
+    w = torch.empty((b, n), dtype=torch.float64, device=a.device)
+    L = intg.lib()
+    L.imago_hermitian_eigvals.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+    L.imago_hermitian_eigvals.restype = ctypes.c_int
+    rc = L.imago_hermitian_eigvals(n, b, a.data_ptr(), w.data_ptr(),
+                                   torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise intg.ImagoError(rc, "imago_hermitian_eigvals")
+    return w
+
+
 def secular_eigenvalues(out, pot_coeffs, num_states=None):
-    """Eigenvalues of H c = E S c per k-point, ascending, [nk, num_states]."""
+    """Eigenvalues of H c = E S c per k-point, ascending, [nk, num_states]:
+    the Cholesky factor L of S (cuSOLVER, batched), A = L^-1 H L^-H, and the
+    eigenvalues of A (hermitian_eigvals)."""
     h, s = secular_matrices(out, pot_coeffs)
     lo = torch.linalg.cholesky(s)
     y = torch.linalg.solve_triangular(lo, h, upper=False)          # L^-1 H
     a = torch.linalg.solve_triangular(lo, y.mH, upper=False)       # L^-1 H L^-H
-    ev = torch.linalg.eigvalsh(a)
+    ev = hermitian_eigvals(a)
     return ev if num_states is None else ev[:, :num_states]

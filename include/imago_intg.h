@@ -261,6 +261,16 @@ IMAGO_API int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
                                      const double *ol_packed, double *h_full,
                                      double *s_full, void *stream);
 
+/*
+ * Eigenvalues of `batch` Hermitian n x n matrices (device memory, (re, im)
+ * interleaved, either storage order) into w [batch][n], ascending, by a
+ * cyclic Jacobi method with each matrix in shared memory (n up to 112,
+ * IMAGO_ERR_RANGE beyond).  The eigenvalue step of the secular equation
+ * (zhegv after its Cholesky reduction, interfaces.F90:73-120).
+ */
+IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
+                                      double *w, void *stream);
+
 /* No counterpart in the reference.  Device scratch of every context comes
  * from one stream-ordered memory pool per device that keeps freed memory
  * for the next context; this hands the pool's unused memory on `device`

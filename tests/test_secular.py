@@ -60,3 +60,21 @@ def test_secular_eigenvalues_match_oracle(imago_lib, name):
         ev = secular.secular_eigenvalues(out, w).cpu().numpy()
     assert ev.shape == ref.shape
     assert np.abs(ev - ref).max() <= EV_TOL, np.abs(ev - ref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 5, 33, 104, 112])
+def test_batched_jacobi_eigenvalues(imago_lib, n):
+    # imago_hermitian_eigvals against LAPACK, including degenerate spectra
+    import torch
+    from imago_b200 import secular
+    rng = np.random.default_rng(n)
+    b = 7
+    x = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    h = (x + np.conj(np.swapaxes(x, 1, 2))) / 2
+    h[0] = np.eye(n) * 2.5                       # fully degenerate
+    h[1] = np.diag(np.arange(n, dtype=float))    # already diagonal
+    ref = np.linalg.eigvalsh(h)
+    got = secular.hermitian_eigvals(torch.as_tensor(h, device="cuda")).cpu().numpy()
+    scale = max(1.0, np.abs(ref).max())
+    assert np.abs(got - ref).max() <= 1e-12 * scale
