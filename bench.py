@@ -307,10 +307,11 @@ def device_outputs(g, torch, dev):
 
 def time_device_builds(g, bufs, stream, steps, flush, torch):
     """Device seconds of each build (outputs in HBM) replayed from the
-    context's CUDA graph (imago_intg_build_graph, captured in the warm-up),
-    with 512 MiB written between builds to flush L2.  The kernel-stage
-    milliseconds come from the same number of plain builds (the graph
-    records no stage events)."""
+    context's CUDA graph (imago_intg_build_graph, captured in the warm-up;
+    the four kinds run concurrently), with 512 MiB written between builds
+    to flush L2.  The kernel-stage milliseconds come from the same number
+    of plain builds with the kinds serialised, so that each stage's time is
+    its own."""
     out = {k: v.data_ptr() for k, v in bufs.items()}
     step_s, kms, launches = [], np.zeros(4), 0
     for _ in range(steps):
@@ -324,11 +325,13 @@ def time_device_builds(g, bufs, stream, steps, flush, torch):
         e.synchronize()
         step_s.append(s.elapsed_time(e) / 1e3)
         launches += g.kernel_stats()[1]
+    g.set_serial(True)  # stage times of each kernel without the overlap
     for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
         g.build(out=out)
         kms += g.kernel_stats()[0]
+    g.set_serial(False)
     return step_s, kms, launches
 
 

@@ -173,14 +173,28 @@ struct imago_ctx {
   DBuf<float> d_cl_d1;
 
   // scratch
-  DBuf<double> blk, M;
+  // Each build kind (OL, KE, NP, EP) has its own scratch and stream (a
+  // lane), forked from `stream` by every call, so that the kinds of one
+  // call run concurrently; only their orthogonalisation waits for the
+  // overlap's coreValeOL (event ev_scv).
+  struct Scratch {
+    DBuf<double> blk, M;
+    DBuf<double2> vv, cv, cc, y;
+  };
+  Scratch scr[4];
+  cudaStream_t kst[4] = {};
+  cudaEvent_t kfork = nullptr, kjoin[4] = {}, ev_scv = nullptr;
+  int lane = 0;
+  bool ol_in_call = false;
+  bool serial = false;   // all kinds on `stream`, one after another
+  cudaStream_t cur() const { return !serial && kst[lane] ? kst[lane] : stream; }
   // host-output staging: one region per output matrix, so that each can be
   // copied out on copy_stream while the next build runs
   DBuf<double> out_stage;
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> cev;
   int cev_used = 0;
-  DBuf<double2> vv, cv, cc, y, s_cv;
+  DBuf<double2> s_cv;
   bool have_ol = false;
   // CUDA-graph capture of the build: no timing events are recorded and EP
   // keeps the chunk size of the last eager build (scratch already sized)
@@ -214,9 +228,14 @@ struct imago_ctx {
       b->release(st);
     for (auto *b : {&d_alpha, &d_basis, &d_site_pos, &d_ptype_z,
                     &d_ptype_nucalpha, &d_palpha, &d_psite_pos, &d_cell,
-                    &d_csize, &d_kxyz, &blk, &M, &out_stage})
+                    &d_csize, &d_kxyz, &out_stage})
       b->release(st);
-    for (auto *b : {&d_phase, &vv, &cv, &cc, &y, &s_cv}) b->release(st);
+    for (auto &sc : scr) {
+      sc.blk.release(st);
+      sc.M.release(st);
+      for (auto *b : {&sc.vv, &sc.cv, &sc.cc, &sc.y}) b->release(st);
+    }
+    for (auto *b : {&d_phase, &s_cv}) b->release(st);
     d_pairs.release(st); d_units.release(st); d_sps.release(st);
     d_terms.release(st); d_btile.release(st); d_simg.release(st);
     d_btile_w.release(st);
@@ -227,6 +246,13 @@ struct imago_ctx {
     for (auto &e : kev) cudaEventDestroy(e);
     for (auto &e : cev) cudaEventDestroy(e);
     if (gexec) cudaGraphExecDestroy(gexec);
+    for (int k = 0; k < 4; ++k) {
+      if (kst[k]) cudaStreamSynchronize(kst[k]);
+      if (kst[k]) cudaStreamDestroy(kst[k]);
+      if (kjoin[k]) cudaEventDestroy(kjoin[k]);
+    }
+    if (kfork) cudaEventDestroy(kfork);
+    if (ev_scv) cudaEventDestroy(ev_scv);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
@@ -870,13 +896,15 @@ size_t term_bytes(const imago_ctx *c) {
 
 int ensure_scratch(imago_ctx *c, int nterm) {
   const size_t V = c->vale_dim, C = c->core_dim, nk = c->nk;
+  imago_ctx::Scratch &S = c->scr[c->lane];
+  cudaStream_t st = c->cur();
   int rc;
-  if ((rc = c->blk.alloc((size_t)c->blk_total * nterm + 1, c->stream))) return rc;
-  if ((rc = c->M.alloc((size_t)c->m_total * nterm + 1, c->stream))) return rc;
-  if ((rc = c->vv.alloc(nk * V * V * nterm + 1, c->stream))) return rc;
-  if ((rc = c->cv.alloc(nk * V * C * nterm + 1, c->stream))) return rc;
-  if ((rc = c->cc.alloc(nk * C * C * nterm + 1, c->stream))) return rc;
-  if ((rc = c->y.alloc(nk * V * C * nterm + 1, c->stream))) return rc;
+  if ((rc = S.blk.alloc((size_t)c->blk_total * nterm + 1, st))) return rc;
+  if ((rc = S.M.alloc((size_t)c->m_total * nterm + 1, st))) return rc;
+  if ((rc = S.vv.alloc(nk * V * V * nterm + 1, st))) return rc;
+  if ((rc = S.cv.alloc(nk * V * C * nterm + 1, st))) return rc;
+  if ((rc = S.cc.alloc(nk * C * C * nterm + 1, st))) return rc;
+  if ((rc = S.y.alloc(nk * V * C * nterm + 1, st))) return rc;
   return IMAGO_OK;
 }
 
@@ -899,7 +927,7 @@ cudaEvent_t next_event(imago_ctx *c) {
 void mark(imago_ctx *c) {
   if (c->capturing) return;
   cudaEvent_t e = next_event(c);
-  if (e) cudaEventRecord(e, c->stream);
+  if (e) cudaEventRecord(e, c->cur());
 }
 
 int class_launches(const imago_ctx *c) {
@@ -921,12 +949,13 @@ int tune_bloch(imago_ctx *c, int nterm) {
       return IMAGO_ERR_CUDA;
     }
   int rc = IMAGO_OK;
-  cudaEventRecord(e[0], c->stream);
+  imago_ctx::Scratch &S = c->scr[c->lane];
+  cudaStream_t st = c->cur();
+  cudaEventRecord(e[0], st);
   for (int wi = 0; wi < kNumBlochWidths && !rc; ++wi) {
     set_bloch_width(c, wi);
-    rc = launch_bloch(c->sys, c->work, nterm, c->M.p, c->vv.p, c->cv.p, c->cc.p,
-                      c->stream);
-    cudaEventRecord(e[wi + 1], c->stream);
+    rc = launch_bloch(c->sys, c->work, nterm, S.M.p, S.vv.p, S.cv.p, S.cc.p, st);
+    cudaEventRecord(e[wi + 1], st);
   }
   if (!rc && cudaEventSynchronize(e[kNumBlochWidths]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
   int best = kNumBlochWidths - 1;
@@ -944,38 +973,43 @@ int tune_bloch(imago_ctx *c, int nterm) {
 
 int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
               double *packed_dev) {
-  cudaStream_t st = c->stream;
+  cudaStream_t st = c->cur();
   int rc = ensure_scratch(c, nterm);
   if (rc) return rc;
+  imago_ctx::Scratch &S = c->scr[c->lane];
   const DevSys &s = c->sys;
   const DevWork &w = c->work;
   c->launches += class_launches(c) + 2 + (c->core_dim > 0 ? 2 : 1);
   mark(c);
   if (kind == KIND_OL || kind == KIND_KE) {
-    rc = launch_prim2c(s, w, c->cls_beg, kind == KIND_KE, c->blk.p, st);
+    rc = launch_prim2c(s, w, c->cls_beg, kind == KIND_KE, S.blk.p, st);
   } else if (kind == KIND_NP) {
-    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, c->blk.p, st);
+    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st);
   } else {
     rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + term0, nterm, false,
-                       c->blk.p, st);
+                       S.blk.p, st);
   }
   if (rc) return rc;
   mark(c);
-  if ((rc = launch_contract(s, w, nterm, c->blk.p, c->M.p, st))) return rc;
+  if ((rc = launch_contract(s, w, nterm, S.blk.p, S.M.p, st))) return rc;
   mark(c);
   if (!c->bloch_tuned && !c->capturing && s.nk > kBlochSmallNk &&
       (rc = tune_bloch(c, nterm)))
     return rc;
-  if ((rc = launch_bloch(s, w, nterm, c->M.p, c->vv.p, c->cv.p, c->cc.p, st)))
+  if ((rc = launch_bloch(s, w, nterm, S.M.p, S.vv.p, S.cv.p, S.cc.p, st)))
     return rc;
   mark(c);
   if (kind == KIND_OL && c->core_dim > 0) {
     const size_t n = (size_t)c->nk * c->vale_dim * c->core_dim;
     if ((rc = c->s_cv.alloc(n, st))) return rc;
-    IMAGO_CUDA(cudaMemcpyAsync(c->s_cv.p, c->cv.p, n * sizeof(double2),
+    IMAGO_CUDA(cudaMemcpyAsync(c->s_cv.p, S.cv.p, n * sizeof(double2),
                                cudaMemcpyDeviceToDevice, st));
+    IMAGO_CUDA(cudaEventRecord(c->ev_scv, st));
+  } else if (c->core_dim > 0 && c->ol_in_call) {
+    // the overlap of this call runs on its own lane
+    IMAGO_CUDA(cudaStreamWaitEvent(st, c->ev_scv, 0));
   }
-  rc = launch_ortho(s, nterm, c->vv.p, c->cv.p, c->cc.p, c->s_cv.p, c->y.p,
+  rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
                     packed_dev, st);
   mark(c);
   return rc;
@@ -1000,12 +1034,12 @@ int copy_out(imago_ctx *c, double *dst, const double *src, size_t n) {
   if (!dst || n == 0) return IMAGO_OK;
   if (c->outputs_on_device) {
     IMAGO_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
-                               cudaMemcpyDeviceToDevice, c->stream));
+                               cudaMemcpyDeviceToDevice, c->cur()));
     return IMAGO_OK;
   }
   cudaEvent_t e = next_copy_event(c);
   if (!e) return IMAGO_ERR_CUDA;
-  IMAGO_CUDA(cudaEventRecord(e, c->stream));
+  IMAGO_CUDA(cudaEventRecord(e, c->cur()));
   IMAGO_CUDA(cudaStreamWaitEvent(c->copy_stream, e, 0));
   IMAGO_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
                              cudaMemcpyDeviceToHost, c->copy_stream));
@@ -1059,11 +1093,11 @@ int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
       im = re + ncv;
     } else if (!re || !im) {
       // one of the two requested on the device: split through y
-      double *scratch = reinterpret_cast<double *>(c->y.p);
+      double *scratch = reinterpret_cast<double *>(c->scr[c->lane].y.p);
       if (!re) re = scratch;
       if (!im) im = scratch + ncv;
     }
-    if ((rc = launch_split_cv(c->sys, c->s_cv.p, re, im, c->stream))) return rc;
+    if ((rc = launch_split_cv(c->sys, c->s_cv.p, re, im, c->cur()))) return rc;
     c->launches += 1;
     if (!c->outputs_on_device) {
       if ((rc = copy_out(c, cv_re, re, ncv))) return rc;
@@ -1130,11 +1164,15 @@ int begin_call(imago_ctx *c) {
 int finish(imago_ctx *c, int rc) {
   if (rc != IMAGO_OK) {
     cudaStreamSynchronize(c->stream);
+    for (cudaStream_t k : c->kst)
+      if (k) cudaStreamSynchronize(k);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     cudaGetLastError();
     return rc;
   }
   IMAGO_CUDA(cudaStreamSynchronize(c->stream));
+  for (cudaStream_t k : c->kst)
+    if (k) IMAGO_CUDA(cudaStreamSynchronize(k));
   if (c->copy_stream) IMAGO_CUDA(cudaStreamSynchronize(c->copy_stream));
   for (int k = 0; k < 4; ++k) c->kernel_ms[k] = 0.0;
   for (int b = 0; b + 4 < c->kev_used; b += 5)
@@ -1153,33 +1191,37 @@ int set_device(imago_ctx *c) {
   return IMAGO_OK;
 }
 
-// Enqueue every build selected by `which` on the context's stream (and its
-// copy stream for host outputs) without waiting for them.
-int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out) {
+// Enqueue every build selected by `which` without waiting for them: each
+// kind on its own lane, forked from the context's stream and joined back
+// into it (EP terms [ep_first, ep_first + ep_count), all by default).
+int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out,
+                  int ep_first = 0, int ep_count = -1) {
+  IMAGO_CUDA(cudaEventRecord(c->kfork, c->stream));
+  c->ol_in_call = (which & IMAGO_OL) != 0;
   int rc = IMAGO_OK;
-  auto rec = [&](int i) {
-    if (!c->capturing) cudaEventRecord(c->ev[i], c->stream);
+  auto run = [&](int kind, auto body) {
+    c->lane = kind;
+    cudaStream_t ks = c->cur();
+    int r = cudaStreamWaitEvent(ks, c->kfork, 0) == cudaSuccess ? IMAGO_OK
+                                                               : IMAGO_ERR_CUDA;
+    if (!c->capturing) cudaEventRecord(c->ev[2 * kind], ks);
+    if (!r) r = body();
+    if (!c->capturing) cudaEventRecord(c->ev[2 * kind + 1], ks);
+    if (cudaEventRecord(c->kjoin[kind], ks) != cudaSuccess ||
+        cudaStreamWaitEvent(c->stream, c->kjoin[kind], 0) != cudaSuccess)
+      r = r ? r : IMAGO_ERR_CUDA;
+    c->lane = 0;
+    return r;
   };
-  if (which & IMAGO_OL) {
-    rec(0);
-    rc = do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im);
-    rec(1);
-  }
-  if (!rc && (which & IMAGO_KE)) {
-    rec(2);
-    rc = do_simple(c, KIND_KE, out->ke_packed);
-    rec(3);
-  }
-  if (!rc && (which & IMAGO_NP)) {
-    rec(4);
-    rc = do_simple(c, KIND_NP, out->np_packed);
-    rec(5);
-  }
-  if (!rc && (which & IMAGO_EP)) {
-    rec(6);
-    rc = do_ep(c, out->ep_packed);
-    rec(7);
-  }
+  if (which & IMAGO_OL)
+    rc = run(KIND_OL, [&] { return do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im); });
+  if (!rc && (which & IMAGO_KE))
+    rc = run(KIND_KE, [&] { return do_simple(c, KIND_KE, out->ke_packed); });
+  if (!rc && (which & IMAGO_NP))
+    rc = run(KIND_NP, [&] { return do_simple(c, KIND_NP, out->np_packed); });
+  if (!rc && (which & IMAGO_EP))
+    rc = run(KIND_EP, [&] { return do_ep(c, out->ep_packed, ep_first, ep_count); });
+  c->ol_in_call = false;
   return rc;
 }
 
@@ -1187,6 +1229,21 @@ bool same_out(const imago_out &a, const imago_out &b) {
   return a.ol_packed == b.ol_packed && a.ol_cv_re == b.ol_cv_re &&
          a.ol_cv_im == b.ol_cv_im && a.ke_packed == b.ke_packed &&
          a.np_packed == b.np_packed && a.ep_packed == b.ep_packed;
+}
+
+// One call of the build API: set-up, the builds of `which` on their lanes,
+// wait, stage times.
+int build_call(imago_ctx *c, unsigned which, const imago_out &o, int ep_first = 0,
+               int ep_count = -1) {
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = begin_call(c))) return finish(c, rc);
+  rc = finish(c, enqueue_build(c, which, &o, ep_first, ep_count));
+  if (!rc)
+    for (int s = 0; s < 4; ++s)
+      if (which & (1u << s))
+        cudaEventElapsedTime(&c->stage_ms[s], c->ev[2 * s], c->ev[2 * s + 1]);
+  return rc;
 }
 
 }  // namespace
@@ -1230,6 +1287,13 @@ int imago_intg_create(const imago_system *sys, const imago_opts *opts,
       c->own_stream = true;
     }
   }
+  for (int k = 0; k < 4 && !rc; ++k)
+    if (cudaStreamCreateWithFlags(&c->kst[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->kjoin[k], cudaEventDisableTiming) != cudaSuccess)
+      rc = IMAGO_ERR_CUDA;
+  if (!rc && (cudaEventCreateWithFlags(&c->kfork, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c->ev_scv, cudaEventDisableTiming) != cudaSuccess))
+    rc = IMAGO_ERR_CUDA;
   if (!rc) {
     for (auto &e : c->ev) cudaEventCreate(&e);
     c->events = true;
@@ -1261,82 +1325,46 @@ int imago_intg_dims(const imago_ctx *c, imago_dims *d) {
 int imago_gauss_overlap_ol(imago_ctx *c, double *packed, double *cv_re,
                            double *cv_im) {
   if (!c) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  cudaEventRecord(c->ev[0], c->stream);
-  rc = do_ol(c, packed, cv_re, cv_im);
-  cudaEventRecord(c->ev[1], c->stream);
-  rc = finish(c, rc);
-  if (!rc) cudaEventElapsedTime(&c->stage_ms[0], c->ev[0], c->ev[1]);
-  return rc;
+  imago_out o{};
+  o.ol_packed = packed;
+  o.ol_cv_re = cv_re;
+  o.ol_cv_im = cv_im;
+  return build_call(c, IMAGO_OL, o);
 }
 
 int imago_gauss_overlap_ke(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  cudaEventRecord(c->ev[2], c->stream);
-  rc = do_simple(c, KIND_KE, packed);
-  cudaEventRecord(c->ev[3], c->stream);
-  rc = finish(c, rc);
-  if (!rc) cudaEventElapsedTime(&c->stage_ms[1], c->ev[2], c->ev[3]);
-  return rc;
+  imago_out o{};
+  o.ke_packed = packed;
+  return build_call(c, IMAGO_KE, o);
 }
 
 int imago_gauss_overlap_np(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  cudaEventRecord(c->ev[4], c->stream);
-  rc = do_simple(c, KIND_NP, packed);
-  cudaEventRecord(c->ev[5], c->stream);
-  rc = finish(c, rc);
-  if (!rc) cudaEventElapsedTime(&c->stage_ms[2], c->ev[4], c->ev[5]);
-  return rc;
+  imago_out o{};
+  o.np_packed = packed;
+  return build_call(c, IMAGO_NP, o);
 }
 
 int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  cudaEventRecord(c->ev[6], c->stream);
-  rc = do_ep(c, packed);
-  cudaEventRecord(c->ev[7], c->stream);
-  rc = finish(c, rc);
-  if (!rc) cudaEventElapsedTime(&c->stage_ms[3], c->ev[6], c->ev[7]);
-  return rc;
+  imago_out o{};
+  o.ep_packed = packed;
+  return build_call(c, IMAGO_EP, o);
 }
 
 int imago_elec_pot_gauss_overlap_range(imago_ctx *c, int first, int count,
                                        double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
   if (first < 0 || count < 0 || first + count > c->pot_dim) return IMAGO_ERR_RANGE;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  cudaEventRecord(c->ev[6], c->stream);
-  if (count > 0) rc = do_ep(c, packed, first, count);
-  cudaEventRecord(c->ev[7], c->stream);
-  rc = finish(c, rc);
-  if (!rc) cudaEventElapsedTime(&c->stage_ms[3], c->ev[6], c->ev[7]);
-  return rc;
+  imago_out o{};
+  o.ep_packed = packed;
+  return build_call(c, count > 0 ? IMAGO_EP : 0u, o, first, count);
 }
 
 int imago_intg_build(imago_ctx *c, unsigned which, const imago_out *out) {
   if (!c || !out) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  rc = finish(c, enqueue_build(c, which, out));
-  if (!rc)
-    for (int s = 0; s < 4; ++s)
-      if (which & (1u << s))
-        cudaEventElapsedTime(&c->stage_ms[s], c->ev[2 * s], c->ev[2 * s + 1]);
-  return rc;
+  return build_call(c, which, *out);
 }
 
 int imago_intg_build_graph(imago_ctx *c, unsigned which, const imago_out *out) {
@@ -1550,6 +1578,16 @@ int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) 
   if (bloch_width) *bloch_width = c->work.bw;
   if (trial_ms)
     for (int i = 0; i < kNumBlochWidths; ++i) trial_ms[i] = c->bloch_ms[i];
+  return IMAGO_OK;
+}
+
+int imago_intg_set_serial(imago_ctx *c, int serial) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (c->gexec) {  // a captured graph keeps its own launch order
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  c->serial = serial != 0;
   return IMAGO_OK;
 }
 

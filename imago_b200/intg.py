@@ -86,6 +86,8 @@ def lib():
         L.imago_intg_kernel_stats.restype = ctypes.c_int
         L.imago_intg_destroy.argtypes = [ctypes.c_void_p]
         L.imago_intg_destroy.restype = None
+        L.imago_intg_set_serial.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.imago_intg_set_serial.restype = ctypes.c_int
         L.imago_intg_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         L.imago_intg_tuning.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
@@ -326,6 +328,12 @@ class IntegralSetup:
         _check(lib().imago_intg_build_graph(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build_graph")
         return out
+
+    def set_serial(self, serial=True):
+        """Run the build kinds one after another on the context's stream
+        (per-kernel timing) instead of concurrently (imago_intg_set_serial)."""
+        _check(lib().imago_intg_set_serial(self._ctx, 1 if serial else 0),
+               "imago_intg_set_serial")
 
     def tuning(self):
         """The phase-sum column width the context measured fastest and the

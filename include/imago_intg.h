@@ -271,6 +271,12 @@ IMAGO_API int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
 IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
                                       double *w, void *stream);
 
+/* No counterpart in the reference.  The builds of one call run each kind
+ * (OL, KE, NP, EP) on a stream of its own, concurrently; serial != 0 runs
+ * them one after another on the context's stream instead, which gives each
+ * kernel stage its own device time in imago_intg_kernel_stats. */
+IMAGO_API int imago_intg_set_serial(imago_ctx *ctx, int serial);
+
 /* No counterpart in the reference.  Device scratch of every context comes
  * from one stream-ordered memory pool per device that keeps freed memory
  * for the next context; this hands the pool's unused memory on `device`
