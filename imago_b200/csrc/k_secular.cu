@@ -137,9 +137,9 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         re[tid] = e;
       }
       __syncthreads();
-      // columns p, q of every row: A <- A J
-      for (int i = tid; i < npair * n; i += kJacobiThreads) {
-        const int k = i / n, row = i % n;
+      // columns p, q of every row: A <- A J (a warp per pair, lanes on rows)
+      for (int k = tid >> 5; k < npair; k += kJacobiThreads / 32)
+      for (int row = tid & 31; row < n; row += 32) {
         const int2 x = pq[k];
         if (x.y >= n) continue;
         const double c = rc[2 * k], sn = rc[2 * k + 1];
@@ -152,9 +152,10 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         A[row * ld + x.y] = make_double2(sn * eap.x + c * aq.x, sn * eap.y + c * aq.y);
       }
       __syncthreads();
-      // rows p, q of every column: A <- J^H A
-      for (int i = tid; i < npair * n; i += kJacobiThreads) {
-        const int k = i / n, col = i % n;
+      // rows p, q of every column: A <- J^H A (a warp per pair, lanes on
+      // columns)
+      for (int k = tid >> 5; k < npair; k += kJacobiThreads / 32)
+      for (int col = tid & 31; col < n; col += 32) {
         const int2 x = pq[k];
         if (x.y >= n) continue;
         const double c = rc[2 * k], sn = rc[2 * k + 1];
