@@ -79,3 +79,29 @@ def test_system_validation():
     s.atom_types[0].num_orb_alphas = [16, 8, 12, 0]
     with pytest.raises(ValueError):
         s.validate()
+
+
+def test_added_entry_points_reject_bad_arguments(imago_lib):
+    # argument checks come before any device work, so they hold without a GPU
+    L = imago_lib
+    vp = ctypes.c_void_p
+    L.imago_intg_set_serial.argtypes = [vp, ctypes.c_int]
+    assert L.imago_intg_set_serial(None, 1) == 1
+    L.imago_intg_build_graph.argtypes = [vp, ctypes.c_uint, vp]
+    assert L.imago_intg_build_graph(None, 15, None) == 1
+    L.imago_intg_tuning.argtypes = [vp, vp, vp]
+    assert L.imago_intg_tuning(None, None, None) == 1
+    L.imago_elec_pot_gauss_overlap_range.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+    assert L.imago_elec_pot_gauss_overlap_range(None, 0, 1, None) == 1
+    out = vp()
+    L.imago_batch_create.argtypes = [ctypes.c_int, vp, vp, ctypes.POINTER(vp)]
+    assert L.imago_batch_create(0, None, None, ctypes.byref(out)) == 1
+    assert not out.value
+    L.imago_batch_build.argtypes = [vp, ctypes.c_uint, vp]
+    assert L.imago_batch_build(None, 15, None) == 1
+    L.imago_batch_size.argtypes = [vp]
+    assert L.imago_batch_size(None) == 0
+    L.imago_hermitian_eigvals.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    assert L.imago_hermitian_eigvals(0, 1, None, None, None) == 1
+    L.imago_secular_matrices.argtypes = [ctypes.c_int] * 3 + [vp] * 8
+    assert L.imago_secular_matrices(0, 1, 0, *([None] * 8)) == 1

@@ -332,3 +332,15 @@ def test_sharded_build_on_one_rank_matches_plain_build(imago_lib):
         assert _same(ref["ep_packed"], got["ep"])
     finally:
         dist.destroy_process_group()
+
+
+def test_serial_and_concurrent_kinds_agree(imago_lib):
+    # the four build kinds on their own concurrent streams, or one after
+    # another on the context's stream: the same matrices bit for bit
+    s = configs.silicon_cubic8(kmesh=(2, 2, 3))
+    with intg.IntegralSetup(s) as g:
+        a = g.build()
+        g.set_serial(True)
+        b = g.build()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
