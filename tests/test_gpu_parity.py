@@ -344,3 +344,28 @@ def test_serial_and_concurrent_kinds_agree(imago_lib):
         b = g.build()
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
+    # an interrupted checkpointed build, resumed, stores exactly the
+    # matrices of one uninterrupted build
+    from imago_b200 import store as st
+    s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+    with intg.IntegralSetup(s) as g:
+        ref = g.build()
+        box = st.IntegralStore.for_setup(str(tmp_path), g)
+
+        def stop(group):
+            if group == box.ep_group(1):
+                raise KeyboardInterrupt
+
+        with pytest.raises(KeyboardInterrupt):
+            st.build_checkpointed(g, box, ep_batch=3, on_group=stop)
+        rest = st.build_checkpointed(g, box)
+        assert rest[0] == box.ep_group(2)
+    got = st.read_all(box)
+    for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed"):
+        assert np.array_equal(ref[k], got[k]), k
+    if g.core_dim > 0:
+        assert np.array_equal(ref["ol_cv_re"], got["ol_cv_re"])
+        assert np.array_equal(ref["ol_cv_im"], got["ol_cv_im"])

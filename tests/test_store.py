@@ -1,0 +1,94 @@
+"""The checkpointed on-disk store (imago_b200.store): the reference's
+group/dataset/status layout, skipping of finished groups, and resumption
+after an interruption.  A fake builder stands in for the GPU here; the
+real builds go through it in test_gpu_parity.py."""
+
+import os
+
+import numpy as np
+import pytest
+
+from imago_b200 import store as st
+
+
+class FakeSetup:
+    """Deterministic packed matrices; counts the builds it runs."""
+
+    def __init__(self, nk=3, V=4, C=2, P=5):
+        self.nk, self.V, self.C, self.P = nk, V, C, P
+        self.np = V * (V + 1) // 2
+        self.calls = []
+
+    def _mat(self, tag):
+        x = np.arange(self.nk * self.np * 2, dtype=float).reshape(self.nk, self.np, 2)
+        return x + 1000.0 * tag
+
+    def gauss_overlap_ol(self):
+        self.calls.append("OL")
+        re = np.full((self.nk, self.V, self.C), 1.5)
+        return self._mat(0), re, -re
+
+    def gauss_overlap_ke(self):
+        self.calls.append("KE")
+        return self._mat(1)
+
+    def gauss_overlap_np(self):
+        self.calls.append("NP")
+        return self._mat(2)
+
+    def elec_pot_gauss_overlap_range(self, first, count):
+        self.calls.append(("EP", first, count))
+        return np.stack([self._mat(10 + t) for t in range(first, first + count)])
+
+
+def _store(tmp_path, f):
+    return st.IntegralStore(str(tmp_path), f.nk, f.np, f.P, f.V, f.C)
+
+
+def test_layout_and_complete_build(tmp_path):
+    f = FakeSetup()
+    s = _store(tmp_path, f)
+    written = st.build_checkpointed(f, s)
+    assert written == [st.OL, st.KE, st.NP] + [s.ep_group(t) for t in range(f.P)]
+    root = os.path.join(str(tmp_path), st.GROUP)
+    assert os.path.exists(os.path.join(root, "atomOverlap", "0000001.npy"))
+    assert os.path.exists(os.path.join(root, "atomOverlapCV", "imag0000003.npy"))
+    assert os.path.exists(os.path.join(root, "atomPotOverlap", "0000005", "0000002.npy"))
+    out = st.read_all(s)
+    assert np.array_equal(out["ke_packed"], f._mat(1))
+    assert np.array_equal(out["ep_packed"][4], f._mat(14))
+    assert np.array_equal(out["ol_cv_im"], -out["ol_cv_re"])
+    # a second run finds everything done and builds nothing
+    f2 = FakeSetup()
+    assert st.build_checkpointed(f2, _store(tmp_path, f2)) == []
+    assert f2.calls == []
+
+
+def test_resume_after_interruption(tmp_path):
+    f = FakeSetup(P=7)
+    s = _store(tmp_path, f)
+
+    def stop(group):
+        if group == s.ep_group(2):
+            raise KeyboardInterrupt
+
+    with pytest.raises(KeyboardInterrupt):
+        st.build_checkpointed(f, s, ep_batch=2, on_group=stop)
+    # terms 0..2 are recorded; term 3 was built in the same run but its
+    # status never set, so it is built again
+    f2 = FakeSetup(P=7)
+    written = st.build_checkpointed(f2, _store(tmp_path, f2), ep_batch=8)
+    assert written == [s.ep_group(t) for t in range(3, 7)]
+    # coreDim > 0: the overlap is rebuilt for the orthogonalisation, not
+    # written again
+    assert f2.calls == ["OL", ("EP", 3, 4)]
+    out = st.read_all(s)
+    for t in range(7):
+        assert np.array_equal(out["ep_packed"][t], f._mat(10 + t))
+
+
+def test_store_refuses_another_system(tmp_path):
+    f = FakeSetup()
+    _store(tmp_path, f)
+    with pytest.raises(ValueError):
+        st.IntegralStore(str(tmp_path), f.nk, f.np, f.P + 1, f.V, f.C)
