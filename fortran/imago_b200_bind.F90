@@ -1,14 +1,17 @@
 ! imago_b200_bind.F90 -- ISO_C_BINDING shim that lets Imago's setupSCF call
-! the B200 integral setup (include/imago_intg.h) in place of its four
+! the B200 integral setup (include/imago_intg.h) in place of its
 ! integral builds.  It is written against the reference's module data and
 ! HDF5 handles:
 !
 !    call gaussOverlapOL(...)      -> call b200GaussOverlapOL(...)
 !    call gaussOverlapKE(...)      -> call b200GaussOverlapKE(...)
+!    call gaussOverlapMV(...)      -> call b200GaussOverlapMV(...)  (rel == 1)
+!    call gaussOverlapHamPSCF(...) -> call b200GaussOverlapHamPSCF(...)  (PSCF)
 !    call gaussOverlapNP(...)      -> call b200GaussOverlapNP(...)
 !    call elecPotGaussOverlap(...) -> call b200ElecPotGaussOverlap(...)
 !
-! (src/imago/imago.F90:262, 268, 284, 293), each with the same arguments.
+! (src/imago/imago.F90:262, 268, 274, 284, 293, 685), each with the same
+! arguments.
 ! Each wrapper skips a matrix whose HDF5 "done" attribute is already 1, as
 ! the reference does, writes the packed valence-valence datasets per
 ! k-point (and coreValeOL for the overlap) and sets the attribute.
@@ -89,6 +92,22 @@ module O_ImagoB200
             & bind(C, name="imago_gauss_overlap_np") result(st)
          import :: c_ptr, c_int, c_double
          type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: packed(*)
+         integer(c_int) :: st
+      end function
+      function imago_gauss_overlap_mv(ctx, packed) &
+            & bind(C, name="imago_gauss_overlap_mv") result(st)
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: packed(*)
+         integer(c_int) :: st
+      end function
+      function imago_ham_pscf(ctx, spin, coeffs, rel, packed) &
+            & bind(C, name="imago_ham_pscf") result(st)
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: spin, rel
+         real(c_double), intent(in) :: coeffs(*)
          real(c_double), intent(out) :: packed(*)
          integer(c_int) :: st
       end function
@@ -352,10 +371,12 @@ contains
       allocate (packed(2, np, numKPoints))
       if (which == 2) then
          st = imago_gauss_overlap_ke(ctx, packed)
+      else if (which == 5) then
+         st = imago_gauss_overlap_mv(ctx, packed)
       else
          st = imago_gauss_overlap_np(ctx, packed)
       endif
-      if (st /= 0) call fail(st, 'gaussOverlapKE/NP')
+      if (st /= 0) call fail(st, 'gaussOverlapKE/MV/NP')
       call writePacked(packed, 2, packedVVDims, did, numKPoints, np)
       call markDone(aid)
    end subroutine b200OneMatrix
@@ -367,6 +388,14 @@ contains
       integer(hid_t), intent(in) :: aid
       call b200OneMatrix(2, packedVVDims, did, aid)
    end subroutine b200GaussOverlapKE
+
+   subroutine b200GaussOverlapMV(packedVVDims, did, aid)
+      use O_KPoints, only: numKPoints
+      integer(hsize_t), dimension(2), intent(in) :: packedVVDims
+      integer(hid_t), dimension(numKPoints), intent(in) :: did
+      integer(hid_t), intent(in) :: aid
+      call b200OneMatrix(5, packedVVDims, did, aid)
+   end subroutine b200GaussOverlapMV
 
    subroutine b200GaussOverlapNP(packedVVDims, did, aid)
       use O_KPoints, only: numKPoints
@@ -398,6 +427,32 @@ contains
          call markDone(aid(t))
       enddo
    end subroutine b200ElecPotGaussOverlap
+
+   ! gaussOverlapHamPSCF + orthoHamPSCF: one packed Hamiltonian per spin
+   ! from potCoeffs(potDim, spin), as imago.F90:685 calls it.
+   subroutine b200GaussOverlapHamPSCF(did, aid)
+      use O_KPoints, only: numKPoints
+      use O_AtomicSites, only: valeDim
+      use O_Potential, only: rel, spin, potCoeffs
+      use O_PSCFIntegralsHDF5, only: packedVVDimsPSCF
+      integer(hid_t), dimension(numKPoints,spin), intent(in) :: did
+      integer(hid_t), intent(in) :: aid
+      real(c_double), allocatable :: packed(:,:,:,:)
+      integer(hsize_t) :: np
+      integer :: h
+      integer(c_int) :: st
+      if (alreadyDone(aid)) return
+      np = int(valeDim, hsize_t) * (valeDim + 1) / 2
+      allocate (packed(2, np, numKPoints, spin))
+      st = imago_ham_pscf(ctx, int(spin, c_int), potCoeffs, int(rel, c_int), &
+            & packed)
+      if (st /= 0) call fail(st, 'gaussOverlapHamPSCF')
+      do h = 1, spin
+         call writePacked(packed(:,:,:,h), 2, packedVVDimsPSCF, did(:,h), &
+               & numKPoints, np)
+      enddo
+      call markDone(aid)
+   end subroutine b200GaussOverlapHamPSCF
 
    subroutine b200Cleanup()
       if (c_associated(ctx)) call imago_intg_destroy(ctx)

@@ -196,6 +196,9 @@ struct imago_ctx {
   int cev_used = 0;
   DBuf<double2> s_cv;
   bool have_ol = false;
+  // PSCF Hamiltonian: accumulated sh blocks per spin, the potential
+  // coefficients, and the packed result when outputs go to the host
+  DBuf<double> ham_blk, ham_w, ham_out;
   // CUDA-graph capture of the build: no timing events are recorded and EP
   // keeps the chunk size of the last eager build (scratch already sized)
   bool capturing = false;
@@ -228,7 +231,7 @@ struct imago_ctx {
       b->release(st);
     for (auto *b : {&d_alpha, &d_basis, &d_site_pos, &d_ptype_z,
                     &d_ptype_nucalpha, &d_palpha, &d_psite_pos, &d_cell,
-                    &d_csize, &d_kxyz, &out_stage})
+                    &d_csize, &d_kxyz, &out_stage, &ham_blk, &ham_w, &ham_out})
       b->release(st);
     for (auto &sc : scr) {
       sc.blk.release(st);
@@ -908,7 +911,7 @@ int ensure_scratch(imago_ctx *c, int nterm) {
   return IMAGO_OK;
 }
 
-enum Kind { KIND_OL = 0, KIND_KE = 1, KIND_NP = 2, KIND_EP = 3 };
+enum Kind { KIND_OL = 0, KIND_KE = 1, KIND_NP = 2, KIND_EP = 3, KIND_MV = 4 };
 
 // One build of `nterm` matrices of one kind, writing packed output to
 // `packed_dev` (device) [nterm][nk][np][2].
@@ -981,8 +984,11 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   const DevWork &w = c->work;
   c->launches += class_launches(c) + 2 + (c->core_dim > 0 ? 2 : 1);
   mark(c);
-  if (kind == KIND_OL || kind == KIND_KE) {
-    rc = launch_prim2c(s, w, c->cls_beg, kind == KIND_KE, S.blk.p, st);
+  if (kind == KIND_OL || kind == KIND_KE || kind == KIND_MV) {
+    const int op = kind == KIND_OL   ? kPrim2cOverlap
+                   : kind == KIND_KE ? kPrim2cKinetic
+                                     : kPrim2cMassVel;
+    rc = launch_prim2c(s, w, c->cls_beg, op, S.blk.p, st);
   } else if (kind == KIND_NP) {
     rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st);
   } else {
@@ -1055,9 +1061,11 @@ size_t cv_doubles(const imago_ctx *c) {
 }
 
 // Host-output staging layout: packed OL, KE, NP, then one region per EP
-// term, then coreValeOL (re, im).  Allocated whole before a call's first
-// build, so no region moves while a copy out of it is pending.
+// term, then MV, then coreValeOL (re, im).  Allocated whole before a call's
+// first build, so no region moves while a copy out of it is pending.
 enum Slot { SLOT_OL = 0, SLOT_KE = 1, SLOT_NP = 2, SLOT_EP = 3 };
+
+int slot_mv(const imago_ctx *c) { return SLOT_EP + c->pot_dim; }
 
 int ensure_out_stage(imago_ctx *c) {
   if (c->outputs_on_device) return IMAGO_OK;
@@ -1068,7 +1076,7 @@ int ensure_out_stage(imago_ctx *c) {
     c->copy_stream = nullptr;
     return IMAGO_ERR_CUDA;
   }
-  const size_t n = packed_doubles(c) * (3 + (size_t)c->pot_dim) + 2 * cv_doubles(c);
+  const size_t n = packed_doubles(c) * (4 + (size_t)c->pot_dim) + 2 * cv_doubles(c);
   return c->out_stage.alloc(n, c->stream);
 }
 
@@ -1089,7 +1097,7 @@ int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
   if (ncv && (cv_re || cv_im)) {
     double *re = cv_re, *im = cv_im;
     if (!c->outputs_on_device) {
-      re = c->out_stage.p + packed_doubles(c) * (3 + (size_t)c->pot_dim);
+      re = c->out_stage.p + packed_doubles(c) * (4 + (size_t)c->pot_dim);
       im = re + ncv;
     } else if (!re || !im) {
       // one of the two requested on the device: split through y
@@ -1110,7 +1118,8 @@ int do_ol(imago_ctx *c, double *packed, double *cv_re, double *cv_im) {
 int do_simple(imago_ctx *c, Kind kind, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
   int rc = IMAGO_OK;
-  double *tgt = packed_target(c, packed, kind == KIND_KE ? SLOT_KE : SLOT_NP);
+  const int slot = kind == KIND_KE ? SLOT_KE : kind == KIND_NP ? SLOT_NP : slot_mv(c);
+  double *tgt = packed_target(c, packed, slot);
   if ((rc = run_build(c, kind, 0, 1, tgt))) return rc;
   if (tgt != packed) rc = copy_out(c, packed, tgt, packed_doubles(c));
   return rc;
@@ -1120,13 +1129,11 @@ int do_simple(imago_ctx *c, Kind kind, double *packed) {
 // one chunk's matrices overlaps building the next.
 constexpr int kEpCopyChunks = 4;
 
-// EP terms [first, first + count); `packed` holds their matrices in order.
-int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
-  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
-  if (count < 0) count = c->pot_dim - first;
+// EP terms run in chunks sized to the scratch budget.  The chunk is fixed
+// on a context's first EP build: its scratch is sized for it, so later
+// builds (and graph captures) reuse it.
+int ep_chunk_size(imago_ctx *c) {
   const int nterm = c->pot_dim;
-  // the chunk is fixed on a context's first EP build: its scratch is sized
-  // for it, so later builds (and graph captures) reuse it
   int chunk = c->ep_chunk;
   if (chunk <= 0) {
     size_t budget = c->scratch_bytes;
@@ -1142,6 +1149,14 @@ int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
       chunk = std::min(chunk, std::max(1, (nterm + kEpCopyChunks - 1) / kEpCopyChunks));
     c->ep_chunk = chunk;
   }
+  return chunk;
+}
+
+// EP terms [first, first + count); `packed` holds their matrices in order.
+int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  if (count < 0) count = c->pot_dim - first;
+  const int chunk = ep_chunk_size(c);
   const size_t npd = packed_doubles(c);
   for (int t0 = first; t0 < first + count; t0 += chunk) {
     const int n = std::min(chunk, first + count - t0);
@@ -1152,6 +1167,68 @@ int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
     if (tgt != user && (rc = copy_out(c, user, tgt, npd * n))) return rc;
   }
   return IMAGO_OK;
+}
+
+// The PSCF Hamiltonian (gaussOverlapHamPSCF, integrals.F90:2860-3606, with
+// orthoHamPSCF 3913-4043): kinetic, mass velocity (rel), nuclear and the
+// potential terms weighted by potCoeffs(potDim, spin), summed over the
+// primitive sh blocks.  The contraction, phase sum and orthogonalisation
+// are linear, so they then run once per spin instead of once per term.
+int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packed) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  cudaStream_t st = c->cur();
+  const DevSys &s = c->sys;
+  const DevWork &w = c->work;
+  const int chunk = ep_chunk_size(c);
+  int rc = ensure_scratch(c, std::max(chunk, spin));
+  if (rc) return rc;
+  imago_ctx::Scratch &S = c->scr[c->lane];
+  const long long n = c->blk_total;
+  if ((rc = c->ham_blk.alloc((size_t)n * spin + 1, st))) return rc;
+  if ((rc = c->ham_w.alloc((size_t)c->pot_dim * spin + 1, st))) return rc;
+  IMAGO_CUDA(cudaMemsetAsync(c->ham_blk.p, 0, sizeof(double) * n * spin, st));
+  if (c->pot_dim > 0)
+    IMAGO_CUDA(cudaMemcpyAsync(c->ham_w.p, coeffs, sizeof(double) * c->pot_dim * spin,
+                               cudaMemcpyHostToDevice, st));
+  const int nchunk = (c->pot_dim + chunk - 1) / chunk;
+  c->launches += class_launches(c) * (2 + (rel ? 1 : 0) + nchunk) +
+                 (2 + (rel ? 1 : 0) + nchunk) + 2 + (c->core_dim > 0 ? 2 : 1);
+  mark(c);
+  if ((rc = launch_prim2c(s, w, c->cls_beg, kPrim2cKinetic, S.blk.p, st))) return rc;
+  if ((rc = launch_block_axpy(S.blk.p, 1, n, nullptr, 0, spin, c->ham_blk.p, st))) return rc;
+  if (rel) {
+    // written negatively, the sign the reference subtracts it with
+    if ((rc = launch_prim2c(s, w, c->cls_beg, kPrim2cMassVel, S.blk.p, st))) return rc;
+    if ((rc = launch_block_axpy(S.blk.p, 1, n, nullptr, 0, spin, c->ham_blk.p, st)))
+      return rc;
+  }
+  if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st))) return rc;
+  if ((rc = launch_block_axpy(S.blk.p, 1, n, nullptr, 0, spin, c->ham_blk.p, st))) return rc;
+  for (int t0 = 0; t0 < c->pot_dim; t0 += chunk) {
+    const int nt = std::min(chunk, c->pot_dim - t0);
+    if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + t0, nt, false, S.blk.p, st)))
+      return rc;
+    if ((rc = launch_block_axpy(S.blk.p, nt, n, c->ham_w.p + t0, c->pot_dim, spin,
+                                c->ham_blk.p, st)))
+      return rc;
+  }
+  mark(c);
+  if ((rc = launch_contract(s, w, spin, c->ham_blk.p, S.M.p, st))) return rc;
+  mark(c);
+  if (!c->bloch_tuned && s.nk > kBlochSmallNk && (rc = tune_bloch(c, spin))) return rc;
+  if ((rc = launch_bloch(s, w, spin, S.M.p, S.vv.p, S.cv.p, S.cc.p, st))) return rc;
+  mark(c);
+  const size_t npd = packed_doubles(c) * spin;
+  double *tgt = packed;
+  if (!c->outputs_on_device) {
+    if ((rc = c->ham_out.alloc(npd, st))) return rc;
+    tgt = c->ham_out.p;
+  }
+  if ((rc = launch_ortho(s, spin, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p, tgt, st)))
+    return rc;
+  mark(c);
+  if (tgt != packed) rc = copy_out(c, packed, tgt, npd);
+  return rc;
 }
 
 int begin_call(imago_ctx *c) {
@@ -1199,14 +1276,18 @@ int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out,
   IMAGO_CUDA(cudaEventRecord(c->kfork, c->stream));
   c->ol_in_call = (which & IMAGO_OL) != 0;
   int rc = IMAGO_OK;
+  // stage times are kept for the four kinds of the lanes; MV follows KE on
+  // the kinetic lane and is not timed
   auto run = [&](int kind, auto body) {
+    const bool timed = kind < 4 && !c->capturing;
+    if (kind == KIND_MV) kind = KIND_KE;
     c->lane = kind;
     cudaStream_t ks = c->cur();
     int r = cudaStreamWaitEvent(ks, c->kfork, 0) == cudaSuccess ? IMAGO_OK
                                                                : IMAGO_ERR_CUDA;
-    if (!c->capturing) cudaEventRecord(c->ev[2 * kind], ks);
+    if (timed) cudaEventRecord(c->ev[2 * kind], ks);
     if (!r) r = body();
-    if (!c->capturing) cudaEventRecord(c->ev[2 * kind + 1], ks);
+    if (timed) cudaEventRecord(c->ev[2 * kind + 1], ks);
     if (cudaEventRecord(c->kjoin[kind], ks) != cudaSuccess ||
         cudaStreamWaitEvent(c->stream, c->kjoin[kind], 0) != cudaSuccess)
       r = r ? r : IMAGO_ERR_CUDA;
@@ -1217,6 +1298,8 @@ int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out,
     rc = run(KIND_OL, [&] { return do_ol(c, out->ol_packed, out->ol_cv_re, out->ol_cv_im); });
   if (!rc && (which & IMAGO_KE))
     rc = run(KIND_KE, [&] { return do_simple(c, KIND_KE, out->ke_packed); });
+  if (!rc && (which & IMAGO_MV))
+    rc = run(KIND_MV, [&] { return do_simple(c, KIND_MV, out->mv_packed); });
   if (!rc && (which & IMAGO_NP))
     rc = run(KIND_NP, [&] { return do_simple(c, KIND_NP, out->np_packed); });
   if (!rc && (which & IMAGO_EP))
@@ -1228,7 +1311,8 @@ int enqueue_build(imago_ctx *c, unsigned which, const imago_out *out,
 bool same_out(const imago_out &a, const imago_out &b) {
   return a.ol_packed == b.ol_packed && a.ol_cv_re == b.ol_cv_re &&
          a.ol_cv_im == b.ol_cv_im && a.ke_packed == b.ke_packed &&
-         a.np_packed == b.np_packed && a.ep_packed == b.ep_packed;
+         a.np_packed == b.np_packed && a.ep_packed == b.ep_packed &&
+         a.mv_packed == b.mv_packed;
 }
 
 // One call of the build API: set-up, the builds of `which` on their lanes,
@@ -1344,6 +1428,26 @@ int imago_gauss_overlap_np(imago_ctx *c, double *packed) {
   imago_out o{};
   o.np_packed = packed;
   return build_call(c, IMAGO_NP, o);
+}
+
+int imago_gauss_overlap_mv(imago_ctx *c, double *packed) {
+  if (!c) return IMAGO_ERR_INVALID;
+  imago_out o{};
+  o.mv_packed = packed;
+  return build_call(c, IMAGO_MV, o);
+}
+
+int imago_ham_pscf(imago_ctx *c, int spin, const double *coeffs, int rel,
+                   double *packed) {
+  if (!c || spin < 1 || spin > 2 || !packed || (!coeffs && c->pot_dim > 0))
+    return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = begin_call(c))) return finish(c, rc);
+  c->lane = KIND_EP;  // the EP lane's scratch is sized for a chunk of terms
+  rc = do_ham(c, spin, coeffs, rel != 0, packed);
+  c->lane = 0;
+  return finish(c, rc);
 }
 
 int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
@@ -1638,10 +1742,10 @@ int imago_kpoint_mesh(const int n[3], const double shift[3],
 
 int imago_prim_eval(int kind, int n, const double *params, const int *cls,
                     double *sh) {
-  if (kind < 0 || kind > 4 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
-  if (kind < 4 && !cls) return IMAGO_ERR_INVALID;
+  if (kind < 0 || kind > 5 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
+  if (kind != 4 && !cls) return IMAGO_ERR_INVALID;
   if (n == 0) return IMAGO_OK;
-  for (int r = 0; kind < 4 && r < n; ++r)
+  for (int r = 0; kind != 4 && r < n; ++r)
     if (cls[2 * r] < 0 || cls[2 * r] > 3 || cls[2 * r + 1] < 0 || cls[2 * r + 1] > 3)
       return IMAGO_ERR_RANGE;
   int ndev = 0;
@@ -1660,7 +1764,7 @@ int imago_prim_eval(int kind, int n, const double *params, const int *cls,
   if (!rc && cudaMemcpy(dp, params, sizeof(double) * 12 * n,
                         cudaMemcpyHostToDevice) != cudaSuccess)
     rc = IMAGO_ERR_CUDA;
-  if (!rc && kind < 4 &&
+  if (!rc && kind != 4 &&
       cudaMemcpy(dc, cls, sizeof(int) * 2 * n, cudaMemcpyHostToDevice) != cudaSuccess)
     rc = IMAGO_ERR_CUDA;
   if (!rc && kind == 4) cudaMemset(dc, 0, sizeof(int) * 2 * n);

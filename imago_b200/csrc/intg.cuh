@@ -119,9 +119,12 @@ struct Term3c {
   int ptype, j;           // EP only
 };
 
+// Two-centre primitive operators of launch_prim2c.
+enum { kPrim2cOverlap = 0, kPrim2cKinetic = 1, kPrim2cMassVel = 2 };
+
 // Launchers (kernels.cu).  All take the stream to run on.
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
-                  bool kinetic, double *blk, cudaStream_t st);
+                  int op, double *blk, cudaStream_t st);
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
                   double *blk, cudaStream_t st);
@@ -132,6 +135,10 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
 int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  const double2 *cv, const double2 *cc, const double2 *s_cv,
                  double2 *y, double *packed, cudaStream_t st);
+// H[q] += sum_t w(t, q) blk[t] over the sh blocks of one term each
+// (n doubles), for the PSCF Hamiltonian.
+int launch_block_axpy(const double *blk, int nterm, long long n, const double *w,
+                      int wstride, int spin, double *H, cudaStream_t st);
 int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
                     cudaStream_t st);
 int launch_phase(const DevSys &s, double2 *phase, cudaStream_t st);

@@ -875,6 +875,36 @@ int launch_split_cv(const DevSys &s, const double2 *cv, double *re, double *im,
   return IMAGO_OK;
 }
 
+// H[q][e] += sum_t w(t, q) blk[t][e] for one or two spins q, w(t, q) =
+// w[q * wstride + t] (the layout of the reference's potCoeffs(potDim, spin))
+// or 1 when w is null.  Terms are added in order, so the sum is
+// reproducible; each element is read once for both spins.
+__global__ void k_block_axpy(const double *__restrict__ blk, int nterm,
+                             long long n, const double *__restrict__ w,
+                             int wstride, int spin, double *H) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    double a0 = H[e], a1 = spin > 1 ? H[n + e] : 0.0;
+    for (int t = 0; t < nterm; ++t) {
+      const double x = blk[t * n + e];
+      a0 += (w ? __ldg(w + t) : 1.0) * x;
+      if (spin > 1) a1 += (w ? __ldg(w + wstride + t) : 1.0) * x;
+    }
+    H[e] = a0;
+    if (spin > 1) H[n + e] = a1;
+  }
+}
+
+int launch_block_axpy(const double *blk, int nterm, long long n, const double *w,
+                      int wstride, int spin, double *H, cudaStream_t st) {
+  if (n == 0 || nterm == 0) return IMAGO_OK;
+  if (spin < 1 || spin > 2) return IMAGO_ERR_INVALID;
+  k_block_axpy<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(
+      blk, nterm, n, w, wstride, spin, H);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
 // phaseFactor(k, cell) = exp(i k.R) (kpoints.f90:578-609), stored cell-major
 // so one image's phases for consecutive k are contiguous.
 __global__ void k_phase(DevSys s, double2 *phase) {

@@ -44,6 +44,15 @@ __device__ void eval_one(int kind, const double *p, double *out) {
     for (int j = 0; j < nsh(LB); ++j) out[i * 16 + j] = blk[i * nsh(LB) + j];
 }
 
+template <int LA, int LB>
+__device__ void eval_mv(const double *p, double *out) {
+  double blk[nsh(LA) * nsh(LB)];
+  prim_mv<LA, LB>(p[0], p[1], p + 3, p + 6, kMassVelPref, blk);
+  for (int i = 0; i < 256; ++i) out[i] = 0.0;
+  for (int i = 0; i < nsh(LA); ++i)
+    for (int j = 0; j < nsh(LB); ++j) out[i * 16 + j] = blk[i * nsh(LB) + j];
+}
+
 static __device__ void eval_one_rt(int la, int lb, int kind, const double *p,
                             double *out) {
   const int L = la + lb;
@@ -91,6 +100,27 @@ __global__ void k_prim_eval(int kind, int n, const double *params,
     return;
   }
   const int la = cls[2 * r], lb = cls[2 * r + 1];
+  if (kind == 5) {  // mass velocity: s/p/d unrolled, f at run time
+    switch (la * 4 + lb) {
+#define IMAGO_EV(a, b) \
+  case a * 4 + b:      \
+    eval_mv<a, b>(p, out); \
+    break;
+      IMAGO_EV(0, 0) IMAGO_EV(0, 1) IMAGO_EV(0, 2) IMAGO_EV(1, 0)
+      IMAGO_EV(1, 1) IMAGO_EV(1, 2) IMAGO_EV(2, 0) IMAGO_EV(2, 1)
+      IMAGO_EV(2, 2)
+#undef IMAGO_EV
+      default: {
+        double blk[256];
+        prim_mv_rt(la, lb, p[0], p[1], p + 3, p + 6, kMassVelPref, blk);
+        for (int i = 0; i < 256; ++i) out[i] = 0.0;
+        for (int i = 0; i < nsh(la); ++i)
+          for (int j = 0; j < nsh(lb); ++j) out[i * 16 + j] = blk[i * nsh(lb) + j];
+        break;
+      }
+    }
+    return;
+  }
   switch (la * 4 + lb) {
 #define IMAGO_EV(a, b) \
   case a * 4 + b:      \

@@ -20,6 +20,28 @@ __global__ void __launch_bounds__(128)
   prim2c<LA, LB, KIN>(q.a1, q.a2, q.A, q.B, blk + sp.boff);
 }
 
+// Mass velocity (built once per SCF run, rel = 1): s/p/d classes unrolled,
+// the f classes through one runtime-class kernel.
+template <int LA, int LB>
+__global__ void __launch_bounds__(128)
+    k_prim_mv(DevSys s, DevWork w, int beg, int end, double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  prim_mv<LA, LB>(q.a1, q.a2, q.A, q.B, -kMassVelPref, blk + sp.boff);
+}
+
+__global__ void __launch_bounds__(128)
+    k_prim_mv_rt(DevSys s, DevWork w, int beg, int end, int la, int lb,
+                 double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  prim_mv_rt(la, lb, q.a1, q.a2, q.A, q.B, -kMassVelPref, blk + sp.boff);
+}
+
 // ------------------------------------------------------------ prim3c --
 // One thread per (shell pair, term).  The site and lattice-image loops are
 // those of nuclearPE (integrals.F90:2533-2698) and electronicPE
@@ -253,8 +275,30 @@ static int prim3c_one(const DevSys &s, const DevWork &w, int beg, int end,
   M(0, 0) M(0, 1) M(0, 2) M(1, 0) M(1, 1) M(1, 2) M(2, 0) M(2, 1) M(2, 2)
 
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
-                  bool kinetic, double *blk, cudaStream_t st) {
+                  int op, double *blk, cudaStream_t st) {
   int rc = IMAGO_OK;
+  if (op == kPrim2cMassVel) {
+#define IMAGO_MV(a, b)                                                        \
+  {                                                                          \
+    const int beg = cls_beg[a * 4 + b], n = cls_beg[a * 4 + b + 1] - beg;    \
+    if (n > 0) {                                                             \
+      k_prim_mv<a, b><<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, beg + n, blk); \
+      IMAGO_CUDA(cudaGetLastError());                                        \
+    }                                                                        \
+  }
+    IMAGO_FOR_SPD_CLASSES(IMAGO_MV)
+#undef IMAGO_MV
+    for (int c = 0; c < 16; ++c) {
+      const int la = c / 4, lb = c % 4;
+      if (la < 3 && lb < 3) continue;
+      const int beg = cls_beg[c], n = cls_beg[c + 1] - beg;
+      if (n <= 0) continue;
+      k_prim_mv_rt<<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, beg + n, la, lb, blk);
+      IMAGO_CUDA(cudaGetLastError());
+    }
+    return IMAGO_OK;
+  }
+  const bool kinetic = op == kPrim2cKinetic;
 #define IMAGO_P2(a, b)                                                       \
   if (rc == IMAGO_OK)                                                       \
     rc = prim2c_one<a, b>(s, w, cls_beg[a * 4 + b], cls_beg[a * 4 + b + 1], \

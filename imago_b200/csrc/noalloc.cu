@@ -67,11 +67,11 @@ int scratch_address(unsigned char **out) {
 
 extern "C" int imago_prim_eval_static(int kind, int n, const double *params,
                                       const int *cls, double *sh) {
-  if (kind < 0 || kind > 4 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
-  if (kind < 4 && !cls) return IMAGO_ERR_INVALID;
+  if (kind < 0 || kind > 5 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
+  if (kind != 4 && !cls) return IMAGO_ERR_INVALID;
   if (n > kMaxRecords) return IMAGO_ERR_RANGE;
   if (n == 0) return IMAGO_OK;
-  for (int r = 0; kind < 4 && r < n; ++r)
+  for (int r = 0; kind != 4 && r < n; ++r)
     if (cls[2 * r] < 0 || cls[2 * r] > 3 || cls[2 * r + 1] < 0 ||
         cls[2 * r + 1] > 3)
       return IMAGO_ERR_RANGE;
@@ -93,7 +93,7 @@ extern "C" int imago_prim_eval_static(int kind, int n, const double *params,
     rc = IMAGO_ERR_CUDA;
   if (!rc) {
     const cudaError_t e =
-        kind < 4 ? cudaMemcpy(dc, cls, sizeof(int) * 2 * n, cudaMemcpyHostToDevice)
+        kind != 4 ? cudaMemcpy(dc, cls, sizeof(int) * 2 * n, cudaMemcpyHostToDevice)
                  : cudaMemset(dc, 0, sizeof(int) * 2 * n);
     if (e != cudaSuccess) rc = IMAGO_ERR_CUDA;
   }

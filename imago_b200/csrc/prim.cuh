@@ -7,6 +7,8 @@
 //
 //  * two-centre overlap and kinetic (overlap2CIntg, kinetic2CIntg): the
 //    Obara-Saika recursions in separable 1D form;
+//  * mass velocity (massvel2CIntg): <nabla^2 a|nabla^2 b> from the same
+//    1D overlap tables, two orders higher;
 //  * three-centre overlap and nuclear (electron3CIntg, nuclear3CIntg):
 //    McMurchie-Davidson.  The product of the two orbital primitives is
 //    expanded in Hermite Gaussians about P with coefficients E_t (they
@@ -188,6 +190,104 @@ __device__ void prim2c(double a1, double a2, const double *A, const double *B,
       pc[p * ncart(LB) + q] = pref * v;
     }
   cart_to_sh<LA, LB>(pc, out);
+}
+
+// (alpha^2 / 8) with alpha the fine structure constant 7.2973525693e-3,
+// the prefactor (fineStructure * 0.001)^2 / 8 of gaussIntegrals.f90:39118.
+constexpr double kFineStructure = 7.2973525693 * 0.001;
+constexpr double kMassVelPref = kFineStructure * kFineStructure / 8.0;
+
+// One axis of the second derivative d^2/dx^2 x^i e^{-a x^2}
+//   = i(i-1) x^{i-2} - 2a(2i+1) x^i + 4a^2 x^{i+2}
+// taken on the left (atom 1), the right (atom 2) or both sides of the
+// overlap table S (which runs two orders past the class on each side).
+template <int IA, int JB>
+__device__ __forceinline__ double d2_left(const double S[IA + 1][JB + 1],
+                                          int i, int j, double a) {
+  double v = -2.0 * a * (2 * i + 1) * S[i][j] + 4.0 * a * a * S[i + 2][j];
+  if (i >= 2) v += i * (i - 1.0) * S[i - 2][j];
+  return v;
+}
+
+template <int IA, int JB>
+__device__ __forceinline__ double d2_right(const double S[IA + 1][JB + 1],
+                                           int i, int j, double b) {
+  double v = -2.0 * b * (2 * j + 1) * S[i][j] + 4.0 * b * b * S[i][j + 2];
+  if (j >= 2) v += j * (j - 1.0) * S[i][j - 2];
+  return v;
+}
+
+template <int IA, int JB>
+__device__ __forceinline__ double d2_both(const double S[IA + 1][JB + 1],
+                                          int i, int j, double a, double b) {
+  double v = -2.0 * a * (2 * i + 1) * d2_right<IA, JB>(S, i, j, b) +
+             4.0 * a * a * d2_right<IA, JB>(S, i + 2, j, b);
+  if (i >= 2) v += i * (i - 1.0) * d2_right<IA, JB>(S, i - 2, j, b);
+  return v;
+}
+
+// Mass-velocity block scale * <a|nabla^4|b> between primitives a1 at A and
+// a2 at B (scale = kMassVelPref gives massvel2CIntg's sh; the build passes
+// its negative, the sign the reference accumulates it with,
+// integrals.F90:1440-1447).  nabla^4 is taken as <nabla^2 a|nabla^2 b>,
+//   sum_x U_x S_y S_z + sum_{x != y} L_x R_y S_z,
+// whose terms carry the size of the result; the reference's recursion seeds
+// on 16 a2^4 <r_B^4> - 80 a2^3 <r_B^2> + 60 a2^2, which cancels to a value
+// of order a1 a2 when a1 << a2.  s, p and d classes only (registers).
+template <int LA, int LB>
+__device__ void prim_mv(double a1, double a2, const double *A, const double *B,
+                        double scale, double *out) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  // per axis: S, L (left d^2), R (right d^2), U (both) for i <= LA, j <= LB;
+  // the extended overlap table lives only while its axis is formed
+  double t[4][3][LA + 1][LB + 1];
+  double d2 = 0.0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    const double X = A[x] - B[x];
+    d2 += X * X;
+    double S[LA + 3][LB + 3];
+    os1d<LA + 2, LB + 2>(P - A[x], P - B[x], inv2p, S);
+#pragma unroll
+    for (int i = 0; i <= LA; ++i)
+#pragma unroll
+      for (int j = 0; j <= LB; ++j) {
+        t[0][x][i][j] = S[i][j];
+        t[1][x][i][j] = d2_left<LA + 2, LB + 2>(S, i, j, a1);
+        t[2][x][i][j] = d2_right<LA + 2, LB + 2>(S, i, j, a2);
+        t[3][x][i][j] = d2_both<LA + 2, LB + 2>(S, i, j, a1, a2);
+      }
+  }
+  const double pref = scale * pow(kPi / zeta, 1.5) * exp(-xi * d2);
+  // one Cartesian pair, evaluated where a harmonic component needs it
+  auto cart = [&](int p, int q) {
+    const int i0 = cart_exp(p, 0), i1 = cart_exp(p, 1), i2 = cart_exp(p, 2);
+    const int j0 = cart_exp(q, 0), j1 = cart_exp(q, 1), j2 = cart_exp(q, 2);
+    const double s0 = t[0][0][i0][j0], s1 = t[0][1][i1][j1], s2 = t[0][2][i2][j2];
+    const double l0 = t[1][0][i0][j0], l1 = t[1][1][i1][j1], l2 = t[1][2][i2][j2];
+    const double r0 = t[2][0][i0][j0], r1 = t[2][1][i1][j1], r2 = t[2][2][i2][j2];
+    const double u0 = t[3][0][i0][j0], u1 = t[3][1][i1][j1], u2 = t[3][2][i2][j2];
+    double v = u0 * s1 * s2 + s0 * u1 * s2 + s0 * s1 * u2;
+    v += (l0 * r1 + r0 * l1) * s2 + (l0 * r2 + r0 * l2) * s1 + (l1 * r2 + r1 * l2) * s0;
+    return pref * v;
+  };
+#pragma unroll
+  for (int s1 = 0; s1 < nsh(LA); ++s1)
+#pragma unroll
+    for (int s2 = 0; s2 < nsh(LB); ++s2) {
+      double v = 0.0;
+#pragma unroll
+      for (int k1 = 0; k1 < 3; ++k1) {
+        if (k1 >= sh_nterm(s1)) break;
+#pragma unroll
+        for (int k2 = 0; k2 < 3; ++k2) {
+          if (k2 >= sh_nterm(s2)) break;
+          v += sh_coef(s1, k1) * sh_coef(s2, k2) * cart(sh_cart(s1, k1), sh_cart(s2, k2));
+        }
+      }
+      out[s1 * nsh(LB) + s2] = v;
+    }
 }
 
 // ---------------------------------------------- McMurchie-Davidson 3C --
@@ -434,6 +534,55 @@ static __device__ __noinline__ void prim2c_rt(int la, int lb, bool kin, double a
             S[0][ax][bx] * S[1][ay][by] * T[2][az][bz];
       else
         v = S[0][ax][bx] * S[1][ay][by] * S[2][az][bz];
+      pc[p * ncb + q] = pref * v;
+    }
+  cart_to_sh_rt(la, lb, pc, out);
+}
+
+// prim_mv for the f classes, with runtime loops over tables in local
+// memory (a fully unrolled f-d or f-f block does not fit the registers).
+static __device__ __noinline__ void prim_mv_rt(int la, int lb, double a1,
+                                               double a2, const double *A,
+                                               const double *B, double scale,
+                                               double *out) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  double t[4][3][4][4];
+  double d2 = 0.0;
+#pragma unroll 1
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    const double X = A[x] - B[x];
+    d2 += X * X;
+    double S[6][6];
+    os1d<5, 5>(P - A[x], P - B[x], inv2p, S);
+#pragma unroll 1
+    for (int i = 0; i <= la; ++i)
+#pragma unroll 1
+      for (int j = 0; j <= lb; ++j) {
+        t[0][x][i][j] = S[i][j];
+        t[1][x][i][j] = d2_left<5, 5>(S, i, j, a1);
+        t[2][x][i][j] = d2_right<5, 5>(S, i, j, a2);
+        t[3][x][i][j] = d2_both<5, 5>(S, i, j, a1, a2);
+      }
+  }
+  const double pref = scale * pow(kPi / zeta, 1.5) * exp(-xi * d2);
+  double pc[ncart(3) * ncart(3)];
+  const int nca = ncart(la), ncb = ncart(lb);
+#pragma unroll 1
+  for (int p = 0; p < nca; ++p)
+#pragma unroll 1
+    for (int q = 0; q < ncb; ++q) {
+      double s[3], l[3], r[3], u[3];
+      for (int x = 0; x < 3; ++x) {
+        const int i = cart_exp(p, x), j = cart_exp(q, x);
+        s[x] = t[0][x][i][j];
+        l[x] = t[1][x][i][j];
+        r[x] = t[2][x][i][j];
+        u[x] = t[3][x][i][j];
+      }
+      double v = u[0] * s[1] * s[2] + s[0] * u[1] * s[2] + s[0] * s[1] * u[2];
+      v += (l[0] * r[1] + r[0] * l[1]) * s[2] + (l[0] * r[2] + r[0] * l[2]) * s[1] +
+           (l[1] * r[2] + r[1] * l[2]) * s[0];
       pc[p * ncb + q] = pref * v;
     }
   cart_to_sh_rt(la, lb, pc, out);

@@ -29,7 +29,7 @@ from .system import ImagoDimsC
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libimago_b200.so")
 
-IMAGO_OL, IMAGO_KE, IMAGO_NP, IMAGO_EP = 1, 2, 4, 8
+IMAGO_OL, IMAGO_KE, IMAGO_NP, IMAGO_EP, IMAGO_MV = 1, 2, 4, 8, 16
 IMAGO_ERR_NO_DEVICE = 7
 
 _LIB = None
@@ -51,7 +51,8 @@ class ImagoOptsC(ctypes.Structure):
 
 class ImagoOutC(ctypes.Structure):
     _fields_ = [("ol_packed", _D), ("ol_cv_re", _D), ("ol_cv_im", _D),
-                ("ke_packed", _D), ("np_packed", _D), ("ep_packed", _D)]
+                ("ke_packed", _D), ("np_packed", _D), ("ep_packed", _D),
+                ("mv_packed", _D)]
 
 
 def lib():
@@ -69,10 +70,12 @@ def lib():
         L.imago_intg_dims.restype = ctypes.c_int
         L.imago_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
         L.imago_gauss_overlap_ol.restype = ctypes.c_int
-        for n in ("imago_gauss_overlap_ke", "imago_gauss_overlap_np",
+        for n in ("imago_gauss_overlap_ke", "imago_gauss_overlap_np", "imago_gauss_overlap_mv",
                   "imago_elec_pot_gauss_overlap"):
             getattr(L, n).argtypes = [ctypes.c_void_p, _D]
             getattr(L, n).restype = ctypes.c_int
+        L.imago_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int, _D]
+        L.imago_ham_pscf.restype = ctypes.c_int
         L.imago_elec_pot_gauss_overlap_range.argtypes = [ctypes.c_void_p, ctypes.c_int,
                                                          ctypes.c_int, _D]
         L.imago_elec_pot_gauss_overlap_range.restype = ctypes.c_int
@@ -150,7 +153,7 @@ def kpoint_mesh(n, shift=(0.0, 0.0, 0.0)):
 
 
 PRIM_KINDS = {"overlap": 0, "kinetic": 1, "electron3c": 2, "nuclear3c": 3,
-              "boys": 4}
+              "boys": 4, "massvel": 5}
 
 
 def prim_eval(kind, params, cls=None):
@@ -193,7 +196,7 @@ def prim_eval_static(kind, params, cls=None):
 
 
 _OUT_NAMES = ("ol_packed", "ol_cv_re", "ol_cv_im", "ke_packed", "np_packed",
-              "ep_packed")
+              "ep_packed", "mv_packed")
 
 
 def _out_struct(out):
@@ -278,6 +281,34 @@ class IntegralSetup:
         _check(lib().imago_gauss_overlap_np(self._ctx, _p(out)), "gaussOverlapNP")
         return out
 
+    def gauss_overlap_mv(self):
+        """Mass velocity (imago_gauss_overlap_mv), the scalar-relativistic
+        term of rel = 1 runs; needs the overlap first when coreDim > 0."""
+        out = self._packed()
+        _check(lib().imago_gauss_overlap_mv(self._ctx, _p(out)), "gaussOverlapMV")
+        return out
+
+    def ham_pscf(self, coeffs, rel=False, out=None):
+        """The PSCF Hamiltonian (imago_ham_pscf): coeffs [potDim] or
+        [potDim, spin] -> [spin, nk, nPacked, 2]; kinetic + nuclear +
+        coefficient-weighted potential terms, minus mass velocity when rel.
+        `out` a device pointer/tensor for outputs_on_device contexts."""
+        c = np.asarray(coeffs, dtype=np.float64)
+        if c.ndim == 1:
+            c = c[:, None]
+        if c.shape[0] != self.pot_dim or c.shape[1] not in (1, 2):
+            raise ValueError("coeffs must be [potDim] or [potDim, spin]")
+        spin = c.shape[1]
+        cf = np.ascontiguousarray(c.T)  # potCoeffs(potDim, spin) column-major
+        if out is None:
+            out = self._packed(spin)
+        ptr = (ctypes.cast(ctypes.c_void_p(out), _D) if isinstance(out, int) else
+               ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D) if hasattr(out, "data_ptr")
+               else _p(out))
+        _check(lib().imago_ham_pscf(self._ctx, spin, _p(cf), 1 if rel else 0, ptr),
+               "gaussOverlapHamPSCF")
+        return out
+
     def elec_pot_gauss_overlap(self):
         out = self._packed(self.pot_dim)
         _check(lib().imago_elec_pot_gauss_overlap(self._ctx, _p(out)),
@@ -299,8 +330,9 @@ class IntegralSetup:
     # -- all matrices in one call --
     def build(self, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP, out=None):
         """Run the selected builds.  `out` maps ol_packed, ol_cv_re, ol_cv_im,
-        ke_packed, np_packed, ep_packed to numpy arrays (host outputs) or
-        integer device pointers (outputs_on_device).  Returns `out`."""
+        ke_packed, np_packed, ep_packed (and mv_packed with IMAGO_MV) to
+        numpy arrays (host outputs) or integer device pointers
+        (outputs_on_device).  Returns `out`."""
         if out is None:
             out = {}
             if which & IMAGO_OL:
@@ -314,6 +346,8 @@ class IntegralSetup:
                 out["np_packed"] = self._packed()
             if which & IMAGO_EP:
                 out["ep_packed"] = self._packed(self.pot_dim)
+            if which & IMAGO_MV:
+                out["mv_packed"] = self._packed()
         s = _out_struct(out)
         _check(lib().imago_intg_build(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build")
@@ -368,6 +402,8 @@ class IntegralSetup:
             n += per
         if which & IMAGO_EP:
             n += per * self.pot_dim
+        if which & IMAGO_MV:
+            n += per
         return n
 
 
@@ -403,7 +439,8 @@ class IntegralBatch:
                             max(d.core_dim, 1), d.pot_dim)
         return {"ol_packed": (nk, npk, 2), "ol_cv_re": (nk, V, C),
                 "ol_cv_im": (nk, V, C), "ke_packed": (nk, npk, 2),
-                "np_packed": (nk, npk, 2), "ep_packed": (P, nk, npk, 2)}
+                "np_packed": (nk, npk, 2), "ep_packed": (P, nk, npk, 2),
+                "mv_packed": (nk, npk, 2)}
 
     def build(self, outs, which=IMAGO_OL | IMAGO_KE | IMAGO_NP | IMAGO_EP):
         """`outs[i]` maps output names of cell i to device pointers or CUDA

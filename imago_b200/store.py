@@ -3,7 +3,8 @@ reference's SCF integral file.
 
 The reference writes its integrals to HDF5 (hdf5SCFIntg.F90:188-460): a
 group atomIntgGroup holding atomOverlap, atomOverlapCV (when coreDim > 0),
-atomKEOverlap, atomNPOverlap and atomPotOverlap/<term>, one dataset per
+atomKEOverlap, atomMVOverlap (scalar-relativistic runs), atomNPOverlap and
+atomPotOverlap/<term>, one dataset per
 k-point named by its 1-based index ("%07d"; coreValeOL as "real%07d" and
 "imag%07d"), and an integer attribute "status" on each group that is set
 to 1 once the group's datasets are written.  setupSCF skips every matrix
@@ -24,8 +25,8 @@ import os
 import numpy as np
 
 GROUP = "atomIntgGroup"
-OL, CV, KE, NP, EP = ("atomOverlap", "atomOverlapCV", "atomKEOverlap",
-                      "atomNPOverlap", "atomPotOverlap")
+OL, CV, KE, MV, NP, EP = ("atomOverlap", "atomOverlapCV", "atomKEOverlap",
+                          "atomMVOverlap", "atomNPOverlap", "atomPotOverlap")
 
 
 def _name(i):
@@ -113,12 +114,14 @@ class IntegralStore:
         return re, im
 
 
-def build_checkpointed(setup, store, ep_batch=8, on_group=None):
-    """Run, in the reference's order, the builds whose status in `store` is
-    not yet 1, writing each group's datasets and then its status.
+def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False):
+    """Run, in the reference's order (imago.F90:260-293: OL, KE, MV when
+    rel, NP, EP), the builds whose status in `store` is not yet 1, writing
+    each group's datasets and then its status.
 
     `setup` is an IntegralSetup with host outputs (or anything with its
-    gauss_overlap_ol / _ke / _np and elec_pot_gauss_overlap_range methods).
+    gauss_overlap_ol / _ke / _mv / _np and elec_pot_gauss_overlap_range
+    methods).
     The overlap is rebuilt on the device whenever a later matrix still has
     to be built and coreDim > 0 (their orthogonalisation needs its
     coreValeOL), but written only if its own status is 0.  EP terms missing
@@ -134,7 +137,11 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None):
             on_group(group)
 
     ep_todo = [t for t in range(store.pot_dim) if store.status(store.ep_group(t)) == 0]
-    later = store.status(KE) == 0 or store.status(NP) == 0 or bool(ep_todo)
+    singles = [(KE, setup.gauss_overlap_ke)]
+    if rel:
+        singles.append((MV, setup.gauss_overlap_mv))
+    singles.append((NP, setup.gauss_overlap_np))
+    later = any(store.status(g) == 0 for g, _ in singles) or bool(ep_todo)
     if store.status(OL) == 0 or (later and store.core_dim > 0):
         ol, re, im = setup.gauss_overlap_ol()
         if store.status(OL) == 0:
@@ -142,7 +149,7 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None):
             if store.core_dim > 0:
                 store.write_cv(re, im)
             done(OL)
-    for group, call in ((KE, setup.gauss_overlap_ke), (NP, setup.gauss_overlap_np)):
+    for group, call in singles:
         if store.status(group) == 0:
             store.write_packed(group, call())
             done(group)
@@ -161,13 +168,16 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None):
     return written
 
 
-def read_all(store):
+def read_all(store, rel=False):
     """Every matrix of a complete store: {"ol_packed", "ol_cv_re",
-    "ol_cv_im", "ke_packed", "np_packed", "ep_packed"} as numpy arrays."""
+    "ol_cv_im", "ke_packed", "np_packed", "ep_packed"}, and "mv_packed"
+    when rel, as numpy arrays."""
     out = {"ol_packed": store.read_packed(OL), "ke_packed": store.read_packed(KE),
            "np_packed": store.read_packed(NP),
            "ep_packed": np.stack([store.read_packed(store.ep_group(t))
                                   for t in range(store.pot_dim)])}
     if store.core_dim > 0:
         out["ol_cv_re"], out["ol_cv_im"] = store.read_cv()
+    if rel:
+        out["mv_packed"] = store.read_packed(MV)
     return out

@@ -64,7 +64,8 @@ enum imago_matrix {
   IMAGO_OL = 1u, /* overlap, timeStamp 8 */
   IMAGO_KE = 2u, /* kinetic energy, timeStamp 9 */
   IMAGO_NP = 4u, /* nuclear potential, timeStamp 10 */
-  IMAGO_EP = 8u  /* every electronic potential term, timeStamp 11 */
+  IMAGO_EP = 8u, /* every electronic potential term, timeStamp 11 */
+  IMAGO_MV = 16u /* mass velocity (rel = 1 only), timeStamp 30 */
 };
 
 /*
@@ -131,6 +132,7 @@ typedef struct imago_out {
   double *ke_packed; /* [nk][nPacked][2] */
   double *np_packed; /* [nk][nPacked][2] */
   double *ep_packed; /* [potDim][nk][nPacked][2] */
+  double *mv_packed; /* [nk][nPacked][2], IMAGO_MV only */
 } imago_out;
 
 /* Sizes of a created context. */
@@ -174,6 +176,23 @@ IMAGO_API int imago_gauss_overlap_ke(imago_ctx *ctx, double *packed);
 /* Nuclear potential: replaces gaussOverlapNP + nuclearPE + ortho(3)
  * (integrals.F90:1531-1942, 2533-2698). */
 IMAGO_API int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
+
+/* Mass velocity, the scalar-relativistic term the reference builds when
+ * rel == 1: replaces gaussOverlapMV + ortho(5) (integrals.F90:1091-1527,
+ * called at imago.F90:270-275).  The kinetic build's screening and lattice
+ * sums with massVel2CIntg accumulated negatively.  Needs the overlap first
+ * when coreDim > 0. */
+IMAGO_API int imago_gauss_overlap_mv(imago_ctx *ctx, double *packed);
+
+/* The PSCF Hamiltonian: replaces gaussOverlapHamPSCF + orthoHamPSCF
+ * (integrals.F90:2860-3606, 3913-4043; called at imago.F90:685).  One
+ * matrix per spin: kinetic + nuclear + sum_t coeffs(t, q) EP_t, minus the
+ * mass velocity when rel != 0, orthogonalised like KE.  coeffs is the
+ * reference's potCoeffs(potDim, spin), column-major: coeffs[q * potDim + t].
+ * packed: [spin][nk][nPacked][2].  spin is 1 or 2.  Needs the overlap first
+ * when coreDim > 0. */
+IMAGO_API int imago_ham_pscf(imago_ctx *ctx, int spin, const double *coeffs, int rel,
+                             double *packed);
 
 /* Every electronic potential term: replaces elecPotGaussOverlap,
  * gaussOverlapEP, electronicPE and ortho(4) for all potDim terms
@@ -296,7 +315,7 @@ IMAGO_API int imago_kpoint_mesh(const int n[3], const double shift[3],
  * reference's generated primitives (gaussIntegrals.f90).  kind: 0 overlap
  * (overlap2CIntg), 1 kinetic (kinetic2CIntg), 2 three-centre overlap
  * (electron3CIntg), 3 three-centre nuclear (nuclear3CIntg), 4 Boys function
- * (boys, F_0..F_6 of params[0]).  Record r reads
+ * (boys, F_0..F_6 of params[0]), 5 mass velocity (massvel2CIntg).  Record r reads
  *   params[r*12 + 0..11] = a1, a2, a3, A[3], B[3], C[3]
  * and cls[2*r + 0..1] = l of atom 1 and atom 2 (0..3); it writes
  * sh[r*256 + i*16 + j] = reference sh(i+1, j+1).  Host pointers.

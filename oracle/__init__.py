@@ -31,7 +31,7 @@ def lib():
         if not os.path.exists(path):
             build()
         L = ctypes.CDLL(path)
-        for name in ("orc_overlap2c", "orc_kinetic2c"):
+        for name in ("orc_overlap2c", "orc_kinetic2c", "orc_massvel2c"):
             f = getattr(L, name)
             f.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D,
                           ctypes.c_int, ctypes.c_int, _D]
@@ -55,6 +55,9 @@ def lib():
         L.orc_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
         L.orc_gauss_overlap_ke.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_np.argtypes = [ctypes.c_void_p, _D]
+        L.orc_gauss_overlap_mv.argtypes = [ctypes.c_void_p, _D]
+        L.orc_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D,
+                                   ctypes.c_int, _D]
         L.orc_elec_pot_gauss_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int,
                                                  ctypes.c_int, _D]
         L.orc_last_times.argtypes = [ctypes.c_void_p, _D, _D]
@@ -78,7 +81,7 @@ def _p(a):
 
 def primitive(kind, la, lb, a1, a2, a3, A, B, C):
     """Reference-layout sh block (nsh(la) x nsh(lb)) from the oracle.
-    kind: overlap, kinetic, electron3c, nuclear3c."""
+    kind: overlap, kinetic, massvel, electron3c, nuclear3c."""
     L = lib()
     sh = np.zeros(256)
     A = np.ascontiguousarray(A, float)
@@ -88,6 +91,8 @@ def primitive(kind, la, lb, a1, a2, a3, A, B, C):
         L.orc_overlap2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
     elif kind == "kinetic":
         L.orc_kinetic2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
+    elif kind == "massvel":
+        L.orc_massvel2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
     elif kind == "electron3c":
         L.orc_electron3c(a1, a2, a3, _p(A), _p(B), _p(C), la, lb, _p(sh))
     elif kind == "nuclear3c":
@@ -150,6 +155,24 @@ class OracleBuild:
         out = self._packed()
         self._check(lib().orc_gauss_overlap_ke(self._ctx, _p(out)), "KE")
         return out[0]
+
+    def mass_velocity(self):
+        out = self._packed()
+        self._check(lib().orc_gauss_overlap_mv(self._ctx, _p(out)), "MV")
+        return out[0]
+
+    def ham_pscf(self, coeffs, rel=False):
+        """gaussOverlapHamPSCF: coeffs [potDim] or [potDim, spin] ->
+        [spin, nk, np, 2]."""
+        coeffs = np.asarray(coeffs, dtype=np.float64)
+        if coeffs.ndim == 1:
+            coeffs = coeffs[:, None]
+        spin = coeffs.shape[1]
+        cf = np.ascontiguousarray(coeffs.T)  # potCoeffs(potDim, spin)
+        out = self._packed(spin)
+        self._check(lib().orc_ham_pscf(self._ctx, spin, _p(cf), 1 if rel else 0,
+                                       _p(out)), "HamPSCF")
+        return out
 
     def nuclear(self):
         out = self._packed()

@@ -31,6 +31,8 @@ void orc_overlap2c(double a1, double a2, const double *A, const double *B,
                    int la, int lb, double *sh);
 void orc_kinetic2c(double a1, double a2, const double *A, const double *B,
                    int la, int lb, double *sh);
+void orc_massvel2c(double a1, double a2, const double *A, const double *B,
+                   int la, int lb, double *sh);
 void orc_electron3c(double a1, double a2, double a3, const double *A,
                     const double *B, const double *C, int la, int lb,
                     double *sh);
@@ -55,6 +57,12 @@ int orc_gauss_overlap_ol(orc_ctx *c, double *packed, double *cv_re,
                          double *cv_im);
 int orc_gauss_overlap_ke(orc_ctx *c, double *packed);
 int orc_gauss_overlap_np(orc_ctx *c, double *packed);
+/* Mass velocity (rel = 1 runs only). */
+int orc_gauss_overlap_mv(orc_ctx *c, double *packed);
+/* The PSCF Hamiltonian: packed [spin][nk][np][2]; coeffs the reference's
+ * potCoeffs(potDim, spin), column-major: coeffs[q * potDim + t]. */
+int orc_ham_pscf(orc_ctx *c, int spin, const double *coeffs, int rel,
+                 double *packed);
 /* Terms [term_lo, term_hi) of the potDim electronic potential terms;
  * packed holds (term_hi - term_lo) matrices. */
 int orc_elec_pot_gauss_overlap(orc_ctx *c, int term_lo, int term_hi,

@@ -529,7 +529,7 @@ void orc_last_counts(const orc_ctx *c, long long *pi, long long *sp,
 
 /* ---------- the integral builds ---------- */
 
-enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3 };
+enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3, K_MV = 4, K_HAM = 5 };
 
 typedef struct {
   /* global matrices for one build (complex, column-major like Fortran) */
@@ -547,6 +547,8 @@ typedef struct {
   int ptype;    /* EP: pot type */
   int pterm;    /* EP: alpha index within the type */
   unsigned char *anyint; /* EP: [i][j][cell] interaction bits */
+  const double *coeffs;  /* HAM: potCoeffs(potDim, spin), column-major */
+  int spin, q, rel;      /* HAM: spins, the spin built, mass velocity */
 } buildspec;
 
 /* saveCurrentPair, intgSaving.F90:346-459 with valeValeSaving 463-510,
@@ -686,6 +688,87 @@ static int three_centre(const orc_ctx *c, const buildspec *bs, int e1, int e2,
   return contrib;
 }
 
+/* The PSCF Hamiltonian of one alpha pair for spin q, gaussOverlapHamPSCF
+ * (integrals.F90:3240-3442): for the first site of each potential type
+ * (potSites%firstPotType), each of the type's alphas weighted by its
+ * potCoeffs entry and then the nuclear term weighted by -Z (skipped when
+ * Z < smallThresh), over the type's sites and their lattice images within
+ * the inline radius logBasisFnThresh (1 - r2/alphaDist) (a1+a2+a3)/(a1+a2)/a3
+ * (3297-3306, evaluated left to right); then + kinetic and, when rel,
+ * - mass velocity (3444-3490).  potCoeffIndex runs over the types' alphas
+ * in that order, which is the EP term order. */
+static void ham_pscf_pair(const orc_ctx *c, const buildspec *bs, int e1, int e2,
+                          int a, int b, double alpha1, double alpha2, double r2,
+                          const double *A, const double *Bp, int la, int lb,
+                          double *acc, long long *ntrip) {
+  double cen = ACENT(c, e1, e2, a, b);
+  double P[3];
+  for (int x = 0; x < 3; ++x) P[x] = cen * (A[x] - Bp[x]) + Bp[x];
+  const int n1 = (la + 1) * (la + 1), n2 = (lb + 1) * (lb + 1);
+  double sh[256];
+  memset(acc, 0, sizeof(double) * 256);
+  int coeff_index = 0;
+  for (int m = 0; m < c->nps; ++m) {
+    if (!c->psite_first[m]) continue;
+    const optype *pt = &c->ptypes[c->psite_type[m]];
+    for (int n = 0; n <= pt->nalpha; ++n) {
+      double coeff = 0.0, alpha3;
+      if (n < pt->nalpha) {
+        coeff = bs->coeffs[(size_t)bs->q * c->pot_dim + coeff_index];
+        ++coeff_index;
+        alpha3 = pt->alphas[n];
+      } else {
+        if (pt->Z < SMALL_THRESH) continue;
+        alpha3 = pt->nucalpha;
+      }
+      double t = c->T * (1 - r2 / ADIST(c, e1, e2, a, b)) * (alpha1 + alpha2 + alpha3) /
+                 (alpha1 + alpha2) / alpha3;
+      for (int o = 0; o < pt->multiplicity; ++o) {
+        const double *Cp = c->psite_pos + 3 * (m + o);
+        double d[3], L2[3], v[3];
+        for (int x = 0; x < 3; ++x) d[x] = P[x] - Cp[x];
+        nearest_lattice(c, d, L2);
+        double c0 = 0.0;
+        for (int x = 0; x < 3; ++x) {
+          v[x] = P[x] - Cp[x] - L2[x];
+          c0 += v[x] * v[x];
+        }
+        if (c0 > t) continue;
+        double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+        for (int p = 0; p < c->ncell; ++p) {
+          if (c->csize[p] > maxr) break;
+          const double *R = c->cell + 3 * p;
+          double sc = (v[0] - R[0]) * (v[0] - R[0]) + (v[1] - R[1]) * (v[1] - R[1]) +
+                      (v[2] - R[2]) * (v[2] - R[2]);
+          if (sc > t) continue;
+          double Cs[3];
+          for (int x = 0; x < 3; ++x) Cs[x] = Cp[x] + L2[x] + R[x];
+          ++*ntrip;
+          if (n < pt->nalpha) {
+            orc_electron3c(alpha1, alpha2, alpha3, A, Bp, Cs, la, lb, sh);
+            for (int i = 0; i < n1; ++i)
+              for (int j = 0; j < n2; ++j)
+                acc[i * 16 + j] = acc[i * 16 + j] + sh[i * 16 + j] * coeff;
+          } else {
+            orc_nuclear3c(alpha1, alpha2, alpha3, A, Bp, Cs, la, lb, sh);
+            for (int i = 0; i < n1; ++i)
+              for (int j = 0; j < n2; ++j)
+                acc[i * 16 + j] = acc[i * 16 + j] - sh[i * 16 + j] * pt->Z;
+          }
+        }
+      }
+    }
+  }
+  orc_kinetic2c(alpha1, alpha2, A, Bp, la, lb, sh);
+  for (int i = 0; i < n1; ++i)
+    for (int j = 0; j < n2; ++j) acc[i * 16 + j] = acc[i * 16 + j] + sh[i * 16 + j];
+  if (bs->rel) {
+    orc_massvel2c(alpha1, alpha2, A, Bp, la, lb, sh);
+    for (int i = 0; i < n1; ++i)
+      for (int j = 0; j < n2; ++j) acc[i * 16 + j] = acc[i * 16 + j] - sh[i * 16 + j];
+  }
+}
+
 /* The atom-pair x lattice x alpha-pair loop nest shared by gaussOverlapOL
  * (integrals.F90:151-652), gaussOverlapKE (656-1090), gaussOverlapNP
  * (1531-1942) and gaussOverlapEP (1946-2356). */
@@ -774,7 +857,15 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
               orc_overlap2c(t1->alphas[a], t2->alphas[b], A, Bp, la, lb, sh);
             else if (bs->kind == K_KE)
               orc_kinetic2c(t1->alphas[a], t2->alphas[b], A, Bp, la, lb, sh);
-            else {
+            else if (bs->kind == K_HAM)
+              ham_pscf_pair(c, bs, e1, e2, a, b, t1->alphas[a], t2->alphas[b], r2, A,
+                            Bp, la, lb, sh, &ntr);
+            else if (bs->kind == K_MV) {
+              /* accumulated with a minus sign (integrals.F90:1440-1447):
+               * a + (-x) c is a - x c exactly */
+              orc_massvel2c(t1->alphas[a], t2->alphas[b], A, Bp, la, lb, sh);
+              for (int q = 0; q < 256; ++q) sh[q] = -sh[q];
+            } else {
               contrib = three_centre(c, bs, e1, e2, a, b, t1->alphas[a],
                                      t2->alphas[b], r2, A, Bp, la, lb, sh,
                                      &ntr);
@@ -803,7 +894,10 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
             M[m1 * ms + m2] = s;
           }
         /* applyPhaseFactors, intgSaving.F90:132-189 */
-        if (max_a1 > 0 || bs->kind != K_OL)
+        /* gaussOverlapMV phases only pairs that used an alpha
+         * (integrals.F90:1458-1480), and gaussOverlapHamPSCF likewise
+         * (3519-3553), as gaussOverlapOL does */
+        if (max_a1 > 0 || (bs->kind != K_OL && bs->kind != K_MV && bs->kind != K_HAM))
           for (int kp = 0; kp < nk; ++kp) {
             double pr = c->phase[2 * ((size_t)kp * c->ncell + k)];
             double pi = c->phase[2 * ((size_t)kp * c->ncell + k) + 1];
@@ -1006,19 +1100,43 @@ static void reset_stats(orc_ctx *c) {
 int orc_gauss_overlap_ol(orc_ctx *c, double *packed, double *cv_re,
                          double *cv_im) {
   reset_stats(c);
-  buildspec bs = {K_OL, 0, 0, NULL};
+  buildspec bs = {K_OL, 0, 0, NULL, NULL, 0, 0, 0};
   return build_one(c, &bs, packed, cv_re, cv_im);
 }
 
 int orc_gauss_overlap_ke(orc_ctx *c, double *packed) {
   reset_stats(c);
-  buildspec bs = {K_KE, 0, 0, NULL};
+  buildspec bs = {K_KE, 0, 0, NULL, NULL, 0, 0, 0};
   return build_one(c, &bs, packed, NULL, NULL);
+}
+
+/* gaussOverlapMV, integrals.F90:1091-1527: the kinetic build's loops with
+ * massVel2CIntg, accumulated negatively, orthogonalised like KE (ortho
+ * opcode 5). */
+int orc_gauss_overlap_mv(orc_ctx *c, double *packed) {
+  reset_stats(c);
+  buildspec bs = {K_MV, 0, 0, NULL, NULL, 0, 0, 0};
+  return build_one(c, &bs, packed, NULL, NULL);
+}
+
+/* gaussOverlapHamPSCF + orthoHamPSCF, integrals.F90:2860-3606 and
+ * 3913-4043: one matrix per spin, each orthogonalised like KE. */
+int orc_ham_pscf(orc_ctx *c, int spin, const double *coeffs, int rel,
+                 double *packed) {
+  if (spin < 1 || spin > 2 || !coeffs) return IMAGO_ERR_INVALID;
+  reset_stats(c);
+  const size_t np = (size_t)c->vale_dim * (c->vale_dim + 1) / 2;
+  for (int q = 0; q < spin; ++q) {
+    buildspec bs = {K_HAM, 0, 0, NULL, coeffs, spin, q, rel};
+    int st = build_one(c, &bs, packed + (size_t)q * 2 * np * c->nk, NULL, NULL);
+    if (st) return st;
+  }
+  return IMAGO_OK;
 }
 
 int orc_gauss_overlap_np(orc_ctx *c, double *packed) {
   reset_stats(c);
-  buildspec bs = {K_NP, 0, 0, NULL};
+  buildspec bs = {K_NP, 0, 0, NULL, NULL, 0, 0, 0};
   return build_one(c, &bs, packed, NULL, NULL);
 }
 
@@ -1045,7 +1163,7 @@ int orc_elec_pot_gauss_overlap(orc_ctx *c, int term_lo, int term_hi,
       /* Terms before the sample are not run: their only effect on later
        * terms is the exact skip bits, which leave the values unchanged. */
       if (term < term_lo) continue;
-      buildspec bs = {K_EP, t, j, bits};
+      buildspec bs = {K_EP, t, j, bits, NULL, 0, 0, 0};
       double l0 = c->t_loops, o0 = c->t_ortho;
       long long a0 = c->n_pair_images, b0 = c->n_shell_pairs, t0 = c->n_triples;
       st = build_one(c, &bs, packed + 2 * np * c->nk * (size_t)(term - term_lo),

@@ -10,6 +10,7 @@
  *
  *   overlap2CIntg  (gaussIntegrals.f90:26-4420)    <a|b>
  *   kinetic2CIntg  (gaussIntegrals.f90:4422-11622) <a|-1/2 nabla^2|b>
+ *   massvel2CIntg  (gaussIntegrals.f90:39070-49402) (alpha^2/8)<a|nabla^4|b>
  *   electron3CIntg (gaussIntegrals.f90:11624-16023) <a|exp(-a3 r_C^2)|b>
  *   nuclear3CIntg  (gaussIntegrals.f90:16223-23039) <a|exp(-a3 r_C^2)/r_C|b>
  *
@@ -220,6 +221,77 @@ void orc_kinetic2c(double a1, double a2, const double *A, const double *B,
       double sx = S[0][u[0]][w[0]], sy = S[1][u[1]][w[1]], sz = S[2][u[2]][w[2]];
       double tx = T[0][u[0]][w[0]], ty = T[1][u[1]][w[1]], tz = T[2][u[2]][w[2]];
       pc[p][q] = pref * (tx * sy * sz + sx * ty * sz + sx * sy * tz);
+    }
+  cart_to_sh(pc, la, lb, sh);
+}
+
+/* Mass-velocity integral (alpha^2 / 8) <a|nabla^4|b>, alpha the fine
+ * structure constant 7.2973525693e-3 (constants.f90:47), the prefactor
+ * (fineStructure * 0.001)^2 / 8 of gaussIntegrals.f90:39118.  The reference
+ * builds it by a Cartesian recursion seeded with the s-s value
+ * 16 a2^4 <r_B^4> - 80 a2^3 <r_B^2> + 60 a2^2 (nabla^4 on the atom-2
+ * Gaussian).  Here it is the symmetric form <nabla^2 a|nabla^2 b>
+ * (two integrations by parts), summed over axis pairs:
+ *   sum_x U_x S_y S_z + sum_{x != y} L_x R_y S_z,
+ * with the 1D second derivative d^2 x^i e^{-a x^2} = i(i-1) x^{i-2}
+ * - 2a(2i+1) x^i + 4a^2 x^{i+2} applied on the left (L), the right (R) or
+ * both (U) of the overlap table.  The s-s seed cancels to a value of order
+ * a1 a2 when a1 << a2; the symmetric form carries that order in each term. */
+static void d2_coef(int i, double a, double c[3]) {
+  c[0] = i * (i - 1.0); /* x^{i-2} */
+  c[1] = -2.0 * a * (2 * i + 1);
+  c[2] = 4.0 * a * a;  /* x^{i+2} */
+}
+
+void orc_massvel2c(double a1, double a2, const double *A, const double *B,
+                   int la, int lb, double *sh) {
+  double zeta = a1 + a2, xi = a1 * a2 / zeta, d2 = 0.0;
+  double S[3][8][8], L[3][4][4], R[3][4][4], U[3][4][4];
+  for (int x = 0; x < 3; ++x) {
+    double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    d2 += (A[x] - B[x]) * (A[x] - B[x]);
+    os_1d(P - A[x], P - B[x], 1.0 / (2.0 * zeta), la + 2, lb + 2, S[x]);
+    for (int i = 0; i <= la; ++i)
+      for (int j = 0; j <= lb; ++j) {
+        double ca[3], cb[3], l = 0.0, r = 0.0, u = 0.0;
+        d2_coef(i, a1, ca);
+        d2_coef(j, a2, cb);
+        for (int p = 0; p < 3; ++p) {
+          int ii = i + 2 * p - 2;
+          if (ii < 0) continue;
+          l += ca[p] * S[x][ii][j];
+          for (int q = 0; q < 3; ++q) {
+            int jj = j + 2 * q - 2;
+            if (jj < 0) continue;
+            u += ca[p] * cb[q] * S[x][ii][jj];
+          }
+        }
+        for (int q = 0; q < 3; ++q) {
+          int jj = j + 2 * q - 2;
+          if (jj >= 0) r += cb[q] * S[x][i][jj];
+        }
+        L[x][i][j] = l;
+        R[x][i][j] = r;
+        U[x][i][j] = u;
+      }
+  }
+  const double fs = 7.2973525693 * 0.001;
+  double pref = fs * fs / 8.0 * pow(ORC_PI / zeta, 1.5) * exp(-xi * d2);
+  double pc[20][20];
+  for (int p = 0; p < NCART[la]; ++p)
+    for (int q = 0; q < NCART[lb]; ++q) {
+      const int *u = CART[p], *w = CART[q];
+      double s[3], l[3], r[3], uu[3];
+      for (int x = 0; x < 3; ++x) {
+        s[x] = S[x][u[x]][w[x]];
+        l[x] = L[x][u[x]][w[x]];
+        r[x] = R[x][u[x]][w[x]];
+        uu[x] = U[x][u[x]][w[x]];
+      }
+      double v = uu[0] * s[1] * s[2] + s[0] * uu[1] * s[2] + s[0] * s[1] * uu[2];
+      v += (l[0] * r[1] + r[0] * l[1]) * s[2] + (l[0] * r[2] + r[0] * l[2]) * s[1] +
+           (l[1] * r[2] + r[1] * l[2]) * s[0];
+      pc[p][q] = pref * v;
     }
   cart_to_sh(pc, la, lb, sh);
 }

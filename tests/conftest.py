@@ -56,3 +56,18 @@ def packed_mismatch(got, ref, atol=ATOL):
            ((ref == 0.0) & (np.abs(got) < ZERO_THRESH + atol))
     d = np.where(flip, 0.0, d)
     return float(d.max()) if d.size else 0.0, int((d > atol).sum())
+
+
+FINE_STRUCTURE = 7.2973525693e-3  # constants.f90:47 (stored there x 1000)
+
+
+def massvel_scale(r):
+    """The size the reference's own massvel2CIntg rounds at.  It seeds its
+    recursion with 16 a2^4 <r_B^4> - 80 a2^3 <r_B^2> + 60 a2^2
+    (gaussIntegrals.f90:39118-39120), terms of order alpha^2/8 a^2 S that
+    cancel to a value of order a1 a2 when a1 << a2, so its rounding is
+    relative to alpha^2/8 max(a1, a2)^2 |S|, not to the result."""
+    import oracle
+    S = oracle.primitive("overlap", r["la"], r["lb"], r["a1"], r["a2"], 0.0,
+                         r["A"], r["B"], r["B"])
+    return FINE_STRUCTURE ** 2 / 8 * max(r["a1"], r["a2"]) ** 2 * np.abs(S).max()

@@ -2,10 +2,10 @@
 own generated kernels.
 
 The reference's primitive integrals live in `src/imago/gaussIntegrals.f90`
-(overlap2CIntg 26-4420, kinetic2CIntg 4422-11622, electron3CIntg
-11624-16023, boys 16080-16221, nuclear3CIntg 16223-23039).  No Fortran
-compiler exists where this script runs, so the script transliterates those
-subroutines statement by statement into Python and executes them with IEEE
+(overlap2CIntg 26-4420, kinetic2CIntg 4422-11622, massvel2CIntg
+39070-49402, electron3CIntg 11624-16023, boys 16080-16221, nuclear3CIntg
+16223-23039).  No Fortran compiler exists where this script runs, so the
+script transliterates those subroutines statement by statement into Python and executes them with IEEE
 double arithmetic, which is what gfortran -O3 (no -ffast-math, no FMA on
 x86-64 baseline) evaluates.  Fortran semantics that matter for the values
 are kept:
@@ -40,6 +40,7 @@ KERNEL_LINES = {
     "electron3CIntg": (11624, 16023),
     "boys": (16080, 16221),
     "nuclear3CIntg": (16223, 23039),
+    "massvel2CIntg": (39070, 49402),
 }
 
 # Class codes built by integrals.F90:533-536: bit 0..3 for atom 1 (s,p,d,f),
@@ -127,9 +128,41 @@ def _powi(x, n):
 POWI_TABLE = [0, 1, 1, 2, 2, 3, 3, 4, 4, 6, 5, 6, 6, 10, 7, 9, 8]
 
 INT_POW = re.compile(r"(\b[A-Za-z_]\w*)\s*\*\*\s*(?:\(\s*(\d+)\s*\)|(\d+))(?![\w.])")
+SLICE_POW = re.compile(r"(\b[A-Za-z_]\w*)\(:\)\s*\*\*\s*(\d+)(?![\w.])")
+PAREN_POW = re.compile(r"\)\s*\*\*\s*(\d+)(?![\w.])")
+
+
+def _apowi(x, n):
+    """Whole-array NAME(:)**n: the same chain per element."""
+    return np.array([_powi(float(v), n) for v in x])
+
+
+def _paren_pow(expr):
+    """(expr)**n with a constant integer n -> _powi((expr), n)."""
+    while True:
+        m = PAREN_POW.search(expr)
+        if not m:
+            return expr
+        depth, i = 0, m.start()
+        while True:
+            if expr[i] == ")":
+                depth += 1
+            elif expr[i] == "(":
+                depth -= 1
+                if depth == 0:
+                    break
+            i -= 1
+        # a function call's parentheses belong to the call: keep its name
+        j = i
+        while j > 0 and (expr[j - 1].isalnum() or expr[j - 1] == "_"):
+            j -= 1
+        expr = (expr[:j] + "_powi(" + expr[j:m.start() + 1] + ", "
+                + m.group(1) + ")" + expr[m.end():])
 
 
 def translate_expr(expr, arrays):
+    expr = SLICE_POW.sub(lambda m: f"_apowi({m.group(1)}, {m.group(2)})", expr)
+    expr = _paren_pow(expr)
     expr = INT_POW.sub(lambda m: f"_powi({m.group(1)}, {m.group(2) or m.group(3)})", expr)
     expr = expr.replace(".eq.", "==").replace(".ne.", "!=")
     expr = expr.replace(".lt.", "<").replace(".le.", "<=")
@@ -252,7 +285,9 @@ def load_kernels(ref_root):
         lines = fh.readlines()
     ns = {
         "FArr": FArr, "_ix": _ix, "f32": f32, "pi": 3.141592653589793,
-        "_powi": _powi,
+        "_powi": _powi, "_apowi": _apowi,
+        # constants.f90:47, a double-kind parameter
+        "fineStructure": float("7.2973525693"),
         "exp": math.exp, "sqrt": math.sqrt, "erf": math.erf, "sum": _fsum,
         "abs": abs, "float": float,
     }
@@ -320,6 +355,7 @@ def main():
                        "A": A, "B": B, "C": C}
                 rec["overlap"] = run_2c(ns, "overlap2CIntg", la, lb, a1, a2, A, B)
                 rec["kinetic"] = run_2c(ns, "kinetic2CIntg", la, lb, a1, a2, A, B)
+                rec["massvel"] = run_2c(ns, "massvel2CIntg", la, lb, a1, a2, A, B)
                 rec["electron3c"] = run_3c(ns, "electron3CIntg", la, lb,
                                            a1, a2, a3, A, B, C)
                 rec["nuclear3c"] = run_3c(ns, "nuclear3CIntg", la, lb,
@@ -381,8 +417,8 @@ def main():
         boys.append({"T": float(T), "F": [F[m] for m in range(1, 8)]})
     out = {
         "source": "src/imago/gaussIntegrals.f90 (overlap2CIntg, kinetic2CIntg,"
-                  " electron3CIntg, boys, nuclear3CIntg) executed statement by"
-                  " statement in IEEE double",
+                  " electron3CIntg, boys, nuclear3CIntg, massvel2CIntg)"
+                  " executed statement by statement in IEEE double",
         "generator": "tests/golden/make_golden.py",
         "records": records,
         "boys": boys,

@@ -105,3 +105,7 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_hermitian_eigvals(0, 1, None, None, None) == 1
     L.imago_secular_matrices.argtypes = [ctypes.c_int] * 3 + [vp] * 8
     assert L.imago_secular_matrices(0, 1, 0, *([None] * 8)) == 1
+    L.imago_gauss_overlap_mv.argtypes = [vp, vp]
+    assert L.imago_gauss_overlap_mv(None, None) == 1
+    L.imago_ham_pscf.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
+    assert L.imago_ham_pscf(None, 1, None, 0, None) == 1

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import packed_mismatch
+from conftest import FINE_STRUCTURE, massvel_scale, packed_mismatch
 from imago_b200 import configs, intg
 
 pytestmark = pytest.mark.gpu
@@ -36,6 +36,31 @@ def test_primitives_match_reference_kernels(imago_lib, golden, kind):
         # relative to the block's largest element; the device uses its own
         # recursions (Obara-Saika 2C, McMurchie-Davidson 3C) and FMA.
         assert np.abs(g[:n1, :n2] - ref).max() <= 1e-12 * scale, (kind, r["la"], r["lb"])
+        assert not np.any(g[n1:, :]) and not np.any(g[:, n2:])
+
+
+def test_massvel_primitives_match_reference_and_oracle(imago_lib, golden):
+    # against the reference's kernel at the size its own cancellation rounds
+    # at, and against the oracle (the same symmetric form) at 1e-12 of its
+    # terms, every class s..f on both sides
+    recs, params, cls = _golden_params(golden, "massvel")
+    got = intg.prim_eval("massvel", params, cls)
+    static = intg.prim_eval_static("massvel", params, cls)
+    assert np.array_equal(got, static)
+    for r, g in zip(recs, got):
+        ref = np.array(r["massvel"])
+        n1, n2 = ref.shape
+        assert np.abs(g[:n1, :n2] - ref).max() <= 1e-12 * massvel_scale(r), (r["la"], r["lb"])
+        orc = oracle.primitive("massvel", r["la"], r["lb"], r["a1"], r["a2"], 0.0,
+                               r["A"], r["B"], r["C"])
+        # the symmetric form's terms are of order alpha^2/8 a1 a2 S; when
+        # a1 << a2 they cancel by a2/a1 too, so rounding (FMA, order) is
+        # relative to that size
+        S = oracle.primitive("overlap", r["la"], r["lb"], r["a1"], r["a2"], 0.0,
+                             r["A"], r["B"], r["C"])
+        terms = FINE_STRUCTURE ** 2 / 8 * r["a1"] * r["a2"] * np.abs(S).max()
+        tol = 1e-12 * max(np.abs(orc).max(), terms)
+        assert np.abs(g[:n1, :n2] - orc).max() <= tol, (r["la"], r["lb"])
         assert not np.any(g[n1:, :]) and not np.any(g[:, n2:])
 
 
@@ -352,7 +377,8 @@ def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
     from imago_b200 import store as st
     s = configs.silicon_cubic8(kmesh=(2, 2, 2))
     with intg.IntegralSetup(s) as g:
-        ref = g.build()
+        ref = g.build(intg.IMAGO_OL | intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP
+                      | intg.IMAGO_MV)
         box = st.IntegralStore.for_setup(str(tmp_path), g)
 
         def stop(group):
@@ -360,12 +386,88 @@ def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
                 raise KeyboardInterrupt
 
         with pytest.raises(KeyboardInterrupt):
-            st.build_checkpointed(g, box, ep_batch=3, on_group=stop)
-        rest = st.build_checkpointed(g, box)
+            st.build_checkpointed(g, box, ep_batch=3, on_group=stop, rel=True)
+        rest = st.build_checkpointed(g, box, rel=True)
         assert rest[0] == box.ep_group(2)
-    got = st.read_all(box)
-    for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed"):
+    got = st.read_all(box, rel=True)
+    for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed", "mv_packed"):
         assert np.array_equal(ref[k], got[k]), k
     if g.core_dim > 0:
         assert np.array_equal(ref["ol_cv_re"], got["ol_cv_re"])
         assert np.array_equal(ref["ol_cv_im"], got["ol_cv_im"])
+
+
+@pytest.mark.parametrize("name", ["small", "f", "silicon8"])
+def test_mass_velocity_build_matches_oracle(imago_lib, name):
+    # gaussOverlapMV: the kinetic build's loops with the mass-velocity
+    # primitive accumulated negatively, orthogonalised like KE; the f system
+    # runs the runtime-class kernel
+    s = {"small": configs.small_test_system,
+         "f": configs.f_test_system,
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3))}[name]()
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    ref = ob.mass_velocity()
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        mv = g.gauss_overlap_mv()
+        both = g.build(intg.IMAGO_OL | intg.IMAGO_KE | intg.IMAGO_MV | intg.IMAGO_EP)
+    _assert_all({"MV": packed_mismatch(mv, ref)})
+    # on the kinetic lane after KE, staged after the EP terms: same values
+    assert np.array_equal(both["mv_packed"], mv)
+    assert np.abs(mv).max() > 0.0
+
+
+def test_mass_velocity_needs_overlap_first(imago_lib):
+    with intg.IntegralSetup(configs.small_test_system()) as g:
+        with pytest.raises(intg.ImagoError) as e:
+            g.gauss_overlap_mv()
+        assert e.value.status == 3
+
+
+@pytest.mark.parametrize("name,spin,rel", [("small", 1, False), ("small", 2, True),
+                                           ("f", 2, False), ("silicon8", 2, True)])
+def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
+    # gaussOverlapHamPSCF: kinetic + nuclear + potCoeffs-weighted potential
+    # terms (- mass velocity) per spin, against the oracle's restatement of
+    # its loop nest (inline screen radius, per-alpha-pair accumulation)
+    s = {"small": configs.small_test_system,
+         "f": configs.f_test_system,
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3))}[name]()
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    rng = np.random.default_rng(11)
+    coeffs = rng.normal(scale=0.5, size=(ob.pot_dim, spin))
+    ref = ob.ham_pscf(coeffs, rel=rel)
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        got = g.ham_pscf(coeffs, rel=rel)
+        # the same matrices from the separate builds, combined afterwards
+        lin = g.gauss_overlap_ke() + g.gauss_overlap_np() + np.tensordot(
+            coeffs.T, g.elec_pot_gauss_overlap(), axes=1)
+        if rel:
+            lin = lin + g.gauss_overlap_mv()
+    assert got.shape == ref.shape == (spin, g.nk, g.npacked, 2)
+    _assert_all({"H%d" % q: packed_mismatch(got[q], ref[q]) for q in range(spin)})
+    # each separate matrix had its |x| < 1e-10 zeroed by the packing
+    # (coreDim > 0), so the combination may differ by 1e-10 per matrix
+    # times its weight
+    _assert_all({"lin%d" % q: packed_mismatch(
+        got[q], lin[q], atol=1e-10 * (3 + np.abs(coeffs[:, q]).sum())) for q in range(spin)})
+
+
+def test_pscf_hamiltonian_device_outputs(imago_lib):
+    import torch
+    s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+    coeffs = np.linspace(-1.0, 1.0, 2 * 64).reshape(-1, 2)
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        host = g.ham_pscf(coeffs[:g.pot_dim])
+    with intg.IntegralSetup(s, outputs_on_device=True) as g:
+        sh = _shapes(g)
+        ol = _device_outputs(torch, {k: sh[k] for k in ("ol_packed", "ol_cv_re", "ol_cv_im")})
+        g.build(intg.IMAGO_OL, out=ol)
+        dev = torch.empty((2, g.nk, g.npacked, 2), dtype=torch.float64, device="cuda")
+        g.ham_pscf(coeffs[:g.pot_dim], out=dev)
+        torch.cuda.synchronize()
+    assert np.array_equal(host, dev.cpu().numpy())

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import massvel_scale
 
 KINDS = ("overlap", "kinetic", "electron3c", "nuclear3c")
 # Relative to the largest element of the block.  The oracle uses its own
@@ -57,3 +58,49 @@ def test_closed_forms_s_s():
     P = (a1 * A + a2 * B) / z
     E = (np.pi / z3) ** 1.5 * np.exp(-xi * d2 - z * a3 / z3 * ((P - C) ** 2).sum())
     assert oracle.primitive("electron3c", 0, 0, a1, a2, a3, A, B, C)[0, 0] == pytest.approx(E, rel=1e-14)
+
+
+def test_massvel_matches_reference_kernel(golden):
+    n = 0
+    for r in golden["records"]:
+        if "massvel" not in r:
+            continue
+        ref = np.array(r["massvel"])
+        got = oracle.primitive("massvel", r["la"], r["lb"], r["a1"], r["a2"],
+                               0.0, r["A"], r["B"], r["C"])
+        # observed <= 2.3e-13 of the scale over all 16 classes
+        assert np.abs(got - ref).max() <= 1e-12 * massvel_scale(r), (r["la"], r["lb"])
+        n += 1
+    assert n == 64
+
+
+def test_massvel_s_s_against_50_digit_value(golden):
+    # The closed s-s form in 50-digit arithmetic: the oracle's symmetric
+    # <nabla^2 a|nabla^2 b> keeps 1e-10 relative accuracy where the
+    # reference's seed has cancelled (a1 << a2), and agrees with the
+    # reference to rounding elsewhere.
+    mp = pytest.importorskip("mpmath")
+    mp.mp.dps = 50
+    fs = mp.mpf("7.2973525693") * mp.mpf("0.001")
+    n = 0
+    for r in golden["records"]:
+        if r["la"] or r["lb"] or "massvel" not in r:
+            continue
+        a1, a2 = mp.mpf(r["a1"]), mp.mpf(r["a2"])
+        A = [mp.mpf(x) for x in r["A"]]
+        B = [mp.mpf(x) for x in r["B"]]
+        z = a1 + a2
+        PB = [(a1 * A[i] + a2 * B[i]) / z - B[i] for i in range(3)]
+        d2 = sum((A[i] - B[i]) ** 2 for i in range(3))
+        S = (mp.pi / z) ** mp.mpf(1.5) * mp.exp(-a1 * a2 / z * d2)
+        p2 = sum(x ** 2 for x in PB)
+        r4 = (sum(x ** 4 for x in PB) + 3 * p2 / z + mp.mpf(9) / (4 * z ** 2)
+              + 2 * ((PB[0] * PB[1]) ** 2 + (PB[0] * PB[2]) ** 2
+                     + (PB[1] * PB[2]) ** 2 + p2 / z + mp.mpf(3) / (4 * z ** 2)))
+        exact = fs ** 2 / 8 * (16 * a2 ** 4 * r4 - 80 * a2 ** 3 * (p2 + 3 / (2 * z))
+                               + 60 * a2 ** 2) * S
+        got = oracle.primitive("massvel", 0, 0, r["a1"], r["a2"], 0.0, r["A"],
+                               r["B"], r["C"])[0, 0]
+        assert abs(got - float(exact)) <= 1e-10 * abs(float(exact))
+        n += 1
+    assert n >= 4

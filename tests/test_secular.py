@@ -78,3 +78,21 @@ def test_batched_jacobi_eigenvalues(imago_lib, n):
     got = secular.hermitian_eigvals(torch.as_tensor(h, device="cuda")).cpu().numpy()
     scale = max(1.0, np.abs(ref).max())
     assert np.abs(got - ref).max() <= 1e-12 * scale
+
+
+def test_oracle_pscf_hamiltonian_is_the_combination_of_its_parts():
+    # gaussOverlapHamPSCF sums kinetic, nuclear, potCoeffs-weighted
+    # potential terms and (rel) minus mass velocity per alpha pair; every
+    # later step is linear, so it equals the same combination of the
+    # separate builds up to rounding and the screen radius's evaluation
+    # order (an ulp of the radius)
+    s = configs.small_test_system()
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=(ob.pot_dim, 2))
+    h = ob.ham_pscf(w, rel=True)
+    lin = (ob.kinetic() + ob.nuclear() + ob.mass_velocity()
+           + np.tensordot(w.T, ob.elec_pot(), axes=1))
+    assert h.shape == lin.shape
+    assert np.abs(h - lin).max() <= 1e-12 * np.abs(lin).max()

@@ -32,6 +32,10 @@ class FakeSetup:
         self.calls.append("KE")
         return self._mat(1)
 
+    def gauss_overlap_mv(self):
+        self.calls.append("MV")
+        return self._mat(3)
+
     def gauss_overlap_np(self):
         self.calls.append("NP")
         return self._mat(2)
@@ -92,3 +96,15 @@ def test_store_refuses_another_system(tmp_path):
     _store(tmp_path, f)
     with pytest.raises(ValueError):
         st.IntegralStore(str(tmp_path), f.nk, f.np, f.P + 1, f.V, f.C)
+
+
+def test_relativistic_run_adds_mass_velocity_in_order(tmp_path):
+    f = FakeSetup()
+    s = _store(tmp_path, f)
+    written = st.build_checkpointed(f, s, rel=True)
+    assert written[:4] == [st.OL, st.KE, st.MV, st.NP]
+    assert f.calls[:4] == ["OL", "KE", "MV", "NP"]
+    assert np.array_equal(st.read_all(s, rel=True)["mv_packed"], f._mat(3))
+    # a later non-relativistic store of the same system skips MV entirely
+    f2 = FakeSetup()
+    assert st.build_checkpointed(f2, _store(tmp_path, f2)) == []
