@@ -7,11 +7,13 @@
 !    call gaussOverlapKE(...)      -> call b200GaussOverlapKE(...)
 !    call gaussOverlapMV(...)      -> call b200GaussOverlapMV(...)  (rel == 1)
 !    call gaussOverlapHamPSCF(...) -> call b200GaussOverlapHamPSCF(...)  (PSCF)
+!    call gaussOverlapDM(...)      -> call b200GaussOverlapDM(...)
+!    call gaussOverlapMM(...)      -> call b200GaussOverlapMM(...)
 !    call gaussOverlapNP(...)      -> call b200GaussOverlapNP(...)
 !    call elecPotGaussOverlap(...) -> call b200ElecPotGaussOverlap(...)
 !
-! (src/imago/imago.F90:262, 268, 274, 284, 293, 685), each with the same
-! arguments.
+! (src/imago/imago.F90:262, 268, 274, 284, 293, 312, 315, 685, 705, 709),
+! each with the same arguments.
 ! Each wrapper skips a matrix whose HDF5 "done" attribute is already 1, as
 ! the reference does, writes the packed valence-valence datasets per
 ! k-point (and coreValeOL for the overlap) and sets the attribute.
@@ -108,6 +110,21 @@ module O_ImagoB200
          type(c_ptr), value :: ctx
          integer(c_int), value :: spin, rel
          real(c_double), intent(in) :: coeffs(*)
+         real(c_double), intent(out) :: packed(*)
+         integer(c_int) :: st
+      end function
+      function imago_gauss_overlap_mm(ctx, packed) &
+            & bind(C, name="imago_gauss_overlap_mm") result(st)
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: packed(*)
+         integer(c_int) :: st
+      end function
+      function imago_gauss_overlap_dm(ctx, center, packed) &
+            & bind(C, name="imago_gauss_overlap_dm") result(st)
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: center(3)
          real(c_double), intent(out) :: packed(*)
          integer(c_int) :: st
       end function
@@ -453,6 +470,54 @@ contains
       enddo
       call markDone(aid)
    end subroutine b200GaussOverlapHamPSCF
+
+   ! gaussOverlapDM / gaussOverlapMM + ortho3Terms: the x, y, z matrices,
+   ! written to did(:,1..3) (integrals3Terms.F90:1538-1546).
+   subroutine b200ThreeTerms(which, valeValeDims, did, aid)
+      use O_KPoints, only: numKPoints
+      use O_AtomicSites, only: valeDim
+      use O_Input, only: dipoleCenter
+      integer, intent(in) :: which
+      integer(hsize_t), dimension(2), intent(in) :: valeValeDims
+      integer(hid_t), dimension(numKPoints,3), intent(in) :: did
+      integer(hid_t), intent(in) :: aid
+      real(c_double), allocatable :: packed(:,:,:,:)
+      real(c_double) :: center(3)
+      integer(hsize_t) :: np
+      integer :: j
+      integer(c_int) :: st
+      if (alreadyDone(aid)) return
+      np = int(valeDim, hsize_t) * (valeDim + 1) / 2
+      allocate (packed(2, np, numKPoints, 3))
+      if (which == 6) then
+         center(:) = dipoleCenter(:)
+         st = imago_gauss_overlap_dm(ctx, center, packed)
+      else
+         st = imago_gauss_overlap_mm(ctx, packed)
+      endif
+      if (st /= 0) call fail(st, 'gaussOverlapDM/MM')
+      do j = 1, 3
+         call writePacked(packed(:,:,:,j), 2, valeValeDims, did(:,j), &
+               & numKPoints, np)
+      enddo
+      call markDone(aid)
+   end subroutine b200ThreeTerms
+
+   subroutine b200GaussOverlapDM(valeValeDims, did, aid)
+      use O_KPoints, only: numKPoints
+      integer(hsize_t), dimension(2), intent(in) :: valeValeDims
+      integer(hid_t), dimension(numKPoints,3), intent(in) :: did
+      integer(hid_t), intent(in) :: aid
+      call b200ThreeTerms(6, valeValeDims, did, aid)
+   end subroutine b200GaussOverlapDM
+
+   subroutine b200GaussOverlapMM(valeValeDims, did, aid)
+      use O_KPoints, only: numKPoints
+      integer(hsize_t), dimension(2), intent(in) :: valeValeDims
+      integer(hid_t), dimension(numKPoints,3), intent(in) :: did
+      integer(hid_t), intent(in) :: aid
+      call b200ThreeTerms(7, valeValeDims, did, aid)
+   end subroutine b200GaussOverlapMM
 
    subroutine b200Cleanup()
       if (c_associated(ctx)) call imago_intg_destroy(ctx)

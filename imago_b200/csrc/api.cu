@@ -199,6 +199,10 @@ struct imago_ctx {
   // PSCF Hamiltonian: accumulated sh blocks per spin, the potential
   // coefficients, and the packed result when outputs go to the host
   DBuf<double> ham_blk, ham_w, ham_out;
+  // momentum / dipole: the dipole centre of the current call and the three
+  // packed matrices when outputs go to the host
+  double dip_center[3] = {0.0, 0.0, 0.0};
+  DBuf<double> vec_out;
   // CUDA-graph capture of the build: no timing events are recorded and EP
   // keeps the chunk size of the last eager build (scratch already sized)
   bool capturing = false;
@@ -231,7 +235,7 @@ struct imago_ctx {
       b->release(st);
     for (auto *b : {&d_alpha, &d_basis, &d_site_pos, &d_ptype_z,
                     &d_ptype_nucalpha, &d_palpha, &d_psite_pos, &d_cell,
-                    &d_csize, &d_kxyz, &out_stage, &ham_blk, &ham_w, &ham_out})
+                    &d_csize, &d_kxyz, &out_stage, &ham_blk, &ham_w, &ham_out, &vec_out})
       b->release(st);
     for (auto &sc : scr) {
       sc.blk.release(st);
@@ -846,6 +850,7 @@ int upload(imago_ctx *c) {
   s.far_lattice = 1.5 * smallest_singular(c->rv) * (1.0 - 1e-6);
   s.real_k = 1;
   for (double x : c->kxyz) s.real_k &= x == 0.0;
+  s.minus_i = 0;
   s.type_nalpha = c->d_type_nalpha.p; s.type_alpha_off = c->d_type_alpha_off.p;
   s.type_nstates = c->d_type_nstates.p; s.type_nvale = c->d_type_nvale.p;
   s.type_state_off = c->d_type_state_off.p; s.type_basis_off = c->d_type_basis_off.p;
@@ -911,7 +916,10 @@ int ensure_scratch(imago_ctx *c, int nterm) {
   return IMAGO_OK;
 }
 
-enum Kind { KIND_OL = 0, KIND_KE = 1, KIND_NP = 2, KIND_EP = 3, KIND_MV = 4 };
+enum Kind {
+  KIND_OL = 0, KIND_KE = 1, KIND_NP = 2, KIND_EP = 3, KIND_MV = 4,
+  KIND_MM = 5, KIND_DM = 6  // three components each
+};
 
 // One build of `nterm` matrices of one kind, writing packed output to
 // `packed_dev` (device) [nterm][nk][np][2].
@@ -980,7 +988,13 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   int rc = ensure_scratch(c, nterm);
   if (rc) return rc;
   imago_ctx::Scratch &S = c->scr[c->lane];
-  const DevSys &s = c->sys;
+  // the momentum matrix takes -i in the phase sum and stays complex at Gamma
+  DevSys sv = c->sys;
+  if (kind == KIND_MM) {
+    sv.minus_i = 1;
+    sv.real_k = 0;
+  }
+  const DevSys &s = sv;
   const DevWork &w = c->work;
   c->launches += class_launches(c) + 2 + (c->core_dim > 0 ? 2 : 1);
   mark(c);
@@ -989,6 +1003,8 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
                    : kind == KIND_KE ? kPrim2cKinetic
                                      : kPrim2cMassVel;
     rc = launch_prim2c(s, w, c->cls_beg, op, S.blk.p, st);
+  } else if (kind == KIND_MM || kind == KIND_DM) {
+    rc = launch_prim2c_vec(s, w, c->cls_beg, kind == KIND_DM, c->dip_center, S.blk.p, st);
   } else if (kind == KIND_NP) {
     rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st);
   } else {
@@ -1128,6 +1144,23 @@ int do_simple(imago_ctx *c, Kind kind, double *packed) {
 // Host outputs: EP runs in at least kEpCopyChunks chunks, so that copying
 // one chunk's matrices overlaps building the next.
 constexpr int kEpCopyChunks = 4;
+
+// Momentum or dipole (gaussOverlapMM / gaussOverlapDM + ortho3Terms,
+// integrals3Terms.F90:64-951, 1388-1608): the x, y, z components as three
+// terms of one build.
+int do_vec(imago_ctx *c, Kind kind, double *packed) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  const size_t npd = packed_doubles(c) * 3;
+  double *tgt = packed;
+  int rc = IMAGO_OK;
+  if (!c->outputs_on_device) {
+    if ((rc = c->vec_out.alloc(npd, c->cur()))) return rc;
+    tgt = c->vec_out.p;
+  }
+  if ((rc = run_build(c, kind, 0, 3, tgt))) return rc;
+  if (tgt != packed) rc = copy_out(c, packed, tgt, npd);
+  return rc;
+}
 
 // EP terms run in chunks sized to the scratch budget.  The chunk is fixed
 // on a context's first EP build: its scratch is sized for it, so later
@@ -1450,6 +1483,26 @@ int imago_ham_pscf(imago_ctx *c, int spin, const double *coeffs, int rel,
   return finish(c, rc);
 }
 
+static int vec_call(imago_ctx *c, Kind kind, const double *center, double *packed) {
+  if (!c || !packed || (kind == KIND_DM && !center)) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = begin_call(c))) return finish(c, rc);
+  for (int x = 0; x < 3; ++x) c->dip_center[x] = center ? center[x] : 0.0;
+  c->lane = KIND_KE;
+  rc = do_vec(c, kind, packed);
+  c->lane = 0;
+  return finish(c, rc);
+}
+
+int imago_gauss_overlap_mm(imago_ctx *c, double *packed) {
+  return vec_call(c, KIND_MM, nullptr, packed);
+}
+
+int imago_gauss_overlap_dm(imago_ctx *c, const double center[3], double *packed) {
+  return vec_call(c, KIND_DM, center, packed);
+}
+
 int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {
   if (!c) return IMAGO_ERR_INVALID;
   imago_out o{};
@@ -1742,7 +1795,7 @@ int imago_kpoint_mesh(const int n[3], const double shift[3],
 
 int imago_prim_eval(int kind, int n, const double *params, const int *cls,
                     double *sh) {
-  if (kind < 0 || kind > 5 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
+  if (kind < 0 || kind > 11 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
   if (kind != 4 && !cls) return IMAGO_ERR_INVALID;
   if (n == 0) return IMAGO_OK;
   for (int r = 0; kind != 4 && r < n; ++r)

@@ -21,6 +21,9 @@ struct DevSys {
   // every k-point is Gamma: all phases are exactly 1, every matrix is real,
   // and the orthogonalisation runs on the real parts only
   int real_k;
+  // the phase sum multiplies by -i (applyPhaseFactors runCode 1,
+  // intgSaving.F90:178-186): the momentum matrix -i<a|d/dx|b> is Hermitian
+  int minus_i;
   // atom types
   const int *type_nalpha, *type_alpha_off, *type_nstates, *type_nvale,
       *type_state_off, *type_basis_off, *type_screen;
@@ -125,6 +128,11 @@ enum { kPrim2cOverlap = 0, kPrim2cKinetic = 1, kPrim2cMassVel = 2 };
 // Launchers (kernels.cu).  All take the stream to run on.
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   int op, double *blk, cudaStream_t st);
+// Momentum (dipole = false) or dipole blocks about `center`: three
+// components per shell pair, component c at blk + c * blk_total.
+int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,
+                      bool dipole, const double center[3], double *blk,
+                      cudaStream_t st);
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
                   double *blk, cudaStream_t st);

@@ -323,7 +323,11 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
         if (e >= ne) continue;
         const double re = ar[mt][nt][i], im = ai[mt][nt][i];
         const int m2 = e / p.ni, m1 = e - m2 * p.ni;
-        scatter(s, p, tk, m1, m2, cs * re - sn * im, cs * im + sn * re, vv, cv, cc);
+        const double xr = cs * re - sn * im, xi = cs * im + sn * re;
+        if (s.minus_i)
+          scatter(s, p, tk, m1, m2, xi, -xr, vv, cv, cc);
+        else
+          scatter(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
       }
   }
 }
@@ -370,8 +374,11 @@ __global__ void __launch_bounds__(kBC)
   for (int k = 0; k < kBlochSmallNk; ++k)
     if (k < nk) {
       const double2 f = shift[k];
-      scatter(s, p, (long long)term * nk + k, m1, m2, f.x * re[k] - f.y * im[k],
-              f.x * im[k] + f.y * re[k], vv, cv, cc);
+      const double xr = f.x * re[k] - f.y * im[k], xi = f.x * im[k] + f.y * re[k];
+      if (s.minus_i)
+        scatter(s, p, (long long)term * nk + k, m1, m2, xi, -xr, vv, cv, cc);
+      else
+        scatter(s, p, (long long)term * nk + k, m1, m2, xr, xi, vv, cv, cc);
     }
 }
 

@@ -53,6 +53,20 @@ __device__ void eval_mv(const double *p, double *out) {
     for (int j = 0; j < nsh(LB); ++j) out[i * 16 + j] = blk[i * nsh(LB) + j];
 }
 
+// One component of the momentum (DIP = false) or dipole blocks (the
+// dipole centre is params 9..11), every class through the runtime-class
+// routine: the build kernels' unrolled s/p/d variants share its arithmetic
+// (vec_factor, the same tables) and are checked by the build tests.
+template <bool DIP>
+__device__ void eval_vec_rt(int la, int lb, int comp, const double *p, double *out) {
+  const int nb = nsh(la) * nsh(lb);
+  double blk[3 * 256];
+  prim_vec_rt<DIP>(la, lb, p[0], p[1], p + 3, p + 6, p + 9, blk, nb);
+  for (int i = 0; i < 256; ++i) out[i] = 0.0;
+  for (int i = 0; i < nsh(la); ++i)
+    for (int j = 0; j < nsh(lb); ++j) out[i * 16 + j] = blk[comp * nb + i * nsh(lb) + j];
+}
+
 static __device__ void eval_one_rt(int la, int lb, int kind, const double *p,
                             double *out) {
   const int L = la + lb;
@@ -100,6 +114,15 @@ __global__ void k_prim_eval(int kind, int n, const double *params,
     return;
   }
   const int la = cls[2 * r], lb = cls[2 * r + 1];
+  if (kind >= 6) {  // momentum (6..8) / dipole (9..11), components x, y, z
+    const int comp = (kind - 6) % 3;
+    const bool dip = kind >= 9;
+    if (dip)
+      eval_vec_rt<true>(la, lb, comp, p, out);
+    else
+      eval_vec_rt<false>(la, lb, comp, p, out);
+    return;
+  }
   if (kind == 5) {  // mass velocity: s/p/d unrolled, f at run time
     switch (la * 4 + lb) {
 #define IMAGO_EV(a, b) \

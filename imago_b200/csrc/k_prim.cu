@@ -42,6 +42,31 @@ __global__ void __launch_bounds__(128)
   prim_mv_rt(la, lb, q.a1, q.a2, q.A, q.B, -kMassVelPref, blk + sp.boff);
 }
 
+// Momentum / dipole: three component blocks per shell pair, component c at
+// blk + c * blk_total.
+template <int LA, int LB, bool DIP>
+__global__ void __launch_bounds__(128)
+    k_prim_vec(DevSys s, DevWork w, int beg, int end, double3 center, double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  const double C[3] = {center.x, center.y, center.z};
+  prim_vec<LA, LB, DIP>(q.a1, q.a2, q.A, q.B, C, blk + sp.boff, w.blk_total);
+}
+
+template <bool DIP>
+__global__ void __launch_bounds__(128)
+    k_prim_vec_rt(DevSys s, DevWork w, int beg, int end, int la, int lb,
+                  double3 center, double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  const double C[3] = {center.x, center.y, center.z};
+  prim_vec_rt<DIP>(la, lb, q.a1, q.a2, q.A, q.B, C, blk + sp.boff, w.blk_total);
+}
+
 // ------------------------------------------------------------ prim3c --
 // One thread per (shell pair, term).  The site and lattice-image loops are
 // those of nuclearPE (integrals.F90:2533-2698) and electronicPE
@@ -317,6 +342,40 @@ int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
     IMAGO_CUDA(cudaGetLastError());
   }
   return rc;
+}
+
+int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,
+                      bool dipole, const double center[3], double *blk,
+                      cudaStream_t st) {
+  const double3 c3 = make_double3(center ? center[0] : 0.0, center ? center[1] : 0.0,
+                                  center ? center[2] : 0.0);
+#define IMAGO_PV(a, b)                                                         \
+  {                                                                           \
+    const int beg = cls_beg[a * 4 + b], n = cls_beg[a * 4 + b + 1] - beg;     \
+    if (n > 0) {                                                              \
+      const unsigned grid = (n + 127) / 128;                                  \
+      if (dipole)                                                             \
+        k_prim_vec<a, b, true><<<grid, 128, 0, st>>>(s, w, beg, beg + n, c3, blk);  \
+      else                                                                    \
+        k_prim_vec<a, b, false><<<grid, 128, 0, st>>>(s, w, beg, beg + n, c3, blk); \
+      IMAGO_CUDA(cudaGetLastError());                                         \
+    }                                                                         \
+  }
+  IMAGO_FOR_SPD_CLASSES(IMAGO_PV)
+#undef IMAGO_PV
+  for (int c = 0; c < 16; ++c) {
+    const int la = c / 4, lb = c % 4;
+    if (la < 3 && lb < 3) continue;
+    const int beg = cls_beg[c], n = cls_beg[c + 1] - beg;
+    if (n <= 0) continue;
+    const unsigned grid = (n + 127) / 128;
+    if (dipole)
+      k_prim_vec_rt<true><<<grid, 128, 0, st>>>(s, w, beg, beg + n, la, lb, c3, blk);
+    else
+      k_prim_vec_rt<false><<<grid, 128, 0, st>>>(s, w, beg, beg + n, la, lb, c3, blk);
+    IMAGO_CUDA(cudaGetLastError());
+  }
+  return IMAGO_OK;
 }
 
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,

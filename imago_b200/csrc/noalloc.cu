@@ -67,7 +67,7 @@ int scratch_address(unsigned char **out) {
 
 extern "C" int imago_prim_eval_static(int kind, int n, const double *params,
                                       const int *cls, double *sh) {
-  if (kind < 0 || kind > 5 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
+  if (kind < 0 || kind > 11 || n < 0 || !params || !sh) return IMAGO_ERR_INVALID;
   if (kind != 4 && !cls) return IMAGO_ERR_INVALID;
   if (n > kMaxRecords) return IMAGO_ERR_RANGE;
   if (n == 0) return IMAGO_OK;

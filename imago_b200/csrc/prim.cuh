@@ -9,6 +9,8 @@
 //    Obara-Saika recursions in separable 1D form;
 //  * mass velocity (massvel2CIntg): <nabla^2 a|nabla^2 b> from the same
 //    1D overlap tables, two orders higher;
+//  * momentum and dipole (momentum2CIntg, dipole3CIntg): three Cartesian
+//    components, the operator moved into one 1D factor;
 //  * three-centre overlap and nuclear (electron3CIntg, nuclear3CIntg):
 //    McMurchie-Davidson.  The product of the two orbital primitives is
 //    expanded in Hermite Gaussians about P with coefficients E_t (they
@@ -288,6 +290,79 @@ __device__ void prim_mv(double a1, double a2, const double *A, const double *B,
       }
       out[s1 * nsh(LB) + s2] = v;
     }
+}
+
+// Momentum <a|d/dx_c|b> (DIP = false) or dipole <a|(r - C)_c|b> (DIP =
+// true) blocks for the three components c, written to out + c * cstride.
+// The operator goes into the component's 1D factor of the overlap table:
+//   dipole: (x - C_x) = x_B + (B_x - C_x) on atom 2's side;
+//   momentum: d/dx x^j e^{-a x^2} = j x^{j-1} - 2 a x^{j+1} on atom 2's
+//   side, or minus the same on atom 1's side (integration by parts), on the
+//   side of the smaller exponent, so that the seed is formed from whichever
+//   of PA = P - A and PB = P - B has not cancelled (the reference seeds
+//   with 2 a1 PA S, gaussIntegrals.f90:23080-23082).
+template <bool DIP, int IA, int JB>
+__device__ __forceinline__ double vec_factor(const double S[IA + 1][JB + 1],
+                                             int i, int j, bool left, double a1,
+                                             double a2, double BC) {
+  if (DIP) return S[i][j + 1] + BC * S[i][j];
+  if (left) return 2.0 * a1 * S[i + 1][j] - (i > 0 ? i * S[i - 1][j] : 0.0);
+  return -2.0 * a2 * S[i][j + 1] + (j > 0 ? j * S[i][j - 1] : 0.0);
+}
+
+// s, p and d classes: bounds known at compile time, tables in registers.
+template <int LA, int LB, bool DIP>
+__device__ void prim_vec(double a1, double a2, const double *A, const double *B,
+                         const double *C, double *out, long long cstride) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  const bool left = a1 <= a2;
+  double S[3][LA + 1][LB + 1], D[3][LA + 1][LB + 1];
+  double d2 = 0.0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    const double X = A[x] - B[x];
+    d2 += X * X;
+    double T[LA + 2][LB + 2];
+    os1d<LA + 1, LB + 1>(P - A[x], P - B[x], inv2p, T);
+    const double BC = DIP ? B[x] - C[x] : 0.0;
+#pragma unroll
+    for (int i = 0; i <= LA; ++i)
+#pragma unroll
+      for (int j = 0; j <= LB; ++j) {
+        S[x][i][j] = T[i][j];
+        D[x][i][j] = vec_factor<DIP, LA + 1, LB + 1>(T, i, j, left, a1, a2, BC);
+      }
+  }
+  const double pref = pow(kPi / zeta, 1.5) * exp(-xi * d2);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    auto cart = [&](int p, int q) {
+      double v = pref;
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const int i = cart_exp(p, x), j = cart_exp(q, x);
+        v *= (x == c) ? D[x][i][j] : S[x][i][j];
+      }
+      return v;
+    };
+#pragma unroll
+    for (int s1 = 0; s1 < nsh(LA); ++s1)
+#pragma unroll
+      for (int s2 = 0; s2 < nsh(LB); ++s2) {
+        double v = 0.0;
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+          if (k1 >= sh_nterm(s1)) break;
+#pragma unroll
+          for (int k2 = 0; k2 < 3; ++k2) {
+            if (k2 >= sh_nterm(s2)) break;
+            v += sh_coef(s1, k1) * sh_coef(s2, k2) * cart(sh_cart(s1, k1), sh_cart(s2, k2));
+          }
+        }
+        out[c * cstride + s1 * nsh(LB) + s2] = v;
+      }
+  }
 }
 
 // ---------------------------------------------- McMurchie-Davidson 3C --
@@ -586,6 +661,55 @@ static __device__ __noinline__ void prim_mv_rt(int la, int lb, double a1,
       pc[p * ncb + q] = pref * v;
     }
   cart_to_sh_rt(la, lb, pc, out);
+}
+
+// prim_vec for the f classes: runtime loops, tables in local memory.
+template <bool DIP>
+__device__ __noinline__ void prim_vec_rt(int la, int lb, double a1, double a2,
+                                         const double *A, const double *B,
+                                         const double *C, double *out,
+                                         long long cstride) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  const bool left = a1 <= a2;
+  double S[3][4][4], D[3][4][4];
+  double d2 = 0.0;
+#pragma unroll 1
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    const double X = A[x] - B[x];
+    d2 += X * X;
+    double T[5][5];
+    os1d<4, 4>(P - A[x], P - B[x], inv2p, T);
+    const double BC = DIP ? B[x] - C[x] : 0.0;
+#pragma unroll 1
+    for (int i = 0; i <= la; ++i)
+#pragma unroll 1
+      for (int j = 0; j <= lb; ++j) {
+        S[x][i][j] = T[i][j];
+        D[x][i][j] = vec_factor<DIP, 4, 4>(T, i, j, left, a1, a2, BC);
+      }
+  }
+  const double pref = pow(kPi / zeta, 1.5) * exp(-xi * d2);
+  const int nca = ncart(la), ncb = ncart(lb), nsa = nsh(la), nsb = nsh(lb);
+  double pc[ncart(3) * ncart(3)];
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll 1
+    for (int p = 0; p < nca; ++p)
+#pragma unroll 1
+      for (int q = 0; q < ncb; ++q) {
+        double v = pref;
+        for (int x = 0; x < 3; ++x) {
+          const int i = cart_exp(p, x), j = cart_exp(q, x);
+          v *= (x == c) ? D[x][i][j] : S[x][i][j];
+        }
+        pc[p * ncb + q] = v;
+      }
+    double blk[256];
+    cart_to_sh_rt(la, lb, pc, blk);
+#pragma unroll 1
+    for (int e = 0; e < nsa * nsb; ++e) out[c * cstride + e] = blk[e];
+  }
 }
 
 static __device__ __noinline__ void accumulate_overlap_q_rt(int L, const double *X,

@@ -71,9 +71,12 @@ def lib():
         L.imago_gauss_overlap_ol.argtypes = [ctypes.c_void_p, _D, _D, _D]
         L.imago_gauss_overlap_ol.restype = ctypes.c_int
         for n in ("imago_gauss_overlap_ke", "imago_gauss_overlap_np", "imago_gauss_overlap_mv",
+                  "imago_gauss_overlap_mm",
                   "imago_elec_pot_gauss_overlap"):
             getattr(L, n).argtypes = [ctypes.c_void_p, _D]
             getattr(L, n).restype = ctypes.c_int
+        L.imago_gauss_overlap_dm.argtypes = [ctypes.c_void_p, _D, _D]
+        L.imago_gauss_overlap_dm.restype = ctypes.c_int
         L.imago_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int, _D]
         L.imago_ham_pscf.restype = ctypes.c_int
         L.imago_elec_pot_gauss_overlap_range.argtypes = [ctypes.c_void_p, ctypes.c_int,
@@ -153,7 +156,9 @@ def kpoint_mesh(n, shift=(0.0, 0.0, 0.0)):
 
 
 PRIM_KINDS = {"overlap": 0, "kinetic": 1, "electron3c": 2, "nuclear3c": 3,
-              "boys": 4, "massvel": 5}
+              "boys": 4, "massvel": 5,
+              "momentum_x": 6, "momentum_y": 7, "momentum_z": 8,
+              "dipole_x": 9, "dipole_y": 10, "dipole_z": 11}
 
 
 def prim_eval(kind, params, cls=None):
@@ -286,6 +291,31 @@ class IntegralSetup:
         term of rel = 1 runs; needs the overlap first when coreDim > 0."""
         out = self._packed()
         _check(lib().imago_gauss_overlap_mv(self._ctx, _p(out)), "gaussOverlapMV")
+        return out
+
+    def _ptr(self, out):
+        if isinstance(out, int):
+            return ctypes.cast(ctypes.c_void_p(out), _D)
+        if hasattr(out, "data_ptr"):
+            return ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D)
+        return _p(out)
+
+    def gauss_overlap_mm(self, out=None):
+        """Momentum matrices -i<a|d/dx_c|b>, c = x, y, z
+        (imago_gauss_overlap_mm): [3, nk, nPacked, 2]."""
+        if out is None:
+            out = self._packed(3)
+        _check(lib().imago_gauss_overlap_mm(self._ctx, self._ptr(out)), "gaussOverlapMM")
+        return out
+
+    def gauss_overlap_dm(self, center, out=None):
+        """Dipole matrices <a|(r - center)_c|b> (imago_gauss_overlap_dm):
+        [3, nk, nPacked, 2]."""
+        c = np.ascontiguousarray(center, dtype=np.float64).reshape(3)
+        if out is None:
+            out = self._packed(3)
+        _check(lib().imago_gauss_overlap_dm(self._ctx, _p(c), self._ptr(out)),
+               "gaussOverlapDM")
         return out
 
     def ham_pscf(self, coeffs, rel=False, out=None):

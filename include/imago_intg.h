@@ -184,6 +184,20 @@ IMAGO_API int imago_gauss_overlap_np(imago_ctx *ctx, double *packed);
  * when coreDim > 0. */
 IMAGO_API int imago_gauss_overlap_mv(imago_ctx *ctx, double *packed);
 
+/* Momentum matrices, the x, y and z components of -i<a|d/dx_c|b>
+ * (Hermitian): replaces gaussOverlapMM + ortho3Terms(7)
+ * (integrals3Terms.F90:511-951, 1388-1608; called at imago.F90:315 and 709
+ * for optical properties).  packed: [3][nk][nPacked][2].  Needs the overlap
+ * first when coreDim > 0. */
+IMAGO_API int imago_gauss_overlap_mm(imago_ctx *ctx, double *packed);
+
+/* Dipole matrices, the x, y and z components of <a|(r - center)_c|b>:
+ * replaces gaussOverlapDM + ortho3Terms(6) (integrals3Terms.F90:64-507;
+ * called at imago.F90:312 and 705).  center is the reference's dipoleCenter
+ * (input.f90:552-594), Cartesian, in bohr.  packed: [3][nk][nPacked][2]. */
+IMAGO_API int imago_gauss_overlap_dm(imago_ctx *ctx, const double center[3],
+                                     double *packed);
+
 /* The PSCF Hamiltonian: replaces gaussOverlapHamPSCF + orthoHamPSCF
  * (integrals.F90:2860-3606, 3913-4043; called at imago.F90:685).  One
  * matrix per spin: kinetic + nuclear + sum_t coeffs(t, q) EP_t, minus the
@@ -315,7 +329,9 @@ IMAGO_API int imago_kpoint_mesh(const int n[3], const double shift[3],
  * reference's generated primitives (gaussIntegrals.f90).  kind: 0 overlap
  * (overlap2CIntg), 1 kinetic (kinetic2CIntg), 2 three-centre overlap
  * (electron3CIntg), 3 three-centre nuclear (nuclear3CIntg), 4 Boys function
- * (boys, F_0..F_6 of params[0]), 5 mass velocity (massvel2CIntg).  Record r reads
+ * (boys, F_0..F_6 of params[0]), 5 mass velocity (massvel2CIntg), 6..8
+ * the x, y, z components of momentum2CIntg and 9..11 those of dipole3CIntg
+ * (operator centre C).  Record r reads
  *   params[r*12 + 0..11] = a1, a2, a3, A[3], B[3], C[3]
  * and cls[2*r + 0..1] = l of atom 1 and atom 2 (0..3); it writes
  * sh[r*256 + i*16 + j] = reference sh(i+1, j+1).  Host pointers.

@@ -36,6 +36,12 @@ def lib():
             f.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D,
                           ctypes.c_int, ctypes.c_int, _D]
             f.restype = None
+        L.orc_momentum2c.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D,
+                                     ctypes.c_int, ctypes.c_int, _D]
+        L.orc_momentum2c.restype = None
+        L.orc_dipole2c.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D,
+                                   ctypes.c_int, ctypes.c_int, _D]
+        L.orc_dipole2c.restype = None
         for name in ("orc_electron3c", "orc_nuclear3c"):
             f = getattr(L, name)
             f.argtypes = [ctypes.c_double] * 3 + [_D, _D, _D, ctypes.c_int,
@@ -56,6 +62,8 @@ def lib():
         L.orc_gauss_overlap_ke.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_np.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_mv.argtypes = [ctypes.c_void_p, _D]
+        L.orc_gauss_overlap_mm.argtypes = [ctypes.c_void_p, _D]
+        L.orc_gauss_overlap_dm.argtypes = [ctypes.c_void_p, _D, _D]
         L.orc_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D,
                                    ctypes.c_int, _D]
         L.orc_elec_pot_gauss_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int,
@@ -77,6 +85,24 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(_D)
+
+
+def primitive_vec(kind, la, lb, a1, a2, A, B, C=None):
+    """Three-component blocks [3, nsh(la), nsh(lb)]: kind momentum
+    (momentum2CIntg) or dipole (dipole3CIntg, operator centre C)."""
+    L = lib()
+    sh = np.zeros(768)
+    A = np.ascontiguousarray(A, float)
+    B = np.ascontiguousarray(B, float)
+    if kind == "momentum":
+        L.orc_momentum2c(a1, a2, _p(A), _p(B), la, lb, _p(sh))
+    elif kind == "dipole":
+        C = np.ascontiguousarray(C, float)
+        L.orc_dipole2c(a1, a2, _p(A), _p(B), _p(C), la, lb, _p(sh))
+    else:
+        raise ValueError(kind)
+    n1, n2 = (la + 1) ** 2, (lb + 1) ** 2
+    return sh.reshape(3, 16, 16)[:, :n1, :n2].copy()
 
 
 def primitive(kind, la, lb, a1, a2, a3, A, B, C):
@@ -160,6 +186,19 @@ class OracleBuild:
         out = self._packed()
         self._check(lib().orc_gauss_overlap_mv(self._ctx, _p(out)), "MV")
         return out[0]
+
+    def momentum(self):
+        """gaussOverlapMM: [3, nk, np, 2] (x, y, z)."""
+        out = self._packed(3)
+        self._check(lib().orc_gauss_overlap_mm(self._ctx, _p(out)), "MM")
+        return out
+
+    def dipole(self, center):
+        """gaussOverlapDM about `center` (xyz): [3, nk, np, 2]."""
+        c = np.ascontiguousarray(center, dtype=np.float64)
+        out = self._packed(3)
+        self._check(lib().orc_gauss_overlap_dm(self._ctx, _p(c), _p(out)), "DM")
+        return out
 
     def ham_pscf(self, coeffs, rel=False):
         """gaussOverlapHamPSCF: coeffs [potDim] or [potDim, spin] ->

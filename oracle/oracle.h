@@ -33,6 +33,11 @@ void orc_kinetic2c(double a1, double a2, const double *A, const double *B,
                    int la, int lb, double *sh);
 void orc_massvel2c(double a1, double a2, const double *A, const double *B,
                    int la, int lb, double *sh);
+/* Three components: sh3[c*256 + i*16 + j] = reference sh(i+1, j+1, c+1). */
+void orc_momentum2c(double a1, double a2, const double *A, const double *B,
+                    int la, int lb, double *sh3);
+void orc_dipole2c(double a1, double a2, const double *A, const double *B,
+                  const double *C, int la, int lb, double *sh3);
 void orc_electron3c(double a1, double a2, double a3, const double *A,
                     const double *B, const double *C, int la, int lb,
                     double *sh);
@@ -59,6 +64,10 @@ int orc_gauss_overlap_ke(orc_ctx *c, double *packed);
 int orc_gauss_overlap_np(orc_ctx *c, double *packed);
 /* Mass velocity (rel = 1 runs only). */
 int orc_gauss_overlap_mv(orc_ctx *c, double *packed);
+/* Momentum (-i d/dx_c, Hermitian) and dipole (r - center)_c matrices,
+ * packed [3][nk][np][2] for c = x, y, z. */
+int orc_gauss_overlap_mm(orc_ctx *c, double *packed);
+int orc_gauss_overlap_dm(orc_ctx *c, const double center[3], double *packed);
 /* The PSCF Hamiltonian: packed [spin][nk][np][2]; coeffs the reference's
  * potCoeffs(potDim, spin), column-major: coeffs[q * potDim + t]. */
 int orc_ham_pscf(orc_ctx *c, int spin, const double *coeffs, int rel,

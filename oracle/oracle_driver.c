@@ -529,7 +529,7 @@ void orc_last_counts(const orc_ctx *c, long long *pi, long long *sp,
 
 /* ---------- the integral builds ---------- */
 
-enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3, K_MV = 4, K_HAM = 5 };
+enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3, K_MV = 4, K_HAM = 5, K_MM = 6, K_DM = 7 };
 
 typedef struct {
   /* global matrices for one build (complex, column-major like Fortran) */
@@ -548,7 +548,9 @@ typedef struct {
   int pterm;    /* EP: alpha index within the type */
   unsigned char *anyint; /* EP: [i][j][cell] interaction bits */
   const double *coeffs;  /* HAM: potCoeffs(potDim, spin), column-major */
-  int spin, q, rel;      /* HAM: spins, the spin built, mass velocity */
+  int spin, q, rel;      /* HAM: spins, the spin built, mass velocity;
+                          * MM, DM: q is the Cartesian component built */
+  const double *center;  /* DM: dipoleCenter */
 } buildspec;
 
 /* saveCurrentPair, intgSaving.F90:346-459 with valeValeSaving 463-510,
@@ -860,7 +862,16 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
             else if (bs->kind == K_HAM)
               ham_pscf_pair(c, bs, e1, e2, a, b, t1->alphas[a], t2->alphas[b], r2, A,
                             Bp, la, lb, sh, &ntr);
-            else if (bs->kind == K_MV) {
+            else if (bs->kind == K_MM || bs->kind == K_DM) {
+              /* one component of momentum2CIntg / dipole3CIntg
+               * (integrals3Terms.F90:398-401, 849-852) */
+              double sh3[768];
+              if (bs->kind == K_MM)
+                orc_momentum2c(t1->alphas[a], t2->alphas[b], A, Bp, la, lb, sh3);
+              else
+                orc_dipole2c(t1->alphas[a], t2->alphas[b], A, Bp, bs->center, la, lb, sh3);
+              memcpy(sh, sh3 + 256 * bs->q, sizeof(double) * 256);
+            } else if (bs->kind == K_MV) {
               /* accumulated with a minus sign (integrals.F90:1440-1447):
                * a + (-x) c is a - x c exactly */
               orc_massvel2c(t1->alphas[a], t2->alphas[b], A, Bp, la, lb, sh);
@@ -905,8 +916,15 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
               for (int m2 = 0; m2 < n2; ++m2) {
                 double *d = cp + 2 * (((size_t)kp * ms + m1) * ms + m2);
                 double x = M[m1 * ms + m2];
-                d[0] = d[0] + pr * x;
-                d[1] = d[1] + pi * x;
+                if (bs->kind == K_MM) {
+                  /* applyPhaseFactors runCode 1: (0,-1) * phase * x,
+                   * intgSaving.F90:178-186 */
+                  d[0] = d[0] + pi * x;
+                  d[1] = d[1] + (-pr) * x;
+                } else {
+                  d[0] = d[0] + pr * x;
+                  d[1] = d[1] + pi * x;
+                }
               }
           }
         if (bs->kind == K_EP && !elec_int) *bit = 0;
@@ -1100,13 +1118,13 @@ static void reset_stats(orc_ctx *c) {
 int orc_gauss_overlap_ol(orc_ctx *c, double *packed, double *cv_re,
                          double *cv_im) {
   reset_stats(c);
-  buildspec bs = {K_OL, 0, 0, NULL, NULL, 0, 0, 0};
+  buildspec bs = {K_OL, 0, 0, NULL, NULL, 0, 0, 0, NULL};
   return build_one(c, &bs, packed, cv_re, cv_im);
 }
 
 int orc_gauss_overlap_ke(orc_ctx *c, double *packed) {
   reset_stats(c);
-  buildspec bs = {K_KE, 0, 0, NULL, NULL, 0, 0, 0};
+  buildspec bs = {K_KE, 0, 0, NULL, NULL, 0, 0, 0, NULL};
   return build_one(c, &bs, packed, NULL, NULL);
 }
 
@@ -1115,7 +1133,7 @@ int orc_gauss_overlap_ke(orc_ctx *c, double *packed) {
  * opcode 5). */
 int orc_gauss_overlap_mv(orc_ctx *c, double *packed) {
   reset_stats(c);
-  buildspec bs = {K_MV, 0, 0, NULL, NULL, 0, 0, 0};
+  buildspec bs = {K_MV, 0, 0, NULL, NULL, 0, 0, 0, NULL};
   return build_one(c, &bs, packed, NULL, NULL);
 }
 
@@ -1127,16 +1145,40 @@ int orc_ham_pscf(orc_ctx *c, int spin, const double *coeffs, int rel,
   reset_stats(c);
   const size_t np = (size_t)c->vale_dim * (c->vale_dim + 1) / 2;
   for (int q = 0; q < spin; ++q) {
-    buildspec bs = {K_HAM, 0, 0, NULL, coeffs, spin, q, rel};
+    buildspec bs = {K_HAM, 0, 0, NULL, coeffs, spin, q, rel, NULL};
     int st = build_one(c, &bs, packed + (size_t)q * 2 * np * c->nk, NULL, NULL);
     if (st) return st;
   }
   return IMAGO_OK;
 }
 
+/* gaussOverlapMM / gaussOverlapDM + ortho3Terms, integrals3Terms.F90:
+ * 64-507, 511-951, 1388-1608: three matrices (x, y, z), each built with the
+ * kinetic build's loops and orthogonalised like KE; the momentum matrix
+ * takes the -i of applyPhaseFactors runCode 1, so it is Hermitian. */
+static int build_vec(orc_ctx *c, int kind, const double *center, double *packed) {
+  reset_stats(c);
+  const size_t np = (size_t)c->vale_dim * (c->vale_dim + 1) / 2;
+  for (int q = 0; q < 3; ++q) {
+    buildspec bs = {kind, 0, 0, NULL, NULL, 0, q, 0, center};
+    int st = build_one(c, &bs, packed + (size_t)q * 2 * np * c->nk, NULL, NULL);
+    if (st) return st;
+  }
+  return IMAGO_OK;
+}
+
+int orc_gauss_overlap_mm(orc_ctx *c, double *packed) {
+  return build_vec(c, K_MM, NULL, packed);
+}
+
+int orc_gauss_overlap_dm(orc_ctx *c, const double center[3], double *packed) {
+  if (!center) return IMAGO_ERR_INVALID;
+  return build_vec(c, K_DM, center, packed);
+}
+
 int orc_gauss_overlap_np(orc_ctx *c, double *packed) {
   reset_stats(c);
-  buildspec bs = {K_NP, 0, 0, NULL, NULL, 0, 0, 0};
+  buildspec bs = {K_NP, 0, 0, NULL, NULL, 0, 0, 0, NULL};
   return build_one(c, &bs, packed, NULL, NULL);
 }
 
@@ -1163,7 +1205,7 @@ int orc_elec_pot_gauss_overlap(orc_ctx *c, int term_lo, int term_hi,
       /* Terms before the sample are not run: their only effect on later
        * terms is the exact skip bits, which leave the values unchanged. */
       if (term < term_lo) continue;
-      buildspec bs = {K_EP, t, j, bits, NULL, 0, 0, 0};
+      buildspec bs = {K_EP, t, j, bits, NULL, 0, 0, 0, NULL};
       double l0 = c->t_loops, o0 = c->t_ortho;
       long long a0 = c->n_pair_images, b0 = c->n_shell_pairs, t0 = c->n_triples;
       st = build_one(c, &bs, packed + 2 * np * c->nk * (size_t)(term - term_lo),

@@ -11,6 +11,8 @@
  *   overlap2CIntg  (gaussIntegrals.f90:26-4420)    <a|b>
  *   kinetic2CIntg  (gaussIntegrals.f90:4422-11622) <a|-1/2 nabla^2|b>
  *   massvel2CIntg  (gaussIntegrals.f90:39070-49402) (alpha^2/8)<a|nabla^4|b>
+ *   momentum2CIntg (gaussIntegrals.f90:23041-39068) <a|d/dx_c|b>, c = x,y,z
+ *   dipole3CIntg   (gaussIntegrals.f90:49404-65510) <a|(r - C)_c|b>
  *   electron3CIntg (gaussIntegrals.f90:11624-16023) <a|exp(-a3 r_C^2)|b>
  *   nuclear3CIntg  (gaussIntegrals.f90:16223-23039) <a|exp(-a3 r_C^2)/r_C|b>
  *
@@ -294,6 +296,61 @@ void orc_massvel2c(double a1, double a2, const double *A, const double *B,
       pc[p][q] = pref * v;
     }
   cart_to_sh(pc, la, lb, sh);
+}
+
+/* Momentum and dipole blocks, three Cartesian components each (the
+ * reference's sh(16,16,3)), sh3[c * 256 + i * 16 + j].  Both move the
+ * operator into one 1D factor of the overlap table, the component's axis
+ * taking the moved factor and the other two the plain overlap factors:
+ *   dipole: (x - C_x) = x_B + (B_x - C_x) on atom 2's side;
+ *   momentum: d/dx x^j e^{-a x^2} = j x^{j-1} - 2 a x^{j+1} on atom 2's
+ *   side, or minus the same on atom 1's side (integration by parts), taken
+ *   on the side of the smaller exponent: the overlap table's PB = P - B
+ *   (PA = P - A) loses digits when P lies near B (near A), and the seed
+ *   -2 a2 PB S = 2 a1 PA S is then formed from the other one.  The
+ *   reference seeds with 2 a1 PA S (gaussIntegrals.f90:23080-23082). */
+static void vec2c(int dipole, double a1, double a2, const double *A,
+                  const double *B, const double *C, int la, int lb,
+                  double *sh3) {
+  double zeta = a1 + a2, xi = a1 * a2 / zeta, d2 = 0.0;
+  double S[3][8][8], D[3][4][4];
+  for (int x = 0; x < 3; ++x) {
+    double P = (a1 * A[x] + a2 * B[x]) / zeta;
+    d2 += (A[x] - B[x]) * (A[x] - B[x]);
+    os_1d(P - A[x], P - B[x], 1.0 / (2.0 * zeta), la + 1, lb + 1, S[x]);
+    for (int i = 0; i <= la; ++i)
+      for (int j = 0; j <= lb; ++j) {
+        if (dipole)
+          D[x][i][j] = S[x][i][j + 1] + (B[x] - C[x]) * S[x][i][j];
+        else if (a1 <= a2)
+          D[x][i][j] = 2.0 * a1 * S[x][i + 1][j] - (i > 0 ? i * S[x][i - 1][j] : 0.0);
+        else
+          D[x][i][j] = -2.0 * a2 * S[x][i][j + 1] + (j > 0 ? j * S[x][i][j - 1] : 0.0);
+      }
+  }
+  double pref = pow(ORC_PI / zeta, 1.5) * exp(-xi * d2);
+  double pc[20][20];
+  for (int c = 0; c < 3; ++c) {
+    for (int p = 0; p < NCART[la]; ++p)
+      for (int q = 0; q < NCART[lb]; ++q) {
+        const int *u = CART[p], *w = CART[q];
+        double v = 1.0;
+        for (int x = 0; x < 3; ++x)
+          v *= (x == c) ? D[x][u[x]][w[x]] : S[x][u[x]][w[x]];
+        pc[p][q] = pref * v;
+      }
+    cart_to_sh(pc, la, lb, sh3 + 256 * c);
+  }
+}
+
+void orc_momentum2c(double a1, double a2, const double *A, const double *B,
+                    int la, int lb, double *sh3) {
+  vec2c(0, a1, a2, A, B, NULL, la, lb, sh3);
+}
+
+void orc_dipole2c(double a1, double a2, const double *A, const double *B,
+                  const double *C, int la, int lb, double *sh3) {
+  vec2c(1, a1, a2, A, B, C, la, lb, sh3);
 }
 
 /* Three-centre overlap: the three Gaussians combine into one of exponent

@@ -71,3 +71,14 @@ def massvel_scale(r):
     S = oracle.primitive("overlap", r["la"], r["lb"], r["a1"], r["a2"], 0.0,
                          r["A"], r["B"], r["B"])
     return FINE_STRUCTURE ** 2 / 8 * max(r["a1"], r["a2"]) ** 2 * np.abs(S).max()
+
+
+def momentum_scale(r):
+    """The size the reference's momentum2CIntg rounds at: it seeds with
+    2 a1 PA S (gaussIntegrals.f90:23080-23082), PA = P - A formed from
+    coordinates of size |A|, |B|, which cancels when a2 << a1."""
+    import oracle
+    S = oracle.primitive("overlap", r["la"], r["lb"], r["a1"], r["a2"], 0.0,
+                         r["A"], r["B"], r["B"])
+    coord = max(np.abs(r["A"]).max(), np.abs(r["B"]).max(), 1.0)
+    return 2 * max(r["a1"], r["a2"]) * coord * np.abs(S).max()

@@ -4,7 +4,7 @@ own generated kernels.
 The reference's primitive integrals live in `src/imago/gaussIntegrals.f90`
 (overlap2CIntg 26-4420, kinetic2CIntg 4422-11622, massvel2CIntg
 39070-49402, electron3CIntg 11624-16023, boys 16080-16221, nuclear3CIntg
-16223-23039).  No Fortran compiler exists where this script runs, so the
+16223-23039, momentum2CIntg 23041-39068, dipole3CIntg 49404-65510).  No Fortran compiler exists where this script runs, so the
 script transliterates those subroutines statement by statement into Python and executes them with IEEE
 double arithmetic, which is what gfortran -O3 (no -ffast-math, no FMA on
 x86-64 baseline) evaluates.  Fortran semantics that matter for the values
@@ -41,6 +41,8 @@ KERNEL_LINES = {
     "boys": (16080, 16221),
     "nuclear3CIntg": (16223, 23039),
     "massvel2CIntg": (39070, 49402),
+    "momentum2CIntg": (23041, 39068),
+    "dipole3CIntg": (49404, 65510),
 }
 
 # Class codes built by integrals.F90:533-536: bit 0..3 for atom 1 (s,p,d,f),
@@ -313,6 +315,17 @@ def run_2c(ns, kern, la, lb, a1, a2, A, B):
             for i in range(1, nsh(la) + 1)]
 
 
+def run_vec(ns, kern, la, lb, a1, a2, A, B, C=None):
+    """Kernels with sh(16,16,3): one block per Cartesian component."""
+    sh = FArr("sh", [16, 16, 3])
+    args = [a1, a2, np.array(A, float), np.array(B, float)]
+    if C is not None:
+        args.append(np.array(C, float))
+    ns[kern](*args, class_code(la, lb), sh)
+    return [[[sh[i, j, c] for j in range(1, nsh(lb) + 1)]
+             for i in range(1, nsh(la) + 1)] for c in range(1, 4)]
+
+
 def run_3c(ns, kern, la, lb, a1, a2, a3, A, B, C):
     sh = FArr("sh", [16, 16])
     ns[kern](a1, a2, a3, np.array(A, float), np.array(B, float),
@@ -356,6 +369,8 @@ def main():
                 rec["overlap"] = run_2c(ns, "overlap2CIntg", la, lb, a1, a2, A, B)
                 rec["kinetic"] = run_2c(ns, "kinetic2CIntg", la, lb, a1, a2, A, B)
                 rec["massvel"] = run_2c(ns, "massvel2CIntg", la, lb, a1, a2, A, B)
+                rec["momentum"] = run_vec(ns, "momentum2CIntg", la, lb, a1, a2, A, B)
+                rec["dipole"] = run_vec(ns, "dipole3CIntg", la, lb, a1, a2, A, B, C)
                 rec["electron3c"] = run_3c(ns, "electron3CIntg", la, lb,
                                            a1, a2, a3, A, B, C)
                 rec["nuclear3c"] = run_3c(ns, "nuclear3CIntg", la, lb,
@@ -417,7 +432,8 @@ def main():
         boys.append({"T": float(T), "F": [F[m] for m in range(1, 8)]})
     out = {
         "source": "src/imago/gaussIntegrals.f90 (overlap2CIntg, kinetic2CIntg,"
-                  " electron3CIntg, boys, nuclear3CIntg, massvel2CIntg)"
+                  " electron3CIntg, boys, nuclear3CIntg, massvel2CIntg,"
+                  " momentum2CIntg, dipole3CIntg)"
                   " executed statement by statement in IEEE double",
         "generator": "tests/golden/make_golden.py",
         "records": records,

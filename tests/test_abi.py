@@ -109,3 +109,7 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_gauss_overlap_mv(None, None) == 1
     L.imago_ham_pscf.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
     assert L.imago_ham_pscf(None, 1, None, 0, None) == 1
+    L.imago_gauss_overlap_mm.argtypes = [vp, vp]
+    assert L.imago_gauss_overlap_mm(None, None) == 1
+    L.imago_gauss_overlap_dm.argtypes = [vp, vp, vp]
+    assert L.imago_gauss_overlap_dm(None, None, None) == 1

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import FINE_STRUCTURE, massvel_scale, packed_mismatch
+from conftest import FINE_STRUCTURE, massvel_scale, momentum_scale, packed_mismatch
 from imago_b200 import configs, intg
 
 pytestmark = pytest.mark.gpu
@@ -62,6 +62,26 @@ def test_massvel_primitives_match_reference_and_oracle(imago_lib, golden):
         tol = 1e-12 * max(np.abs(orc).max(), terms)
         assert np.abs(g[:n1, :n2] - orc).max() <= tol, (r["la"], r["lb"])
         assert not np.any(g[n1:, :]) and not np.any(g[:, n2:])
+
+
+def test_momentum_dipole_primitives_match_reference_and_oracle(imago_lib, golden):
+    # kinds 6..8 / 9..11: the x, y, z components, every class s..f
+    recs, params, cls = _golden_params(golden, "momentum")
+    for c, axis in enumerate("xyz"):
+        mom = intg.prim_eval("momentum_" + axis, params, cls)
+        dip = intg.prim_eval("dipole_" + axis, params, cls)
+        assert np.array_equal(dip, intg.prim_eval_static("dipole_" + axis, params, cls))
+        for r, gm, gd in zip(recs, mom, dip):
+            n1, n2 = (r["la"] + 1) ** 2, (r["lb"] + 1) ** 2
+            ref = np.array(r["momentum"][c])
+            scale = max(np.abs(ref).max(), momentum_scale(r))
+            assert np.abs(gm[:n1, :n2] - ref).max() <= 1e-12 * scale, (axis, r["la"], r["lb"])
+            orc = oracle.primitive_vec("momentum", r["la"], r["lb"], r["a1"], r["a2"],
+                                       r["A"], r["B"])[c]
+            assert np.abs(gm[:n1, :n2] - orc).max() <= 1e-12 * scale
+            ref = np.array(r["dipole"][c])
+            assert np.abs(gd[:n1, :n2] - ref).max() <= 1e-12 * np.abs(ref).max(), (axis, r["la"], r["lb"])
+            assert not np.any(gm[n1:, :]) and not np.any(gd[:, n2:])
 
 
 def test_boys_follows_reference_branches(imago_lib, golden):
@@ -471,3 +491,32 @@ def test_pscf_hamiltonian_device_outputs(imago_lib):
         g.ham_pscf(coeffs[:g.pot_dim], out=dev)
         torch.cuda.synchronize()
     assert np.array_equal(host, dev.cpu().numpy())
+
+
+@pytest.mark.parametrize("name", ["small", "f", "silicon8", "gamma"])
+def test_momentum_and_dipole_builds_match_oracle(imago_lib, name):
+    # gaussOverlapMM / gaussOverlapDM + ortho3Terms: three matrices each;
+    # the momentum matrix takes -i in the phase sum and stays complex at
+    # Gamma (the "gamma" system, where the other matrices are real)
+    s = {"small": configs.small_test_system,
+         "f": configs.f_test_system,
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3)),
+         "gamma": lambda: configs.silicon_cubic8(kmesh=(1, 1, 1),
+                                                 shift=(0.5, 0.5, 0.5))}[name]()
+    center = np.array([0.7, -0.4, 1.1])
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    ref_mm, ref_dm = ob.momentum(), ob.dipole(center)
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        mm = g.gauss_overlap_mm()
+        dm = g.gauss_overlap_dm(center)
+    assert mm.shape == dm.shape == (3, g.nk, g.npacked, 2)
+    res = {}
+    for c in range(3):
+        res["MM%d" % c] = packed_mismatch(mm[c], ref_mm[c])
+        res["DM%d" % c] = packed_mismatch(dm[c], ref_dm[c])
+    _assert_all(res)
+    assert np.abs(mm).max() > 0.0 and np.abs(dm).max() > 0.0
+    if name == "gamma":
+        assert np.abs(mm[..., 1]).max() > 0.0  # imaginary off-diagonal kept

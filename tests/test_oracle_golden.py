@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import massvel_scale
+from conftest import massvel_scale, momentum_scale
 
 KINDS = ("overlap", "kinetic", "electron3c", "nuclear3c")
 # Relative to the largest element of the block.  The oracle uses its own
@@ -104,3 +104,23 @@ def test_massvel_s_s_against_50_digit_value(golden):
         assert abs(got - float(exact)) <= 1e-10 * abs(float(exact))
         n += 1
     assert n >= 4
+
+
+def test_momentum_and_dipole_match_reference_kernels(golden):
+    # three components each; momentum at the size the reference's own seed
+    # rounds at (observed <= 3.1e-16 of it), dipole at 1e-12 of the block
+    n = 0
+    for r in golden["records"]:
+        if "momentum" not in r:
+            continue
+        ref = np.array(r["momentum"])
+        got = oracle.primitive_vec("momentum", r["la"], r["lb"], r["a1"], r["a2"],
+                                   r["A"], r["B"])
+        scale = max(np.abs(ref).max(), momentum_scale(r))
+        assert np.abs(got - ref).max() <= 1e-12 * scale, (r["la"], r["lb"])
+        ref = np.array(r["dipole"])
+        got = oracle.primitive_vec("dipole", r["la"], r["lb"], r["a1"], r["a2"],
+                                   r["A"], r["B"], r["C"])
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (r["la"], r["lb"])
+        n += 1
+    assert n == 64
