@@ -1031,8 +1031,12 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
     // the overlap of this call runs on its own lane
     IMAGO_CUDA(cudaStreamWaitEvent(st, c->ev_scv, 0));
   }
-  rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
-                    packed_dev, st);
+  if (kind == KIND_DM)
+    rc = launch_ortho_general(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
+                              packed_dev, st);
+  else
+    rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
+                      packed_dev, st);
   mark(c);
   return rc;
 }

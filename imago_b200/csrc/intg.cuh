@@ -143,6 +143,12 @@ int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
 int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  const double2 *cv, const double2 *cc, const double2 *s_cv,
                  double2 *y, double *packed, cudaStream_t st);
+// The same for a matrix whose core-core block is not Hermitian (dipole):
+// the reference's zher2k-then-makeValeVale sequence as it stands.
+int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,
+                         const double2 *cv, const double2 *cc,
+                         const double2 *s_cv, double2 *y, double *packed,
+                         cudaStream_t st);
 // H[q] += sum_t w(t, q) blk[t] over the sh blocks of one term each
 // (n doubles), for the PSCF Hamiltonian.
 int launch_block_axpy(const double *blk, int nterm, long long n, const double *w,

@@ -474,12 +474,13 @@ __device__ __forceinline__ double2 ocombine(double t1, double t2, double t3) {
               : make_double2(t1 - t2, t3 - t1 - t2);
 }
 
-// Y(c, v) = X_cv(c, v) - 1/2 sum_l X_cc(c, l) S(l, v).  Operands are staged
-// through registers one K stage ahead of the MMAs.
+// Y(c, v) = X_cv(c, v) - ycc sum_l X_cc(c, l) S(l, v), ycc = 1/2 for a
+// Hermitian X_cc (the her2k form) and 1 for the general form below.
+// Operands are staged through registers one K stage ahead of the MMAs.
 template <bool REAL>
 __global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_y(DevSys s, const double2 *cv, const double2 *cc,
-              const double2 *s_cv, double2 *y) {
+              const double2 *s_cv, double2 *y, double ycc) {
   __shared__ OStage st;
   const int V = s.vale_dim, C = s.core_dim;
   const int ntc = (C + kOT - 1) / kOT;
@@ -535,7 +536,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
         if (c >= C || v >= V) continue;
         const double2 x = X[(long long)v * C + c];
         const double2 p = ocombine<false, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
-        Y[(long long)v * C + c] = make_double2(x.x - 0.5 * p.x, x.y - 0.5 * p.y);
+        Y[(long long)v * C + c] = make_double2(x.x - ycc * p.x, x.y - ycc * p.y);
       }
 }
 
@@ -850,12 +851,72 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
   dim3 gy(tcv * tvv, s.nk, nterm);
   dim3 gw(tvv * (tvv + 1) / 2, s.nk, nterm);
   if (s.real_k) {
-    k_ortho_y<true><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
+    k_ortho_y<true><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 0.5);
     k_ortho_w<true><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
   } else {
-    k_ortho_y<false><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y);
+    k_ortho_y<false><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 0.5);
     k_ortho_w<false><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
   }
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+// The orthogonalisation of a matrix whose core-core block is not Hermitian
+// (the dipole matrix: <a|(r - C)|b> is not invariant under the lattice
+// translation that relates a pair's two orientations).  The reference's
+// sequence is applied as it stands: zher2k (VV - S^H X_cv - X_cv^H S, its
+// diagonal made real), then + S^H X_cc S (makeValeVale,
+// intgOrtho.F90:23-213).  With Y = X_cv - X_cc S from k_ortho_y (ycc = 1):
+//   W = VV - S^H Y - X_cv^H S, and on the diagonal Im W -= Im VV,
+// which leaves there the imaginary part of S^H X_cc S alone.  One thread
+// per packed element, CUDA cores: the dipole is built once per run.
+__global__ void __launch_bounds__(256)
+    k_ortho_general_w(DevSys s, const double2 *vv, const double2 *y,
+                      const double2 *cv, const double2 *s_cv, double *packed) {
+  const int k = blockIdx.y, term = blockIdx.z;
+  const int V = s.vale_dim, C = s.core_dim;
+  const long long np = (long long)V * (V + 1) / 2;
+  const long long tk = (long long)term * s.nk + k;
+  const double2 *VVt = vv + tk * V * V;
+  const double2 *Y = y + tk * V * C, *X = cv + tk * V * C;
+  const double2 *S = s_cv + (long long)k * V * C;
+  double *out = packed + 2 * tk * np;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+       idx < np; idx += (long long)gridDim.x * blockDim.x) {
+    int col = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while ((long long)col * (col + 1) / 2 > idx) --col;
+    while ((long long)(col + 1) * (col + 2) / 2 <= idx) ++col;
+    const int row = (int)(idx - (long long)col * (col + 1) / 2);
+    const double2 *sr = S + (long long)row * C, *sc = S + (long long)col * C;
+    const double2 *yc = Y + (long long)col * C, *xr = X + (long long)row * C;
+    double wr = 0.0, wi = 0.0;
+    for (int c = 0; c < C; ++c) {
+      const double2 a = sr[c], b = yc[c], u = xr[c], v = sc[c];
+      // conj(a) b + conj(u) v
+      wr += a.x * b.x + a.y * b.y + u.x * v.x + u.y * v.y;
+      wi += a.x * b.y - a.y * b.x + u.x * v.y - u.y * v.x;
+    }
+    const double2 e = VVt[(long long)col * V + row];
+    double2 w = make_double2(e.x - wr, e.y - wi);
+    if (row == col) w.y -= e.y;
+    store_packed(out, idx, w);
+  }
+}
+
+int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,
+                         const double2 *cv, const double2 *cc,
+                         const double2 *s_cv, double2 *y, double *packed,
+                         cudaStream_t st) {
+  const int V = s.vale_dim, C = s.core_dim;
+  if (nterm == 0) return IMAGO_OK;
+  if (C == 0) return launch_ortho(s, nterm, vv, cv, cc, s_cv, y, packed, st);
+  const int tcv = (C + kOT - 1) / kOT, tvv = (V + kOT - 1) / kOT;
+  k_ortho_y<false><<<dim3(tcv * tvv, s.nk, nterm), kOThreads, 0, st>>>(s, cv, cc, s_cv,
+                                                                      y, 1.0);
+  IMAGO_CUDA(cudaGetLastError());
+  const long long np = (long long)V * (V + 1) / 2;
+  dim3 g((unsigned)std::min<long long>((np + 255) / 256, 4 * 148), s.nk, nterm);
+  k_ortho_general_w<<<g, 256, 0, st>>>(s, vv, y, cv, s_cv, packed);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
