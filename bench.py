@@ -386,6 +386,46 @@ def time_secular(bufs, pot_dim, stream, torch, steps=3):
     return float(np.median(ts))
 
 
+def adjacent_builds(g, bufs, stream, torch, dev, reps=5):
+    """Device milliseconds (median of `reps`, CUDA events on the library's
+    stream, outputs resident in HBM) of the builds beside the SCF set on the
+    same system: mass velocity, the momentum and dipole matrices (three
+    each), the PSCF Hamiltonian for one spin and for two spins with mass
+    velocity (synthetic potential coefficients), and KE + NP + all EP terms,
+    the matrices the Hamiltonian combines, for comparison.  The overlap of
+    the main run is resident, as these builds need."""
+    from imago_b200 import intg
+    n = g.nk * g.npacked * 2
+    z = lambda m: torch.empty(m * n, dtype=torch.float64, device=dev)
+    mv, v3, h1, h2 = z(1), z(3), z(1), z(2)
+    w = np.random.default_rng(1).normal(scale=0.5, size=(g.pot_dim, 2))
+    parts = {k: bufs[k].data_ptr() for k in ("ke_packed", "np_packed", "ep_packed")}
+    cases = {
+        "mass_velocity": lambda: g.build(intg.IMAGO_MV, {"mv_packed": mv.data_ptr()}),
+        "momentum_xyz": lambda: g.gauss_overlap_mm(out=v3),
+        "dipole_xyz": lambda: g.gauss_overlap_dm([0.5, 0.5, 0.5], out=v3),
+        "ham_pscf_spin1": lambda: g.ham_pscf(w[:, :1], out=h1),
+        "ham_pscf_spin2_rel": lambda: g.ham_pscf(w, rel=True, out=h2),
+        "ke_np_ep_separate": lambda: g.build(intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP,
+                                             parts),
+    }
+    out = {}
+    for name, fn in cases.items():
+        fn()
+        ts = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        out[name + "_ms"] = float(np.median(ts))
+    out["stat"] = f"median of {reps}, device events on the library's stream"
+    return out
+
+
 def silica_headline(args, local, stream, torch):
     """The 162-atom alpha-quartz build at Gamma (device time, end to end
     and the oracle on the host cores), reported beside the main line."""
@@ -638,6 +678,9 @@ def run_ours(args):
 
     tuning = g.tuning()
     secular_s = time_secular(bufs, P, stream, torch)
+    adjacent = None
+    if world == 1 and args.workload == "si8" and not args.no_adjacent:
+        adjacent = adjacent_builds(g, bufs, stream, torch, dev)
     e2e = time_e2e(system, local, stream, bufs, 5, torch)
 
     flops = algorithmic_flops(g)
@@ -685,6 +728,8 @@ def run_ours(args):
             "tuning": tuning,
             "secular_step_s": secular_s,
         }
+        if adjacent:
+            line["adjacent_builds"] = adjacent
         if args.workload == "si8" and list(args.kmesh) != [8, 8, 8]:
             line["note"] = (f"k-mesh {args.kmesh} (profiling case, not the "
                             f"measured workload)")
@@ -724,6 +769,9 @@ def main():
                          "matrices over the ranks (strong scaling)")
     ap.add_argument("--no-silica", action="store_true",
                     help="skip the 162-atom quartz report of the default run")
+    ap.add_argument("--no-adjacent", action="store_true",
+                    help="skip the timings of the mass-velocity, momentum, "
+                         "dipole and PSCF Hamiltonian builds")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -1367,6 +1367,32 @@ int build_call(imago_ctx *c, unsigned which, const imago_out &o, int ep_first = 
   return rc;
 }
 
+// One build on lane `lane`, forked from the context's stream and joined back
+// into it, so it is ordered after the caller's earlier work on that stream.
+template <class Body>
+int on_lane(imago_ctx *c, int lane, Body body) {
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = begin_call(c))) return finish(c, rc);
+  c->lane = lane;
+  cudaStream_t ks = c->cur();
+  if (cudaEventRecord(c->kfork, c->stream) != cudaSuccess ||
+      cudaStreamWaitEvent(ks, c->kfork, 0) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  if (!rc) rc = body();
+  if (cudaEventRecord(c->kjoin[lane], ks) != cudaSuccess ||
+      cudaStreamWaitEvent(c->stream, c->kjoin[lane], 0) != cudaSuccess)
+    rc = rc ? rc : IMAGO_ERR_CUDA;
+  c->lane = 0;
+  return finish(c, rc);
+}
+
+int vec_call(imago_ctx *c, Kind kind, const double *center, double *packed) {
+  if (!c || !packed || (kind == KIND_DM && !center)) return IMAGO_ERR_INVALID;
+  for (int x = 0; x < 3; ++x) c->dip_center[x] = center ? center[x] : 0.0;
+  return on_lane(c, KIND_KE, [&] { return do_vec(c, kind, packed); });
+}
+
 }  // namespace
 
 extern "C" {
@@ -1478,26 +1504,10 @@ int imago_ham_pscf(imago_ctx *c, int spin, const double *coeffs, int rel,
                    double *packed) {
   if (!c || spin < 1 || spin > 2 || !packed || (!coeffs && c->pot_dim > 0))
     return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  c->lane = KIND_EP;  // the EP lane's scratch is sized for a chunk of terms
-  rc = do_ham(c, spin, coeffs, rel != 0, packed);
-  c->lane = 0;
-  return finish(c, rc);
+  // the EP lane: its scratch is sized for a chunk of terms
+  return on_lane(c, KIND_EP, [&] { return do_ham(c, spin, coeffs, rel != 0, packed); });
 }
 
-static int vec_call(imago_ctx *c, Kind kind, const double *center, double *packed) {
-  if (!c || !packed || (kind == KIND_DM && !center)) return IMAGO_ERR_INVALID;
-  int rc = set_device(c);
-  if (rc) return rc;
-  if ((rc = begin_call(c))) return finish(c, rc);
-  for (int x = 0; x < 3; ++x) c->dip_center[x] = center ? center[x] : 0.0;
-  c->lane = KIND_KE;
-  rc = do_vec(c, kind, packed);
-  c->lane = 0;
-  return finish(c, rc);
-}
 
 int imago_gauss_overlap_mm(imago_ctx *c, double *packed) {
   return vec_call(c, KIND_MM, nullptr, packed);
