@@ -199,6 +199,7 @@ struct imago_ctx {
   // PSCF Hamiltonian: accumulated sh blocks per spin, the potential
   // coefficients, and the packed result when outputs go to the host
   DBuf<double> ham_blk, ham_w, ham_out;
+  int ham_mode = 0;  // 0 by system size and spin, 1 block sums, 2 fused
   // momentum / dipole: the dipole centre of the current call and the three
   // packed matrices when outputs go to the host
   double dip_center[3] = {0.0, 0.0, 0.0};
@@ -1207,30 +1208,63 @@ int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
 }
 
 // The PSCF Hamiltonian (gaussOverlapHamPSCF, integrals.F90:2860-3606, with
-// orthoHamPSCF 3913-4043): kinetic, mass velocity (rel), nuclear and the
-// potential terms weighted by potCoeffs(potDim, spin), summed over the
-// primitive sh blocks.  The contraction, phase sum and orthogonalisation
-// are linear, so they then run once per spin instead of once per term.
+// orthoHamPSCF 3913-4043): the potential terms weighted by potCoeffs(potDim,
+// spin), then the kinetic, mass-velocity (rel) and nuclear blocks added.
+// The contraction, phase sum and orthogonalisation are linear, so they then
+// run once per spin instead of once per term.  The potential terms are
+// summed either in registers per shell pair (k_prim3c_ham: one thread per
+// shell pair runs all terms, one spin per pass) or, for small systems and
+// two spins, as the EP build's per-term blocks added with their weights
+// (k_block_axpy): one thread per (shell pair, term) keeps a small system's
+// GPU busy, and two spins share one pass over the terms
+// (imago_intg_set_ham_mode forces either).  Measured on one
+// B200: 62k shell pairs (Si8) 2.9 ms by blocks, 4.2 ms fused; 1.36M (162-atom
+// quartz) 51 ms by blocks, 37 ms fused; two spins on quartz 53 ms by blocks,
+// 70 ms fused.
+constexpr long long kHamFusedMinPairs = 300000;
+
 int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packed) {
   if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
   cudaStream_t st = c->cur();
   const DevSys &s = c->sys;
   const DevWork &w = c->work;
-  const int chunk = ep_chunk_size(c);
-  int rc = ensure_scratch(c, std::max(chunk, spin));
+  int rc = ensure_scratch(c, spin);
   if (rc) return rc;
   imago_ctx::Scratch &S = c->scr[c->lane];
   const long long n = c->blk_total;
   if ((rc = c->ham_blk.alloc((size_t)n * spin + 1, st))) return rc;
   if ((rc = c->ham_w.alloc((size_t)c->pot_dim * spin + 1, st))) return rc;
-  IMAGO_CUDA(cudaMemsetAsync(c->ham_blk.p, 0, sizeof(double) * n * spin, st));
+  const bool fused = c->pot_dim > 0 &&
+                     (c->ham_mode == 2 ||
+                      (c->ham_mode == 0 && spin == 1 &&
+                       (long long)c->sps.size() >= kHamFusedMinPairs));
+  const int chunk = fused ? 0 : ep_chunk_size(c);
+  if (!fused && (rc = ensure_scratch(c, std::max(chunk, spin)))) return rc;
+  if (!fused)
+    IMAGO_CUDA(cudaMemsetAsync(c->ham_blk.p, 0, sizeof(double) * n * spin, st));
   if (c->pot_dim > 0)
     IMAGO_CUDA(cudaMemcpyAsync(c->ham_w.p, coeffs, sizeof(double) * c->pot_dim * spin,
                                cudaMemcpyHostToDevice, st));
-  const int nchunk = (c->pot_dim + chunk - 1) / chunk;
-  c->launches += class_launches(c) * (2 + (rel ? 1 : 0) + nchunk) +
+  const int nchunk = fused || c->pot_dim == 0 ? 0 : (c->pot_dim + chunk - 1) / chunk;
+  c->launches += class_launches(c) * (2 + (rel ? 1 : 0) + (fused ? spin : nchunk)) +
                  (2 + (rel ? 1 : 0) + nchunk) + 2 + (c->core_dim > 0 ? 2 : 1);
   mark(c);
+  if (fused) {
+    for (int h = 0; h < spin; ++h)
+      if ((rc = launch_prim3c_ham(s, w, c->cls_beg, c->d_terms.p, c->pot_dim,
+                                  c->ham_w.p + (size_t)h * c->pot_dim,
+                                  c->ham_blk.p + (size_t)h * n, st)))
+        return rc;
+  } else {
+    for (int t0 = 0; t0 < c->pot_dim; t0 += chunk) {
+      const int nt = std::min(chunk, c->pot_dim - t0);
+      if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + t0, nt, false, S.blk.p, st)))
+        return rc;
+      if ((rc = launch_block_axpy(S.blk.p, nt, n, c->ham_w.p + t0, c->pot_dim, spin,
+                                  c->ham_blk.p, st)))
+        return rc;
+    }
+  }
   if ((rc = launch_prim2c(s, w, c->cls_beg, kPrim2cKinetic, S.blk.p, st))) return rc;
   if ((rc = launch_block_axpy(S.blk.p, 1, n, nullptr, 0, spin, c->ham_blk.p, st))) return rc;
   if (rel) {
@@ -1241,14 +1275,6 @@ int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packe
   }
   if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st))) return rc;
   if ((rc = launch_block_axpy(S.blk.p, 1, n, nullptr, 0, spin, c->ham_blk.p, st))) return rc;
-  for (int t0 = 0; t0 < c->pot_dim; t0 += chunk) {
-    const int nt = std::min(chunk, c->pot_dim - t0);
-    if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + t0, nt, false, S.blk.p, st)))
-      return rc;
-    if ((rc = launch_block_axpy(S.blk.p, nt, n, c->ham_w.p + t0, c->pot_dim, spin,
-                                c->ham_blk.p, st)))
-      return rc;
-  }
   mark(c);
   if ((rc = launch_contract(s, w, spin, c->ham_blk.p, S.M.p, st))) return rc;
   mark(c);
@@ -1749,6 +1775,12 @@ int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) 
   if (bloch_width) *bloch_width = c->work.bw;
   if (trial_ms)
     for (int i = 0; i < kNumBlochWidths; ++i) trial_ms[i] = c->bloch_ms[i];
+  return IMAGO_OK;
+}
+
+int imago_intg_set_ham_mode(imago_ctx *c, int mode) {
+  if (!c || mode < 0 || mode > 2) return IMAGO_ERR_INVALID;
+  c->ham_mode = mode;
   return IMAGO_OK;
 }
 

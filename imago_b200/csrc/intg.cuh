@@ -128,6 +128,11 @@ enum { kPrim2cOverlap = 0, kPrim2cKinetic = 1, kPrim2cMassVel = 2 };
 // Launchers (kernels.cu).  All take the stream to run on.
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   int op, double *blk, cudaStream_t st);
+// The PSCF Hamiltonian's potential terms for one spin, summed in registers
+// per shell pair: H = sum_t coef[t] EP_t (sh blocks, written, not added).
+int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
+                      const Term3c *terms_dev, int nterm, const double *coef,
+                      double *H, cudaStream_t st);
 // Momentum (dipole = false) or dipole blocks about `center`: three
 // components per shell pair, component c at blk + c * blk_total.
 int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,

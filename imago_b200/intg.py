@@ -77,6 +77,8 @@ def lib():
             getattr(L, n).restype = ctypes.c_int
         L.imago_gauss_overlap_dm.argtypes = [ctypes.c_void_p, _D, _D]
         L.imago_gauss_overlap_dm.restype = ctypes.c_int
+        L.imago_intg_set_ham_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.imago_intg_set_ham_mode.restype = ctypes.c_int
         L.imago_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int, _D]
         L.imago_ham_pscf.restype = ctypes.c_int
         L.imago_elec_pot_gauss_overlap_range.argtypes = [ctypes.c_void_p, ctypes.c_int,
@@ -299,6 +301,13 @@ class IntegralSetup:
         if hasattr(out, "data_ptr"):
             return ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D)
         return _p(out)
+
+    def set_ham_mode(self, mode):
+        """How ham_pscf sums the potential terms (imago_intg_set_ham_mode):
+        "auto", "blocks" (per-term blocks added with their weights) or
+        "fused" (all terms of a shell pair in registers, a pass per spin)."""
+        m = {"auto": 0, "blocks": 1, "fused": 2}[mode]
+        _check(lib().imago_intg_set_ham_mode(self._ctx, m), "imago_intg_set_ham_mode")
 
     def gauss_overlap_mm(self, out=None):
         """Momentum matrices -i<a|d/dx_c|b>, c = x, y, z

@@ -208,6 +208,13 @@ IMAGO_API int imago_gauss_overlap_dm(imago_ctx *ctx, const double center[3],
 IMAGO_API int imago_ham_pscf(imago_ctx *ctx, int spin, const double *coeffs, int rel,
                              double *packed);
 
+/* How imago_ham_pscf sums the potential terms (no counterpart in the
+ * reference): 0 chooses by system size and spin, 1 builds each term's
+ * primitive blocks and adds them with their weights, 2 sums all terms of a
+ * shell pair in registers, one pass per spin.  The results agree to
+ * rounding; the choice is a matter of speed. */
+IMAGO_API int imago_intg_set_ham_mode(imago_ctx *ctx, int mode);
+
 /* Every electronic potential term: replaces elecPotGaussOverlap,
  * gaussOverlapEP, electronicPE and ortho(4) for all potDim terms
  * (integrals.F90:1946-2531, 2700-2858). */

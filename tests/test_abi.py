@@ -113,3 +113,5 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_gauss_overlap_mm(None, None) == 1
     L.imago_gauss_overlap_dm.argtypes = [vp, vp, vp]
     assert L.imago_gauss_overlap_dm(None, None, None) == 1
+    L.imago_intg_set_ham_mode.argtypes = [vp, ctypes.c_int]
+    assert L.imago_intg_set_ham_mode(None, 0) == 1

@@ -462,6 +462,11 @@ def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
     with intg.IntegralSetup(s) as g:
         g.gauss_overlap_ol()
         got = g.ham_pscf(coeffs, rel=rel)
+        # the potential terms summed in registers instead of by blocks
+        g.set_ham_mode("fused")
+        fused = g.ham_pscf(coeffs, rel=rel)
+        g.set_ham_mode("blocks")
+        blocks = g.ham_pscf(coeffs, rel=rel)
         # the same matrices from the separate builds, combined afterwards
         lin = g.gauss_overlap_ke() + g.gauss_overlap_np() + np.tensordot(
             coeffs.T, g.elec_pot_gauss_overlap(), axes=1)
@@ -469,6 +474,8 @@ def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
             lin = lin + g.gauss_overlap_mv()
     assert got.shape == ref.shape == (spin, g.nk, g.npacked, 2)
     _assert_all({"H%d" % q: packed_mismatch(got[q], ref[q]) for q in range(spin)})
+    _assert_all({"fused%d" % q: packed_mismatch(fused[q], ref[q]) for q in range(spin)})
+    _assert_all({"blocks%d" % q: packed_mismatch(blocks[q], ref[q]) for q in range(spin)})
     # each separate matrix had its |x| < 1e-10 zeroed by the packing
     # (coreDim > 0), so the combination may differ by 1e-10 per matrix
     # times its weight
