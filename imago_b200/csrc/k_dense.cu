@@ -540,13 +540,15 @@ __global__ void __launch_bounds__(kOThreads, 4)
       }
 }
 
-// Upper tiles (J <= I) of W = S^H Y + Y^H S as one K loop over the stacked
-// core index (S;Y)^H (Y;S), then VV'(j, i) = VV(j, i) - W(j, i) packed at
-// i(i+1)/2 + j.
+// Upper tiles (J <= I) of W = S^H Y + X2^H S as one K loop over the stacked
+// core index (S;X2)^H (Y;S), then VV'(j, i) = VV(j, i) - W(j, i) packed at
+// i(i+1)/2 + j.  The her2k form passes X2 = Y and makes the diagonal real;
+// the general form (`general`, X2 = X_cv, Y = X_cv - X_cc S) keeps on the
+// diagonal the imaginary part of S^H X_cc S = -Im W there.
 template <bool REAL>
 __global__ void __launch_bounds__(kOThreads, 4)
-    k_ortho_w(DevSys s, const double2 *vv, const double2 *y,
-              const double2 *s_cv, double *packed) {
+    k_ortho_w(DevSys s, const double2 *vv, const double2 *y, const double2 *x2,
+              const double2 *s_cv, double *packed, bool general) {
   __shared__ OStage st;
   const int V = s.vale_dim, C = s.core_dim;
   // upper-triangular tile index -> (J, I), J <= I
@@ -559,7 +561,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
   const int k = blockIdx.y, term = blockIdx.z;
   const long long tk = (long long)term * s.nk + k;
   const double2 *S = s_cv + (long long)k * V * C;
-  const double2 *Y = y + tk * V * C;
+  const double2 *Y = y + tk * V * C, *X2 = x2 + tk * V * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K2 = 2 * C;
   double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
@@ -576,7 +578,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
       const int j = J * kOT + r, ii = I * kOT + r;
       double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
       if (l < K2) {
-        const double2 *Aop = l < C ? S : Y;   // (S; Y), conjugated in the MMA
+        const double2 *Aop = l < C ? S : X2;  // (S; X2), conjugated in the MMA
         const double2 *Bop = l < C ? Y : S;   // (Y; S)
         const int lc = l < C ? l : l - C;
         if (j < V) a = Aop[(long long)j * C + lc];
@@ -619,7 +621,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
         const double2 p = ocombine<true, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
         v.x -= p.x;
         v.y -= p.y;
-        if (row == col) v.y = 0.0;  // zherk/zher2k keep the diagonal real
+        if (row == col) v.y = general ? -p.y : 0.0;  // zher2k keeps it real
         if (fabs(v.x) < kPackThresh) v.x = 0.0;
         if (fabs(v.y) < kPackThresh) v.y = 0.0;
         const long long idx = (long long)col * (col + 1) / 2 + row;
@@ -852,10 +854,10 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
   dim3 gw(tvv * (tvv + 1) / 2, s.nk, nterm);
   if (s.real_k) {
     k_ortho_y<true><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 0.5);
-    k_ortho_w<true><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
+    k_ortho_w<true><<<gw, kOThreads, 0, st>>>(s, vv, y, y, s_cv, packed, false);
   } else {
     k_ortho_y<false><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 0.5);
-    k_ortho_w<false><<<gw, kOThreads, 0, st>>>(s, vv, y, s_cv, packed);
+    k_ortho_w<false><<<gw, kOThreads, 0, st>>>(s, vv, y, y, s_cv, packed, false);
   }
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
@@ -866,43 +868,9 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
 // translation that relates a pair's two orientations).  The reference's
 // sequence is applied as it stands: zher2k (VV - S^H X_cv - X_cv^H S, its
 // diagonal made real), then + S^H X_cc S (makeValeVale,
-// intgOrtho.F90:23-213).  With Y = X_cv - X_cc S from k_ortho_y (ycc = 1):
-//   W = VV - S^H Y - X_cv^H S, and on the diagonal Im W -= Im VV,
-// which leaves there the imaginary part of S^H X_cc S alone.  One thread
-// per packed element, CUDA cores: the dipole is built once per run.
-__global__ void __launch_bounds__(256)
-    k_ortho_general_w(DevSys s, const double2 *vv, const double2 *y,
-                      const double2 *cv, const double2 *s_cv, double *packed) {
-  const int k = blockIdx.y, term = blockIdx.z;
-  const int V = s.vale_dim, C = s.core_dim;
-  const long long np = (long long)V * (V + 1) / 2;
-  const long long tk = (long long)term * s.nk + k;
-  const double2 *VVt = vv + tk * V * V;
-  const double2 *Y = y + tk * V * C, *X = cv + tk * V * C;
-  const double2 *S = s_cv + (long long)k * V * C;
-  double *out = packed + 2 * tk * np;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-       idx < np; idx += (long long)gridDim.x * blockDim.x) {
-    int col = (int)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
-    while ((long long)col * (col + 1) / 2 > idx) --col;
-    while ((long long)(col + 1) * (col + 2) / 2 <= idx) ++col;
-    const int row = (int)(idx - (long long)col * (col + 1) / 2);
-    const double2 *sr = S + (long long)row * C, *sc = S + (long long)col * C;
-    const double2 *yc = Y + (long long)col * C, *xr = X + (long long)row * C;
-    double wr = 0.0, wi = 0.0;
-    for (int c = 0; c < C; ++c) {
-      const double2 a = sr[c], b = yc[c], u = xr[c], v = sc[c];
-      // conj(a) b + conj(u) v
-      wr += a.x * b.x + a.y * b.y + u.x * v.x + u.y * v.y;
-      wi += a.x * b.y - a.y * b.x + u.x * v.y - u.y * v.x;
-    }
-    const double2 e = VVt[(long long)col * V + row];
-    double2 w = make_double2(e.x - wr, e.y - wi);
-    if (row == col) w.y -= e.y;
-    store_packed(out, idx, w);
-  }
-}
-
+// intgOrtho.F90:23-213).  With Y = X_cv - X_cc S (k_ortho_y, ycc = 1) that
+// is W = VV - S^H Y - X_cv^H S, the diagonal keeping Im(S^H X_cc S):
+// k_ortho_w's general form, on the tensor cores like the her2k form.
 int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,
                          const double2 *cv, const double2 *cc,
                          const double2 *s_cv, double2 *y, double *packed,
@@ -914,9 +882,8 @@ int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,
   k_ortho_y<false><<<dim3(tcv * tvv, s.nk, nterm), kOThreads, 0, st>>>(s, cv, cc, s_cv,
                                                                       y, 1.0);
   IMAGO_CUDA(cudaGetLastError());
-  const long long np = (long long)V * (V + 1) / 2;
-  dim3 g((unsigned)std::min<long long>((np + 255) / 256, 4 * 148), s.nk, nterm);
-  k_ortho_general_w<<<g, 256, 0, st>>>(s, vv, y, cv, s_cv, packed);
+  k_ortho_w<false><<<dim3(tvv * (tvv + 1) / 2, s.nk, nterm), kOThreads, 0, st>>>(
+      s, vv, y, cv, s_cv, packed, true);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
