@@ -2,11 +2,12 @@
 // packed integrals (secularEqnSCF, secularEqn.F90:135-186).
 //
 // For each k-point the reference accumulates, in this order, the packed
-// nuclear, kinetic and electronic-potential matrices,
-//   H = NP + KE + sum_j w_j EP_j,
+// nuclear, kinetic, mass-velocity (rel = 1 only) and electronic-potential
+// matrices,
+//   H = NP + KE (+ MV) + sum_j w_j EP_j,
 // through readPackedMatrixAccum (matrixSubs.F90:339-375), whose factor rule
-// is: a factor of exactly 0.0 adds the matrix unscaled (that is how KE is
-// added), any other factor multiplies it -- so a potential coefficient of
+// is: a factor of exactly 0.0 adds the matrix unscaled (that is how KE and
+// MV are added), any other factor multiplies it -- so a potential coefficient of
 // exactly zero adds its term with weight one.  It then unpacks H and the
 // overlap S into the upper triangle of full matrices (unpackMatrix,
 // matrixSubs.F90:405-433) for zhegv(1, 'V', 'U').  Here both triangles are
@@ -22,9 +23,9 @@ constexpr size_t kJacobiMaxSmem = 216 * 1024;
 namespace {
 
 __global__ void k_secular(int V, long long np, int nk, int pot_dim,
-                          const double *npm, const double *ke, const double *ep,
-                          const double *w, const double *ol, double2 *h,
-                          double2 *s) {
+                          const double *npm, const double *ke, const double *mv,
+                          const double *ep, const double *w, const double *ol,
+                          double2 *h, double2 *s) {
   const long long n = (long long)nk * np;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n;
        g += (long long)gridDim.x * blockDim.x) {
@@ -36,6 +37,10 @@ __global__ void k_secular(int V, long long np, int nk, int pot_dim,
     const int row = (int)(idx - (long long)col * (col + 1) / 2);
     const long long pk = 2 * ((long long)k * np + idx);
     double re = npm[pk] + ke[pk], im = npm[pk + 1] + ke[pk + 1];
+    if (mv) {
+      re = re + mv[pk];
+      im = im + mv[pk + 1];
+    }
     for (int j = 0; j < pot_dim; ++j) {
       const double f = w[j] == 0.0 ? 1.0 : w[j];
       const long long pj = 2 * (((long long)j * nk + k) * np + idx);
@@ -220,13 +225,14 @@ extern "C" int imago_hermitian_eigvals(int n, int batch, const double *a,
   return IMAGO_OK;
 }
 
-extern "C" int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
-                                      const double *np_packed,
-                                      const double *ke_packed,
-                                      const double *ep_packed,
-                                      const double *pot_coeffs,
-                                      const double *ol_packed, double *h_full,
-                                      double *s_full, void *stream) {
+extern "C" int imago_secular_matrices_rel(int vale_dim, int num_kpoints, int pot_dim,
+                                          const double *np_packed,
+                                          const double *ke_packed,
+                                          const double *mv_packed,
+                                          const double *ep_packed,
+                                          const double *pot_coeffs,
+                                          const double *ol_packed, double *h_full,
+                                          double *s_full, void *stream) {
   if (vale_dim <= 0 || num_kpoints <= 0 || pot_dim < 0 || !np_packed ||
       !ke_packed || (pot_dim > 0 && (!ep_packed || !pot_coeffs)) || !ol_packed ||
       !h_full || !s_full)
@@ -235,9 +241,21 @@ extern "C" int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim
   const long long n = np * num_kpoints;
   const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 148 * 16);
   imago::k_secular<<<grid, 256, 0, (cudaStream_t)stream>>>(
-      vale_dim, np, num_kpoints, pot_dim, np_packed, ke_packed, ep_packed,
+      vale_dim, np, num_kpoints, pot_dim, np_packed, ke_packed, mv_packed, ep_packed,
       pot_coeffs, ol_packed, reinterpret_cast<double2 *>(h_full),
       reinterpret_cast<double2 *>(s_full));
   if (cudaGetLastError() != cudaSuccess) return IMAGO_ERR_CUDA;
   return IMAGO_OK;
+}
+
+extern "C" int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
+                                      const double *np_packed,
+                                      const double *ke_packed,
+                                      const double *ep_packed,
+                                      const double *pot_coeffs,
+                                      const double *ol_packed, double *h_full,
+                                      double *s_full, void *stream) {
+  return imago_secular_matrices_rel(vale_dim, num_kpoints, pot_dim, np_packed,
+                                    ke_packed, nullptr, ep_packed, pot_coeffs,
+                                    ol_packed, h_full, s_full, stream);
 }

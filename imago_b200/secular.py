@@ -23,7 +23,9 @@ from . import intg
 
 
 def secular_matrices(out, pot_coeffs, stream=None):
-    """Full Hermitian H and S [nk, V, V] (complex128, CUDA) for every k."""
+    """Full Hermitian H and S [nk, V, V] (complex128, CUDA) for every k;
+    with out["mv_packed"] (a scalar-relativistic run) H includes the mass
+    velocity, added after KE as the reference does."""
     npk = out["np_packed"]
     nk, npacked = npk.shape[0], npk.shape[1]
     V = int((int((8 * npacked + 1) ** 0.5) - 1) // 2)
@@ -36,16 +38,18 @@ def secular_matrices(out, pot_coeffs, stream=None):
         raise ValueError(f"{w.numel()} coefficients for {P} potential terms")
     h = torch.empty((nk, V, V), dtype=torch.complex128, device=npk.device)
     s = torch.empty_like(h)
+    mv = out.get("mv_packed")
     L = intg.lib()
-    L.imago_secular_matrices.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 8
-    L.imago_secular_matrices.restype = ctypes.c_int
+    L.imago_secular_matrices_rel.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 9
+    L.imago_secular_matrices_rel.restype = ctypes.c_int
     st = torch.cuda.current_stream().cuda_stream if stream is None else stream
-    rc = L.imago_secular_matrices(
+    rc = L.imago_secular_matrices_rel(
         V, nk, P, npk.data_ptr(), out["ke_packed"].data_ptr(),
+        mv.data_ptr() if mv is not None else None,
         ep.data_ptr() if P else None, w.data_ptr() if P else None,
         out["ol_packed"].data_ptr(), h.data_ptr(), s.data_ptr(), st)
     if rc:
-        raise intg.ImagoError(rc, "imago_secular_matrices")
+        raise intg.ImagoError(rc, "imago_secular_matrices_rel")
     # stored [k][col][row]: the matrix is the transpose of each slice
     return h.transpose(-2, -1), s.transpose(-2, -1)
 

@@ -301,6 +301,19 @@ IMAGO_API int imago_secular_matrices(int vale_dim, int num_kpoints, int pot_dim,
                                      const double *ol_packed, double *h_full,
                                      double *s_full, void *stream);
 
+/* imago_secular_matrices for a scalar-relativistic run (rel == 1): the
+ * mass-velocity matrix is added after KE with factor 0.0, i.e. unscaled
+ * (secularEqn.F90:157-163), H = NP + KE + MV + sum_j w_j EP_j.  mv_packed
+ * may be null, which is imago_secular_matrices. */
+IMAGO_API int imago_secular_matrices_rel(int vale_dim, int num_kpoints, int pot_dim,
+                                         const double *np_packed,
+                                         const double *ke_packed,
+                                         const double *mv_packed,
+                                         const double *ep_packed,
+                                         const double *pot_coeffs,
+                                         const double *ol_packed, double *h_full,
+                                         double *s_full, void *stream);
+
 /*
  * Eigenvalues of `batch` Hermitian n x n matrices (device memory, (re, im)
  * interleaved, either storage order) into w [batch][n], ascending, by a

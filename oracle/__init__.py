@@ -257,9 +257,11 @@ class OracleBuild:
         return o
 
 
-def secular_eigenvalues(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed):
+def secular_eigenvalues(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed,
+                        mv_packed=None):
     """The secular equation of one SCF step on the CPU, as secularEqnSCF
-    (secularEqn.F90:135-186) does it: H = NP + KE + sum_j w_j EP_j in that
+    (secularEqn.F90:135-186) does it: H = NP + KE (+ MV for a
+    scalar-relativistic run) + sum_j w_j EP_j in that
     order with readPackedMatrixAccum's rule (a factor of exactly 0.0 adds
     the matrix unscaled, matrixSubs.F90:369-373), upper triangles unpacked
     (matrixSubs.F90:405-433), then LAPACK's generalised Hermitian solver
@@ -275,6 +277,8 @@ def secular_eigenvalues(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed):
     for k in range(nk):
         hp = np_packed[k, :, 0] + 1j * np_packed[k, :, 1]
         hp = hp + (ke_packed[k, :, 0] + 1j * ke_packed[k, :, 1])
+        if mv_packed is not None:  # rel == 1, secularEqn.F90:157-163
+            hp = hp + (mv_packed[k, :, 0] + 1j * mv_packed[k, :, 1])
         for j, w in enumerate(pot_coeffs):
             f = 1.0 if w == 0.0 else w
             hp = hp + (ep_packed[j, k, :, 0] + 1j * ep_packed[j, k, :, 1]) * f

@@ -37,8 +37,10 @@ def test_zero_factor_adds_the_matrix_unscaled():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small", "si8_2x2x2"])
-def test_secular_eigenvalues_match_oracle(imago_lib, name):
+@pytest.mark.parametrize("name,rel", [("small", False), ("si8_2x2x2", False),
+                                      ("small", True)])
+def test_secular_eigenvalues_match_oracle(imago_lib, name, rel):
+    # rel: a scalar-relativistic step, the mass velocity added after KE
     import torch
     from imago_b200 import secular
     s = (configs.small_test_system() if name == "small"
@@ -46,8 +48,9 @@ def test_secular_eigenvalues_match_oracle(imago_lib, name):
     ob = oracle.OracleBuild(s)
     ol = ob.overlap()[0]
     ke, npm, ep = ob.kinetic(), ob.nuclear(), ob.elec_pot()
+    mv = ob.mass_velocity() if rel else None
     w = _coefficients(ep.shape[0])
-    ref = oracle.secular_eigenvalues(npm, ke, ep, w, ol)
+    ref = oracle.secular_eigenvalues(npm, ke, ep, w, ol, mv_packed=mv)
     dev = torch.device("cuda", 0)
     with intg.IntegralSetup(s, outputs_on_device=True) as g:
         C = max(g.core_dim, 1)
@@ -55,8 +58,11 @@ def test_secular_eigenvalues_match_oracle(imago_lib, name):
                   "ol_cv_im": (g.nk, g.vale_dim, C), "ke_packed": (g.nk, g.npacked, 2),
                   "np_packed": (g.nk, g.npacked, 2),
                   "ep_packed": (g.pot_dim, g.nk, g.npacked, 2)}
+        if rel:
+            shapes["mv_packed"] = (g.nk, g.npacked, 2)
         out = {k: torch.empty(v, dtype=torch.float64, device=dev) for k, v in shapes.items()}
-        g.build(out=out)
+        which = intg.IMAGO_OL | intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP
+        g.build(which | (intg.IMAGO_MV if rel else 0), out=out)
         ev = secular.secular_eigenvalues(out, w).cpu().numpy()
     assert ev.shape == ref.shape
     assert np.abs(ev - ref).max() <= EV_TOL, np.abs(ev - ref).max()
@@ -96,3 +102,17 @@ def test_oracle_pscf_hamiltonian_is_the_combination_of_its_parts():
            + np.tensordot(w.T, ob.elec_pot(), axes=1))
     assert h.shape == lin.shape
     assert np.abs(h - lin).max() <= 1e-12 * np.abs(lin).max()
+
+
+def test_mass_velocity_shifts_the_oracle_eigenvalues():
+    # rel adds -p^4/8c^2: every eigenvalue moves down, by a few per cent
+    # at most (the most at the highest states, where p^4 is largest)
+    s = configs.small_test_system()
+    ob = oracle.OracleBuild(s)
+    ol = ob.overlap()[0]
+    ke, npm, ep, mv = ob.kinetic(), ob.nuclear(), ob.elec_pot(), ob.mass_velocity()
+    w = _coefficients(ep.shape[0])
+    a = oracle.secular_eigenvalues(npm, ke, ep, w, ol)
+    b = oracle.secular_eigenvalues(npm, ke, ep, w, ol, mv_packed=mv)
+    assert np.all(b <= a + 1e-12)
+    assert np.all(a - b <= 0.05 * (np.abs(a) + 1.0))
