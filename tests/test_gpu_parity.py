@@ -527,3 +527,32 @@ def test_momentum_and_dipole_builds_match_oracle(imago_lib, name):
     assert np.abs(mm).max() > 0.0 and np.abs(dm).max() > 0.0
     if name == "gamma":
         assert np.abs(mm[..., 1]).max() > 0.0  # imaginary off-diagonal kept
+
+
+def test_adjacent_builds_on_device_outputs_and_graph(imago_lib):
+    # outputs_on_device: the mass velocity inside a captured build graph and
+    # the momentum / dipole matrices written straight to device memory agree
+    # bit for bit with the host-output builds
+    import torch
+    s = configs.silicon_cubic8(kmesh=(2, 2, 3))
+    center = [0.3, 0.1, -0.2]
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        mv_h, mm_h, dm_h = g.gauss_overlap_mv(), g.gauss_overlap_mm(), g.gauss_overlap_dm(center)
+    which = intg.IMAGO_OL | intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP | intg.IMAGO_MV
+    with intg.IntegralSetup(s, outputs_on_device=True) as g:
+        sh = _shapes(g)
+        sh["mv_packed"] = (g.nk, g.npacked, 2)
+        got = _device_outputs(torch, sh)
+        for _ in range(2):  # eager build and capture, then a replay
+            got["mv_packed"].fill_(np.nan)
+            g.build_graph(got, which=which)
+            torch.cuda.synchronize()
+            assert np.array_equal(got["mv_packed"].cpu().numpy(), mv_h)
+        v3 = torch.full((3, g.nk, g.npacked, 2), np.nan, dtype=torch.float64, device="cuda")
+        g.gauss_overlap_mm(out=v3)
+        torch.cuda.synchronize()
+        assert np.array_equal(v3.cpu().numpy(), mm_h)
+        g.gauss_overlap_dm(center, out=v3)
+        torch.cuda.synchronize()
+        assert np.array_equal(v3.cpu().numpy(), dm_h)
