@@ -386,7 +386,7 @@ def time_secular(bufs, pot_dim, stream, torch, steps=3):
     return float(np.median(ts))
 
 
-def adjacent_builds(g, bufs, stream, torch, dev, reps=5):
+def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     """Device milliseconds (median of `reps`, CUDA events on the library's
     stream, outputs resident in HBM) of the builds beside the SCF set on the
     same system: mass velocity, the momentum and dipole matrices (three
@@ -400,6 +400,7 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5):
     mv, v3, h1, h2 = z(1), z(3), z(1), z(2)
     w = np.random.default_rng(1).normal(scale=0.5, size=(g.pot_dim, 2))
     parts = {k: bufs[k].data_ptr() for k in ("ke_packed", "np_packed", "ep_packed")}
+    g.set_ham_mode(ham_mode)
     cases = {
         "mass_velocity": lambda: g.build(intg.IMAGO_MV, {"mv_packed": mv.data_ptr()}),
         "momentum_xyz": lambda: g.gauss_overlap_mm(out=v3),
@@ -423,6 +424,8 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5):
             ts.append(a.elapsed_time(b))
         out[name + "_ms"] = float(np.median(ts))
     out["stat"] = f"median of {reps}, device events on the library's stream"
+    out["ham_mode"] = ham_mode
+    g.set_ham_mode("auto")
     return out
 
 
@@ -680,7 +683,7 @@ def run_ours(args):
     secular_s = time_secular(bufs, P, stream, torch)
     adjacent = None
     if world == 1 and args.workload == "si8" and not args.no_adjacent:
-        adjacent = adjacent_builds(g, bufs, stream, torch, dev)
+        adjacent = adjacent_builds(g, bufs, stream, torch, dev, ham_mode=args.ham_mode)
     e2e = time_e2e(system, local, stream, bufs, 5, torch)
 
     flops = algorithmic_flops(g)
@@ -769,6 +772,10 @@ def main():
                          "matrices over the ranks (strong scaling)")
     ap.add_argument("--no-silica", action="store_true",
                     help="skip the 162-atom quartz report of the default run")
+    ap.add_argument("--ham-mode", default="auto", choices=["auto", "blocks", "fused"],
+                    help="how the PSCF Hamiltonian of the adjacent builds sums "
+                         "its potential terms (profiling the fused kernel on a "
+                         "small case)")
     ap.add_argument("--no-adjacent", action="store_true",
                     help="skip the timings of the mass-velocity, momentum, "
                          "dipole and PSCF Hamiltonian builds")
