@@ -772,7 +772,8 @@ def main():
                          "matrices over the ranks (strong scaling)")
     ap.add_argument("--no-silica", action="store_true",
                     help="skip the 162-atom quartz report of the default run")
-    ap.add_argument("--ham-mode", default="auto", choices=["auto", "blocks", "fused"],
+    ap.add_argument("--ham-mode", default="auto",
+                    choices=["auto", "blocks", "fused", "fused1"],
                     help="how the PSCF Hamiltonian of the adjacent builds sums "
                          "its potential terms (profiling the fused kernel on a "
                          "small case)")

@@ -199,7 +199,8 @@ struct imago_ctx {
   // PSCF Hamiltonian: accumulated sh blocks per spin, the potential
   // coefficients, and the packed result when outputs go to the host
   DBuf<double> ham_blk, ham_w, ham_out;
-  int ham_mode = 0;  // 0 by system size and spin, 1 block sums, 2 fused
+  // 0 by system size and spin, 1 block sums, 2 fused, 3 fused one lane
+  int ham_mode = 0;
   // momentum / dipole: the dipole centre of the current call and the three
   // packed matrices when outputs go to the host
   double dip_center[3] = {0.0, 0.0, 0.0};
@@ -1211,16 +1212,15 @@ int do_ep(imago_ctx *c, double *packed, int first = 0, int count = -1) {
 // orthoHamPSCF 3913-4043): the potential terms weighted by potCoeffs(potDim,
 // spin), then the kinetic, mass-velocity (rel) and nuclear blocks added.
 // The contraction, phase sum and orthogonalisation are linear, so they then
-// run once per spin instead of once per term.  The potential terms are
-// summed either in registers per shell pair (k_prim3c_ham: one thread per
-// shell pair runs all terms, one spin per pass) or, for small systems and
-// two spins, as the EP build's per-term blocks added with their weights
-// (k_block_axpy): one thread per (shell pair, term) keeps a small system's
-// GPU busy, and two spins share one pass over the terms
-// (imago_intg_set_ham_mode forces either).  Measured on one
-// B200: 62k shell pairs (Si8) 2.9 ms by blocks, 4.2 ms fused; 1.36M (162-atom
-// quartz) 51 ms by blocks, 37 ms fused; two spins on quartz 53 ms by blocks,
-// 70 ms fused.
+// run once per spin instead of once per term.  For one spin the potential
+// terms are summed in registers per shell pair (k_prim3c_ham; four lanes
+// per pair below kHamFusedMinPairs shell pairs, so that a small system
+// fills the GPU); for two spins, which would run that term loop twice, as
+// the EP build's per-term blocks added with their weights (k_block_axpy).
+// imago_intg_set_ham_mode forces either.  Measured on one B200, spin 1:
+// Si8 (62k shell pairs) 2.6 ms fused with four lanes, 4.2 ms with one,
+// 2.9 ms by blocks; 162-atom quartz (1.36M) 37 ms fused, 51 ms by blocks.
+// Two spins: Si8 4.2 ms fused, 3.2 ms by blocks; quartz 70 and 53 ms.
 constexpr long long kHamFusedMinPairs = 300000;
 
 int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packed) {
@@ -1235,9 +1235,10 @@ int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packe
   if ((rc = c->ham_blk.alloc((size_t)n * spin + 1, st))) return rc;
   if ((rc = c->ham_w.alloc((size_t)c->pot_dim * spin + 1, st))) return rc;
   const bool fused = c->pot_dim > 0 &&
-                     (c->ham_mode == 2 ||
-                      (c->ham_mode == 0 && spin == 1 &&
-                       (long long)c->sps.size() >= kHamFusedMinPairs));
+                     (c->ham_mode >= 2 || (c->ham_mode == 0 && spin == 1));
+  // a small system's shell pairs get four lanes each
+  const int lanes =
+      c->ham_mode == 3 || (long long)c->sps.size() >= kHamFusedMinPairs ? 1 : 4;
   const int chunk = fused ? 0 : ep_chunk_size(c);
   if (!fused && (rc = ensure_scratch(c, std::max(chunk, spin)))) return rc;
   if (!fused)
@@ -1252,7 +1253,7 @@ int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packe
   if (fused) {
     for (int h = 0; h < spin; ++h)
       if ((rc = launch_prim3c_ham(s, w, c->cls_beg, c->d_terms.p, c->pot_dim,
-                                  c->ham_w.p + (size_t)h * c->pot_dim,
+                                  c->ham_w.p + (size_t)h * c->pot_dim, lanes,
                                   c->ham_blk.p + (size_t)h * n, st)))
         return rc;
   } else {
@@ -1779,7 +1780,7 @@ int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) 
 }
 
 int imago_intg_set_ham_mode(imago_ctx *c, int mode) {
-  if (!c || mode < 0 || mode > 2) return IMAGO_ERR_INVALID;
+  if (!c || mode < 0 || mode > 3) return IMAGO_ERR_INVALID;
   c->ham_mode = mode;
   return IMAGO_OK;
 }

@@ -130,9 +130,10 @@ int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   int op, double *blk, cudaStream_t st);
 // The PSCF Hamiltonian's potential terms for one spin, summed in registers
 // per shell pair: H = sum_t coef[t] EP_t (sh blocks, written, not added).
+// lanes (1 or 4) threads share a shell pair's terms (s, p, d classes).
 int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
                       const Term3c *terms_dev, int nterm, const double *coef,
-                      double *H, cudaStream_t st);
+                      int lanes, double *H, cudaStream_t st);
 // Momentum (dipole = false) or dipole blocks about `center`: three
 // components per shell pair, component c at blk + c * blk_total.
 int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,

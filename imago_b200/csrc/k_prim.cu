@@ -169,72 +169,89 @@ __global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
 }
 
 // The potential terms of the PSCF Hamiltonian (gaussOverlapHamPSCF,
-// integrals.F90:3240-3442) for one spin, fused: one thread per shell pair
-// runs every term's site and image loops of k_prim3c, weighting each term
-// by its coefficient coef[t] times (pi/z3)^1.5, into one Hermite
-// accumulator, and writes one Hermite-to-spherical transform to
-// H + sp.boff.  The per-term blocks of the EP build are never formed.
-template <int LA, int LB>
+// integrals.F90:3240-3442) for one spin, fused: T adjacent lanes of a warp
+// share a shell pair, each running the site and image loops of k_prim3c for
+// every T-th term, weighting the term by its coefficient coef[t] times
+// (pi/z3)^1.5, into its Hermite accumulator; the T accumulators are summed
+// by warp shuffles and the first lane writes one Hermite-to-spherical
+// transform to H + sp.boff.  The per-term blocks of the EP build are never
+// formed.  T > 1 gives a small system's shell pairs enough threads.
+template <int LA, int LB, int T>
 __global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
     k_prim3c_ham(DevSys s, DevWork w, int beg, int n, const Term3c *terms, int nterm,
                  const double *coef, double *H) {
   constexpr int L = LA + LB;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n) return;
-  const DSp sp = w.sps[w.sp_by_cls[beg + g]];
-  const SpGeom q = sp_geom(s, w, sp);
-  const double cen = q.a1s / (q.a1s + q.a2s);
-  const double adist = s.T / q.a2s / cen;
-  const double frac = 1 - q.r2 / adist;
-  double Ps[3], Pt[3];
-  const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
-  double pm = 0.0;
-#pragma unroll
-  for (int x = 0; x < 3; ++x) {
-    Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
-    Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
-    const double e = Ps[x] - 0.5 * (q.A[x] + q.B[x]);
-    pm += e * e;
-  }
-  pm = sqrt(pm);
-  const float pmf = __double2float_ru(pm);
+  static_assert(32 % T == 0, "a shell pair's lanes stay in one warp");
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int pair = (int)(g / T), sub = (int)(g % T);
+  // lanes past the last pair stay for the shuffles below
+  const bool live = pair < n;
   double Q[nherm(L)];
 #pragma unroll
   for (int i = 0; i < nherm(L); ++i) Q[i] = 0.0;
-  for (int tl = 0; tl < nterm; ++tl) {
-    const Term3c tm = terms[tl];
-    const int pt = tm.ptype;
-    const double a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
-    const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
-    // alphaPotDist (gaussRelations.f90:187-196)
-    const double t = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
-    const double z3e = zeta + a3, mu = zeta * a3 / z3e;
-    const double wt = coef[tl] * pow(kPi / z3e, 1.5);
-    const float tf = __double2float_ru(t);
-    const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
-    for (int cb = s0 - s0 % kSiteCluster; cb < s1; cb += kSiteCluster) {
-      if (w.cl_d1 &&
-          beyond(w.cl_d1[(long long)sp.unit * w.ncl + cb / kSiteCluster], pmf, tf))
-        continue;
-      const int lo = max(cb, s0), hi = min(cb + kSiteCluster, s1);
-      for (int site = lo; site < hi; ++site) {
-        double L2[3], v[3], c0;
-        if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
-        const double *C = s.psite_pos + 3 * site;
-        const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-        for (int nc = 0; nc < s.ncell; ++nc) {
-          if (s.csize[nc] > maxr) break;
-          const double *R = s.cell + 3 * nc;
-          const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-          if (dx * dx + dy * dy + dz * dz > t) continue;
-          double X[3];
+  DSp sp{};
+  SpGeom q{};
+  if (live) {
+    sp = w.sps[w.sp_by_cls[beg + pair]];
+    q = sp_geom(s, w, sp);
+    const double cen = q.a1s / (q.a1s + q.a2s);
+    const double adist = s.T / q.a2s / cen;
+    const double frac = 1 - q.r2 / adist;
+    double Ps[3], Pt[3];
+    const double zeta = q.a1 + q.a2;
+    double pm = 0.0;
 #pragma unroll
-          for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-          accumulate_overlap_q<L>(X, mu, wt, Q);
+    for (int x = 0; x < 3; ++x) {
+      Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
+      Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+      const double e = Ps[x] - 0.5 * (q.A[x] + q.B[x]);
+      pm += e * e;
+    }
+    pm = sqrt(pm);
+    const float pmf = __double2float_ru(pm);
+    for (int tl = sub; tl < nterm; tl += T) {
+      const Term3c tm = terms[tl];
+      const int pt = tm.ptype;
+      const double a3 = s.palpha[s.ptype_alpha_off[pt] + tm.j];
+      const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
+      // alphaPotDist (gaussRelations.f90:187-196)
+      const double t = frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s);
+      const double z3e = zeta + a3, mu = zeta * a3 / z3e;
+      const double wt = coef[tl] * pow(kPi / z3e, 1.5);
+      const float tf = __double2float_ru(t);
+      const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
+      for (int cb = s0 - s0 % kSiteCluster; cb < s1; cb += kSiteCluster) {
+        if (w.cl_d1 &&
+            beyond(w.cl_d1[(long long)sp.unit * w.ncl + cb / kSiteCluster], pmf, tf))
+          continue;
+        const int lo = max(cb, s0), hi = min(cb + kSiteCluster, s1);
+        for (int site = lo; site < hi; ++site) {
+          double L2[3], v[3], c0;
+          if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+          const double *C = s.psite_pos + 3 * site;
+          const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+          for (int nc = 0; nc < s.ncell; ++nc) {
+            if (s.csize[nc] > maxr) break;
+            const double *R = s.cell + 3 * nc;
+            const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+            if (dx * dx + dy * dy + dz * dz > t) continue;
+            double X[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+            accumulate_overlap_q<L>(X, mu, wt, Q);
+          }
         }
       }
     }
   }
+  if (T > 1) {
+#pragma unroll
+    for (int off = T / 2; off > 0; off /= 2)
+#pragma unroll
+      for (int i = 0; i < nherm(L); ++i) Q[i] += __shfl_xor_sync(0xffffffffu, Q[i], off);
+  }
+  if (!live || sub != 0) return;
+  const double xi = q.a1 * q.a2 / (q.a1 + q.a2);
   hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, exp(-xi * q.r2), Q, H + sp.boff);
 }
 
@@ -510,14 +527,21 @@ int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,
 
 int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
                       const Term3c *terms_dev, int nterm, const double *coef,
-                      double *H, cudaStream_t st) {
+                      int lanes, double *H, cudaStream_t st) {
   if (nterm <= 0) return IMAGO_OK;
+  if (lanes != 1 && lanes != 4) return IMAGO_ERR_INVALID;
 #define IMAGO_PH(a, b)                                                          \
   {                                                                            \
     const int beg = cls_beg[a * 4 + b], n = cls_beg[a * 4 + b + 1] - beg;      \
     if (n > 0) {                                                               \
-      k_prim3c_ham<a, b><<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, n, terms_dev, \
-                                                          nterm, coef, H);     \
+      const long long nt = (long long)n * lanes;                               \
+      const unsigned grid = (unsigned)((nt + 127) / 128);                      \
+      if (lanes == 4)                                                          \
+        k_prim3c_ham<a, b, 4><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev,   \
+                                                    nterm, coef, H);           \
+      else                                                                     \
+        k_prim3c_ham<a, b, 1><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev,   \
+                                                    nterm, coef, H);           \
       IMAGO_CUDA(cudaGetLastError());                                          \
     }                                                                          \
   }

@@ -304,9 +304,10 @@ class IntegralSetup:
 
     def set_ham_mode(self, mode):
         """How ham_pscf sums the potential terms (imago_intg_set_ham_mode):
-        "auto", "blocks" (per-term blocks added with their weights) or
-        "fused" (all terms of a shell pair in registers, a pass per spin)."""
-        m = {"auto": 0, "blocks": 1, "fused": 2}[mode]
+        "auto", "blocks" (per-term blocks added with their weights),
+        "fused" (all terms of a shell pair in registers, a pass per spin,
+        four lanes per shell pair on small systems) or "fused1" (one lane)."""
+        m = {"auto": 0, "blocks": 1, "fused": 2, "fused1": 3}[mode]
         _check(lib().imago_intg_set_ham_mode(self._ctx, m), "imago_intg_set_ham_mode")
 
     def gauss_overlap_mm(self, out=None):

@@ -209,10 +209,11 @@ IMAGO_API int imago_ham_pscf(imago_ctx *ctx, int spin, const double *coeffs, int
                              double *packed);
 
 /* How imago_ham_pscf sums the potential terms (no counterpart in the
- * reference): 0 chooses by system size and spin, 1 builds each term's
- * primitive blocks and adds them with their weights, 2 sums all terms of a
- * shell pair in registers, one pass per spin.  The results agree to
- * rounding; the choice is a matter of speed. */
+ * reference): 0 chooses by spin count and system size, 1 builds each
+ * term's primitive blocks and adds them with their weights, 2 sums all
+ * terms of a shell pair in registers (one pass per spin; several lanes per
+ * shell pair on small systems), 3 as 2 with one lane per shell pair.  The
+ * results agree to rounding; the choice is a matter of speed. */
 IMAGO_API int imago_intg_set_ham_mode(imago_ctx *ctx, int mode);
 
 /* Every electronic potential term: replaces elecPotGaussOverlap,

@@ -465,6 +465,8 @@ def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
         # the potential terms summed in registers instead of by blocks
         g.set_ham_mode("fused")
         fused = g.ham_pscf(coeffs, rel=rel)
+        g.set_ham_mode("fused1")
+        fused1 = g.ham_pscf(coeffs, rel=rel)
         g.set_ham_mode("blocks")
         blocks = g.ham_pscf(coeffs, rel=rel)
         # the same matrices from the separate builds, combined afterwards
@@ -475,6 +477,7 @@ def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
     assert got.shape == ref.shape == (spin, g.nk, g.npacked, 2)
     _assert_all({"H%d" % q: packed_mismatch(got[q], ref[q]) for q in range(spin)})
     _assert_all({"fused%d" % q: packed_mismatch(fused[q], ref[q]) for q in range(spin)})
+    _assert_all({"fused1_%d" % q: packed_mismatch(fused1[q], ref[q]) for q in range(spin)})
     _assert_all({"blocks%d" % q: packed_mismatch(blocks[q], ref[q]) for q in range(spin)})
     # each separate matrix had its |x| < 1e-10 zeroed by the packing
     # (coreDim > 0), so the combination may differ by 1e-10 per matrix
