@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <utility>
 #include <atomic>
 #include <mutex>
 #include <thread>
@@ -69,6 +71,29 @@ cudaMemPool_t scratch_pool() {
   return g_pools[dev];
 }
 
+// An allocator whose resize leaves trivial elements uninitialised: the
+// work arrays of a large cell (millions of shell pairs) are then first
+// written, and their pages first touched, by the threads that fill them.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U> &) {}
+  template <class U, class... A>
+  void construct(U *q, A &&...a) {
+    if constexpr (sizeof...(A) == 0)
+      ::new ((void *)q) U;
+    else
+      ::new ((void *)q) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 template <class T>
 struct DBuf {
   T *p = nullptr;
@@ -88,7 +113,8 @@ struct DBuf {
     n = count;
     return IMAGO_OK;
   }
-  int upload(const std::vector<T> &v, cudaStream_t st) {
+  template <class Vec>
+  int upload(const Vec &v, cudaStream_t st) {
     int rc = alloc(v.empty() ? 1 : v.size(), st);
     if (rc) return rc;
     if (!v.empty())
@@ -141,9 +167,9 @@ struct imago_ctx {
 
   // work lists
   std::vector<DPair> pairs;
-  std::vector<DUnit> units;
-  std::vector<DSp> sps;
-  std::vector<int> sp_by_cls;
+  HostVec<DUnit> units;
+  HostVec<DSp> sps;
+  HostVec<int> sp_by_cls;
   std::vector<int2> btile;
   // tensor-core phase-sum tiles for each tuned width, concatenated, and
   // where each width's list starts
@@ -574,10 +600,16 @@ int read_system(imago_ctx *c, const imago_system *s) {
 // The pair / image / alpha-pair screens of integrals.F90:323-569.
 // Work lists of a contiguous range of atom pairs, with indices and offsets
 // local to the range; build_work joins the ranges in order.
+// Shell pairs sort by class and, within a class, by the pair's own part of
+// the three-centre screening radius^2 in four buckets (kSortKeys keys).
+constexpr int kSortKeys = 16 * 4;
+
 struct PairWork {
   std::vector<DPair> pairs;
   std::vector<DUnit> units;
   std::vector<DSp> sps;
+  std::vector<unsigned char> key;  // sort key of each shell pair
+  int hist[kSortKeys] = {};
   long long moff = 0, boff = 0;
   int rc = IMAGO_OK;
 };
@@ -654,6 +686,15 @@ void build_pairs(const imago_ctx *c, const std::vector<int2> &ij, size_t lo,
             sp.boff = w.boff;
             w.boff += nsh(sp.la) * nsh(sp.lb);
             w.sps.push_back(sp);
+            // the pair's own part of the three-centre screening radius^2,
+            // frac T / (a1 + a2) (gaussRelations alphaNucDist/alphaPotDist
+            // without the third exponent)
+            const double reach =
+                (1.0 - r2 / adist(a, b)) * c->T / (s1.alphas[a] + s2.alphas[b]);
+            const int bucket = reach > 64.0 ? 0 : reach > 16.0 ? 1 : reach > 4.0 ? 2 : 3;
+            const int key = (sp.la * 4 + sp.lb) * 4 + bucket;
+            w.key.push_back((unsigned char)key);
+            ++w.hist[key];
           }
         }
         u.spend = (int)w.sps.size();
@@ -699,71 +740,70 @@ int build_work(imago_ctx *c) {
   parallel_ranges(ij.size(), nchunk, [&](size_t k, size_t lo, size_t hi) {
     build_pairs(c, ij, lo, hi, part[k]);
   });
-  long long moff = 0, boff = 0;
-  size_t np = 0, nu = 0, ns = 0;
-  for (const PairWork &w : part) {
+  // offsets of each part in the merged arrays, then the parts copied (and
+  // their shell pairs' sort positions scattered) in parallel
+  const size_t nparts = part.size();
+  std::vector<size_t> pb(nparts + 1, 0), ub(nparts + 1, 0), sb(nparts + 1, 0);
+  std::vector<long long> mb(nparts + 1, 0), bb(nparts + 1, 0);
+  for (size_t k = 0; k < nparts; ++k) {
+    const PairWork &w = part[k];
     if (w.rc) return w.rc;
-    np += w.pairs.size();
-    nu += w.units.size();
-    ns += w.sps.size();
+    pb[k + 1] = pb[k] + w.pairs.size();
+    ub[k + 1] = ub[k] + w.units.size();
+    sb[k + 1] = sb[k] + w.sps.size();
+    mb[k + 1] = mb[k] + w.moff;
+    bb[k + 1] = bb[k] + w.boff;
   }
-  c->pairs.reserve(np);
-  c->units.reserve(nu);
-  c->sps.reserve(ns);
-  for (const PairWork &w : part) {
-    const int pb = (int)c->pairs.size(), ub = (int)c->units.size();
-    const int sb = (int)c->sps.size();
-    for (DPair p : w.pairs) {
-      p.ubeg += ub;
-      p.uend += ub;
-      p.moff += moff;
-      c->pairs.push_back(p);
-    }
-    for (DUnit u : w.units) {
-      u.pair += pb;
-      u.spbeg += sb;
-      u.spend += sb;
-      c->units.push_back(u);
-    }
-    for (DSp sp : w.sps) {
-      sp.unit += ub;
-      sp.boff += boff;
-      c->sps.push_back(sp);
-    }
-    moff += w.moff;
-    boff += w.boff;
+  c->pairs.resize(pb[nparts]);
+  c->units.resize(ub[nparts]);
+  c->sps.resize(sb[nparts]);
+  c->blk_total = bb[nparts];
+  c->m_total = mb[nparts];
+  // Shell pairs by class and, within a class, by reach bucket (above 64,
+  // 16, 4 bohr^2 and below), stable in unit order: a warp then holds shell
+  // pairs of similar reach, whose site screens agree.  The order only maps
+  // threads to shell pairs.  A stable counting sort, each part scattering
+  // its own shell pairs from its offsets per key.
+  std::vector<long long> start(kSortKeys + 1, 0);
+  for (size_t k = 0; k < nparts; ++k)
+    for (int q = 0; q < kSortKeys; ++q) start[q + 1] += part[k].hist[q];
+  for (int q = 0; q < kSortKeys; ++q) start[q + 1] += start[q];
+  std::vector<long long> off((size_t)nparts * kSortKeys);
+  {
+    std::vector<long long> run(start.begin(), start.end() - 1);
+    for (size_t k = 0; k < nparts; ++k)
+      for (int q = 0; q < kSortKeys; ++q) {
+        off[k * kSortKeys + q] = run[q];
+        run[q] += part[k].hist[q];
+      }
   }
-  c->blk_total = boff;
-  c->m_total = moff;
-  // Shell pairs by class and, within a class, by the pair's own part of
-  // the three-centre screening radius^2, frac T / (a1 + a2) (gaussRelations
-  // alphaNucDist/alphaPotDist without the third exponent), in four buckets
-  // (above 64, 16, 4 bohr^2 and below), stable in unit order: a warp then
-  // holds shell pairs of similar reach, whose site screens agree.  The
-  // order only maps threads to shell pairs.
-  std::vector<int> key(c->sps.size());
-  for (size_t q = 0; q < c->sps.size(); ++q) {
-    const DSp &sp = c->sps[q];
-    const DUnit &u = c->units[sp.unit];
-    const DPair &p = c->pairs[u.pair];
-    const HType &s1 = c->types[c->type_screen[p.ti]];
-    const HType &s2 = c->types[c->type_screen[p.tj]];
-    const double x1 = s1.alphas[sp.a], x2 = s2.alphas[sp.b];
-    const double frac = 1.0 - u.r2 / (c->T / x2 / (x1 / (x1 + x2)));
-    const double reach = frac * c->T / (x1 + x2);
-    const int bucket = reach > 64.0 ? 0 : reach > 16.0 ? 1 : reach > 4.0 ? 2 : 3;
-    key[q] = (sp.la * 4 + sp.lb) * 4 + bucket;
-  }
-  // stable counting sort over the 16 x 4 keys
-  constexpr int kKeys = 16 * 4;
-  std::vector<int> start(kKeys + 1, 0), idx(c->sps.size());
-  for (int k : key) ++start[k + 1];
-  for (int k = 0; k < kKeys; ++k) start[k + 1] += start[k];
-  for (size_t q = 0; q < key.size(); ++q) idx[start[key[q]]++] = (int)q;
-  c->sp_by_cls = idx;
-  for (int k = 0; k <= 16; ++k) c->cls_beg[k] = 0;
-  for (const DSp &sp : c->sps) c->cls_beg[sp.la * 4 + sp.lb + 1] += 1;
-  for (int k = 0; k < 16; ++k) c->cls_beg[k + 1] += c->cls_beg[k];
+  c->sp_by_cls.resize(sb[nparts]);
+  parallel_ranges(sb[nparts], nparts, [&](size_t k, size_t, size_t) {
+    const PairWork &w = part[k];
+    for (size_t q = 0; q < w.pairs.size(); ++q) {
+      DPair p = w.pairs[q];
+      p.ubeg += (int)ub[k];
+      p.uend += (int)ub[k];
+      p.moff += mb[k];
+      c->pairs[pb[k] + q] = p;
+    }
+    for (size_t q = 0; q < w.units.size(); ++q) {
+      DUnit u = w.units[q];
+      u.pair += (int)pb[k];
+      u.spbeg += (int)sb[k];
+      u.spend += (int)sb[k];
+      c->units[ub[k] + q] = u;
+    }
+    long long *o = &off[k * kSortKeys];
+    for (size_t q = 0; q < w.sps.size(); ++q) {
+      DSp sp = w.sps[q];
+      sp.unit += (int)ub[k];
+      sp.boff += bb[k];
+      c->sps[sb[k] + q] = sp;
+      c->sp_by_cls[o[w.key[q]]++] = (int)(sb[k] + q);
+    }
+  });
+  for (int k = 0; k <= 16; ++k) c->cls_beg[k] = (int)start[4 * k];
   // phase-sum tiles: every pair (also those with no image, whose blocks
   // are written as zeros) in column tiles of kBlochCols block elements
   c->btile.clear();
