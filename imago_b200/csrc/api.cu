@@ -1481,9 +1481,12 @@ int imago_intg_create(const imago_system *sys, const imago_opts *opts,
     delete c;
     return IMAGO_ERR_NO_DEVICE;
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, c->device) != cudaSuccess ||
-      prop.major != 10) {
+  // one attribute, not cudaGetDeviceProperties, which queries them all and
+  // costs milliseconds on every context
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c->device) !=
+          cudaSuccess ||
+      major != 10) {
     cudaGetLastError();
     delete c;
     return IMAGO_ERR_NO_DEVICE;
