@@ -417,14 +417,15 @@ def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
         assert np.array_equal(ref["ol_cv_im"], got["ol_cv_im"])
 
 
-@pytest.mark.parametrize("name", ["small", "f", "silicon8"])
+@pytest.mark.parametrize("name", ["small", "f", "silicon8", "nocore"])
 def test_mass_velocity_build_matches_oracle(imago_lib, name):
     # gaussOverlapMV: the kinetic build's loops with the mass-velocity
     # primitive accumulated negatively, orthogonalised like KE; the f system
     # runs the runtime-class kernel
     s = {"small": configs.small_test_system,
          "f": configs.f_test_system,
-         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3))}[name]()
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3)),
+         "nocore": configs.no_core_test_system}[name]()
     ob = oracle.OracleBuild(s)
     ob.overlap()
     ref = ob.mass_velocity()
@@ -446,14 +447,16 @@ def test_mass_velocity_needs_overlap_first(imago_lib):
 
 
 @pytest.mark.parametrize("name,spin,rel", [("small", 1, False), ("small", 2, True),
-                                           ("f", 2, False), ("silicon8", 2, True)])
+                                           ("f", 2, False), ("silicon8", 2, True),
+                                           ("nocore", 1, True)])
 def test_pscf_hamiltonian_matches_oracle(imago_lib, name, spin, rel):
     # gaussOverlapHamPSCF: kinetic + nuclear + potCoeffs-weighted potential
     # terms (- mass velocity) per spin, against the oracle's restatement of
     # its loop nest (inline screen radius, per-alpha-pair accumulation)
     s = {"small": configs.small_test_system,
          "f": configs.f_test_system,
-         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3))}[name]()
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3)),
+         "nocore": configs.no_core_test_system}[name]()
     ob = oracle.OracleBuild(s)
     ob.overlap()
     rng = np.random.default_rng(11)
@@ -503,7 +506,7 @@ def test_pscf_hamiltonian_device_outputs(imago_lib):
     assert np.array_equal(host, dev.cpu().numpy())
 
 
-@pytest.mark.parametrize("name", ["small", "f", "silicon8", "gamma"])
+@pytest.mark.parametrize("name", ["small", "f", "silicon8", "gamma", "nocore"])
 def test_momentum_and_dipole_builds_match_oracle(imago_lib, name):
     # gaussOverlapMM / gaussOverlapDM + ortho3Terms: three matrices each;
     # the momentum matrix takes -i in the phase sum and stays complex at
@@ -512,7 +515,8 @@ def test_momentum_and_dipole_builds_match_oracle(imago_lib, name):
          "f": configs.f_test_system,
          "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3)),
          "gamma": lambda: configs.silicon_cubic8(kmesh=(1, 1, 1),
-                                                 shift=(0.5, 0.5, 0.5))}[name]()
+                                                 shift=(0.5, 0.5, 0.5)),
+         "nocore": configs.no_core_test_system}[name]()
     center = np.array([0.7, -0.4, 1.1])
     ob = oracle.OracleBuild(s)
     ob.overlap()
