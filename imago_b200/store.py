@@ -3,8 +3,10 @@ reference's SCF integral file.
 
 The reference writes its integrals to HDF5 (hdf5SCFIntg.F90:188-460): a
 group atomIntgGroup holding atomOverlap, atomOverlapCV (when coreDim > 0),
-atomKEOverlap, atomMVOverlap (scalar-relativistic runs), atomNPOverlap and
-atomPotOverlap/<term>, one dataset per
+atomKEOverlap, atomMVOverlap (scalar-relativistic runs), atomNPOverlap,
+atomPotOverlap/<term>, and atomDMOverlap/<axis> and atomMMOverlap/<axis>
+(dipole and momentum matrices, axes x, y, z as 1..3, one status for the
+three; hdf5SCFIntg.F90:227-267, 383-396), one dataset per
 k-point named by its 1-based index ("%07d"; coreValeOL as "real%07d" and
 "imag%07d"), and an integer attribute "status" on each group that is set
 to 1 once the group's datasets are written.  setupSCF skips every matrix
@@ -27,6 +29,7 @@ import numpy as np
 GROUP = "atomIntgGroup"
 OL, CV, KE, MV, NP, EP = ("atomOverlap", "atomOverlapCV", "atomKEOverlap",
                           "atomMVOverlap", "atomNPOverlap", "atomPotOverlap")
+DM, MM = "atomDMOverlap", "atomMMOverlap"
 
 
 def _name(i):
@@ -99,6 +102,17 @@ class IntegralStore:
         return np.stack([np.load(os.path.join(d, _name(k) + ".npy"))
                          for k in range(self.nk)])
 
+    def write_xyz(self, group, packed3):
+        """packed3 [3, nk, V(V+1)/2, 2]: the x, y, z matrices in subgroups
+        1..3 of `group`."""
+        packed3 = np.asarray(packed3)
+        assert packed3.shape == (3, self.nk, self.npacked, 2), packed3.shape
+        for c in range(3):
+            self.write_packed(f"{group}/{_name(c)}", packed3[c])
+
+    def read_xyz(self, group):
+        return np.stack([self.read_packed(f"{group}/{_name(c)}") for c in range(3)])
+
     def write_cv(self, re, im):
         d = self._dir(CV)
         for k in range(self.nk):
@@ -114,10 +128,12 @@ class IntegralStore:
         return re, im
 
 
-def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False):
-    """Run, in the reference's order (imago.F90:260-293: OL, KE, MV when
-    rel, NP, EP), the builds whose status in `store` is not yet 1, writing
-    each group's datasets and then its status.
+def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False,
+                       dipole_center=None, momentum=False):
+    """Run, in the reference's order (imago.F90:260-315: OL, KE, MV when
+    rel, NP, EP, then the dipole matrices about `dipole_center` and the
+    momentum matrices when asked for), the builds whose status in `store`
+    is not yet 1, writing each group's datasets and then its status.
 
     `setup` is an IntegralSetup with host outputs (or anything with its
     gauss_overlap_ol / _ke / _mv / _np and elec_pot_gauss_overlap_range
@@ -141,7 +157,13 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False):
     if rel:
         singles.append((MV, setup.gauss_overlap_mv))
     singles.append((NP, setup.gauss_overlap_np))
-    later = any(store.status(g) == 0 for g, _ in singles) or bool(ep_todo)
+    triples = []
+    if dipole_center is not None:
+        triples.append((DM, lambda: setup.gauss_overlap_dm(dipole_center)))
+    if momentum:
+        triples.append((MM, setup.gauss_overlap_mm))
+    later = (any(store.status(g) == 0 for g, _ in singles + triples)
+             or bool(ep_todo))
     if store.status(OL) == 0 or (later and store.core_dim > 0):
         ol, re, im = setup.gauss_overlap_ol()
         if store.status(OL) == 0:
@@ -165,13 +187,18 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False):
             store.write_packed(store.ep_group(first + j), mats[j])
             done(store.ep_group(first + j))
         i += count
+    for group, call in triples:
+        if store.status(group) == 0:
+            store.write_xyz(group, call())
+            done(group)
     return written
 
 
-def read_all(store, rel=False):
+def read_all(store, rel=False, dipole=False, momentum=False):
     """Every matrix of a complete store: {"ol_packed", "ol_cv_re",
     "ol_cv_im", "ke_packed", "np_packed", "ep_packed"}, and "mv_packed"
-    when rel, as numpy arrays."""
+    when rel, "dm_packed" / "mm_packed" ([3, ...]) when asked for, as
+    numpy arrays."""
     out = {"ol_packed": store.read_packed(OL), "ke_packed": store.read_packed(KE),
            "np_packed": store.read_packed(NP),
            "ep_packed": np.stack([store.read_packed(store.ep_group(t))
@@ -180,4 +207,8 @@ def read_all(store, rel=False):
         out["ol_cv_re"], out["ol_cv_im"] = store.read_cv()
     if rel:
         out["mv_packed"] = store.read_packed(MV)
+    if dipole:
+        out["dm_packed"] = store.read_xyz(DM)
+    if momentum:
+        out["mm_packed"] = store.read_xyz(MM)
     return out

@@ -405,12 +405,17 @@ def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
             if group == box.ep_group(1):
                 raise KeyboardInterrupt
 
+        center = (0.25, -0.5, 0.75)
         with pytest.raises(KeyboardInterrupt):
-            st.build_checkpointed(g, box, ep_batch=3, on_group=stop, rel=True)
-        rest = st.build_checkpointed(g, box, rel=True)
-        assert rest[0] == box.ep_group(2)
-    got = st.read_all(box, rel=True)
-    for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed", "mv_packed"):
+            st.build_checkpointed(g, box, ep_batch=3, on_group=stop, rel=True,
+                                  dipole_center=center, momentum=True)
+        rest = st.build_checkpointed(g, box, rel=True, dipole_center=center, momentum=True)
+        assert rest[0] == box.ep_group(2) and rest[-2:] == [st.DM, st.MM]
+        ref["dm_packed"] = g.gauss_overlap_dm(center)
+        ref["mm_packed"] = g.gauss_overlap_mm()
+    got = st.read_all(box, rel=True, dipole=True, momentum=True)
+    for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed", "mv_packed",
+              "dm_packed", "mm_packed"):
         assert np.array_equal(ref[k], got[k]), k
     if g.core_dim > 0:
         assert np.array_equal(ref["ol_cv_re"], got["ol_cv_re"])

@@ -36,6 +36,14 @@ class FakeSetup:
         self.calls.append("MV")
         return self._mat(3)
 
+    def gauss_overlap_dm(self, center):
+        self.calls.append(("DM", tuple(center)))
+        return np.stack([self._mat(20 + c) for c in range(3)])
+
+    def gauss_overlap_mm(self):
+        self.calls.append("MM")
+        return np.stack([self._mat(30 + c) for c in range(3)])
+
     def gauss_overlap_np(self):
         self.calls.append("NP")
         return self._mat(2)
@@ -108,3 +116,23 @@ def test_relativistic_run_adds_mass_velocity_in_order(tmp_path):
     # a later non-relativistic store of the same system skips MV entirely
     f2 = FakeSetup()
     assert st.build_checkpointed(f2, _store(tmp_path, f2)) == []
+
+
+def test_dipole_and_momentum_groups(tmp_path):
+    # atomDMOverlap/<axis>/<k> and atomMMOverlap/<axis>/<k>, one status
+    # each, built after the potential terms
+    f = FakeSetup(P=2)
+    s = _store(tmp_path, f)
+    written = st.build_checkpointed(f, s, dipole_center=(0.5, 0.0, 0.0), momentum=True)
+    assert written[-2:] == [st.DM, st.MM]
+    assert f.calls[-2:] == [("DM", (0.5, 0.0, 0.0)), "MM"]
+    root = os.path.join(str(tmp_path), st.GROUP)
+    assert os.path.exists(os.path.join(root, "atomDMOverlap", "0000003", "0000002.npy"))
+    out = st.read_all(s, dipole=True, momentum=True)
+    assert np.array_equal(out["dm_packed"][1], f._mat(21))
+    assert np.array_equal(out["mm_packed"][2], f._mat(32))
+    # a rerun with everything recorded builds nothing, the overlap included
+    f2 = FakeSetup(P=2)
+    assert st.build_checkpointed(f2, _store(tmp_path, f2), dipole_center=(0.5, 0.0, 0.0),
+                                 momentum=True) == []
+    assert f2.calls == []
