@@ -430,8 +430,9 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
 
 
 def silica_headline(args, local, stream, torch):
-    """The 162-atom alpha-quartz build at Gamma (device time, end to end
-    and the oracle on the host cores), reported beside the main line."""
+    """The 162-atom alpha-quartz build at Gamma (device time, end to end,
+    the builds beside the SCF set, and the oracle on the host cores),
+    reported beside the main line."""
     from imago_b200 import intg
     wl = "quartz-gamma"
     system = system_for(wl)
@@ -452,6 +453,9 @@ def silica_headline(args, local, stream, torch):
            "vale_dim": g.vale_dim, "core_dim": g.core_dim, "pot_terms": g.pot_dim,
            "pair_images": g.num_pair_images, "shell_pairs": g.num_shell_pairs,
            "gpu_launches": int(launches), "clocks": clk.summary()}
+    if not args.no_adjacent:
+        out["adjacent_builds"] = adjacent_builds(g, bufs, stream, torch, dev, reps=3,
+                                                 ham_mode=args.ham_mode)
     g.close()
     out["e2e"] = time_e2e(system, local, stream, bufs, 3, torch)
     del bufs, flush
