@@ -1208,6 +1208,48 @@ int do_vec(imago_ctx *c, Kind kind, double *packed) {
   return rc;
 }
 
+// The overlap with a plane wave e^{-i dK.r} for the three wave vectors dK
+// (gaussKOverlap + ortho3Terms(8), integrals3Terms.F90:956-1384,
+// 1388-1608): the complex primitive's real and imaginary parts are six
+// real terms of one contraction, summed with the Bloch phases into the
+// full (not Hermitian) matrices, orthogonalised on the full matrix and
+// written as real and imaginary planes [axis][k][col][row].
+int do_kov(imago_ctx *c, const double *dk, double *re, double *im) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  cudaStream_t st = c->cur();
+  int rc = ensure_scratch(c, 6);
+  if (rc) return rc;
+  imago_ctx::Scratch &S = c->scr[c->lane];
+  const size_t n = (size_t)3 * c->nk * c->vale_dim * c->vale_dim;
+  double *tre = re, *tim = im;
+  if (!c->outputs_on_device) {
+    if ((rc = c->vec_out.alloc(2 * n + 1, st))) return rc;
+    tre = c->vec_out.p;
+    tim = tre + n;
+  }
+  KovWaves q;
+  for (int x = 0; x < 9; ++x) q.q[x] = dk[x];
+  const DevSys &s = c->sys;
+  const DevWork &w = c->work;
+  c->launches += class_launches(c) + 2 + (c->core_dim > 0 ? 2 : 1);
+  mark(c);
+  if ((rc = launch_prim_kov(s, w, c->cls_beg, q, S.blk.p, st))) return rc;
+  mark(c);
+  if ((rc = launch_contract(s, w, 6, S.blk.p, S.M.p, st))) return rc;
+  mark(c);
+  if ((rc = launch_bloch_kov(s, w, S.M.p, S.vv.p, S.cv.p, S.cc.p, st))) return rc;
+  mark(c);
+  if (c->core_dim > 0 && c->ol_in_call) IMAGO_CUDA(cudaStreamWaitEvent(st, c->ev_scv, 0));
+  if ((rc = launch_ortho_full(s, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p, tre, tim, st)))
+    return rc;
+  mark(c);
+  if (tre != re) {
+    if ((rc = copy_out(c, re, tre, n))) return rc;
+    rc = copy_out(c, im, tim, n);
+  }
+  return rc;
+}
+
 // EP terms run in chunks sized to the scratch budget.  The chunk is fixed
 // on a context's first EP build: its scratch is sized for it, so later
 // builds (and graph captures) reuse it.
@@ -1585,6 +1627,13 @@ int imago_gauss_overlap_mm(imago_ctx *c, double *packed) {
 
 int imago_gauss_overlap_dm(imago_ctx *c, const double center[3], double *packed) {
   return vec_call(c, KIND_DM, center, packed);
+}
+
+int imago_gauss_koverlap(imago_ctx *c, const double dk[9], double *re, double *im) {
+  if (!c || !dk || !re || !im) return IMAGO_ERR_INVALID;
+  for (int x = 0; x < 9; ++x)
+    if (!std::isfinite(dk[x])) return IMAGO_ERR_INVALID;
+  return on_lane(c, KIND_KE, [&] { return do_kov(c, dk, re, im); });
 }
 
 int imago_elec_pot_gauss_overlap(imago_ctx *c, double *packed) {

@@ -134,6 +134,25 @@ int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
 int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
                       const Term3c *terms_dev, int nterm, const double *coef,
                       int lanes, double *H, cudaStream_t st);
+// The three wave vectors of a K-overlap build, q[3 * axis + xyz].
+struct KovWaves {
+  double q[9];
+};
+// K-overlap primitive blocks: real and imaginary parts of axis a as terms
+// 2a and 2a + 1 (blk + t * blk_total).
+int launch_prim_kov(const DevSys &s, const DevWork &w, const int *cls_beg,
+                    const KovWaves &dk, double *blk, cudaStream_t st);
+// The K-overlap's complex phase sum (M: 6 real terms) with the full saving
+// of the reference (block (j, i) the dagger of block (i, j), a diagonal
+// block replaced by its dagger): vv/cv/cc hold 3 complex terms.
+int launch_bloch_kov(const DevSys &s, const DevWork &w, const double *M, double2 *vv,
+                     double2 *cv, double2 *cc, cudaStream_t st);
+// The K-overlap's orthogonalisation on the full matrix, no Hermitian form:
+// W = VV - S^H X_cv - X_cv^H S + S^H X_cc S, 3 terms, written as real and
+// imaginary [term][k][col][row] planes.
+int launch_ortho_full(const DevSys &s, const double2 *vv, const double2 *cv,
+                      const double2 *cc, const double2 *s_cv, double2 *y, double *re,
+                      double *im, cudaStream_t st);
 // Momentum (dipole = false) or dipole blocks about `center`: three
 // components per shell pair, component c at blk + c * blk_total.
 int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,

@@ -545,19 +545,26 @@ __global__ void __launch_bounds__(kOThreads, 4)
 // i(i+1)/2 + j.  The her2k form passes X2 = Y and makes the diagonal real;
 // the general form (`general`, X2 = X_cv, Y = X_cv - X_cc S) keeps on the
 // diagonal the imaginary part of S^H X_cc S = -Im W there.
-template <bool REAL>
+template <bool REAL, bool FULL = false>
 __global__ void __launch_bounds__(kOThreads, 4)
     k_ortho_w(DevSys s, const double2 *vv, const double2 *y, const double2 *x2,
-              const double2 *s_cv, double *packed, bool general) {
+              const double2 *s_cv, double *packed, bool general, double *im_plane = nullptr) {
   __shared__ OStage st;
   const int V = s.vale_dim, C = s.core_dim;
-  // upper-triangular tile index -> (J, I), J <= I
-  int t = blockIdx.x, I = 0;
-  while (t > I) {
-    t -= I + 1;
-    ++I;
+  // upper-triangular tile index -> (J, I), J <= I; FULL: every tile
+  int I = 0, J = 0;
+  if (FULL) {
+    const int tvv = (V + kOT - 1) / kOT;
+    J = blockIdx.x % tvv;
+    I = blockIdx.x / tvv;
+  } else {
+    int t = blockIdx.x;
+    while (t > I) {
+      t -= I + 1;
+      ++I;
+    }
+    J = t;
   }
-  const int J = t;
   const int k = blockIdx.y, term = blockIdx.z;
   const long long tk = (long long)term * s.nk + k;
   const double2 *S = s_cv + (long long)k * V * C;
@@ -567,7 +574,7 @@ __global__ void __launch_bounds__(kOThreads, 4)
   double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
   // on a diagonal tile the warp owning rows 16..31 x columns 0..15 lies
   // wholly below the diagonal, which is never stored
-  const bool lower = J == I && (warp >> 1) > (warp & 1);
+  const bool lower = !FULL && J == I && (warp >> 1) > (warp & 1);
   double2 ra[kOLoads], rb[kOLoads];
   auto fetch = [&](int l0) {
 #pragma unroll
@@ -616,11 +623,17 @@ __global__ void __launch_bounds__(kOThreads, 4)
       for (int i = 0; i < 2; ++i) {
         const int row = J * kOT + r0 + 8 * mt + (lane >> 2);
         const int col = I * kOT + cb + 8 * nt + 2 * (lane & 3) + i;
-        if (row >= V || col >= V || row > col) continue;
+        if (row >= V || col >= V || (!FULL && row > col)) continue;
         double2 v = VVt[(long long)col * V + row];
         const double2 p = ocombine<true, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
         v.x -= p.x;
         v.y -= p.y;
+        if (FULL) {  // the whole matrix as real and imaginary planes
+          const long long o = (tk * V + col) * (long long)V + row;
+          packed[o] = v.x;
+          im_plane[o] = v.y;
+          continue;
+        }
         if (row == col) v.y = general ? -p.y : 0.0;  // zher2k keeps it real
         if (fabs(v.x) < kPackThresh) v.x = 0.0;
         if (fabs(v.y) < kPackThresh) v.y = 0.0;
@@ -859,6 +872,117 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
     k_ortho_y<false><<<gy, kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 0.5);
     k_ortho_w<false><<<gw, kOThreads, 0, st>>>(s, vv, y, y, s_cv, packed, false);
   }
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+// ------------------------------------------------------------ K-overlap --
+// saveCurrentPair with saveFull = 1 (intgSaving.F90:346-459, 513-551,
+// 555-608, 654-690): block (i, j) takes the pair's element, block (j, i)
+// its conjugate at the transposed place; for i == j the dagger, written
+// second in the reference, replaces the block, so only it is written.
+__device__ __forceinline__ void scatter_full(const DevSys &s, const DPair &p,
+                                             long long tk, int m1, int m2,
+                                             double re, double im, double2 *vv,
+                                             double2 *cv, double2 *cc) {
+  const int V = s.vale_dim, C = s.core_dim;
+  const int v1 = s.type_nvale[p.ti], v2 = s.type_nvale[p.tj];
+  const bool same = p.i == p.j;
+  if (m1 < v1 && m2 < v2) {
+    const int r = s.site_cum_vale[p.i] + m1, c = s.site_cum_vale[p.j] + m2;
+    if (!same) vv[tk * V * V + (long long)c * V + r] = make_double2(re, im);
+    vv[tk * V * V + (long long)r * V + c] = make_double2(re, -im);
+    return;
+  }
+  if (C == 0) return;
+  if (m1 >= v1 && m2 < v2) {
+    if (same) return;
+    const int row = s.site_cum_core[p.i] + (m1 - v1);
+    const int col = s.site_cum_vale[p.j] + m2;
+    cv[tk * V * C + (long long)col * C + row] = make_double2(re, im);
+  } else if (m1 < v1) {
+    const int row = s.site_cum_core[p.j] + (m2 - v2);
+    const int col = s.site_cum_vale[p.i] + m1;
+    cv[tk * V * C + (long long)col * C + row] = make_double2(re, -im);
+  } else {
+    const int r1 = s.site_cum_core[p.i] + (m1 - v1);
+    const int r2 = s.site_cum_core[p.j] + (m2 - v2);
+    if (!same) cc[tk * C * C + (long long)r2 * C + r1] = make_double2(re, im);
+    cc[tk * C * C + (long long)r1 * C + r2] = make_double2(re, -im);
+  }
+}
+
+// The K-overlap phase sum (cmplxApplyPhaseFactors, intgSaving.F90:192-238;
+// then kPointLatticeOriginShift): the complex contracted blocks are the
+// real terms 2 axis and 2 axis + 1 of M.  One thread per (block element,
+// k-point, axis), CUDA cores: the build runs once per optical run.
+__global__ void __launch_bounds__(256)
+    k_bloch_kov(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
+                double2 *cc) {
+  const int2 bt = w.btile[blockIdx.x];
+  const DPair p = w.pairs[bt.x];
+  const int ne = p.ni * p.nj, nk = s.nk;
+  const int e = bt.y * kBlochCols + (threadIdx.x & (kBlochCols - 1));
+  const int k = blockIdx.y * (256 / kBlochCols) + threadIdx.x / kBlochCols;
+  const int ax = blockIdx.z;
+  if (e >= ne || k >= nk) return;
+  const double *Mr = M + (long long)(2 * ax) * w.m_total + p.moff + e;
+  const double *Mi = M + (long long)(2 * ax + 1) * w.m_total + p.moff + e;
+  double ar = 0.0, ai = 0.0;
+  for (int u = p.ubeg; u < p.uend; ++u) {
+    const long long o = (long long)(u - p.ubeg) * ne;
+    const double xr = Mr[o], xi = Mi[o];
+    const double2 f = s.phase[(long long)w.units[u].cell * nk + k];
+    ar = ar + (f.x * xr - f.y * xi);
+    ai = ai + (f.x * xi + f.y * xr);
+  }
+  const double *kv = s.kxyz + 3 * k;
+  const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
+  if (fabs(dot) >= kSmallThresh) {
+    double sn, cs;
+    sincos(dot, &sn, &cs);
+    const double r = cs * ar - sn * ai;
+    ai = cs * ai + sn * ar;
+    ar = r;
+  }
+  const int m2 = e / p.ni, m1 = e - m2 * p.ni;
+  scatter_full(s, p, (long long)ax * nk + k, m1, m2, ar, ai, vv, cv, cc);
+}
+
+int launch_bloch_kov(const DevSys &s, const DevWork &w, const double *M, double2 *vv,
+                     double2 *cv, double2 *cc, cudaStream_t st) {
+  if (w.nbtile == 0) return IMAGO_OK;
+  constexpr int kPerBlock = 256 / kBlochCols;
+  dim3 grid(w.nbtile, (s.nk + kPerBlock - 1) / kPerBlock, 3);
+  k_bloch_kov<<<grid, 256, 0, st>>>(s, w, M, vv, cv, cc);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+__global__ void k_vv_planes(long long n, const double2 *vv, double *re, double *im) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    re[i] = vv[i].x;
+    im[i] = vv[i].y;
+  }
+}
+
+int launch_ortho_full(const DevSys &s, const double2 *vv, const double2 *cv,
+                      const double2 *cc, const double2 *s_cv, double2 *y, double *re,
+                      double *im, cudaStream_t st) {
+  const int V = s.vale_dim, C = s.core_dim;
+  if (C == 0) {
+    const long long n = 3LL * s.nk * V * V;
+    k_vv_planes<<<(unsigned)std::min<long long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(
+        n, vv, re, im);
+    IMAGO_CUDA(cudaGetLastError());
+    return IMAGO_OK;
+  }
+  const int tcv = (C + kOT - 1) / kOT, tvv = (V + kOT - 1) / kOT;
+  k_ortho_y<false><<<dim3(tcv * tvv, s.nk, 3), kOThreads, 0, st>>>(s, cv, cc, s_cv, y, 1.0);
+  IMAGO_CUDA(cudaGetLastError());
+  k_ortho_w<false, true><<<dim3(tvv * tvv, s.nk, 3), kOThreads, 0, st>>>(
+      s, vv, y, cv, s_cv, re, true, im);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }

@@ -559,6 +559,33 @@ int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
   return IMAGO_OK;
 }
 
+// K-overlap: for the three wave vectors, the real and imaginary blocks of
+// each shell pair as terms 2 axis and 2 axis + 1.
+__global__ void __launch_bounds__(128)
+    k_prim_kov(DevSys s, DevWork w, int beg, int end, int la, int lb, KovWaves dk,
+               double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+#pragma unroll 1
+  for (int ax = 0; ax < 3; ++ax)
+    prim_kov(la, lb, q.a1, q.a2, q.A, q.B, dk.q + 3 * ax,
+             blk + (long long)(2 * ax) * w.blk_total + sp.boff,
+             blk + (long long)(2 * ax + 1) * w.blk_total + sp.boff);
+}
+
+int launch_prim_kov(const DevSys &s, const DevWork &w, const int *cls_beg,
+                    const KovWaves &dk, double *blk, cudaStream_t st) {
+  for (int c = 0; c < 16; ++c) {
+    const int beg = cls_beg[c], n = cls_beg[c + 1] - beg;
+    if (n <= 0) continue;
+    k_prim_kov<<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, beg + n, c / 4, c % 4, dk, blk);
+    IMAGO_CUDA(cudaGetLastError());
+  }
+  return IMAGO_OK;
+}
+
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
                   double *blk, cudaStream_t st) {

@@ -712,6 +712,77 @@ __device__ __noinline__ void prim_vec_rt(int la, int lb, double a1, double a2,
   }
 }
 
+// Overlap with a plane wave, <a|exp(-i q.r)|b> (KOverlap2CIntg), complex,
+// as two real blocks.  The product Gaussian times exp(-i q x) is
+// exp(-i q P - q^2/(4p)) times a Gaussian about P' = P - i q/(2p): the 1D
+// recursion runs with the complex PA' = PA - i q/(2p), PB' = PB - i q/(2p)
+// and each axis carries sqrt(pi/p) exp(-xi X^2) exp(-q^2/(4p)) exp(-i q P).
+// Runtime loops (every class; the build runs once per optical run).
+static __device__ __noinline__ void prim_kov(int la, int lb, double a1, double a2,
+                                             const double *A, const double *B,
+                                             const double *q, double *out_re,
+                                             double *out_im) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  double Sr[3][4][4], Si[3][4][4], fr[3], fi[3];
+#pragma unroll 1
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta, X = A[x] - B[x];
+    const double ar = P - A[x], br = P - B[x], sh = -q[x] * inv2p;
+    Sr[x][0][0] = 1.0;
+    Si[x][0][0] = 0.0;
+    for (int i = 0; i < la; ++i) {
+      double vr = ar * Sr[x][i][0] - sh * Si[x][i][0];
+      double vi = ar * Si[x][i][0] + sh * Sr[x][i][0];
+      if (i > 0) {
+        vr += i * inv2p * Sr[x][i - 1][0];
+        vi += i * inv2p * Si[x][i - 1][0];
+      }
+      Sr[x][i + 1][0] = vr;
+      Si[x][i + 1][0] = vi;
+    }
+    for (int j = 0; j < lb; ++j)
+      for (int i = 0; i <= la; ++i) {
+        double vr = br * Sr[x][i][j] - sh * Si[x][i][j];
+        double vi = br * Si[x][i][j] + sh * Sr[x][i][j];
+        if (i > 0) {
+          vr += i * inv2p * Sr[x][i - 1][j];
+          vi += i * inv2p * Si[x][i - 1][j];
+        }
+        if (j > 0) {
+          vr += j * inv2p * Sr[x][i][j - 1];
+          vi += j * inv2p * Si[x][i][j - 1];
+        }
+        Sr[x][i][j + 1] = vr;
+        Si[x][i][j + 1] = vi;
+      }
+    const double mag = sqrt(kPi / zeta) * exp(-xi * X * X) * exp(-q[x] * q[x] / (4.0 * zeta));
+    double sn, cs;
+    sincos(q[x] * P, &sn, &cs);
+    fr[x] = mag * cs;
+    fi[x] = -mag * sn;
+  }
+  double pcr[ncart(3) * ncart(3)], pci[ncart(3) * ncart(3)];
+  const int nca = ncart(la), ncb = ncart(lb);
+#pragma unroll 1
+  for (int p = 0; p < nca; ++p)
+#pragma unroll 1
+    for (int c = 0; c < ncb; ++c) {
+      double vr = 1.0, vi = 0.0;
+      for (int x = 0; x < 3; ++x) {
+        const int i = cart_exp(p, x), j = cart_exp(c, x);
+        const double gr = Sr[x][i][j] * fr[x] - Si[x][i][j] * fi[x];
+        const double gi = Sr[x][i][j] * fi[x] + Si[x][i][j] * fr[x];
+        const double nr = vr * gr - vi * gi, ni = vr * gi + vi * gr;
+        vr = nr;
+        vi = ni;
+      }
+      pcr[p * ncb + c] = vr;
+      pci[p * ncb + c] = vi;
+    }
+  cart_to_sh_rt(la, lb, pcr, out_re);
+  cart_to_sh_rt(la, lb, pci, out_im);
+}
+
 static __device__ __noinline__ void accumulate_overlap_q_rt(int L, const double *X,
                                                      double mu, double w,
                                                      double *Q) {

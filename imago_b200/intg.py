@@ -77,6 +77,8 @@ def lib():
             getattr(L, n).restype = ctypes.c_int
         L.imago_gauss_overlap_dm.argtypes = [ctypes.c_void_p, _D, _D]
         L.imago_gauss_overlap_dm.restype = ctypes.c_int
+        L.imago_gauss_koverlap.argtypes = [ctypes.c_void_p, _D, _D, _D]
+        L.imago_gauss_koverlap.restype = ctypes.c_int
         L.imago_intg_set_ham_mode.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.imago_intg_set_ham_mode.restype = ctypes.c_int
         L.imago_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int, _D]
@@ -327,6 +329,21 @@ class IntegralSetup:
         _check(lib().imago_gauss_overlap_dm(self._ctx, _p(c), self._ptr(out)),
                "gaussOverlapDM")
         return out
+
+    def gauss_koverlap(self, dk, re=None, im=None):
+        """The overlap with a plane wave <a|exp(-i dK_c . r)|b> for three
+        wave vectors dk [3, 3] (row c is dK_c, bohr^-1)
+        (imago_gauss_koverlap): full complex matrices, returned as real and
+        imaginary planes [3, nk, V, V] indexed [c, k, col, row]."""
+        q = np.ascontiguousarray(dk, dtype=np.float64).reshape(9)
+        shape = (3, self.nk, self.vale_dim, self.vale_dim)
+        if re is None:
+            re = np.zeros(shape)
+        if im is None:
+            im = np.zeros(shape)
+        _check(lib().imago_gauss_koverlap(self._ctx, _p(q), self._ptr(re), self._ptr(im)),
+               "gaussKOverlap")
+        return re, im
 
     def ham_pscf(self, coeffs, rel=False, out=None):
         """The PSCF Hamiltonian (imago_ham_pscf): coeffs [potDim] or

@@ -198,6 +198,17 @@ IMAGO_API int imago_gauss_overlap_mm(imago_ctx *ctx, double *packed);
 IMAGO_API int imago_gauss_overlap_dm(imago_ctx *ctx, const double center[3],
                                      double *packed);
 
+/* The overlap with a plane wave, <a|exp(-i dK_c . r)|b> for three wave
+ * vectors dK_c (dk[3*c .. 3*c+2], bohr^-1; the reference passes
+ * recipVectors(:, c) / numAxialKPoints(c)): replaces gaussKOverlap +
+ * ortho3Terms(8) (integrals3Terms.F90:956-1384, 1388-1608; called at
+ * imago.F90:319 for the Berry-phase polarisation).  The matrices are not
+ * Hermitian, so they are returned whole as real and imaginary planes,
+ * re/im[(c * nk + k) * valeDim * valeDim + col * valeDim + row], unscreened.
+ * Needs the overlap first when coreDim > 0. */
+IMAGO_API int imago_gauss_koverlap(imago_ctx *ctx, const double dk[9], double *re,
+                                   double *im);
+
 /* The PSCF Hamiltonian: replaces gaussOverlapHamPSCF + orthoHamPSCF
  * (integrals.F90:2860-3606, 3913-4043; called at imago.F90:685).  One
  * matrix per spin: kinetic + nuclear + sum_t coeffs(t, q) EP_t, minus the

@@ -42,6 +42,9 @@ def lib():
         L.orc_dipole2c.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D,
                                    ctypes.c_int, ctypes.c_int, _D]
         L.orc_dipole2c.restype = None
+        L.orc_koverlap2c.argtypes = [ctypes.c_double, ctypes.c_double, _D, _D, _D,
+                                     ctypes.c_int, ctypes.c_int, _D]
+        L.orc_koverlap2c.restype = None
         for name in ("orc_electron3c", "orc_nuclear3c"):
             f = getattr(L, name)
             f.argtypes = [ctypes.c_double] * 3 + [_D, _D, _D, ctypes.c_int,
@@ -64,6 +67,7 @@ def lib():
         L.orc_gauss_overlap_mv.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_mm.argtypes = [ctypes.c_void_p, _D]
         L.orc_gauss_overlap_dm.argtypes = [ctypes.c_void_p, _D, _D]
+        L.orc_gauss_koverlap.argtypes = [ctypes.c_void_p, _D, _D, _D]
         L.orc_ham_pscf.argtypes = [ctypes.c_void_p, ctypes.c_int, _D,
                                    ctypes.c_int, _D]
         L.orc_elec_pot_gauss_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int,
@@ -103,6 +107,16 @@ def primitive_vec(kind, la, lb, a1, a2, A, B, C=None):
         raise ValueError(kind)
     n1, n2 = (la + 1) ** 2, (lb + 1) ** 2
     return sh.reshape(3, 16, 16)[:, :n1, :n2].copy()
+
+
+def primitive_koverlap(la, lb, a1, a2, A, B, dK):
+    """<a|exp(-i dK.r)|b> (KOverlap2CIntg) as a complex [nsh(la), nsh(lb)]."""
+    sh = np.zeros(512)
+    arr = [np.ascontiguousarray(v, float) for v in (A, B, dK)]
+    lib().orc_koverlap2c(a1, a2, _p(arr[0]), _p(arr[1]), _p(arr[2]), la, lb, _p(sh))
+    c = sh[0::2] + 1j * sh[1::2]
+    n1, n2 = (la + 1) ** 2, (lb + 1) ** 2
+    return c.reshape(16, 16)[:n1, :n2].copy()
 
 
 def primitive(kind, la, lb, a1, a2, a3, A, B, C):
@@ -199,6 +213,18 @@ class OracleBuild:
         out = self._packed(3)
         self._check(lib().orc_gauss_overlap_dm(self._ctx, _p(c), _p(out)), "DM")
         return out
+
+    def koverlap(self, dk):
+        """gaussKOverlap for the three wave vectors dk [3, 3] (axis, xyz):
+        complex [3, nk, V, V] (row, col)."""
+        dk = np.ascontiguousarray(dk, dtype=np.float64).reshape(9)
+        nk = self.nk
+        V = self.vale_dim
+        re = np.zeros((3, nk, V, V))
+        im = np.zeros_like(re)
+        self._check(lib().orc_gauss_koverlap(self._ctx, _p(dk), _p(re), _p(im)), "KOV")
+        # planes are [col][row]: transpose to [row][col]
+        return (re + 1j * im).transpose(0, 1, 3, 2)
 
     def ham_pscf(self, coeffs, rel=False):
         """gaussOverlapHamPSCF: coeffs [potDim] or [potDim, spin] ->

@@ -38,6 +38,9 @@ void orc_momentum2c(double a1, double a2, const double *A, const double *B,
                     int la, int lb, double *sh3);
 void orc_dipole2c(double a1, double a2, const double *A, const double *B,
                   const double *C, int la, int lb, double *sh3);
+/* <a|exp(-i dK.r)|b>: sh2[2*(i*16 + j) + 0/1] = Re/Im sh(i+1, j+1). */
+void orc_koverlap2c(double a1, double a2, const double *A, const double *B,
+                    const double *dK, int la, int lb, double *sh2);
 void orc_electron3c(double a1, double a2, double a3, const double *A,
                     const double *B, const double *C, int la, int lb,
                     double *sh);
@@ -68,6 +71,9 @@ int orc_gauss_overlap_mv(orc_ctx *c, double *packed);
  * packed [3][nk][np][2] for c = x, y, z. */
 int orc_gauss_overlap_mm(orc_ctx *c, double *packed);
 int orc_gauss_overlap_dm(orc_ctx *c, const double center[3], double *packed);
+/* K-overlap: dk[3 * axis + xyz] the three wave vectors; re, im full
+ * [3][nk][V][V] planes, column-major per k. */
+int orc_gauss_koverlap(orc_ctx *c, const double *dk, double *re, double *im);
 /* The PSCF Hamiltonian: packed [spin][nk][np][2]; coeffs the reference's
  * potCoeffs(potDim, spin), column-major: coeffs[q * potDim + t]. */
 int orc_ham_pscf(orc_ctx *c, int spin, const double *coeffs, int rel,

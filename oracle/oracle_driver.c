@@ -529,7 +529,8 @@ void orc_last_counts(const orc_ctx *c, long long *pi, long long *sp,
 
 /* ---------- the integral builds ---------- */
 
-enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3, K_MV = 4, K_HAM = 5, K_MM = 6, K_DM = 7 };
+enum { K_OL = 0, K_KE = 1, K_NP = 2, K_EP = 3, K_MV = 4, K_HAM = 5, K_MM = 6, K_DM = 7,
+       K_KOV = 8 };
 
 typedef struct {
   /* global matrices for one build (complex, column-major like Fortran) */
@@ -550,7 +551,7 @@ typedef struct {
   const double *coeffs;  /* HAM: potCoeffs(potDim, spin), column-major */
   int spin, q, rel;      /* HAM: spins, the spin built, mass velocity;
                           * MM, DM: q is the Cartesian component built */
-  const double *center;  /* DM: dipoleCenter */
+  const double *center;  /* DM: dipoleCenter; KOV: the wave vector dK */
 } buildspec;
 
 /* saveCurrentPair, intgSaving.F90:346-459 with valeValeSaving 463-510,
@@ -611,6 +612,65 @@ static void save_pair(const orc_ctx *c, gmats *g, int i, int j,
           d[0] = CP(k, v1 + b, v2 + a)[0];
           d[1] = -CP(k, v1 + b, v2 + a)[1];
         }
+  }
+#undef CP
+}
+
+/* saveCurrentPair with saveFull = 1 (intgSaving.F90:346-459, 513-551,
+ * 555-608, 654-690): block (i, j) takes the pair, block (j, i) its dagger;
+ * for i == j the dagger, written second, replaces the block. */
+static void save_pair_full(const orc_ctx *c, gmats *g, int i, int j,
+                           const double *cp, int ms) {
+  const otype *t1 = &c->types[c->site_type[i]], *t2 = &c->types[c->site_type[j]];
+  int v1 = t1->nvale, v2 = t2->nvale, c1 = t1->ncore, c2 = t2->ncore;
+  int vi = c->cum_vale[i], vj = c->cum_vale[j];
+  int ci = c->cum_core[i], cj = c->cum_core[j];
+#define CP(k, a, b) (cp + 2 * (((size_t)(k) * ms + (a)) * ms + (b)))
+  for (int k = 0; k < c->nk; ++k) {
+    for (int a = 0; a < v1; ++a)
+      for (int b = 0; b < v2; ++b) {
+        double *d = VV(g, c, k, vi + a, vj + b);
+        d[0] = CP(k, a, b)[0];
+        d[1] = CP(k, a, b)[1];
+      }
+    for (int a = 0; a < v2; ++a)
+      for (int b = 0; b < v1; ++b) {
+        double *d = VV(g, c, k, vj + a, vi + b);
+        d[0] = CP(k, b, a)[0];
+        d[1] = -CP(k, b, a)[1];
+      }
+  }
+  if (c->core_dim == 0) return;
+  if (c1 != 0)
+    for (int k = 0; k < c->nk; ++k)
+      for (int a = 0; a < c1; ++a)
+        for (int b = 0; b < v2; ++b) {
+          double *d = CV(g, c, k, ci + a, vj + b);
+          d[0] = CP(k, v1 + a, b)[0];
+          d[1] = CP(k, v1 + a, b)[1];
+        }
+  if (c2 != 0)
+    for (int k = 0; k < c->nk; ++k)
+      for (int a = 0; a < c2; ++a)
+        for (int b = 0; b < v1; ++b) {
+          double *d = CV(g, c, k, cj + a, vi + b);
+          d[0] = CP(k, b, v2 + a)[0];
+          d[1] = -CP(k, b, v2 + a)[1];
+        }
+  if (c1 == 0 || c2 == 0) return;
+  for (int k = 0; k < c->nk; ++k) {
+    for (int a = 0; a < c1; ++a)
+      for (int b = 0; b < c2; ++b) {
+        double *d = CC(g, c, k, ci + a, cj + b);
+        d[0] = CP(k, v1 + a, v2 + b)[0];
+        d[1] = CP(k, v1 + a, v2 + b)[1];
+      }
+    for (int a = 0; a < c2; ++a)
+      for (int b = 0; b < c1; ++b) {
+        double *d = CC(g, c, k, cj + a, ci + b);
+        d[0] = CP(k, v1 + b, v2 + a)[0];
+        d[1] = -CP(k, v1 + b, v2 + a)[1];
+      }
   }
 #undef CP
 }
@@ -787,7 +847,10 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
     double *cp = malloc(sizeof(double) * 2 * (size_t)nk * ms * ms);
     double *X = malloc(sizeof(double) * 16 * (size_t)ma * ms);
     double *M = malloc(sizeof(double) * (size_t)ms * ms);
-    double sh[256];
+    /* KOV: imaginary parts of X and M */
+    double *X2 = bs->kind == K_KOV ? malloc(sizeof(double) * 16 * (size_t)ma * ms) : NULL;
+    double *M2 = bs->kind == K_KOV ? malloc(sizeof(double) * (size_t)ms * ms) : NULL;
+    double sh[256], sh2[512];
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 1)
 #endif
@@ -832,6 +895,7 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
         if (r2 > lim) continue;
         ++npi;
         memset(X, 0, sizeof(double) * 16 * (size_t)ma * ms);
+        if (X2) memset(X2, 0, sizeof(double) * 16 * (size_t)ma * ms);
         int max_a1 = 0;
         int nmin = t1->nalpha < t2->nalpha ? t1->nalpha : t2->nalpha;
         for (int l = 0; l < nmin; ++l) {
@@ -862,7 +926,11 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
             else if (bs->kind == K_HAM)
               ham_pscf_pair(c, bs, e1, e2, a, b, t1->alphas[a], t2->alphas[b], r2, A,
                             Bp, la, lb, sh, &ntr);
-            else if (bs->kind == K_MM || bs->kind == K_DM) {
+            else if (bs->kind == K_KOV) {
+              /* KOverlap2CIntg, complex (integrals3Terms.F90:1293-1297) */
+              orc_koverlap2c(t1->alphas[a], t2->alphas[b], A, Bp, bs->center, la, lb, sh2);
+              for (int q = 0; q < 256; ++q) sh[q] = sh2[2 * q];
+            } else if (bs->kind == K_MM || bs->kind == K_DM) {
               /* one component of momentum2CIntg / dipole3CIntg
                * (integrals3Terms.F90:398-401, 849-852) */
               double sh3[768];
@@ -890,6 +958,11 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
                 for (int lm1 = 0; lm1 < nl; ++lm1)
                   X[((size_t)lm1 * ma + a) * ms + m] =
                       X[((size_t)lm1 * ma + a) * ms + m] + sh[lm1 * 16 + lm2] * cb;
+                if (X2)
+                  for (int lm1 = 0; lm1 < nl; ++lm1)
+                    X2[((size_t)lm1 * ma + a) * ms + m] =
+                        X2[((size_t)lm1 * ma + a) * ms + m] +
+                        sh2[2 * (lm1 * 16 + lm2) + 1] * cb;
               }
               if (a + 1 > max_a1) max_a1 = a + 1;
             }
@@ -903,6 +976,13 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
             for (int a = 0; a < max_a1; ++a)
               s = s + t1->basis[a * n1 + m1] * X[((size_t)lm1 * ma + a) * ms + m2];
             M[m1 * ms + m2] = s;
+            if (M2) {
+              /* cmplxMultWithBasisFn1 */
+              double s2 = 0.0;
+              for (int a = 0; a < max_a1; ++a)
+                s2 = s2 + t1->basis[a * n1 + m1] * X2[((size_t)lm1 * ma + a) * ms + m2];
+              M2[m1 * ms + m2] = s2;
+            }
           }
         /* applyPhaseFactors, intgSaving.F90:132-189 */
         /* gaussOverlapMV phases only pairs that used an alpha
@@ -916,7 +996,13 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
               for (int m2 = 0; m2 < n2; ++m2) {
                 double *d = cp + 2 * (((size_t)kp * ms + m1) * ms + m2);
                 double x = M[m1 * ms + m2];
-                if (bs->kind == K_MM) {
+                if (bs->kind == K_KOV) {
+                  /* cmplxApplyPhaseFactors: phase * (x + i x2),
+                   * intgSaving.F90:218-230 */
+                  const double x2 = M2[m1 * ms + m2];
+                  d[0] = d[0] + (pr * x - pi * x2);
+                  d[1] = d[1] + (pr * x2 + pi * x);
+                } else if (bs->kind == K_MM) {
                   /* applyPhaseFactors runCode 1: (0,-1) * phase * x,
                    * intgSaving.F90:178-186 */
                   d[0] = d[0] + pi * x;
@@ -944,9 +1030,14 @@ static int pair_loops(orc_ctx *c, const buildspec *bs, gmats *g) {
             }
         }
       }
-      save_pair(c, g, i, j, cp, ms);
+      if (bs->kind == K_KOV)
+        save_pair_full(c, g, i, j, cp, ms);
+      else
+        save_pair(c, g, i, j, cp, ms);
     }
     free(cp);
+    free(X2);
+    free(M2);
     free(X);
     free(M);
   }
@@ -1114,6 +1205,82 @@ static void reset_stats(orc_ctx *c) {
   c->t_loops = c->t_ortho = 0.0;
   c->n_pair_images = c->n_shell_pairs = c->n_triples = 0;
 }
+
+/* ortho3Terms(8) (integrals3Terms.F90:1388-1608 with intgOrtho.F90
+ * valeCoreCoreVale / makeValeVale, fullFlag 1): on the full matrix,
+ *   W = VV - S^H X_cv - X_cv^H S + S^H X_cc S,
+ * no Hermitian form, no diagonal rule, no zeroing; written as the real and
+ * imaginary valeVale planes, column-major per k: re[(k*V + col)*V + row]. */
+static void ortho_full(orc_ctx *c, gmats *g, double *re, double *im) {
+  const int V = c->vale_dim, C = c->core_dim;
+  for (int k = 0; k < c->nk; ++k) {
+    double *orr = re + (size_t)k * V * V, *oi = im + (size_t)k * V * V;
+    if (C == 0) {
+      for (int col = 0; col < V; ++col)
+        for (int row = 0; row < V; ++row) {
+          orr[(size_t)col * V + row] = VV(g, c, k, row, col)[0];
+          oi[(size_t)col * V + row] = VV(g, c, k, row, col)[1];
+        }
+      continue;
+    }
+    const double *S = c->s_cv + 2 * (size_t)k * V * C;
+#define SCV(row, col) (S + 2 * ((size_t)(col) * C + (row)))
+    double *vc = malloc(sizeof(double) * 2 * (size_t)C * V);
+    for (int ci = 0; ci < C; ++ci)
+      for (int v = 0; v < V; ++v) {
+        double sr = 0, si = 0;
+        for (int l = 0; l < C; ++l) {
+          const double *a = SCV(l, v), *b = CC(g, c, k, l, ci);
+          sr += a[0] * b[0] + a[1] * b[1];
+          si += a[0] * b[1] - a[1] * b[0];
+        }
+        vc[2 * ((size_t)v * C + ci)] = sr;
+        vc[2 * ((size_t)v * C + ci) + 1] = si;
+      }
+    for (int i = 0; i < V; ++i)
+      for (int j = 0; j < V; ++j) {
+        double ar = 0, ai = 0, br = 0, bi = 0, cr = 0, cim = 0;
+        for (int l = 0; l < C; ++l) {
+          const double *sj = SCV(l, j), *xi_ = CV(g, c, k, l, i);
+          const double *xj = CV(g, c, k, l, j), *si_ = SCV(l, i);
+          ar += sj[0] * xi_[0] + sj[1] * xi_[1];
+          ai += sj[0] * xi_[1] - sj[1] * xi_[0];
+          br += xj[0] * si_[0] + xj[1] * si_[1];
+          bi += xj[0] * si_[1] - xj[1] * si_[0];
+          const double *w = vc + 2 * ((size_t)j * C + l);
+          cr += w[0] * si_[0] - w[1] * si_[1];
+          cim += w[0] * si_[1] + w[1] * si_[0];
+        }
+        const double *d = VV(g, c, k, j, i);
+        orr[(size_t)i * V + j] = (d[0] - ar - br) + cr;
+        oi[(size_t)i * V + j] = (d[1] - ai - bi) + cim;
+      }
+#undef SCV
+    free(vc);
+  }
+}
+
+/* gaussKOverlap + ortho3Terms(8) (integrals3Terms.F90:956-1384): three
+ * complex matrices, one per wave vector dK[axis] (the reference's
+ * recipVectors(:, axis) / numAxialKPoints(axis)), as real and imaginary
+ * full planes [3][nk][V][V]. */
+int orc_gauss_koverlap(orc_ctx *c, const double *dk, double *re, double *im) {
+  if (c->core_dim > 0 && !c->have_ol) return IMAGO_ERR_NEED_OVERLAP;
+  reset_stats(c);
+  const size_t vv = (size_t)c->nk * c->vale_dim * c->vale_dim;
+  for (int q = 0; q < 3; ++q) {
+    gmats g;
+    int st = alloc_gmats(c, &g);
+    if (st) return st;
+    buildspec bs = {K_KOV, 0, 0, NULL, NULL, 0, q, 0, dk + 3 * q};
+    st = pair_loops(c, &bs, &g);
+    if (!st) ortho_full(c, &g, re + q * vv, im + q * vv);
+    free_gmats(&g);
+    if (st) return st;
+  }
+  return IMAGO_OK;
+}
+
 
 int orc_gauss_overlap_ol(orc_ctx *c, double *packed, double *cv_re,
                          double *cv_im) {

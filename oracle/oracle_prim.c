@@ -13,6 +13,7 @@
  *   massvel2CIntg  (gaussIntegrals.f90:39070-49402) (alpha^2/8)<a|nabla^4|b>
  *   momentum2CIntg (gaussIntegrals.f90:23041-39068) <a|d/dx_c|b>, c = x,y,z
  *   dipole3CIntg   (gaussIntegrals.f90:49404-65510) <a|(r - C)_c|b>
+ *   KOverlap2CIntg (gaussIntegrals.f90:129408-135102) <a|exp(-i dK.r)|b>
  *   electron3CIntg (gaussIntegrals.f90:11624-16023) <a|exp(-a3 r_C^2)|b>
  *   nuclear3CIntg  (gaussIntegrals.f90:16223-23039) <a|exp(-a3 r_C^2)/r_C|b>
  *
@@ -351,6 +352,79 @@ void orc_momentum2c(double a1, double a2, const double *A, const double *B,
 void orc_dipole2c(double a1, double a2, const double *A, const double *B,
                   const double *C, int la, int lb, double *sh3) {
   vec2c(1, a1, a2, A, B, C, la, lb, sh3);
+}
+
+/* Overlap with a plane wave, <a|exp(-i dK.r)|b> (complex).  The product
+ * Gaussian times exp(-i q x) is exp(-i q P - q^2/(4p)) times a Gaussian
+ * about P' = P - i q/(2p), so the 1D recursion runs with the complex
+ * PA' = PA - i q/(2p), PB' = PB - i q/(2p) and each axis carries
+ * sqrt(pi/p) exp(-xi X^2) exp(-q^2/(4p)) exp(-i q P).  The reference
+ * writes the same shift as Hermite-polynomial terms (hermite_term(1) =
+ * -i q/(2p); hermite_term(2) - hermite_term(1)^2 = 1/(2p),
+ * gaussIntegrals.f90:129450-129470).  sh2[2 * (i*16 + j) + 0/1] = re/im. */
+void orc_koverlap2c(double a1, double a2, const double *A, const double *B,
+                    const double *dK, int la, int lb, double *sh2) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  double Sr[3][8][8], Si[3][8][8], pr[3], pi_[3];
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta, X = A[x] - B[x];
+    const double ar = P - A[x], br = P - B[x], sh = -dK[x] * inv2p;  /* imag shift */
+    /* S_{i+1,j} = PA' S_ij + (i S_{i-1,j} + j S_{i,j-1}) / (2p), complex */
+    Sr[x][0][0] = 1.0;
+    Si[x][0][0] = 0.0;
+    for (int i = 0; i < la; ++i) {
+      double vr = ar * Sr[x][i][0] - sh * Si[x][i][0];
+      double vi = ar * Si[x][i][0] + sh * Sr[x][i][0];
+      if (i > 0) {
+        vr += i * inv2p * Sr[x][i - 1][0];
+        vi += i * inv2p * Si[x][i - 1][0];
+      }
+      Sr[x][i + 1][0] = vr;
+      Si[x][i + 1][0] = vi;
+    }
+    for (int j = 0; j < lb; ++j)
+      for (int i = 0; i <= la; ++i) {
+        double vr = br * Sr[x][i][j] - sh * Si[x][i][j];
+        double vi = br * Si[x][i][j] + sh * Sr[x][i][j];
+        if (i > 0) {
+          vr += i * inv2p * Sr[x][i - 1][j];
+          vi += i * inv2p * Si[x][i - 1][j];
+        }
+        if (j > 0) {
+          vr += j * inv2p * Sr[x][i][j - 1];
+          vi += j * inv2p * Si[x][i][j - 1];
+        }
+        Sr[x][i][j + 1] = vr;
+        Si[x][i][j + 1] = vi;
+      }
+    const double mag = sqrt(ORC_PI / zeta) * exp(-xi * X * X) *
+                       exp(-dK[x] * dK[x] / (4.0 * zeta));
+    pr[x] = mag * cos(dK[x] * P);
+    pi_[x] = -mag * sin(dK[x] * P);
+  }
+  double pcr[20][20], pci[20][20];
+  for (int p = 0; p < NCART[la]; ++p)
+    for (int q = 0; q < NCART[lb]; ++q) {
+      double vr = 1.0, vi = 0.0;
+      for (int x = 0; x < 3; ++x) {
+        const int i = CART[p][x], j = CART[q][x];
+        /* times S_x(i, j) * pref_x */
+        const double fr = Sr[x][i][j] * pr[x] - Si[x][i][j] * pi_[x];
+        const double fi = Sr[x][i][j] * pi_[x] + Si[x][i][j] * pr[x];
+        const double nr = vr * fr - vi * fi, ni = vr * fi + vi * fr;
+        vr = nr;
+        vi = ni;
+      }
+      pcr[p][q] = vr;
+      pci[p][q] = vi;
+    }
+  double shr[256], shi[256];
+  cart_to_sh(pcr, la, lb, shr);
+  cart_to_sh(pci, la, lb, shi);
+  for (int k = 0; k < 256; ++k) {
+    sh2[2 * k] = shr[k];
+    sh2[2 * k + 1] = shi[k];
+  }
 }
 
 /* Three-centre overlap: the three Gaussians combine into one of exponent

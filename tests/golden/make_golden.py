@@ -4,7 +4,8 @@ own generated kernels.
 The reference's primitive integrals live in `src/imago/gaussIntegrals.f90`
 (overlap2CIntg 26-4420, kinetic2CIntg 4422-11622, massvel2CIntg
 39070-49402, electron3CIntg 11624-16023, boys 16080-16221, nuclear3CIntg
-16223-23039, momentum2CIntg 23041-39068, dipole3CIntg 49404-65510).  No Fortran compiler exists where this script runs, so the
+16223-23039, momentum2CIntg 23041-39068, dipole3CIntg 49404-65510,
+KOverlap2CIntg 129408-135102).  No Fortran compiler exists where this script runs, so the
 script transliterates those subroutines statement by statement into Python and executes them with IEEE
 double arithmetic, which is what gfortran -O3 (no -ffast-math, no FMA on
 x86-64 baseline) evaluates.  Fortran semantics that matter for the values
@@ -44,6 +45,8 @@ KERNEL_LINES = {
     "momentum2CIntg": (23041, 39068),
     "dipole3CIntg": (49404, 65510),
 }
+# Kernels whose local arrays are assigned whole rows or are complex.
+NUMPY_KERNELS = {"KOverlap2CIntg": (129408, 135102)}
 
 # Class codes built by integrals.F90:533-536: bit 0..3 for atom 1 (s,p,d,f),
 # bit 4..7 for atom 2.
@@ -80,6 +83,34 @@ class FArr:
         self.d[self._key(k)] = float(v)
 
 
+class NArr:
+    """1-based Fortran array backed by numpy, for kernels that assign whole
+    rows (`Hn(1,:) = ...`) or hold complex values; `:` is the token ALL."""
+
+    def __init__(self, name, dims, cplx=False):
+        self.name = name
+        self.a = np.zeros(dims, dtype=complex if cplx else float)
+
+    def _k(self, k):
+        if not isinstance(k, tuple):
+            k = (k,)
+        return tuple(i if isinstance(i, slice) else int(i) - 1 for i in k)
+
+    def __getitem__(self, k):
+        v = self.a[self._k(k)]
+        return v if isinstance(v, np.ndarray) else v.item()
+
+    def __setitem__(self, k, v):
+        self.a[self._k(k)] = v
+
+
+ALL = slice(None)
+
+
+def _exp(x):
+    return math.exp(x) if isinstance(x, float) else np.exp(x)
+
+
 def _fsum(x):
     s = 0.0
     for v in x:
@@ -88,11 +119,13 @@ def _fsum(x):
 
 
 def _ix(arr, *k):
-    if isinstance(arr, FArr):
+    if isinstance(arr, (FArr, NArr)):
         return arr[k if len(k) > 1 else k[0]]
     # numpy vector from a whole-array assignment
     assert len(k) == 1
-    return float(arr[int(k[0]) - 1])
+    if isinstance(k[0], slice):
+        return arr
+    return arr[int(k[0]) - 1].item()
 
 
 REAL_LIT = re.compile(
@@ -136,7 +169,9 @@ PAREN_POW = re.compile(r"\)\s*\*\*\s*(\d+)(?![\w.])")
 
 def _apowi(x, n):
     """Whole-array NAME(:)**n: the same chain per element."""
-    return np.array([_powi(float(v), n) for v in x])
+    if isinstance(x, NArr):
+        x = x.a
+    return np.array([_powi(v.item() if hasattr(v, "item") else v, n) for v in x])
 
 
 def _paren_pow(expr):
@@ -162,8 +197,12 @@ def _paren_pow(expr):
                 + m.group(1) + ")" + expr[m.end():])
 
 
+ALL_INDEX = re.compile(r"(?<=[(,])\s*:\s*(?=[,)])")
+
+
 def translate_expr(expr, arrays):
     expr = SLICE_POW.sub(lambda m: f"_apowi({m.group(1)}, {m.group(2)})", expr)
+    expr = ALL_INDEX.sub("ALL", expr)
     expr = _paren_pow(expr)
     expr = INT_POW.sub(lambda m: f"_powi({m.group(1)}, {m.group(2) or m.group(3)})", expr)
     expr = expr.replace(".eq.", "==").replace(".ne.", "!=")
@@ -210,9 +249,11 @@ def read_subroutine(lines, start, end):
     return joined
 
 
-def transpile(name, stmts):
-    """Return python source of a function `name(**kw)` for one subroutine."""
+def transpile(name, stmts, numpy_arrays=False):
+    """Return python source of a function `name(**kw)` for one subroutine.
+    numpy_arrays: local arrays as NArr (whole-row assignments, complex)."""
     arrays = set()
+    cplx = set()
     decl_lines = []
     params = None
     py = []
@@ -225,7 +266,7 @@ def transpile(name, stmts):
         if low.startswith("end subroutine") or low.startswith("use ") \
                 or low.startswith("implicit"):
             continue
-        if low.startswith("real") or low.startswith("integer"):
+        if low.startswith("real") or low.startswith("integer") or low.startswith("complex"):
             m = re.search(r"dimension\s*\(([^)]*)\)\s*(?:,\s*intent\s*\([^)]*\))?\s*::\s*(.*)$", s)
             if m:
                 dims = [int(x) for x in m.group(1).split(",")]
@@ -233,6 +274,8 @@ def transpile(name, stmts):
                     v = v.strip()
                     arrays.add(v)
                     decl_lines.append((v, dims))
+                    if low.startswith("complex"):
+                        cplx.add(v)
             continue
         pad = "    " * indent
         m = re.match(r"(else\s*if|if)\s*\((.*)\)\s*then$", s, re.I)
@@ -267,6 +310,7 @@ def transpile(name, stmts):
             lhs, idx, rhs = m.group(1), m.group(3), m.group(4)
             rhs = translate_expr(rhs, arrays)
             if idx is not None:
+                idx = ",".join("ALL" if q.strip() == ":" else q for q in idx.split(","))
                 idx = translate_expr(idx, arrays)
                 py.append(pad + f"{lhs}[{idx}] = {rhs}")
             else:
@@ -277,7 +321,10 @@ def transpile(name, stmts):
     for v, dims in decl_lines:
         if v in params.split(","):
             continue
-        head.append(f"    {v} = FArr('{v}', {dims})")
+        if numpy_arrays:
+            head.append(f"    {v} = NArr('{v}', {dims}, {v in cplx})")
+        else:
+            head.append(f"    {v} = FArr('{v}', {dims})")
     return "\n".join(head + py) + "\n"
 
 
@@ -287,14 +334,18 @@ def load_kernels(ref_root):
         lines = fh.readlines()
     ns = {
         "FArr": FArr, "_ix": _ix, "f32": f32, "pi": 3.141592653589793,
-        "_powi": _powi, "_apowi": _apowi,
+        "_powi": _powi, "_apowi": _apowi, "NArr": NArr, "ALL": ALL,
+        "cmplx": lambda re, im, kind=None: complex(re, im), "double": 8,
         # constants.f90:47, a double-kind parameter
         "fineStructure": float("7.2973525693"),
-        "exp": math.exp, "sqrt": math.sqrt, "erf": math.erf, "sum": _fsum,
+        "exp": _exp, "sqrt": math.sqrt, "erf": math.erf, "sum": _fsum,
         "abs": abs, "float": float,
     }
     for name, (a, b) in KERNEL_LINES.items():
         src = transpile(name, read_subroutine(lines, a, b))
+        exec(compile(src, f"<{name}>", "exec"), ns)
+    for name, (a, b) in NUMPY_KERNELS.items():
+        src = transpile(name, read_subroutine(lines, a, b), numpy_arrays=True)
         exec(compile(src, f"<{name}>", "exec"), ns)
     return ns
 
@@ -324,6 +375,15 @@ def run_vec(ns, kern, la, lb, a1, a2, A, B, C=None):
     ns[kern](*args, class_code(la, lb), sh)
     return [[[sh[i, j, c] for j in range(1, nsh(lb) + 1)]
              for i in range(1, nsh(la) + 1)] for c in range(1, 4)]
+
+
+def run_k(ns, la, lb, a1, a2, A, B, dK):
+    """KOverlap2CIntg: complex sh(16,16) as [re, im] pairs."""
+    sh = NArr("sh", [16, 16], True)
+    ns["KOverlap2CIntg"](a1, a2, np.array(A, float), np.array(B, float),
+                         np.array(dK, float), class_code(la, lb), sh)
+    return [[[sh[i, j].real, sh[i, j].imag] for j in range(1, nsh(lb) + 1)]
+            for i in range(1, nsh(la) + 1)]
 
 
 def run_3c(ns, kern, la, lb, a1, a2, a3, A, B, C):
@@ -371,6 +431,11 @@ def main():
                 rec["massvel"] = run_2c(ns, "massvel2CIntg", la, lb, a1, a2, A, B)
                 rec["momentum"] = run_vec(ns, "momentum2CIntg", la, lb, a1, a2, A, B)
                 rec["dipole"] = run_vec(ns, "dipole3CIntg", la, lb, a1, a2, A, B, C)
+                # a wave vector of the size of a reciprocal-lattice vector
+                # over a k-point count (gaussKOverlap's deltaK)
+                dK = (np.sin(np.arange(3) + 7 * la + 3 * lb + rep) * 0.6).tolist()
+                rec["dK"] = dK
+                rec["koverlap"] = run_k(ns, la, lb, a1, a2, A, B, dK)
                 rec["electron3c"] = run_3c(ns, "electron3CIntg", la, lb,
                                            a1, a2, a3, A, B, C)
                 rec["nuclear3c"] = run_3c(ns, "nuclear3CIntg", la, lb,
@@ -433,7 +498,7 @@ def main():
     out = {
         "source": "src/imago/gaussIntegrals.f90 (overlap2CIntg, kinetic2CIntg,"
                   " electron3CIntg, boys, nuclear3CIntg, massvel2CIntg,"
-                  " momentum2CIntg, dipole3CIntg)"
+                  " momentum2CIntg, dipole3CIntg, KOverlap2CIntg)"
                   " executed statement by statement in IEEE double",
         "generator": "tests/golden/make_golden.py",
         "records": records,

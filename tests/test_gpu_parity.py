@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import FINE_STRUCTURE, massvel_scale, momentum_scale, packed_mismatch
+from conftest import ATOL, FINE_STRUCTURE, massvel_scale, momentum_scale, packed_mismatch
 from imago_b200 import configs, intg
 
 pytestmark = pytest.mark.gpu
@@ -568,3 +568,50 @@ def test_adjacent_builds_on_device_outputs_and_graph(imago_lib):
         g.gauss_overlap_dm(center, out=v3)
         torch.cuda.synchronize()
         assert np.array_equal(v3.cpu().numpy(), dm_h)
+
+
+def _wave_vectors(s):
+    # the reference's recipVectors(:, axis) / numAxialKPoints(axis); a fixed
+    # set where the system has no k-point mesh
+    if s.kmesh is None:
+        return np.array([[0.31, 0.0, 0.05], [0.0, 0.27, -0.08], [0.12, 0.1, 0.35]])
+    recip = 2.0 * np.pi * np.linalg.inv(np.asarray(s.real_vectors)).T
+    return recip / np.asarray(s.kmesh[0], float)[:, None]
+
+
+@pytest.mark.parametrize("name", ["small", "f", "silicon8", "gamma", "nocore"])
+def test_koverlap_build_matches_oracle(imago_lib, name):
+    # gaussKOverlap + ortho3Terms(8): the full (not Hermitian) matrices of
+    # <a|exp(-i dK.r)|b>, real and imaginary planes, nothing zeroed
+    s = {"small": configs.small_test_system,
+         "f": configs.f_test_system,
+         "silicon8": lambda: configs.silicon_cubic8(kmesh=(2, 2, 3)),
+         "gamma": lambda: configs.silicon_cubic8(kmesh=(1, 1, 1),
+                                                 shift=(0.5, 0.5, 0.5)),
+         "nocore": configs.no_core_test_system}[name]()
+    dk = _wave_vectors(s)
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    ref = ob.koverlap(dk).transpose(0, 1, 3, 2)  # [axis, k, col, row]
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        re, im = g.gauss_koverlap(dk)
+        re0, im0 = g.gauss_koverlap(np.zeros((3, 3)))
+        ol = g.gauss_overlap_ol()[0]
+    assert re.shape == (3, g.nk, g.vale_dim, g.vale_dim)
+    err = max(np.abs(re - ref.real).max(), np.abs(im - ref.imag).max())
+    assert err <= ATOL, err
+    # the matrices are not Hermitian and keep an imaginary part at Gamma
+    full = re[0, 0] + 1j * im[0, 0]
+    assert np.abs(full - full.conj().T).max() > 1e-6
+    assert np.abs(im).max() > 1e-6
+    # dK = 0: the overlap itself, whose packed upper triangle is zeroed
+    # below 1e-10
+    V = g.vale_dim
+    rows, cols = np.triu_indices(V)
+    idx = cols * (cols + 1) // 2 + rows
+    for k in range(g.nk):
+        for ax in range(3):
+            d = packed_mismatch(np.stack([re0[ax, k][cols, rows], im0[ax, k][cols, rows]], -1),
+                                ol[k][idx])
+            assert d[1] == 0, d

@@ -124,3 +124,44 @@ def test_momentum_and_dipole_match_reference_kernels(golden):
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (r["la"], r["lb"])
         n += 1
     assert n == 64
+
+
+def test_koverlap_matches_reference_kernel(golden):
+    # <a|exp(-i dK.r)|b>, complex, at random wave vectors of |dK| ~ 1
+    # bohr^-1 (a few times the reference's recipVectors / numAxialKPoints)
+    n = 0
+    for r in golden["records"]:
+        if "koverlap" not in r:
+            continue
+        ref = np.array(r["koverlap"])
+        ref = ref[..., 0] + 1j * ref[..., 1]
+        got = oracle.primitive_koverlap(r["la"], r["lb"], r["a1"], r["a2"],
+                                        r["A"], r["B"], r["dK"])
+        assert got.shape == ref.shape
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (r["la"], r["lb"])
+        n += 1
+    assert n == 64
+
+
+def test_koverlap_at_zero_wave_vector_is_the_overlap():
+    # exp(-i 0.r) = 1: the plane-wave overlap of dK = 0 is the orthogonalised
+    # overlap itself, here unpacked from its Hermitian upper triangle
+    from imago_b200 import configs
+    s = configs.small_test_system()
+    ob = oracle.OracleBuild(s)
+    ol = ob.overlap()[0]
+    kov = ob.koverlap(np.zeros((3, 3)))
+    V = ob.vale_dim
+    iu = np.triu_indices(V)
+    for k in range(ob.nk):
+        full = np.zeros((V, V), complex)
+        p = ol[k, :, 0] + 1j * ol[k, :, 1]
+        # packed column-major upper triangle: index col (col + 1) / 2 + row
+        cols, rows = iu[1], iu[0]
+        order = np.argsort(cols * (cols + 1) // 2 + rows)
+        full[rows[order], cols[order]] = p
+        full = full + np.conj(np.triu(full, 1)).T
+        for ax in range(3):
+            # the packed overlap zeroes entries below 1e-10; the full planes
+            # do not
+            assert np.abs(kov[ax, k] - full).max() <= 1e-10
