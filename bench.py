@@ -390,7 +390,9 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     """Device milliseconds (median of `reps`, CUDA events on the library's
     stream, outputs resident in HBM) of the builds beside the SCF set on the
     same system: mass velocity, the momentum and dipole matrices (three
-    each), the PSCF Hamiltonian for one spin and for two spins with mass
+    each), the plane-wave overlaps for the three wave vectors
+    b_c / n_c (reciprocal lattice vector over the k-mesh divisions; b_c at
+    Gamma), the PSCF Hamiltonian for one spin and for two spins with mass
     velocity (synthetic potential coefficients), and KE + NP + all EP terms,
     the matrices the Hamiltonian combines, for comparison.  The overlap of
     the main run is resident, as these builds need."""
@@ -400,11 +402,18 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     mv, v3, h1, h2 = z(1), z(3), z(1), z(2)
     w = np.random.default_rng(1).normal(scale=0.5, size=(g.pot_dim, 2))
     parts = {k: bufs[k].data_ptr() for k in ("ke_packed", "np_packed", "ep_packed")}
+    nvv = 3 * g.nk * g.vale_dim * g.vale_dim
+    kre, kim = (torch.empty(nvv, dtype=torch.float64, device=dev) for _ in range(2))
+    sysm = g.system
+    dk = 2.0 * np.pi * np.linalg.inv(np.asarray(sysm.real_vectors)).T
+    if sysm.kmesh is not None:
+        dk = dk / np.asarray(sysm.kmesh[0], float)[:, None]
     g.set_ham_mode(ham_mode)
     cases = {
         "mass_velocity": lambda: g.build(intg.IMAGO_MV, {"mv_packed": mv.data_ptr()}),
         "momentum_xyz": lambda: g.gauss_overlap_mm(out=v3),
         "dipole_xyz": lambda: g.gauss_overlap_dm([0.5, 0.5, 0.5], out=v3),
+        "plane_wave_xyz": lambda: g.gauss_koverlap(dk, re=kre, im=kim),
         "ham_pscf_spin1": lambda: g.ham_pscf(w[:, :1], out=h1),
         "ham_pscf_spin2_rel": lambda: g.ham_pscf(w, rel=True, out=h2),
         "ke_np_ep_separate": lambda: g.build(intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP,

@@ -9,10 +9,12 @@
 !    call gaussOverlapHamPSCF(...) -> call b200GaussOverlapHamPSCF(...)  (PSCF)
 !    call gaussOverlapDM(...)      -> call b200GaussOverlapDM(...)
 !    call gaussOverlapMM(...)      -> call b200GaussOverlapMM(...)
+!    call gaussKOverlap(...)       -> call b200GaussKOverlap(...)
 !    call gaussOverlapNP(...)      -> call b200GaussOverlapNP(...)
 !    call elecPotGaussOverlap(...) -> call b200ElecPotGaussOverlap(...)
 !
-! (src/imago/imago.F90:262, 268, 274, 284, 293, 312, 315, 685, 705, 709),
+! (src/imago/imago.F90:262, 268, 274, 284, 293, 312, 315, 319, 321, 685,
+! 705, 709, 714, 716),
 ! each with the same arguments.
 ! Each wrapper skips a matrix whose HDF5 "done" attribute is already 1, as
 ! the reference does, writes the packed valence-valence datasets per
@@ -30,7 +32,9 @@ module O_ImagoB200
    implicit none
    private
    public :: b200Setup, b200GaussOverlapOL, b200GaussOverlapKE, &
-         & b200GaussOverlapNP, b200ElecPotGaussOverlap, b200Cleanup
+         & b200GaussOverlapMV, b200GaussOverlapNP, b200ElecPotGaussOverlap, &
+         & b200GaussOverlapHamPSCF, b200GaussOverlapDM, b200GaussOverlapMM, &
+         & b200GaussKOverlap, b200Cleanup
 
    type, bind(C) :: imago_system
       real(c_double) :: real_vectors(9)
@@ -126,6 +130,14 @@ module O_ImagoB200
          type(c_ptr), value :: ctx
          real(c_double), intent(in) :: center(3)
          real(c_double), intent(out) :: packed(*)
+         integer(c_int) :: st
+      end function
+      function imago_gauss_koverlap(ctx, dk, re, im) &
+            & bind(C, name="imago_gauss_koverlap") result(st)
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: dk(9)
+         real(c_double), intent(out) :: re(*), im(*)
          integer(c_int) :: st
       end function
       function imago_elec_pot_gauss_overlap(ctx, packed) &
@@ -518,6 +530,46 @@ contains
       integer(hid_t), intent(in) :: aid
       call b200ThreeTerms(7, valeValeDims, did, aid)
    end subroutine b200GaussOverlapMM
+
+   ! gaussKOverlap + ortho3Terms(8/9): the overlaps with exp(-i dK_c . r),
+   ! dK_c = recipVectors(:,c) / numAxialKPoints(c), written as the full real
+   ! (did1) and imaginary (did2) valence planes per k-point and axis, with
+   ! the dimensions the reference writes them with
+   ! (integrals3Terms.F90:1549-1556).  As in the reference, plusG does not
+   ! enter the integrals (integrals3Terms.F90:1287-1298); the caller's
+   ! handles decide which group (KOverlap or KOverlapPlusG) is written.
+   subroutine b200GaussKOverlap(valeValeDims, did1, did2, aid, plusG)
+      use O_KPoints, only: numKPoints, numAxialKPoints
+      use O_AtomicSites, only: valeDim
+      use O_Lattice, only: recipVectors
+      integer(hsize_t), dimension(2), intent(in) :: valeValeDims
+      integer(hid_t), dimension(numKPoints,3), intent(in) :: did1, did2
+      integer(hid_t), intent(in) :: aid
+      real(double), dimension(3,3), intent(in) :: plusG
+      real(c_double), allocatable :: re(:,:,:,:), im(:,:,:,:)
+      real(c_double) :: dk(3,3)
+      integer :: i, j, hdferr
+      integer(c_int) :: st
+      if (alreadyDone(aid)) return
+      do j = 1, 3
+         dk(:,j) = recipVectors(:,j) / numAxialKPoints(j)
+      enddo
+      allocate (re(valeDim, valeDim, numKPoints, 3))
+      allocate (im(valeDim, valeDim, numKPoints, 3))
+      st = imago_gauss_koverlap(ctx, dk, re, im)
+      if (st /= 0) call fail(st, 'gaussKOverlap')
+      do j = 1, 3
+         do i = 1, numKPoints
+            call h5dwrite_f(did1(i,j), H5T_NATIVE_DOUBLE, re(:,:,i,j), &
+                  & valeValeDims, hdferr)
+            if (hdferr /= 0) stop 'failed to write Koverlap vale vale'
+            call h5dwrite_f(did2(i,j), H5T_NATIVE_DOUBLE, im(:,:,i,j), &
+                  & valeValeDims, hdferr)
+            if (hdferr /= 0) stop 'failed to write Koverlap vale vale'
+         enddo
+      enddo
+      call markDone(aid)
+   end subroutine b200GaussKOverlap
 
    subroutine b200Cleanup()
       if (c_associated(ctx)) call imago_intg_destroy(ctx)

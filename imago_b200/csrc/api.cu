@@ -948,13 +948,26 @@ int ensure_scratch(imago_ctx *c, int nterm) {
   const size_t V = c->vale_dim, C = c->core_dim, nk = c->nk;
   imago_ctx::Scratch &S = c->scr[c->lane];
   cudaStream_t st = c->cur();
+  const size_t nblk = (size_t)c->blk_total * nterm + 1, nm = (size_t)c->m_total * nterm + 1;
+  const size_t nvv = nk * V * V * nterm + 1, ncv = nk * V * C * nterm + 1;
+  const size_t ncc = nk * C * C * nterm + 1;
+  // A captured build graph holds these buffers' addresses: a build that
+  // needs more (more terms per pass, as the three- and six-term builds
+  // do) drops the graph before the old buffers are freed, and the next
+  // imago_intg_build_graph call captures anew.
+  auto grows = [](const auto &b, size_t n) { return !b.p || n > b.n; };
+  if (c->gexec && (grows(S.blk, nblk) || grows(S.M, nm) || grows(S.vv, nvv) ||
+                   grows(S.cv, ncv) || grows(S.cc, ncc) || grows(S.y, ncv))) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
   int rc;
-  if ((rc = S.blk.alloc((size_t)c->blk_total * nterm + 1, st))) return rc;
-  if ((rc = S.M.alloc((size_t)c->m_total * nterm + 1, st))) return rc;
-  if ((rc = S.vv.alloc(nk * V * V * nterm + 1, st))) return rc;
-  if ((rc = S.cv.alloc(nk * V * C * nterm + 1, st))) return rc;
-  if ((rc = S.cc.alloc(nk * C * C * nterm + 1, st))) return rc;
-  if ((rc = S.y.alloc(nk * V * C * nterm + 1, st))) return rc;
+  if ((rc = S.blk.alloc(nblk, st))) return rc;
+  if ((rc = S.M.alloc(nm, st))) return rc;
+  if ((rc = S.vv.alloc(nvv, st))) return rc;
+  if ((rc = S.cv.alloc(ncv, st))) return rc;
+  if ((rc = S.cc.alloc(ncc, st))) return rc;
+  if ((rc = S.y.alloc(ncv, st))) return rc;
   return IMAGO_OK;
 }
 

@@ -543,14 +543,15 @@ def test_momentum_and_dipole_builds_match_oracle(imago_lib, name):
 
 def test_adjacent_builds_on_device_outputs_and_graph(imago_lib):
     # outputs_on_device: the mass velocity inside a captured build graph and
-    # the momentum / dipole matrices written straight to device memory agree
-    # bit for bit with the host-output builds
+    # the momentum / dipole / plane-wave matrices written straight to device
+    # memory agree bit for bit with the host-output builds
     import torch
     s = configs.silicon_cubic8(kmesh=(2, 2, 3))
     center = [0.3, 0.1, -0.2]
     with intg.IntegralSetup(s) as g:
         g.gauss_overlap_ol()
         mv_h, mm_h, dm_h = g.gauss_overlap_mv(), g.gauss_overlap_mm(), g.gauss_overlap_dm(center)
+        kov_h = g.gauss_koverlap(_wave_vectors(s))
     which = intg.IMAGO_OL | intg.IMAGO_KE | intg.IMAGO_NP | intg.IMAGO_EP | intg.IMAGO_MV
     with intg.IntegralSetup(s, outputs_on_device=True) as g:
         sh = _shapes(g)
@@ -568,6 +569,25 @@ def test_adjacent_builds_on_device_outputs_and_graph(imago_lib):
         g.gauss_overlap_dm(center, out=v3)
         torch.cuda.synchronize()
         assert np.array_equal(v3.cpu().numpy(), dm_h)
+        # the plane-wave overlaps into device planes; their six-term pass
+        # grows the scratch the graph was captured on, which drops the
+        # graph: the next build_graph call captures anew and reproduces
+        # every matrix
+        dk = _wave_vectors(s)
+        kre = torch.full((3, g.nk, g.vale_dim, g.vale_dim), np.nan, dtype=torch.float64,
+                         device="cuda")
+        kim = torch.full_like(kre, np.nan)
+        g.gauss_koverlap(dk, re=kre, im=kim)
+        torch.cuda.synchronize()
+        assert np.array_equal(kre.cpu().numpy(), kov_h[0])
+        assert np.array_equal(kim.cpu().numpy(), kov_h[1])
+        first = {k: v.cpu().numpy() for k, v in got.items()}
+        for v in got.values():
+            v.fill_(np.nan)
+        g.build_graph(got, which=which)
+        torch.cuda.synchronize()
+        for k, v in got.items():
+            assert np.array_equal(v.cpu().numpy(), first[k]), k
 
 
 def _wave_vectors(s):
