@@ -230,14 +230,54 @@ __device__ __forceinline__ void scatter(const DevSys &s, const DPair &p,
   }
 }
 
+// ------------------------------------------------------------ K-overlap --
+// saveCurrentPair with saveFull = 1 (intgSaving.F90:346-459, 513-551,
+// 555-608, 654-690): block (i, j) takes the pair's element, block (j, i)
+// its conjugate at the transposed place; for i == j the dagger, written
+// second in the reference, replaces the block, so only it is written.
+__device__ __forceinline__ void scatter_full(const DevSys &s, const DPair &p,
+                                             long long tk, int m1, int m2,
+                                             double re, double im, double2 *vv,
+                                             double2 *cv, double2 *cc) {
+  const int V = s.vale_dim, C = s.core_dim;
+  const int v1 = s.type_nvale[p.ti], v2 = s.type_nvale[p.tj];
+  const bool same = p.i == p.j;
+  if (m1 < v1 && m2 < v2) {
+    const int r = s.site_cum_vale[p.i] + m1, c = s.site_cum_vale[p.j] + m2;
+    if (!same) vv[tk * V * V + (long long)c * V + r] = make_double2(re, im);
+    vv[tk * V * V + (long long)r * V + c] = make_double2(re, -im);
+    return;
+  }
+  if (C == 0) return;
+  if (m1 >= v1 && m2 < v2) {
+    if (same) return;
+    const int row = s.site_cum_core[p.i] + (m1 - v1);
+    const int col = s.site_cum_vale[p.j] + m2;
+    cv[tk * V * C + (long long)col * C + row] = make_double2(re, im);
+  } else if (m1 < v1) {
+    const int row = s.site_cum_core[p.j] + (m2 - v2);
+    const int col = s.site_cum_vale[p.i] + m1;
+    cv[tk * V * C + (long long)col * C + row] = make_double2(re, -im);
+  } else {
+    const int r1 = s.site_cum_core[p.i] + (m1 - v1);
+    const int r2 = s.site_cum_core[p.j] + (m2 - v2);
+    if (!same) cc[tk * C * C + (long long)r2 * C + r1] = make_double2(re, im);
+    cc[tk * C * C + (long long)r1 * C + r2] = make_double2(re, -im);
+  }
+}
+
 // Tensor-core phase sum over a (pair, BC-column tile, 32 k-points, term):
 // 2 x BC/16 warps, each a 16 k x 16 column tile.  Rows of m_s are BC + 4
 // doubles and rows of ph_s 34 complex values, both 8 mod 32 bank words, so
 // the 4 k rows of a fragment read fall on distinct banks in each wavefront.
 constexpr int kBKP = kBK + 2;
 
-template <int BC>
-__global__ void __launch_bounds__(4 * BC, 256 / BC)
+// KOV: the plane-wave overlap's complex blocks, the real and imaginary
+// parts being terms 2 z and 2 z + 1 of M (z = blockIdx.z, the wave
+// vector): the image loop runs once per part into its own accumulators,
+// and the epilogue saves both orientations (scatter_full).
+template <int BC, bool KOV = false>
+__global__ void __launch_bounds__(4 * BC, (KOV ? 128 : 256) / BC)
     k_bloch(DevSys s, DevWork w, const double *M, double2 *vv, double2 *cv,
             double2 *cc) {
   constexpr int T = 4 * BC, NWC = BC / 16;
@@ -252,8 +292,9 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
   const int nu = p.uend - p.ubeg;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wk = (warp / NWC) * 16, wc = (warp % NWC) * 16;  // warp tile origin
-  const double *Mt = M + (long long)term * w.m_total + p.moff;
-  double ar[2][2][2] = {}, ai[2][2][2] = {};
+  constexpr int NP = KOV ? 2 : 1;
+  const double *Mt = nullptr;
+  double ar[NP][2][2][2] = {}, ai[NP][2][2][2] = {};
   auto issue = [&](int u0, int buf) {
 #pragma unroll
     for (int q = 0; q < PH; ++q) {
@@ -275,6 +316,9 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
+#pragma unroll
+  for (int part = 0; part < NP; ++part) {
+  Mt = M + (long long)(KOV ? 2 * term + part : term) * w.m_total + p.moff;
   if (nu > 0) issue(0, 0);
   for (int u0 = 0, buf = 0; u0 < nu; u0 += kBU, buf ^= 1) {
     if (u0 + kBU < nu) {
@@ -298,11 +342,12 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
-          dmma(ar[mt][nt][0], ar[mt][nt][1], a[mt].x, b[nt]);
-          dmma(ai[mt][nt][0], ai[mt][nt][1], a[mt].y, b[nt]);
+          dmma(ar[part][mt][nt][0], ar[part][mt][nt][1], a[mt].x, b[nt]);
+          dmma(ai[part][mt][nt][0], ai[part][mt][nt][1], a[mt].y, b[nt]);
         }
     }
     __syncthreads();  // this stage's buffer is refilled two stages on
+  }
   }
   // epilogue: origin shift (kPointLatticeOriginShift, intgSaving.F90:241-292,
   // skipped when |k.L0| < smallThresh) and the scatter
@@ -321,10 +366,14 @@ __global__ void __launch_bounds__(4 * BC, 256 / BC)
       for (int i = 0; i < 2; ++i) {
         const int e = c0 + wc + nt * 8 + 2 * (lane & 3) + i;
         if (e >= ne) continue;
-        const double re = ar[mt][nt][i], im = ai[mt][nt][i];
+        // KOV: (phase) x (Mr + i Mi)
+        const double re = KOV ? ar[0][mt][nt][i] - ai[NP - 1][mt][nt][i] : ar[0][mt][nt][i];
+        const double im = KOV ? ai[0][mt][nt][i] + ar[NP - 1][mt][nt][i] : ai[0][mt][nt][i];
         const int m2 = e / p.ni, m1 = e - m2 * p.ni;
         const double xr = cs * re - sn * im, xi = cs * im + sn * re;
-        if (s.minus_i)
+        if (KOV)
+          scatter_full(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
+        else if (s.minus_i)
           scatter(s, p, tk, m1, m2, xi, -xr, vv, cv, cc);
         else
           scatter(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
@@ -876,42 +925,6 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
   return IMAGO_OK;
 }
 
-// ------------------------------------------------------------ K-overlap --
-// saveCurrentPair with saveFull = 1 (intgSaving.F90:346-459, 513-551,
-// 555-608, 654-690): block (i, j) takes the pair's element, block (j, i)
-// its conjugate at the transposed place; for i == j the dagger, written
-// second in the reference, replaces the block, so only it is written.
-__device__ __forceinline__ void scatter_full(const DevSys &s, const DPair &p,
-                                             long long tk, int m1, int m2,
-                                             double re, double im, double2 *vv,
-                                             double2 *cv, double2 *cc) {
-  const int V = s.vale_dim, C = s.core_dim;
-  const int v1 = s.type_nvale[p.ti], v2 = s.type_nvale[p.tj];
-  const bool same = p.i == p.j;
-  if (m1 < v1 && m2 < v2) {
-    const int r = s.site_cum_vale[p.i] + m1, c = s.site_cum_vale[p.j] + m2;
-    if (!same) vv[tk * V * V + (long long)c * V + r] = make_double2(re, im);
-    vv[tk * V * V + (long long)r * V + c] = make_double2(re, -im);
-    return;
-  }
-  if (C == 0) return;
-  if (m1 >= v1 && m2 < v2) {
-    if (same) return;
-    const int row = s.site_cum_core[p.i] + (m1 - v1);
-    const int col = s.site_cum_vale[p.j] + m2;
-    cv[tk * V * C + (long long)col * C + row] = make_double2(re, im);
-  } else if (m1 < v1) {
-    const int row = s.site_cum_core[p.j] + (m2 - v2);
-    const int col = s.site_cum_vale[p.i] + m1;
-    cv[tk * V * C + (long long)col * C + row] = make_double2(re, -im);
-  } else {
-    const int r1 = s.site_cum_core[p.i] + (m1 - v1);
-    const int r2 = s.site_cum_core[p.j] + (m2 - v2);
-    if (!same) cc[tk * C * C + (long long)r2 * C + r1] = make_double2(re, im);
-    cc[tk * C * C + (long long)r1 * C + r2] = make_double2(re, -im);
-  }
-}
-
 // The K-overlap phase sum (cmplxApplyPhaseFactors, intgSaving.F90:192-238;
 // then kPointLatticeOriginShift): the complex contracted blocks are the
 // real terms 2 axis and 2 axis + 1 of M.  One thread per (block element,
@@ -952,6 +965,25 @@ __global__ void __launch_bounds__(256)
 int launch_bloch_kov(const DevSys &s, const DevWork &w, const double *M, double2 *vv,
                      double2 *cv, double2 *cc, cudaStream_t st) {
   if (w.nbtile == 0) return IMAGO_OK;
+  if (s.nk > kBlochSmallNk) {  // the tensor-core phase sum at the tuned width
+    if (w.nbtile_w == 0) return IMAGO_OK;
+    dim3 grid(w.nbtile_w, (s.nk + kBK - 1) / kBK, 3);
+    switch (w.bw) {
+      case bloch_width(0):
+        k_bloch<bloch_width(0), true><<<grid, 4 * bloch_width(0), 0, st>>>(s, w, M, vv, cv, cc);
+        break;
+      case bloch_width(1):
+        k_bloch<bloch_width(1), true><<<grid, 4 * bloch_width(1), 0, st>>>(s, w, M, vv, cv, cc);
+        break;
+      case bloch_width(2):
+        k_bloch<bloch_width(2), true><<<grid, 4 * bloch_width(2), 0, st>>>(s, w, M, vv, cv, cc);
+        break;
+      default:
+        return IMAGO_ERR_INVALID;
+    }
+    IMAGO_CUDA(cudaGetLastError());
+    return IMAGO_OK;
+  }
   constexpr int kPerBlock = 256 / kBlochCols;
   dim3 grid(w.nbtile, (s.nk + kPerBlock - 1) / kPerBlock, 3);
   k_bloch_kov<<<grid, 256, 0, st>>>(s, w, M, vv, cv, cc);

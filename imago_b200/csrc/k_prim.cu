@@ -564,23 +564,45 @@ int launch_prim3c_ham(const DevSys &s, const DevWork &w, const int *cls_beg,
 __global__ void __launch_bounds__(128)
     k_prim_kov(DevSys s, DevWork w, int beg, int end, int la, int lb, KovWaves dk,
                double *blk) {
-  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x, ax = blockIdx.y;
   if (g >= end) return;
   const DSp sp = w.sps[w.sp_by_cls[g]];
   const SpGeom q = sp_geom(s, w, sp);
-#pragma unroll 1
-  for (int ax = 0; ax < 3; ++ax)
-    prim_kov(la, lb, q.a1, q.a2, q.A, q.B, dk.q + 3 * ax,
-             blk + (long long)(2 * ax) * w.blk_total + sp.boff,
-             blk + (long long)(2 * ax + 1) * w.blk_total + sp.boff);
+  prim_kov(la, lb, q.a1, q.a2, q.A, q.B, dk.q + 3 * ax,
+           blk + (long long)(2 * ax) * w.blk_total + sp.boff,
+           blk + (long long)(2 * ax + 1) * w.blk_total + sp.boff);
 }
 
+template <int LA, int LB>
+__global__ void __launch_bounds__(128)
+    k_prim_kov_t(DevSys s, DevWork w, int beg, int end, KovWaves dk, double *blk) {
+  const int g = beg + blockIdx.x * blockDim.x + threadIdx.x, ax = blockIdx.y;
+  if (g >= end) return;
+  const DSp sp = w.sps[w.sp_by_cls[g]];
+  const SpGeom q = sp_geom(s, w, sp);
+  prim_kov_t<LA, LB>(q.a1, q.a2, q.A, q.B, dk.q + 3 * ax,
+                     blk + (long long)(2 * ax) * w.blk_total + sp.boff,
+                     blk + (long long)(2 * ax + 1) * w.blk_total + sp.boff);
+}
+
+// One thread per (shell pair, wave vector): s, p and d classes unrolled,
+// f classes through the runtime routine.
 int launch_prim_kov(const DevSys &s, const DevWork &w, const int *cls_beg,
                     const KovWaves &dk, double *blk, cudaStream_t st) {
   for (int c = 0; c < 16; ++c) {
     const int beg = cls_beg[c], n = cls_beg[c + 1] - beg;
     if (n <= 0) continue;
-    k_prim_kov<<<(n + 127) / 128, 128, 0, st>>>(s, w, beg, beg + n, c / 4, c % 4, dk, blk);
+    const dim3 grid((n + 127) / 128, 3);
+    switch (c) {
+#define IMAGO_KOV(a, b)                                                                 \
+  case a * 4 + b:                                                                       \
+    k_prim_kov_t<a, b><<<grid, 128, 0, st>>>(s, w, beg, beg + n, dk, blk);              \
+    break;
+      IMAGO_FOR_SPD_CLASSES(IMAGO_KOV)
+#undef IMAGO_KOV
+      default:
+        k_prim_kov<<<grid, 128, 0, st>>>(s, w, beg, beg + n, c / 4, c % 4, dk, blk);
+    }
     IMAGO_CUDA(cudaGetLastError());
   }
   return IMAGO_OK;

@@ -712,6 +712,77 @@ __device__ __noinline__ void prim_vec_rt(int la, int lb, double a1, double a2,
   }
 }
 
+// The plane-wave overlap for one wave vector q with compile-time classes
+// (s, p, d): the same complex-shifted recursion as prim_kov below, its
+// tables and the Cartesian products unrolled into registers.
+template <int LA, int LB>
+__device__ void prim_kov_t(double a1, double a2, const double *A, const double *B,
+                           const double *q, double *out_re, double *out_im) {
+  const double zeta = a1 + a2, xi = a1 * a2 / zeta, inv2p = 1.0 / (2.0 * zeta);
+  double Sr[3][LA + 1][LB + 1], Si[3][LA + 1][LB + 1], fr[3], fi[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double P = (a1 * A[x] + a2 * B[x]) / zeta, X = A[x] - B[x];
+    const double ar = P - A[x], br = P - B[x], sh = -q[x] * inv2p;
+    Sr[x][0][0] = 1.0;
+    Si[x][0][0] = 0.0;
+#pragma unroll
+    for (int i = 0; i < LA; ++i) {
+      double vr = ar * Sr[x][i][0] - sh * Si[x][i][0];
+      double vi = ar * Si[x][i][0] + sh * Sr[x][i][0];
+      if (i > 0) {
+        vr += i * inv2p * Sr[x][i - 1][0];
+        vi += i * inv2p * Si[x][i - 1][0];
+      }
+      Sr[x][i + 1][0] = vr;
+      Si[x][i + 1][0] = vi;
+    }
+#pragma unroll
+    for (int j = 0; j < LB; ++j)
+#pragma unroll
+      for (int i = 0; i <= LA; ++i) {
+        double vr = br * Sr[x][i][j] - sh * Si[x][i][j];
+        double vi = br * Si[x][i][j] + sh * Sr[x][i][j];
+        if (i > 0) {
+          vr += i * inv2p * Sr[x][i - 1][j];
+          vi += i * inv2p * Si[x][i - 1][j];
+        }
+        if (j > 0) {
+          vr += j * inv2p * Sr[x][i][j - 1];
+          vi += j * inv2p * Si[x][i][j - 1];
+        }
+        Sr[x][i][j + 1] = vr;
+        Si[x][i][j + 1] = vi;
+      }
+    const double mag = sqrt(kPi / zeta) * exp(-xi * X * X) * exp(-q[x] * q[x] / (4.0 * zeta));
+    double sn, cs;
+    sincos(q[x] * P, &sn, &cs);
+    fr[x] = mag * cs;
+    fi[x] = -mag * sn;
+  }
+  double pcr[ncart(LA) * ncart(LB)], pci[ncart(LA) * ncart(LB)];
+#pragma unroll
+  for (int p = 0; p < ncart(LA); ++p)
+#pragma unroll
+    for (int c = 0; c < ncart(LB); ++c) {
+      double vr = 1.0, vi = 0.0;
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const int i = cart_exp(p, x), j = cart_exp(c, x);
+        const double gr = Sr[x][i][j] * fr[x] - Si[x][i][j] * fi[x];
+        const double gi = Sr[x][i][j] * fi[x] + Si[x][i][j] * fr[x];
+        const double nr = vr * gr - vi * gi, ni = vr * gi + vi * gr;
+        vr = nr;
+        vi = ni;
+      }
+      pcr[p * ncart(LB) + c] = vr;
+      pci[p * ncart(LB) + c] = vi;
+    }
+  cart_to_sh<LA, LB>(pcr, out_re);
+  cart_to_sh<LA, LB>(pci, out_im);
+}
+
+
 // Overlap with a plane wave, <a|exp(-i q.r)|b> (KOverlap2CIntg), complex,
 // as two real blocks.  The product Gaussian times exp(-i q x) is
 // exp(-i q P - q^2/(4p)) times a Gaussian about P' = P - i q/(2p): the 1D
