@@ -404,10 +404,7 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     parts = {k: bufs[k].data_ptr() for k in ("ke_packed", "np_packed", "ep_packed")}
     nvv = 3 * g.nk * g.vale_dim * g.vale_dim
     kre, kim = (torch.empty(nvv, dtype=torch.float64, device=dev) for _ in range(2))
-    sysm = g.system
-    dk = 2.0 * np.pi * np.linalg.inv(np.asarray(sysm.real_vectors)).T
-    if sysm.kmesh is not None:
-        dk = dk / np.asarray(sysm.kmesh[0], float)[:, None]
+    dk = intg.koverlap_wave_vectors(g.system)
     g.set_ham_mode(ham_mode)
     cases = {
         "mass_velocity": lambda: g.build(intg.IMAGO_MV, {"mv_packed": mv.data_ptr()}),

@@ -223,6 +223,19 @@ def _out_struct(out):
     return s
 
 
+def koverlap_wave_vectors(system, num_axial=None):
+    """The wave vectors of the reference's gaussKOverlap
+    (integrals3Terms.F90:1293-1297): recipVectors(:, c) / numAxialKPoints(c)
+    as rows c of a [3, 3] array (bohr^-1), recipVectors as
+    initializeLattice forms them (lattice.f90:200-214).  num_axial
+    defaults to the system's k-point mesh, else one point per axis."""
+    a = np.asarray(system.real_vectors, dtype=np.float64)
+    recip = 2.0 * np.pi * np.linalg.inv(a).T
+    if num_axial is None:
+        num_axial = system.kmesh[0] if system.kmesh is not None else (1, 1, 1)
+    return recip / np.asarray(num_axial, dtype=np.float64)[:, None]
+
+
 class IntegralSetup:
     """One system staged on the GPU: imago_intg_create .. imago_intg_destroy.
 

@@ -6,7 +6,10 @@ group atomIntgGroup holding atomOverlap, atomOverlapCV (when coreDim > 0),
 atomKEOverlap, atomMVOverlap (scalar-relativistic runs), atomNPOverlap,
 atomPotOverlap/<term>, and atomDMOverlap/<axis> and atomMMOverlap/<axis>
 (dipole and momentum matrices, axes x, y, z as 1..3, one status for the
-three; hdf5SCFIntg.F90:227-267, 383-396), one dataset per
+three; hdf5SCFIntg.F90:227-267, 383-396), atomKOverlap/<axis> and
+atomKOverlapPlusG/<axis> (the plane-wave overlaps, full valence matrices
+as "real%07d" and "imag%07d"; hdf5SCFIntg.F90:235-275, 398-423), one
+dataset per
 k-point named by its 1-based index ("%07d"; coreValeOL as "real%07d" and
 "imag%07d"), and an integer attribute "status" on each group that is set
 to 1 once the group's datasets are written.  setupSCF skips every matrix
@@ -30,6 +33,7 @@ GROUP = "atomIntgGroup"
 OL, CV, KE, MV, NP, EP = ("atomOverlap", "atomOverlapCV", "atomKEOverlap",
                           "atomMVOverlap", "atomNPOverlap", "atomPotOverlap")
 DM, MM = "atomDMOverlap", "atomMMOverlap"
+KOV, KOVG = "atomKOverlap", "atomKOverlapPlusG"
 
 
 def _name(i):
@@ -113,6 +117,25 @@ class IntegralStore:
     def read_xyz(self, group):
         return np.stack([self.read_packed(f"{group}/{_name(c)}") for c in range(3)])
 
+    def write_planes(self, group, re, im):
+        """re, im [3, nk, V, V] indexed (axis, k, col, row), the memory
+        order of the reference's (valeDim, valeDim) Fortran datasets: the
+        full matrices of each axis in subgroups 1..3 of `group`."""
+        shape = (3, self.nk, self.vale_dim, self.vale_dim)
+        assert np.shape(re) == shape and np.shape(im) == shape, np.shape(re)
+        for c in range(3):
+            d = self._dir(f"{group}/{_name(c)}")
+            for k in range(self.nk):
+                np.save(os.path.join(d, "real" + _name(k) + ".npy"), np.asarray(re[c][k]))
+                np.save(os.path.join(d, "imag" + _name(k) + ".npy"), np.asarray(im[c][k]))
+
+    def read_planes(self, group):
+        def part(name):
+            return np.stack([np.stack([
+                np.load(os.path.join(self.root, group, _name(c), name + _name(k) + ".npy"))
+                for k in range(self.nk)]) for c in range(3)])
+        return part("real"), part("imag")
+
     def write_cv(self, re, im):
         d = self._dir(CV)
         for k in range(self.nk):
@@ -129,11 +152,15 @@ class IntegralStore:
 
 
 def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False,
-                       dipole_center=None, momentum=False):
-    """Run, in the reference's order (imago.F90:260-315: OL, KE, MV when
-    rel, NP, EP, then the dipole matrices about `dipole_center` and the
-    momentum matrices when asked for), the builds whose status in `store`
-    is not yet 1, writing each group's datasets and then its status.
+                       dipole_center=None, momentum=False, plane_wave=False):
+    """Run, in the reference's order (imago.F90:260-323: OL, KE, MV when
+    rel, NP, EP, then the dipole matrices about `dipole_center`, the
+    momentum matrices and the plane-wave overlaps when asked for), the
+    builds whose status in `store` is not yet 1, writing each group's
+    datasets and then its status.  The plane-wave overlaps fill
+    atomKOverlap and atomKOverlapPlusG with the same matrices, as the
+    reference does (its plusG argument does not enter the integrals,
+    integrals3Terms.F90:1287-1298).
 
     `setup` is an IntegralSetup with host outputs (or anything with its
     gauss_overlap_ol / _ke / _mv / _np and elec_pot_gauss_overlap_range
@@ -162,8 +189,9 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False,
         triples.append((DM, lambda: setup.gauss_overlap_dm(dipole_center)))
     if momentum:
         triples.append((MM, setup.gauss_overlap_mm))
+    planes = [g for g in ((KOV, KOVG) if plane_wave else ()) if store.status(g) == 0]
     later = (any(store.status(g) == 0 for g, _ in singles + triples)
-             or bool(ep_todo))
+             or bool(ep_todo) or bool(planes))
     if store.status(OL) == 0 or (later and store.core_dim > 0):
         ol, re, im = setup.gauss_overlap_ol()
         if store.status(OL) == 0:
@@ -191,14 +219,21 @@ def build_checkpointed(setup, store, ep_batch=8, on_group=None, rel=False,
         if store.status(group) == 0:
             store.write_xyz(group, call())
             done(group)
+    if planes:
+        from imago_b200.intg import koverlap_wave_vectors
+        re, im = setup.gauss_koverlap(koverlap_wave_vectors(setup.system))
+        for group in planes:
+            store.write_planes(group, re, im)
+            done(group)
     return written
 
 
-def read_all(store, rel=False, dipole=False, momentum=False):
+def read_all(store, rel=False, dipole=False, momentum=False, plane_wave=False):
     """Every matrix of a complete store: {"ol_packed", "ol_cv_re",
     "ol_cv_im", "ke_packed", "np_packed", "ep_packed"}, and "mv_packed"
-    when rel, "dm_packed" / "mm_packed" ([3, ...]) when asked for, as
-    numpy arrays."""
+    when rel, "dm_packed" / "mm_packed" ([3, ...]) and "kov_re" /
+    "kov_im" ([3, nk, V, V], from atomKOverlap) when asked for, as numpy
+    arrays."""
     out = {"ol_packed": store.read_packed(OL), "ke_packed": store.read_packed(KE),
            "np_packed": store.read_packed(NP),
            "ep_packed": np.stack([store.read_packed(store.ep_group(t))
@@ -211,4 +246,6 @@ def read_all(store, rel=False, dipole=False, momentum=False):
         out["dm_packed"] = store.read_xyz(DM)
     if momentum:
         out["mm_packed"] = store.read_xyz(MM)
+    if plane_wave:
+        out["kov_re"], out["kov_im"] = store.read_planes(KOV)
     return out

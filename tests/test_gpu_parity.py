@@ -409,13 +409,15 @@ def test_checkpointed_build_resumes_to_the_same_matrices(imago_lib, tmp_path):
         with pytest.raises(KeyboardInterrupt):
             st.build_checkpointed(g, box, ep_batch=3, on_group=stop, rel=True,
                                   dipole_center=center, momentum=True)
-        rest = st.build_checkpointed(g, box, rel=True, dipole_center=center, momentum=True)
-        assert rest[0] == box.ep_group(2) and rest[-2:] == [st.DM, st.MM]
+        rest = st.build_checkpointed(g, box, rel=True, dipole_center=center, momentum=True,
+                                     plane_wave=True)
+        assert rest[0] == box.ep_group(2) and rest[-4:] == [st.DM, st.MM, st.KOV, st.KOVG]
         ref["dm_packed"] = g.gauss_overlap_dm(center)
         ref["mm_packed"] = g.gauss_overlap_mm()
-    got = st.read_all(box, rel=True, dipole=True, momentum=True)
+        ref["kov_re"], ref["kov_im"] = g.gauss_koverlap(intg.koverlap_wave_vectors(s))
+    got = st.read_all(box, rel=True, dipole=True, momentum=True, plane_wave=True)
     for k in ("ol_packed", "ke_packed", "np_packed", "ep_packed", "mv_packed",
-              "dm_packed", "mm_packed"):
+              "dm_packed", "mm_packed", "kov_re", "kov_im"):
         assert np.array_equal(ref[k], got[k]), k
     if g.core_dim > 0:
         assert np.array_equal(ref["ol_cv_re"], got["ol_cv_re"])
@@ -591,12 +593,8 @@ def test_adjacent_builds_on_device_outputs_and_graph(imago_lib):
 
 
 def _wave_vectors(s):
-    # the reference's recipVectors(:, axis) / numAxialKPoints(axis); a fixed
-    # set where the system has no k-point mesh
-    if s.kmesh is None:
-        return np.array([[0.31, 0.0, 0.05], [0.0, 0.27, -0.08], [0.12, 0.1, 0.35]])
-    recip = 2.0 * np.pi * np.linalg.inv(np.asarray(s.real_vectors)).T
-    return recip / np.asarray(s.kmesh[0], float)[:, None]
+    # the reference's recipVectors(:, axis) / numAxialKPoints(axis)
+    return intg.koverlap_wave_vectors(s)
 
 
 @pytest.mark.parametrize("name", ["small", "f", "silicon8", "gamma", "nocore"])

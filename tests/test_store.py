@@ -15,7 +15,9 @@ class FakeSetup:
     """Deterministic packed matrices; counts the builds it runs."""
 
     def __init__(self, nk=3, V=4, C=2, P=5):
+        from imago_b200 import configs
         self.nk, self.V, self.C, self.P = nk, V, C, P
+        self.system = configs.silicon_cubic8(kmesh=(2, 2, 3))
         self.np = V * (V + 1) // 2
         self.calls = []
 
@@ -47,6 +49,12 @@ class FakeSetup:
     def gauss_overlap_np(self):
         self.calls.append("NP")
         return self._mat(2)
+
+    def gauss_koverlap(self, dk):
+        self.calls.append(("KOV", np.asarray(dk).round(12).tobytes()))
+        x = np.arange(3 * self.nk * self.V * self.V, dtype=float)
+        x = x.reshape(3, self.nk, self.V, self.V)
+        return x + 40000.0, -x
 
     def elec_pot_gauss_overlap_range(self, first, count):
         self.calls.append(("EP", first, count))
@@ -135,4 +143,33 @@ def test_dipole_and_momentum_groups(tmp_path):
     f2 = FakeSetup(P=2)
     assert st.build_checkpointed(f2, _store(tmp_path, f2), dipole_center=(0.5, 0.0, 0.0),
                                  momentum=True) == []
+    assert f2.calls == []
+
+
+def test_plane_wave_groups(tmp_path):
+    # atomKOverlap/<axis>/real<k>, imag<k> and the same matrices in
+    # atomKOverlapPlusG, from one build with dK_c = b_c / n_c, after the
+    # momentum matrices; a rerun builds nothing
+    from imago_b200 import intg
+    f = FakeSetup(P=1)
+    s = _store(tmp_path, f)
+    written = st.build_checkpointed(f, s, momentum=True, plane_wave=True)
+    assert written[-3:] == [st.MM, st.KOV, st.KOVG]
+    kov = [c for c in f.calls if isinstance(c, tuple) and c[0] == "KOV"]
+    assert len(kov) == 1
+    dk = intg.koverlap_wave_vectors(f.system)
+    assert kov[0][1] == dk.round(12).tobytes()
+    # b_c . a_c = 2 pi, so dK_c . a_c = 2 pi / n_c
+    a = np.asarray(f.system.real_vectors)
+    assert np.allclose(np.einsum("cx,cx->c", dk, a), 2 * np.pi / np.array([2, 2, 3]))
+    root = os.path.join(str(tmp_path), st.GROUP)
+    for g in ("atomKOverlap", "atomKOverlapPlusG"):
+        assert os.path.exists(os.path.join(root, g, "0000003", "imag0000003.npy"))
+    out = st.read_all(s, momentum=True, plane_wave=True)
+    re, im = f.gauss_koverlap(dk)
+    assert np.array_equal(out["kov_re"], re) and np.array_equal(out["kov_im"], im)
+    assert np.array_equal(s.read_planes(st.KOVG)[1], im)
+    f2 = FakeSetup(P=1)
+    assert st.build_checkpointed(f2, _store(tmp_path, f2), momentum=True,
+                                 plane_wave=True) == []
     assert f2.calls == []
