@@ -1642,6 +1642,27 @@ int imago_gauss_overlap_dm(imago_ctx *c, const double center[3], double *packed)
   return vec_call(c, KIND_DM, center, packed);
 }
 
+int imago_packed_traces(int vale_dim, int num_kpoints, int nmat, const double *mats,
+                        int nrho, const double *rho, double *traces, void *stream) {
+  if (vale_dim <= 0 || num_kpoints <= 0 || nmat < 0 || nmat > 65535 || nrho < 1 ||
+      nrho > 2 || (nmat > 0 && (!mats || !rho || !traces)))
+    return IMAGO_ERR_INVALID;
+  if (nmat == 0) return IMAGO_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemPool_t pool = scratch_pool();
+  if (!pool) return IMAGO_ERR_NO_DEVICE;
+  const size_t n = packed_traces_work(vale_dim, num_kpoints, nmat, nrho);
+  void *part = nullptr;
+  if (cudaMallocFromPoolAsync(&part, n * sizeof(double), pool, st) != cudaSuccess) {
+    cudaGetLastError();
+    return IMAGO_ERR_NOMEM;
+  }
+  const int rc = launch_packed_traces(vale_dim, num_kpoints, nmat, mats, nrho, rho,
+                                      static_cast<double *>(part), traces, st);
+  cudaFreeAsync(part, st);
+  return rc;
+}
+
 int imago_gauss_koverlap(imago_ctx *c, const double dk[9], double *re, double *im) {
   if (!c || !dk || !re || !im) return IMAGO_ERR_INVALID;
   for (int x = 0; x < 9; ++x)

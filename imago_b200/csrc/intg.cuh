@@ -186,4 +186,10 @@ int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
 int launch_prim_eval(int kind, int n, const double *params, const int *cls,
                      double *sh, cudaStream_t st);
 
+// makeValenceRho's traces of packed matrices against packed densities
+// (k_secular.cu); `part` holds packed_traces_work(...) doubles.
+size_t packed_traces_work(int vale_dim, int nk, int nmat, int nrho);
+int launch_packed_traces(int vale_dim, int nk, int nmat, const double *mats, int nrho,
+                         const double *rho, double *part, double *traces, cudaStream_t st);
+
 }  // namespace imago

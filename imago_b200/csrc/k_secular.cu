@@ -190,6 +190,105 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
 
 }  // namespace
 
+// ------------------------------------------------------------ traces --
+// makeValenceRho's traces (valeCharge.F90:218-291): for each packed
+// Hermitian matrix M_m and packed density R_s, summed over k-points,
+//   matrixElementMult(M, R) = 2 sum_{off-diagonal} (Mre Rre + Mim Rim)
+//                             + sum_{diagonal} Mre Rre
+// (matrixSubs.F90:66-109).  One CTA per (chunk of one k-point's packed
+// elements, matrix): each thread walks its elements kTrThreads apart and
+// follows the packed column they fall in (column c holds c + 1 elements
+// from c (c + 1) / 2, the last one diagonal), so no element's row and
+// column are computed from scratch.  Partial sums go to part[m][k][chunk]
+// [s] and k_trace_sum adds them in that fixed order: the result does not
+// depend on the schedule.  HBM-bound: 16 bytes of M per element and R
+// from L2 when the densities fit.
+constexpr int kTrThreads = 256;
+constexpr int kTrPerThread = 16;
+constexpr long long kTrChunk = (long long)kTrThreads * kTrPerThread;
+
+__global__ void __launch_bounds__(kTrThreads)
+    k_packed_traces(long long np, int nk, int nchunk, const double2 *mats, int nrho,
+                    const double2 *rho, double *part) {
+  const int m = blockIdx.y;
+  const int k = blockIdx.x / nchunk, chunk = blockIdx.x - k * nchunk;
+  const long long e0 = chunk * kTrChunk;
+  const long long e1 = e0 + kTrChunk < np ? e0 + kTrChunk : np;
+  const double2 *M = mats + ((long long)m * nk + k) * np;
+  const double2 *R0 = rho + (long long)k * np;
+  const double2 *R1 = rho + ((long long)nk + k) * np;
+  double a0 = 0.0, a1 = 0.0;
+  long long e = e0 + threadIdx.x;
+  if (e < e1) {
+    long long c = (long long)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
+    while (c * (c + 1) / 2 > e) --c;
+    while ((c + 1) * (c + 2) / 2 <= e) ++c;
+    long long end = (c + 1) * (c + 2) / 2;  // one past column c
+    for (; e < e1; e += kTrThreads) {
+      while (e >= end) {
+        ++c;
+        end += c + 1;
+      }
+      const double2 x = M[e];
+      const bool diag = e == end - 1;
+      const double2 r = R0[e];
+      a0 += diag ? x.x * r.x : 2.0 * (x.x * r.x + x.y * r.y);
+      if (nrho > 1) {
+        const double2 q = R1[e];
+        a1 += diag ? x.x * q.x : 2.0 * (x.x * q.x + x.y * q.y);
+      }
+    }
+  }
+  __shared__ double red[2][kTrThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][warp] = a0;
+    red[1][warp] = a1;
+  }
+  __syncthreads();
+  if (threadIdx.x < nrho) {
+    double t = 0.0;
+    for (int w = 0; w < kTrThreads / 32; ++w) t += red[threadIdx.x][w];
+    part[(((long long)m * nk + k) * nchunk + chunk) * nrho + threadIdx.x] = t;
+  }
+}
+
+__global__ void k_trace_sum(int nmat, int nrho, long long nper, const double *part,
+                            double *traces) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nmat * nrho) return;
+  const int m = i / nrho, s = i - m * nrho;
+  double t = 0.0;
+  for (long long j = 0; j < nper; ++j) t += part[((long long)m * nper + j) * nrho + s];
+  traces[i] = t;
+}
+
+size_t packed_traces_work(int vale_dim, int nk, int nmat, int nrho) {
+  const long long np = (long long)vale_dim * (vale_dim + 1) / 2;
+  const long long nchunk = (np + kTrChunk - 1) / kTrChunk;
+  return (size_t)nmat * nk * nchunk * nrho;
+}
+
+int launch_packed_traces(int vale_dim, int nk, int nmat, const double *mats, int nrho,
+                         const double *rho, double *part, double *traces, cudaStream_t st) {
+  const long long np = (long long)vale_dim * (vale_dim + 1) / 2;
+  const int nchunk = (int)((np + kTrChunk - 1) / kTrChunk);
+  const dim3 grid((unsigned)((long long)nk * nchunk), (unsigned)nmat);
+  k_packed_traces<<<grid, kTrThreads, 0, st>>>(np, nk, nchunk,
+                                              reinterpret_cast<const double2 *>(mats), nrho,
+                                              reinterpret_cast<const double2 *>(rho), part);
+  IMAGO_CUDA(cudaGetLastError());
+  k_trace_sum<<<(nmat * nrho + 127) / 128, 128, 0, st>>>(nmat, nrho,
+                                                         (long long)nk * nchunk, part, traces);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
 size_t jacobi_smem(int n) {
   const int m = n + (n & 1);
   return sizeof(double2) * (size_t)n * (n + 1) + sizeof(double) * m +

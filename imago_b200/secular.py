@@ -87,3 +87,20 @@ def secular_eigenvalues(out, pot_coeffs, num_states=None):
     a = torch.linalg.solve_triangular(lo, y.mH, upper=False)       # L^-1 H L^-H
     ev = hermitian_eigvals(a)
     return ev if num_states is None else ev[:, :num_states]
+
+
+def secular_eigensystem(out, pot_coeffs, num_states=None):
+    """Eigenvalues [nk, num_states] (ascending) and eigenvectors
+    [nk, V, num_states] of H c = E S c per k-point, the vectors normalised
+    as zhegv(1, 'V', 'U') returns them (c^H S c = 1): A = L^-1 H L^-H is
+    diagonalised by cuSOLVER through torch.linalg.eigh and the vectors
+    taken back by c = L^-H y."""
+    h, s = secular_matrices(out, pot_coeffs)
+    lo = torch.linalg.cholesky(s)
+    y = torch.linalg.solve_triangular(lo, h, upper=False)
+    a = torch.linalg.solve_triangular(lo, y.mH, upper=False)
+    ev, vec = torch.linalg.eigh(a)
+    c = torch.linalg.solve_triangular(lo.mH, vec, upper=True)
+    if num_states is not None:
+        ev, c = ev[:, :num_states], c[:, :, :num_states]
+    return ev, c

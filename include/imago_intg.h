@@ -198,6 +198,20 @@ IMAGO_API int imago_gauss_overlap_mm(imago_ctx *ctx, double *packed);
 IMAGO_API int imago_gauss_overlap_dm(imago_ctx *ctx, const double center[3],
                                      double *packed);
 
+/* The traces of makeValenceRho (valeCharge.F90:218-291) on the device:
+ *   traces[m * nrho + s] = sum over k of matrixElementMult(M_m(k), R_s(k))
+ *     = sum_k [ 2 sum_{off-diagonal} (Re M Re R + Im M Im R)
+ *               + sum_{diagonal} Re M Re R ]   (matrixSubs.F90:66-109)
+ * for nmat packed Hermitian matrices mats [nmat][nk][nPacked][2] (OL, NP,
+ * KE, MV or the potential terms EP_j) and nrho (1 or 2) packed densities
+ * rho [nrho][nk][nPacked][2] (for spin 2 the reference's total and
+ * difference densities).  All pointers are device memory; the call is
+ * ordered on `stream` and does not synchronise.  The partial sums are
+ * added in a fixed order, so the result is reproducible. */
+IMAGO_API int imago_packed_traces(int vale_dim, int num_kpoints, int nmat,
+                                  const double *mats, int nrho, const double *rho,
+                                  double *traces, void *stream);
+
 /* The overlap with a plane wave, <a|exp(-i dK_c . r)|b> for three wave
  * vectors dK_c (dk[3*c .. 3*c+2], bohr^-1; the reference passes
  * recipVectors(:, c) / numAxialKPoints(c)): replaces gaussKOverlap +

@@ -315,3 +315,168 @@ def secular_eigenvalues(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed,
         S[iu] = sp[pidx]
         out[k] = scipy.linalg.eigh(H, S, lower=False, eigvals_only=True)
     return out
+
+
+def _secular_hs(np_packed, ke_packed, ep_packed, pot_coeffs, ol_packed, mv_packed, k):
+    """H and S of k-point k, upper triangles, as secular_eigenvalues forms them."""
+    npk = np_packed.shape[1]
+    V = int((int((8 * npk + 1) ** 0.5) - 1) // 2)
+    iu = np.triu_indices(V)
+    pidx = iu[1] * (iu[1] + 1) // 2 + iu[0]
+    hp = np_packed[k, :, 0] + 1j * np_packed[k, :, 1]
+    hp = hp + (ke_packed[k, :, 0] + 1j * ke_packed[k, :, 1])
+    if mv_packed is not None:
+        hp = hp + (mv_packed[k, :, 0] + 1j * mv_packed[k, :, 1])
+    for j, w in enumerate(pot_coeffs):
+        f = 1.0 if w == 0.0 else w
+        hp = hp + (ep_packed[j, k, :, 0] + 1j * ep_packed[j, k, :, 1]) * f
+    sp = ol_packed[k, :, 0] + 1j * ol_packed[k, :, 1]
+    H = np.zeros((V, V), complex)
+    S = np.zeros((V, V), complex)
+    H[iu] = hp[pidx]
+    S[iu] = sp[pidx]
+    return H, S
+
+
+def populate_standard(eigenvalues, num_electrons, kpoint_weights=None):
+    """populateStandard (populate.F90:190-483) statement by statement, with
+    Python loops (small cases only): eigenvalues [nk, spin, numStates].
+    Returns (population [nk, spin, numStates], occupiedEnergy,
+    occupiedEnergyIndex (0-based), bandGap, gapKindCode)."""
+    small, metal_gap = 1.0e-8, 1.0e-3    # constants.f90:49, populate.F90
+    e = np.asarray(eigenvalues, dtype=np.float64)
+    nk, spin, ns = e.shape
+    kw = [2.0 / nk] * nk if kpoint_weights is None else list(kpoint_weights)
+    temp = [e[i, j, k] for i in range(nk) for j in range(spin) for k in range(ns)]
+    n = len(temp)
+    index = sorted(range(n), key=lambda i: temp[i])   # stable, ascending
+    srt = [temp[i] for i in index]
+    wt = lambda idx: kw[idx // (ns * spin)] / float(spin)
+    pop = [0.0] * n
+    populated = 0.0
+    ne = float(num_electrons)
+    occ = None
+    for i in range(n):
+        pop[index[i]] = wt(index[i])
+        populated = populated + pop[index[i]]
+        if populated > ne:
+            pop[index[i]] = wt(index[i]) + ne - populated
+            populated = ne
+        if abs(ne - populated) < small:
+            occ = i
+            break
+    if occ is None:
+        raise ValueError("fewer states than electrons")
+    occ_e = srt[occ]
+    lo = hi = occ
+    degen = pop[index[occ]]
+    possible = wt(index[occ])
+    while hi + 1 < n and abs(occ_e - srt[hi + 1]) <= small:
+        hi += 1
+        possible = possible + wt(index[hi])
+    while lo > 0 and abs(occ_e - srt[lo - 1]) <= small:
+        lo -= 1
+        possible = possible + wt(index[lo])
+        degen = degen + wt(index[lo])
+    for i in range(lo, hi + 1):
+        pop[index[i]] = degen / possible * wt(index[i])
+    occ = hi
+    occ_e = srt[occ]
+    if occ >= n - 1:
+        gap, kind = 0.0, 0
+    else:
+        gap = srt[occ + 1] - srt[occ]
+        if gap <= metal_gap:
+            gap, kind = 0.0, 0
+        else:
+            vbm, cbm = index[occ] // (ns * spin), index[occ + 1] // (ns * spin)
+            kind = 1 if vbm == cbm else 2
+    return np.array(pop).reshape(nk, spin, ns), occ_e, occ, gap, kind
+
+
+def matrix_element_mult(m1, m2):
+    """matrixElementMult (matrixSubs.F90:66-109) on one packed pair
+    [nPacked, 2]: off-diagonal re*re + im*im, diagonal re*re / 2, times 2."""
+    npk = m1.shape[0]
+    V = int((int((8 * npk + 1) ** 0.5) - 1) // 2)
+    t = 0.0
+    d = 0
+    for i in range(1, V + 1):
+        seg = slice(d, d + i - 1)
+        t += float(np.dot(m1[seg, 0], m2[seg, 0]) + np.dot(m1[seg, 1], m2[seg, 1]))
+        d += i
+        t += m1[d - 1, 0] * m2[d - 1, 0] / 2.0
+    return t * 2.0
+
+
+def valence_rho(np_packed, ke_packed, ep_packed, ol_packed, pot_coeffs, num_electrons,
+                num_states, mv_packed=None, kpoint_weights=None):
+    """One step of secularEqnSCF, populateStandard and makeValenceRho's
+    traces (valeCharge.F90:34-488) on the CPU: LAPACK's eigh(H, S) per k
+    and spin (pot_coeffs [potDim, spin]), rank-one updates of the upper
+    triangle per occupied state, packMatrix, matrixElementMult.  Returns a
+    dict named as the reference's variables, plus "population"."""
+    import scipy.linalg
+    w = np.asarray(pot_coeffs, dtype=np.float64)
+    if w.ndim == 1:
+        w = w[:, None]
+    spin = w.shape[1]
+    nk = np_packed.shape[0]
+    ev = np.zeros((nk, spin, num_states))
+    vecs = {}
+    for k in range(nk):
+        for s in range(spin):
+            H, S = _secular_hs(np_packed, ke_packed, ep_packed, w[:, s], ol_packed,
+                               mv_packed, k)
+            e, c = scipy.linalg.eigh(H, S, lower=False)
+            ev[k, s] = e[:num_states]
+            vecs[k, s] = c[:, :num_states]
+    pop, occ_e, _, gap, kind = populate_standard(ev, num_electrons, kpoint_weights)
+    V = vecs[0, 0].shape[0]
+    iu = np.triu_indices(V)
+    pidx = iu[1] * (iu[1] + 1) // 2 + iu[0]
+    order = np.argsort(pidx)
+    npk = V * (V + 1) // 2
+    mats = {"chargeDensityTrace": ol_packed, "nucPotTrace": np_packed,
+            "kineticEnergyTrace": ke_packed}
+    if mv_packed is not None:
+        mats["massVelocityTrace"] = mv_packed
+    res = {key: np.zeros(spin) for key in mats}
+    res["potRho"] = np.zeros((ep_packed.shape[0], spin))
+    res["electronEnergy"] = np.zeros(spin)
+    for k in range(nk):
+        rho = []
+        for s in range(spin):
+            r = np.zeros((V, V), complex)
+            for j in range(num_states):
+                f = pop[k, :, j]
+                if np.abs(f).sum() < 1.0e-8:
+                    continue
+                res["electronEnergy"][s] += f[s] * ev[k, s, j]
+                c = vecs[k, s][:, j]
+                r += f[s] * np.outer(c, np.conj(c))
+            p = np.zeros((npk, 2))
+            p[:, 0] = r[iu][order].real
+            p[:, 1] = r[iu][order].imag
+            rho.append(p)
+        if spin == 2:
+            rho = [rho[0] + rho[1], rho[0] - rho[1]]
+        for s in range(spin):
+            for key, m in mats.items():
+                res[key][s] += matrix_element_mult(m[k], rho[s])
+            for t in range(ep_packed.shape[0]):
+                res["potRho"][t, s] += matrix_element_mult(ep_packed[t, k], rho[s])
+    mv = res.get("massVelocityTrace", np.zeros(spin))
+    ke, nuc, pr = res["kineticEnergyTrace"], res["nucPotTrace"], res["potRho"]
+    if spin == 1:
+        res["sumElecEnergy"] = np.array([(w[:, 0] * pr[:, 0]).sum() + ke[0] + mv[0] + nuc[0]])
+    else:
+        res["sumElecEnergy"] = np.array([
+            0.5 * ((w[:, 0] * (pr[:, 0] + pr[:, 1])).sum() + ke[0] + ke[1] + mv[0] + mv[1]
+                   + nuc[0] + nuc[1]),
+            0.5 * ((w[:, 1] * (pr[:, 0] - pr[:, 1])).sum() + ke[0] - ke[1] + mv[0] - mv[1]
+                   + nuc[0] - nuc[1])])
+    res["population"] = pop
+    res["occupiedEnergy"], res["bandGap"], res["gapKindCode"] = occ_e, gap, kind
+    res["eigenvalues"] = ev
+    return res
