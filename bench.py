@@ -386,6 +386,53 @@ def time_secular(bufs, pot_dim, stream, torch, steps=3):
     return float(np.median(ts))
 
 
+def time_valence_rho(bufs, pot_dim, stream, torch, steps=3):
+    """One SCF step's valence charge from the resident builds
+    (imago_b200.charge): eigenvalues and eigenvectors, the populations (host,
+    half as many electrons as valence states), and the density traces
+    against OL, NP, KE and every EP term; median wall seconds of the step
+    with the device synchronised on both sides.  Then the trace kernel alone
+    over the EP terms (device events): its time and HBM bandwidth, the
+    algorithmic bytes being the EP matrices read once (potDim x nk x
+    nPacked x 16)."""
+    import time
+    from imago_b200 import charge, secular
+    w = -0.5 * np.ones(pot_dim)
+    out = {k: bufs[k] for k in ("np_packed", "ke_packed", "ep_packed", "ol_packed")}
+    nk, npk = out["np_packed"].shape[0], out["np_packed"].shape[1]
+    V = int((int((8 * npk + 1) ** 0.5) - 1) // 2)
+    ne = V // 2
+    ts = []
+    with torch.cuda.stream(stream):
+        for rep in range(steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e, c = secular.secular_eigensystem(out, w)
+            pop = charge.populate_standard(e.cpu().numpy()[:, None, :], ne)
+            r = charge.valence_rho(out, [e], [c], pop["population"], w)
+            torch.cuda.synchronize()
+            if rep:
+                ts.append(time.perf_counter() - t0)
+        rho = charge.packed_density(c, pop["population"][:, 0, :])[None]
+        charge.packed_traces(out["ep_packed"], rho, nk, V)
+        kt = []
+        for _ in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            charge.packed_traces(out["ep_packed"], rho, nk, V)
+            b.record(stream)
+            b.synchronize()
+            kt.append(a.elapsed_time(b))
+    nbytes = pot_dim * nk * npk * 16
+    kms = float(np.median(kt))
+    return {"valence_step_s": float(np.median(ts)), "num_electrons": ne,
+            "charge_trace": float(r["chargeDensityTrace"][0]),
+            "trace_kernel_ms": kms, "trace_bytes": nbytes,
+            "trace_gbs": nbytes / (kms * 1e-3) / 1e9,
+            "stat": f"median of {steps}"}
+
+
 def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     """Device milliseconds (median of `reps`, CUDA events on the library's
     stream, outputs resident in HBM) of the builds beside the SCF set on the
@@ -691,6 +738,7 @@ def run_ours(args):
 
     tuning = g.tuning()
     secular_s = time_secular(bufs, P, stream, torch)
+    valence = time_valence_rho(bufs, P, stream, torch)
     adjacent = None
     if world == 1 and args.workload == "si8" and not args.no_adjacent:
         adjacent = adjacent_builds(g, bufs, stream, torch, dev, ham_mode=args.ham_mode)
@@ -740,6 +788,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "tuning": tuning,
             "secular_step_s": secular_s,
+            "valence_rho": valence,
         }
         if adjacent:
             line["adjacent_builds"] = adjacent

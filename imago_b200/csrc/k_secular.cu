@@ -67,11 +67,16 @@ __global__ void k_secular(int V, long long np, int nk, int pot_dim,
 // J_qp = -s e^{-i phi} (columns first, then rows).  Sweeps stop when the
 // off-diagonal Frobenius norm is below 1e-14 of the whole, at most
 // kJacobiMaxSweeps; the diagonal is then returned in ascending order.
+// With `vec`, the rotations are also accumulated, V <- V J from V = I, in
+// `vec` itself (column-major while the sweeps run, so the lanes of a warp,
+// on rows, touch consecutive addresses), and at the end the columns are
+// written in the order of the eigenvalues, vec[b][row][j] the row-th
+// component of the j-th eigenvector (A V = V diag(w)).
 constexpr int kJacobiThreads = 512;
 constexpr int kJacobiMaxSweeps = 30;
 
 __global__ void __launch_bounds__(kJacobiThreads, 1)
-    k_jacobi_eigvals(int n, const double2 *a, double *w) {
+    k_jacobi_eigvals(int n, const double2 *a, double *w, double2 *vec) {
   extern __shared__ double2 jsm[];
   const int ld = n + 1, m = n + (n & 1), npair = m / 2;
   double2 *A = jsm;
@@ -83,6 +88,10 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   const double2 *src = a + (size_t)blockIdx.x * n * n;
   for (int i = tid; i < n * n; i += kJacobiThreads)
     A[(i / n) * ld + i % n] = src[i];
+  double2 *Vt = vec ? vec + (size_t)blockIdx.x * n * n : nullptr;  // Vt[col * n + row]
+  if (Vt)
+    for (int i = tid; i < n * n; i += kJacobiThreads)
+      Vt[i] = make_double2(i / n == i % n ? 1.0 : 0.0, 0.0);
   __syncthreads();
   for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
     // convergence: off-diagonal part of the Frobenius norm
@@ -155,6 +164,15 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
         const double2 eap = make_double2(e.x * ap.x - e.y * ap.y, e.x * ap.y + e.y * ap.x);
         A[row * ld + x.x] = make_double2(c * ap.x - sn * ceq.x, c * ap.y - sn * ceq.y);
         A[row * ld + x.y] = make_double2(sn * eap.x + c * aq.x, sn * eap.y + c * aq.y);
+        if (Vt) {  // the same column rotation of V
+          const double2 vp = Vt[(size_t)x.x * n + row], vq = Vt[(size_t)x.y * n + row];
+          const double2 cvq = make_double2(e.x * vq.x + e.y * vq.y, e.x * vq.y - e.y * vq.x);
+          const double2 evp = make_double2(e.x * vp.x - e.y * vp.y, e.x * vp.y + e.y * vp.x);
+          Vt[(size_t)x.x * n + row] =
+              make_double2(c * vp.x - sn * cvq.x, c * vp.y - sn * cvq.y);
+          Vt[(size_t)x.y * n + row] =
+              make_double2(sn * evp.x + c * vq.x, sn * evp.y + c * vq.y);
+        }
       }
       __syncthreads();
       // rows p, q of every column: A <- J^H A (a warp per pair, lanes on
@@ -177,6 +195,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
   }
   // ascending order by rank (ties by index)
   double *out = w + (size_t)blockIdx.x * n;
+  int *inv = reinterpret_cast<int *>(pq);  // inv[rank] = index, m >= n ints
   for (int i = tid; i < n; i += kJacobiThreads) {
     const double d = A[i * ld + i].x;
     int rank = 0;
@@ -185,6 +204,15 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
       rank += dj < d || (dj == d && j < i);
     }
     out[rank] = d;
+    inv[rank] = i;
+  }
+  if (!Vt) return;
+  __syncthreads();  // the diagonal is read: A's storage takes V
+  for (int i = tid; i < n * n; i += kJacobiThreads) A[(i / n) * ld + i % n] = Vt[i];
+  __syncthreads();
+  for (int o = tid; o < n * n; o += kJacobiThreads) {
+    const int row = o / n, j = o % n;
+    Vt[o] = A[inv[j] * ld + row];
   }
 }
 
@@ -297,8 +325,8 @@ size_t jacobi_smem(int n) {
 
 }  // namespace imago
 
-extern "C" int imago_hermitian_eigvals(int n, int batch, const double *a,
-                                       double *w, void *stream) {
+extern "C" int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
+                                    double *vec, void *stream) {
   if (n <= 0 || batch < 0 || !a || !w) return IMAGO_ERR_INVALID;
   if (batch == 0) return IMAGO_OK;
   const size_t smem = imago::jacobi_smem(n);
@@ -319,9 +347,14 @@ extern "C" int imago_hermitian_eigvals(int n, int batch, const double *a,
     attr_set[dev] = true;
   }
   imago::k_jacobi_eigvals<<<batch, imago::kJacobiThreads, smem, (cudaStream_t)stream>>>(
-      n, reinterpret_cast<const double2 *>(a), w);
+      n, reinterpret_cast<const double2 *>(a), w, reinterpret_cast<double2 *>(vec));
   if (cudaGetLastError() != cudaSuccess) return IMAGO_ERR_CUDA;
   return IMAGO_OK;
+}
+
+extern "C" int imago_hermitian_eigvals(int n, int batch, const double *a,
+                                       double *w, void *stream) {
+  return imago_hermitian_eigh(n, batch, a, w, nullptr, stream);
 }
 
 extern "C" int imago_secular_matrices_rel(int vale_dim, int num_kpoints, int pot_dim,

@@ -77,6 +77,27 @@ def hermitian_eigvals(a):
     return w
 
 
+def hermitian_eigh(a):
+    """Ascending eigenvalues [b, n] and unit eigenvectors [b, n, n] (in
+    columns) of a batch of Hermitian matrices [b, n, n] (complex128, CUDA):
+    imago_hermitian_eigh (the Jacobi kernel accumulating its rotations) up
+    to n = 112, cuSOLVER through torch beyond."""
+    b, n = a.shape[0], a.shape[-1]
+    if n > JACOBI_MAX_N:
+        return torch.linalg.eigh(a)
+    a = a.contiguous()
+    w = torch.empty((b, n), dtype=torch.float64, device=a.device)
+    v = torch.empty((b, n, n), dtype=torch.complex128, device=a.device)
+    L = intg.lib()
+    L.imago_hermitian_eigh.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 4
+    L.imago_hermitian_eigh.restype = ctypes.c_int
+    rc = L.imago_hermitian_eigh(n, b, a.data_ptr(), w.data_ptr(), v.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise intg.ImagoError(rc, "imago_hermitian_eigh")
+    return w, v
+
+
 def secular_eigenvalues(out, pot_coeffs, num_states=None):
     """Eigenvalues of H c = E S c per k-point, ascending, [nk, num_states]:
     the Cholesky factor L of S (cuSOLVER, batched), A = L^-1 H L^-H, and the
@@ -93,13 +114,13 @@ def secular_eigensystem(out, pot_coeffs, num_states=None):
     """Eigenvalues [nk, num_states] (ascending) and eigenvectors
     [nk, V, num_states] of H c = E S c per k-point, the vectors normalised
     as zhegv(1, 'V', 'U') returns them (c^H S c = 1): A = L^-1 H L^-H is
-    diagonalised by cuSOLVER through torch.linalg.eigh and the vectors
-    taken back by c = L^-H y."""
+    diagonalised by hermitian_eigh and the vectors taken back by
+    c = L^-H y."""
     h, s = secular_matrices(out, pot_coeffs)
     lo = torch.linalg.cholesky(s)
     y = torch.linalg.solve_triangular(lo, h, upper=False)
     a = torch.linalg.solve_triangular(lo, y.mH, upper=False)
-    ev, vec = torch.linalg.eigh(a)
+    ev, vec = hermitian_eigh(a)
     c = torch.linalg.solve_triangular(lo.mH, vec, upper=True)
     if num_states is not None:
         ev, c = ev[:, :num_states], c[:, :, :num_states]

@@ -350,6 +350,15 @@ IMAGO_API int imago_secular_matrices_rel(int vale_dim, int num_kpoints, int pot_
 IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
                                       double *w, void *stream);
 
+/* imago_hermitian_eigvals with the eigenvectors: a is stored row-major,
+ * a[b][row][col], and vec [batch][n][n] (device, (re, im) interleaved)
+ * receives vec[b][row][j], the row-th component of the unit eigenvector of
+ * w[b][j] (the columns of V with A V = V diag(w)), accumulated from the
+ * Jacobi rotations.  The eigenvector step of zhegv(1, 'V', 'U') after its
+ * Cholesky reduction (interfaces.F90:73-120). */
+IMAGO_API int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
+                                   double *vec, void *stream);
+
 /* No counterpart in the reference.  The builds of one call run each kind
  * (OL, KE, NP, EP) on a stream of its own, concurrently; serial != 0 runs
  * them one after another on the context's stream instead, which gives each

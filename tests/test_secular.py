@@ -86,6 +86,32 @@ def test_batched_jacobi_eigenvalues(imago_lib, n):
     assert np.abs(got - ref).max() <= 1e-12 * scale
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 5, 33, 104, 112])
+def test_batched_jacobi_eigenvectors(imago_lib, n):
+    # imago_hermitian_eigh: A V = V diag(w), V unitary, w as LAPACK's, on
+    # random and degenerate spectra
+    import torch
+    from imago_b200 import secular
+    rng = np.random.default_rng(100 + n)
+    b = 6
+    x = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    h = (x + np.conj(np.swapaxes(x, 1, 2))) / 2
+    h[0] = np.eye(n) * 2.5
+    if n > 3:  # a three-fold level inside a random spectrum
+        q, _ = np.linalg.qr(x[1])
+        d = np.sort(rng.normal(size=n))
+        d[1:4] = d[1]
+        h[1] = (q * d) @ np.conj(q.T)
+    w, v = secular.hermitian_eigh(torch.as_tensor(h, device="cuda"))
+    w, v = w.cpu().numpy(), v.cpu().numpy()
+    scale = max(1.0, np.abs(h).max())
+    assert np.abs(w - np.linalg.eigvalsh(h)).max() <= 1e-12 * scale * n
+    for i in range(b):
+        assert np.abs(h[i] @ v[i] - v[i] * w[i]).max() <= 1e-11 * scale * n
+        assert np.abs(np.conj(v[i].T) @ v[i] - np.eye(n)).max() <= 1e-12 * n
+
+
 def test_oracle_pscf_hamiltonian_is_the_combination_of_its_parts():
     # gaussOverlapHamPSCF sums kinetic, nuclear, potCoeffs-weighted
     # potential terms and (rel) minus mass velocity per alpha pair; every
