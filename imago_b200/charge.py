@@ -83,6 +83,78 @@ def populate_standard(eigenvalues, num_electrons, kpoint_weights=None):
             "occupied_index": occ, "band_gap": float(gap), "gap_kind": kind}
 
 
+def step_function(x, step_range):
+    """stepFunction (mathSubs.f90:164-185): 0 above the range, 1 below it,
+    the Fermi function 1 / (1 + e^x) between."""
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(over="ignore"):
+        f = 1.0 / (1.0 + np.exp(np.minimum(x, step_range)))
+    return np.where(x > step_range, 0.0, np.where(x < -step_range, 1.0, f))
+
+
+def populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
+                      fermi_search_limit, kpoint_weights=None, standard=None):
+    """populateSmearing (populate.F90:486-620): the Fermi level bisected
+    (at most 500 steps) between the standard population's highest occupied
+    state minus fermi_search_limit and the next state plus it, every state
+    taking weight x stepFunction((E - E_F) / thermal_sigma,
+    max_thermal_range) until the charge is within smallThresh of
+    numElectrons.  Energies in Hartree (the reference divides its eV inputs
+    by hartree, input.f90:369-383).  `standard` is populate_standard's
+    result for the same arguments (computed when absent).  Returns
+    {"population", "fermi_energy", "iterations", "charge"}."""
+    e = np.asarray(eigenvalues, dtype=np.float64)
+    nk, spin, ns = e.shape
+    if standard is None:
+        standard = populate_standard(e, num_electrons, kpoint_weights)
+    kw = (np.full(nk, 2.0 / nk) if kpoint_weights is None
+          else np.asarray(kpoint_weights, dtype=np.float64))
+    flat = e.reshape(-1)
+    order = np.argsort(flat, kind="stable")
+    srt = flat[order]
+    w = kw[order // (ns * spin)] / float(spin)
+    occ = standard["occupied_index"]
+    lo = srt[occ] - fermi_search_limit
+    hi = srt[min(occ + 1, srt.size - 1)] + fermi_search_limit
+    ne = float(num_electrons)
+    pop = np.zeros(srt.size)
+    ef, charge, it = 0.5 * (lo + hi), 0.0, 0
+    for it in range(1, 501):
+        ef = 0.5 * (lo + hi)
+        f = step_function((srt - ef) / thermal_sigma, max_thermal_range)
+        p = w * f
+        # the reference's loop stops at the first state the step function
+        # zeroes; the energies ascend, so every later one is zero too
+        charge = float(np.cumsum(p)[-1])
+        pop = np.zeros(srt.size)
+        pop[order] = p
+        if abs(charge - ne) < SMALL_THRESH:
+            break
+        if charge < ne:
+            lo = ef
+        else:
+            hi = ef
+    return {"population": pop.reshape(nk, spin, ns), "fermi_energy": float(ef),
+            "iterations": it, "charge": charge}
+
+
+def populate_states(eigenvalues, num_electrons, kpoint_weights=None, thermal_sigma=0.0,
+                    max_thermal_range=0.0, fermi_search_limit=0.0):
+    """populateStates (populate.F90:150-187): the standard population, then
+    the thermal smearing when thermal_sigma is not zero.  The XANES/ELNES
+    core-hole correction (excitedQN_n) is not part of this step."""
+    std = populate_standard(eigenvalues, num_electrons, kpoint_weights)
+    if thermal_sigma == 0.0:
+        return std
+    sm = populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
+                           fermi_search_limit, kpoint_weights, standard=std)
+    out = dict(std)
+    out["population"] = sm["population"]
+    out["occupied_energy"] = sm["fermi_energy"]
+    out["smearing_iterations"] = sm["iterations"]
+    return out
+
+
 _PACK_CACHE = {}
 
 

@@ -394,6 +394,52 @@ def populate_standard(eigenvalues, num_electrons, kpoint_weights=None):
     return np.array(pop).reshape(nk, spin, ns), occ_e, occ, gap, kind
 
 
+def populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
+                      fermi_search_limit, kpoint_weights=None):
+    """populateSmearing (populate.F90:486-620) statement by statement with
+    Python loops and stepFunction (mathSubs.f90:164-185), after
+    populate_standard.  Returns (population, occupiedEnergy, iterations)."""
+    import math
+    e = np.asarray(eigenvalues, dtype=np.float64)
+    nk, spin, ns = e.shape
+    _, _, occ, _, _ = populate_standard(e, num_electrons, kpoint_weights)
+    kw = [2.0 / nk] * nk if kpoint_weights is None else list(kpoint_weights)
+    temp = [e[i, j, k] for i in range(nk) for j in range(spin) for k in range(ns)]
+    n = len(temp)
+    index = sorted(range(n), key=lambda i: temp[i])
+    srt = [temp[i] for i in index]
+
+    def step(x, r):
+        if x > r:
+            return 0.0
+        if x < -r:
+            return 1.0
+        return 1.0 / (1.0 + math.exp(x))
+
+    lo = srt[occ] - fermi_search_limit
+    hi = srt[min(occ + 1, n - 1)] + fermi_search_limit
+    ne = float(num_electrons)
+    pop = [0.0] * n
+    ef, it = 0.0, 0
+    for it in range(1, 501):
+        ef = 0.5 * (lo + hi)
+        charge = 0.0
+        pop = [0.0] * n
+        for j in range(n):
+            f = step((srt[j] - ef) / thermal_sigma, max_thermal_range)
+            if f == 0.0:
+                break
+            pop[index[j]] = (kw[index[j] // (ns * spin)] / float(spin)) * f
+            charge = charge + pop[index[j]]
+        if abs(charge - ne) < 1.0e-8:
+            break
+        if charge < ne:
+            lo = ef
+        else:
+            hi = ef
+    return np.array(pop).reshape(nk, spin, ns), ef, it
+
+
 def matrix_element_mult(m1, m2):
     """matrixElementMult (matrixSubs.F90:66-109) on one packed pair
     [nPacked, 2]: off-diagonal re*re + im*im, diagonal re*re / 2, times 2."""

@@ -61,6 +61,37 @@ def test_populate_shares_a_degenerate_level():
         charge.populate_standard(e, 9)
 
 
+@pytest.mark.parametrize("seed", range(5))
+def test_smearing_matches_oracle(seed):
+    # thermal smearing: sigma from 0.01 to 0.5 eV, in Hartree
+    rng = np.random.default_rng(50 + seed)
+    nk, spin, ns = int(rng.integers(1, 5)), int(rng.integers(1, 3)), int(rng.integers(5, 14))
+    e = _spectrum(rng, nk, spin, ns, degenerate=seed == 4) * 0.3
+    kw = rng.uniform(0.5, 1.5, nk)
+    kw *= 2.0 / kw.sum()
+    hartree = 27.21138386
+    for sigma_ev in (0.01, 0.1, 0.5):
+        ne = int(rng.integers(1, ns))
+        args = (e, ne, sigma_ev / hartree, 20.0, 1.0 / hartree)
+        got = charge.populate_smearing(*args, kpoint_weights=kw)
+        pop, ef, it = oracle.populate_smearing(*args, kpoint_weights=kw)
+        assert got["iterations"] == it and got["fermi_energy"] == ef, (seed, sigma_ev)
+        assert np.allclose(got["population"], pop, rtol=0, atol=1e-14)
+        assert abs(got["population"].sum() - ne) < 1e-8
+        both = charge.populate_states(e, ne, kw, *args[2:])
+        assert np.array_equal(both["population"], got["population"])
+
+
+def test_smearing_tends_to_the_standard_population():
+    # a gapped spectrum and a sigma far below the gap: the Fermi function
+    # is a step at the gap, so the smeared population is the standard one
+    e = np.array([[[-1.0, -0.5, 0.5]], [[-0.9, -0.4, 0.6]]])
+    std = charge.populate_standard(e, 4)
+    sm = charge.populate_smearing(e, 4, 0.001, 50.0, 0.05)
+    assert np.allclose(sm["population"], std["population"], atol=1e-12)
+    assert -0.4 < sm["fermi_energy"] < 0.5
+
+
 def test_oracle_charge_trace_counts_the_electrons():
     # Tr(rho S) = sum_j f_j c_j^H S c_j = sum_j f_j = numElectrons
     s = configs.small_test_system()
