@@ -633,3 +633,24 @@ def test_koverlap_build_matches_oracle(imago_lib, name):
             d = packed_mismatch(np.stack([re0[ax, k][cols, rows], im0[ax, k][cols, rows]], -1),
                                 ol[k][idx])
             assert d[1] == 0, d
+
+
+def test_koverlap_at_zero_wave_vector_is_the_overlap_quartz(imago_lib):
+    # the 162-atom quartz cell at Gamma (V = 1566, C = 378, the tiled
+    # orthogonalisation): with dK = 0 every plane-wave matrix is the
+    # orthogonalised overlap, full, whose packed upper triangle the overlap
+    # build zeroes below 1e-10
+    s = configs.quartz_supercell(seed=3, gamma=True)
+    with intg.IntegralSetup(s) as g:
+        ol = g.gauss_overlap_ol()[0]
+        re, im = g.gauss_koverlap(np.zeros((3, 3)))
+        V = g.vale_dim
+    rows, cols = np.triu_indices(V)
+    idx = cols * (cols + 1) // 2 + rows
+    for ax in range(3):
+        got = np.stack([re[ax, 0][cols, rows], im[ax, 0][cols, rows]], -1)
+        d = packed_mismatch(got, ol[0][idx])
+        assert d[1] == 0, (ax, d)
+        # and the full matrix is Hermitian
+        full = re[ax, 0] + 1j * im[ax, 0]
+        assert np.abs(full - full.conj().T).max() <= 1e-10
