@@ -224,47 +224,53 @@ __global__ void __launch_bounds__(kJacobiThreads, 1)
 //   matrixElementMult(M, R) = 2 sum_{off-diagonal} (Mre Rre + Mim Rim)
 //                             + sum_{diagonal} Mre Rre
 // (matrixSubs.F90:66-109).  One CTA per (chunk of one k-point's packed
-// elements, matrix): each thread walks its elements kTrThreads apart and
-// follows the packed column they fall in (column c holds c + 1 elements
-// from c (c + 1) / 2, the last one diagonal), so no element's row and
-// column are computed from scratch.  Partial sums go to part[m][k][chunk]
-// [s] and k_trace_sum adds them in that fixed order: the result does not
+// elements, matrix): every element is first taken as an off-diagonal one
+// (contiguous loads, 32-bit indices), then the chunk's diagonal elements,
+// at c (c + 3) / 2 for column c, are corrected to the diagonal weight.
+// Partial sums go to part[m][k][chunk][s] and k_trace_sum adds them in
+// that fixed order: the result does not
 // depend on the schedule.  HBM-bound: 16 bytes of M per element and R
 // from L2 when the densities fit.
 constexpr int kTrThreads = 256;
 constexpr int kTrPerThread = 16;
 constexpr long long kTrChunk = (long long)kTrThreads * kTrPerThread;
 
+template <int NRHO>
 __global__ void __launch_bounds__(kTrThreads)
-    k_packed_traces(long long np, int nk, int nchunk, const double2 *mats, int nrho,
+    k_packed_traces(long long np, int nk, int nchunk, const double2 *mats,
                     const double2 *rho, double *part) {
   const int m = blockIdx.y;
   const int k = blockIdx.x / nchunk, chunk = blockIdx.x - k * nchunk;
   const long long e0 = chunk * kTrChunk;
-  const long long e1 = e0 + kTrChunk < np ? e0 + kTrChunk : np;
-  const double2 *M = mats + ((long long)m * nk + k) * np;
-  const double2 *R0 = rho + (long long)k * np;
-  const double2 *R1 = rho + ((long long)nk + k) * np;
+  const int len = (int)(e0 + kTrChunk < np ? kTrChunk : np - e0);
+  const double2 *M = mats + ((long long)m * nk + k) * np + e0;
+  const double2 *R0 = rho + (long long)k * np + e0;
+  const double2 *R1 = rho + ((long long)nk + k) * np + e0;
+  // every element as an off-diagonal one ...
   double a0 = 0.0, a1 = 0.0;
-  long long e = e0 + threadIdx.x;
-  if (e < e1) {
-    long long c = (long long)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
-    while (c * (c + 1) / 2 > e) --c;
-    while ((c + 1) * (c + 2) / 2 <= e) ++c;
-    long long end = (c + 1) * (c + 2) / 2;  // one past column c
-    for (; e < e1; e += kTrThreads) {
-      while (e >= end) {
-        ++c;
-        end += c + 1;
-      }
-      const double2 x = M[e];
-      const bool diag = e == end - 1;
-      const double2 r = R0[e];
-      a0 += diag ? x.x * r.x : 2.0 * (x.x * r.x + x.y * r.y);
-      if (nrho > 1) {
-        const double2 q = R1[e];
-        a1 += diag ? x.x * q.x : 2.0 * (x.x * q.x + x.y * q.y);
-      }
+#pragma unroll 4
+  for (int i = threadIdx.x; i < len; i += kTrThreads) {
+    const double2 x = M[i], r = R0[i];
+    a0 += x.x * r.x + x.y * r.y;
+    if (NRHO > 1) {
+      const double2 q = R1[i];
+      a1 += x.x * q.x + x.y * q.y;
+    }
+  }
+  a0 *= 2.0;
+  a1 *= 2.0;
+  // ... then the diagonal ones (packed index c (c + 3) / 2) of the chunk
+  // corrected to Re M Re R: minus (Re M Re R + 2 Im M Im R)
+  long long c = (long long)((sqrt(9.0 + 8.0 * (double)e0) - 3.0) * 0.5);
+  while (c > 0 && (c - 1) * (c + 2) / 2 >= e0) --c;
+  while (c * (c + 3) / 2 < e0) ++c;
+  for (long long d = c + threadIdx.x; d * (d + 3) / 2 < e0 + len; d += kTrThreads) {
+    const int i = (int)(d * (d + 3) / 2 - e0);
+    const double2 x = M[i], r = R0[i];
+    a0 -= x.x * r.x + 2.0 * x.y * r.y;
+    if (NRHO > 1) {
+      const double2 q = R1[i];
+      a1 -= x.x * q.x + 2.0 * x.y * q.y;
     }
   }
   __shared__ double red[2][kTrThreads / 32];
@@ -279,10 +285,10 @@ __global__ void __launch_bounds__(kTrThreads)
     red[1][warp] = a1;
   }
   __syncthreads();
-  if (threadIdx.x < nrho) {
+  if (threadIdx.x < NRHO) {
     double t = 0.0;
     for (int w = 0; w < kTrThreads / 32; ++w) t += red[threadIdx.x][w];
-    part[(((long long)m * nk + k) * nchunk + chunk) * nrho + threadIdx.x] = t;
+    part[(((long long)m * nk + k) * nchunk + chunk) * NRHO + threadIdx.x] = t;
   }
 }
 
@@ -307,9 +313,12 @@ int launch_packed_traces(int vale_dim, int nk, int nmat, const double *mats, int
   const long long np = (long long)vale_dim * (vale_dim + 1) / 2;
   const int nchunk = (int)((np + kTrChunk - 1) / kTrChunk);
   const dim3 grid((unsigned)((long long)nk * nchunk), (unsigned)nmat);
-  k_packed_traces<<<grid, kTrThreads, 0, st>>>(np, nk, nchunk,
-                                              reinterpret_cast<const double2 *>(mats), nrho,
-                                              reinterpret_cast<const double2 *>(rho), part);
+  const double2 *m2 = reinterpret_cast<const double2 *>(mats);
+  const double2 *r2 = reinterpret_cast<const double2 *>(rho);
+  if (nrho > 1)
+    k_packed_traces<2><<<grid, kTrThreads, 0, st>>>(np, nk, nchunk, m2, r2, part);
+  else
+    k_packed_traces<1><<<grid, kTrThreads, 0, st>>>(np, nk, nchunk, m2, r2, part);
   IMAGO_CUDA(cudaGetLastError());
   k_trace_sum<<<(nmat * nrho + 127) / 128, 128, 0, st>>>(nmat, nrho,
                                                          (long long)nk * nchunk, part, traces);
