@@ -292,14 +292,18 @@ __global__ void __launch_bounds__(kTrThreads)
   }
 }
 
-__global__ void k_trace_sum(int nmat, int nrho, long long nper, const double *part,
-                            double *traces) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nmat * nrho) return;
-  const int m = i / nrho, s = i - m * nrho;
+// One warp per trace: lane l adds partials l, l + 32, ... in order, then
+// the lanes' sums are combined in a fixed butterfly, so the result does not
+// depend on the schedule.
+__global__ void __launch_bounds__(32)
+    k_trace_sum(int nrho, long long nper, const double *part, double *traces) {
+  const int i = blockIdx.x, m = i / nrho, s = i - m * nrho;
   double t = 0.0;
-  for (long long j = 0; j < nper; ++j) t += part[((long long)m * nper + j) * nrho + s];
-  traces[i] = t;
+  for (long long j = threadIdx.x; j < nper; j += 32)
+    t += part[((long long)m * nper + j) * nrho + s];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (threadIdx.x == 0) traces[i] = t;
 }
 
 size_t packed_traces_work(int vale_dim, int nk, int nmat, int nrho) {
@@ -320,8 +324,7 @@ int launch_packed_traces(int vale_dim, int nk, int nmat, const double *mats, int
   else
     k_packed_traces<1><<<grid, kTrThreads, 0, st>>>(np, nk, nchunk, m2, r2, part);
   IMAGO_CUDA(cudaGetLastError());
-  k_trace_sum<<<(nmat * nrho + 127) / 128, 128, 0, st>>>(nmat, nrho,
-                                                         (long long)nk * nchunk, part, traces);
+  k_trace_sum<<<nmat * nrho, 32, 0, st>>>(nrho, (long long)nk * nchunk, part, traces);
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }
