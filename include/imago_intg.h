@@ -2,12 +2,19 @@
  * imago_intg.h -- C ABI of the B200 integral setup for Imago.
  *
  * This library replaces the four integral builds that Imago's setupSCF
- * (src/imago/imago.F90:103-377) calls:
+ * (src/imago/imago.F90:103-377) calls on every SCF run:
  *
  *   gaussOverlapOL      src/imago/integrals.F90:151   (called imago.F90:262)
  *   gaussOverlapKE      src/imago/integrals.F90:656   (called imago.F90:268)
  *   gaussOverlapNP      src/imago/integrals.F90:1531  (called imago.F90:284)
  *   elecPotGaussOverlap src/imago/integrals.F90:2357  (called imago.F90:293)
+ *
+ * and the builds beside them: gaussOverlapMV (integrals.F90:1091, rel = 1),
+ * gaussOverlapHamPSCF (integrals.F90:2860), gaussOverlapDM / gaussOverlapMM
+ * / gaussKOverlap (integrals3Terms.F90:64, 511, 956).  For the SCF step
+ * that consumes them it provides the secular matrices (secularEqn.F90),
+ * batched Hermitian eigenvalues and eigenvectors (after zhegv's Cholesky
+ * reduction) and the density traces of makeValenceRho (valeCharge.F90).
  *
  * Each build sums the two- or three-centre Gaussian integrals over lattice
  * images within the reference's cutoffs, phases them onto every k-point,
