@@ -5,9 +5,9 @@ traces of the density matrix against the integral matrices.
     rho = valence_rho(out, eigenvalues, eigenvectors, pop["population"],
                       pot_coeffs)
 
-populate_standard is populateStandard (populate.F90:190-483, the
-population without thermal smearing): host work over the sorted
-eigenvalues, as in the reference.  valence_rho is the trace part of
+populate_states is populateStates (populate.F90:150-620: the standard
+population and the thermal smearing) in the library's host code
+(imago_populate_states), over the sorted eigenvalues as in the reference.  valence_rho is the trace part of
 makeValenceRho (valeCharge.F90:34-526): per k-point the density
 rho = sum_j f_j c_j c_j^H of the occupied states (a batched complex GEMM,
 cuBLAS through torch), packed like the integrals, and its traces against
@@ -24,135 +24,66 @@ import torch
 from . import intg
 
 SMALL_THRESH = 1.0e-8      # smallThresh, constants.f90:49
-METAL_GAP_THRESH = 1.0e-3  # populate.F90 metalGapThresh
-
-
-def populate_standard(eigenvalues, num_electrons, kpoint_weights=None):
-    """populateStandard (populate.F90:190-483) for eigenvalues [nk, spin,
-    numStates] (energyEigenValues(state, k, spin) in the reference).  Every
-    state takes kPointWeight(k) / spin electrons in ascending energy until
-    numElectrons are placed, the last one the remainder; the states within
-    smallThresh of that energy then share the degenerate charge in
-    proportion to their weights.  kpoint_weights default to 2 / nk (the
-    mesh weights, kpoints.f90:816).  Returns {"population": [nk, spin,
-    numStates], "occupied_energy", "occupied_index" (0-based, into the
-    sorted list), "band_gap", "gap_kind" (0 metal, 1 direct, 2 indirect)}."""
-    e = np.asarray(eigenvalues, dtype=np.float64)
-    nk, spin, ns = e.shape
-    kw = (np.full(nk, 2.0 / nk) if kpoint_weights is None
-          else np.asarray(kpoint_weights, dtype=np.float64))
-    flat = e.reshape(-1)        # (k, spin, state), state fastest
-    n = flat.size
-    order = np.argsort(flat, kind="stable")
-    srt = flat[order]
-    w = kw[order // (ns * spin)] / float(spin)
-    ne = float(num_electrons)
-    pop = np.zeros(n)
-    # the running total, added in the reference's order
-    run = np.cumsum(w)
-    hit = np.nonzero((run > ne) | (np.abs(ne - run) < SMALL_THRESH))[0]
-    if hit.size == 0:
-        raise ValueError("fewer states than electrons")
-    occ = int(hit[0])
-    pop[order[:occ + 1]] = w[:occ + 1]
-    if run[occ] > ne:
-        pop[order[occ]] = w[occ] + ne - run[occ]
-    occ_e = srt[occ]
-    lo = hi = occ
-    degen = pop[order[occ]]
-    possible = w[occ]
-    while hi + 1 < n and abs(occ_e - srt[hi + 1]) <= SMALL_THRESH:
-        hi += 1
-        possible += w[hi]
-    while lo > 0 and abs(occ_e - srt[lo - 1]) <= SMALL_THRESH:
-        lo -= 1
-        possible += w[lo]
-        degen += w[lo]
-    pop[order[lo:hi + 1]] = degen / possible * w[lo:hi + 1]
-    occ = hi
-    occ_e = srt[occ]
-    gap, kind = 0.0, 0
-    if occ < n - 1:
-        gap = srt[occ + 1] - srt[occ]
-        if gap <= METAL_GAP_THRESH:
-            gap = 0.0
-        else:
-            vbm, cbm = order[occ] // (ns * spin), order[occ + 1] // (ns * spin)
-            kind = 1 if vbm == cbm else 2
-    return {"population": pop.reshape(nk, spin, ns), "occupied_energy": float(occ_e),
-            "occupied_index": occ, "band_gap": float(gap), "gap_kind": kind}
-
-
-def step_function(x, step_range):
-    """stepFunction (mathSubs.f90:164-185): 0 above the range, 1 below it,
-    the Fermi function 1 / (1 + e^x) between."""
-    x = np.asarray(x, dtype=np.float64)
-    with np.errstate(over="ignore"):
-        f = 1.0 / (1.0 + np.exp(np.minimum(x, step_range)))
-    return np.where(x > step_range, 0.0, np.where(x < -step_range, 1.0, f))
-
-
-def populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
-                      fermi_search_limit, kpoint_weights=None, standard=None):
-    """populateSmearing (populate.F90:486-620): the Fermi level bisected
-    (at most 500 steps) between the standard population's highest occupied
-    state minus fermi_search_limit and the next state plus it, every state
-    taking weight x stepFunction((E - E_F) / thermal_sigma,
-    max_thermal_range) until the charge is within smallThresh of
-    numElectrons.  Energies in Hartree (the reference divides its eV inputs
-    by hartree, input.f90:369-383).  `standard` is populate_standard's
-    result for the same arguments (computed when absent).  Returns
-    {"population", "fermi_energy", "iterations", "charge"}."""
-    e = np.asarray(eigenvalues, dtype=np.float64)
-    nk, spin, ns = e.shape
-    if standard is None:
-        standard = populate_standard(e, num_electrons, kpoint_weights)
-    kw = (np.full(nk, 2.0 / nk) if kpoint_weights is None
-          else np.asarray(kpoint_weights, dtype=np.float64))
-    flat = e.reshape(-1)
-    order = np.argsort(flat, kind="stable")
-    srt = flat[order]
-    w = kw[order // (ns * spin)] / float(spin)
-    occ = standard["occupied_index"]
-    lo = srt[occ] - fermi_search_limit
-    hi = srt[min(occ + 1, srt.size - 1)] + fermi_search_limit
-    ne = float(num_electrons)
-    pop = np.zeros(srt.size)
-    ef, charge, it = 0.5 * (lo + hi), 0.0, 0
-    for it in range(1, 501):
-        ef = 0.5 * (lo + hi)
-        f = step_function((srt - ef) / thermal_sigma, max_thermal_range)
-        p = w * f
-        # the reference's loop stops at the first state the step function
-        # zeroes; the energies ascend, so every later one is zero too
-        charge = float(np.cumsum(p)[-1])
-        pop = np.zeros(srt.size)
-        pop[order] = p
-        if abs(charge - ne) < SMALL_THRESH:
-            break
-        if charge < ne:
-            lo = ef
-        else:
-            hi = ef
-    return {"population": pop.reshape(nk, spin, ns), "fermi_energy": float(ef),
-            "iterations": it, "charge": charge}
 
 
 def populate_states(eigenvalues, num_electrons, kpoint_weights=None, thermal_sigma=0.0,
                     max_thermal_range=0.0, fermi_search_limit=0.0):
-    """populateStates (populate.F90:150-187): the standard population, then
-    the thermal smearing when thermal_sigma is not zero.  The XANES/ELNES
-    core-hole correction (excitedQN_n) is not part of this step."""
-    std = populate_standard(eigenvalues, num_electrons, kpoint_weights)
+    """populateStates (populate.F90:150-620) through imago_populate_states:
+    populateStandard and, when thermal_sigma is not zero, populateSmearing,
+    for eigenvalues [nk, spin, numStates] (energyEigenValues(state, k, spin)
+    in the reference; Hartree).  Every state takes kPointWeight(k) / spin
+    electrons in ascending energy until numElectrons are placed, the last
+    one the remainder, and the states within smallThresh of that energy
+    share the degenerate charge; with smearing, the Fermi level is bisected
+    and each state takes its weight times the clipped Fermi function.
+    kpoint_weights default to 2 / nk (the mesh weights, kpoints.f90:816);
+    thermal_sigma and fermi_search_limit in Hartree (the reference divides
+    its eV inputs by hartree, input.f90:369-383).  The XANES/ELNES core-hole
+    correction (excitedQN_n) is not part of this step.  Returns
+    {"population": [nk, spin, numStates], "occupied_energy" (the Fermi level
+    when smearing), "occupied_index" (0-based, into the sorted list),
+    "band_gap", "gap_kind" (0 metal, 1 direct, 2 indirect),
+    "smearing_iterations"}."""
+    e = np.ascontiguousarray(eigenvalues, dtype=np.float64)
+    nk, spin, ns = e.shape
+    kw = None if kpoint_weights is None else np.ascontiguousarray(kpoint_weights,
+                                                                  dtype=np.float64)
+    pop = np.zeros_like(e)
+    info = np.zeros(5)
+    L = intg.lib()
+    L.imago_populate_states.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2 + \
+        [ctypes.c_double] * 4 + [ctypes.c_void_p] * 2
+    L.imago_populate_states.restype = ctypes.c_int
+    dp = lambda a: None if a is None else a.ctypes.data
+    rc = L.imago_populate_states(nk, spin, ns, dp(e), dp(kw), float(num_electrons),
+                                 float(thermal_sigma), float(max_thermal_range),
+                                 float(fermi_search_limit), dp(pop), dp(info))
+    if rc == 8:
+        raise ValueError("fewer states than electrons")
+    if rc:
+        raise intg.ImagoError(rc, "imago_populate_states")
+    return {"population": pop, "occupied_energy": float(info[0]),
+            "occupied_index": int(info[3]), "band_gap": float(info[1]),
+            "gap_kind": int(info[2]), "smearing_iterations": int(info[4])}
+
+
+def populate_standard(eigenvalues, num_electrons, kpoint_weights=None):
+    """populateStandard (populate.F90:190-483): populate_states without
+    thermal smearing."""
+    return populate_states(eigenvalues, num_electrons, kpoint_weights)
+
+
+def populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
+                      fermi_search_limit, kpoint_weights=None):
+    """populateSmearing (populate.F90:486-620) after populateStandard:
+    {"population", "fermi_energy", "iterations", "charge"}."""
     if thermal_sigma == 0.0:
-        return std
-    sm = populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_range,
-                           fermi_search_limit, kpoint_weights, standard=std)
-    out = dict(std)
-    out["population"] = sm["population"]
-    out["occupied_energy"] = sm["fermi_energy"]
-    out["smearing_iterations"] = sm["iterations"]
-    return out
+        raise ValueError("thermal_sigma must not be zero")
+    r = populate_states(eigenvalues, num_electrons, kpoint_weights, thermal_sigma,
+                        max_thermal_range, fermi_search_limit)
+    return {"population": r["population"], "fermi_energy": r["occupied_energy"],
+            "iterations": r["smearing_iterations"],
+            "charge": float(r["population"].sum())}
 
 
 _PACK_CACHE = {}

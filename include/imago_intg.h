@@ -205,6 +205,25 @@ IMAGO_API int imago_gauss_overlap_mm(imago_ctx *ctx, double *packed);
 IMAGO_API int imago_gauss_overlap_dm(imago_ctx *ctx, const double center[3],
                                      double *packed);
 
+/* populateStates (populate.F90:150-620) on the host: populateStandard
+ * and, when thermal_sigma is not zero, populateSmearing.  eigenvalues
+ * [nk][spin][numStates] (Hartree), kpoint_weights [nk] or NULL for the mesh
+ * weights 2 / nk (kpoints.f90:816); thermal_sigma, max_thermal_range and
+ * fermi_search_limit as the reference holds them after input.f90:369-383
+ * (sigma and limit in Hartree, the range in units of sigma).  population
+ * [nk][spin][numStates] receives electronPopulation; info[5] the highest
+ * occupied energy (the Fermi level when smearing), the band gap, the gap
+ * kind (0 metal, 1 direct, 2 indirect), the 0-based sorted index of the
+ * highest occupied state and the number of Fermi-level bisections.
+ * IMAGO_ERR_RANGE when the states hold fewer than num_electrons.  No
+ * device work. */
+IMAGO_API int imago_populate_states(int num_kpoints, int spin, int num_states,
+                                    const double *eigenvalues,
+                                    const double *kpoint_weights, double num_electrons,
+                                    double thermal_sigma, double max_thermal_range,
+                                    double fermi_search_limit, double *population,
+                                    double *info);
+
 /* The traces of makeValenceRho (valeCharge.F90:218-291) on the device:
  *   traces[m * nrho + s] = sum over k of matrixElementMult(M_m(k), R_s(k))
  *     = sum_k [ 2 sum_{off-diagonal} (Re M Re R + Im M Im R)

@@ -117,6 +117,9 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_gauss_koverlap(None, None, None, None) == 1
     L.imago_hermitian_eigh.argtypes = [ctypes.c_int, ctypes.c_int] + [vp] * 4
     assert L.imago_hermitian_eigh(0, 1, None, None, None, None) == 1
+    L.imago_populate_states.argtypes = [ctypes.c_int] * 3 + [vp] * 2 + \
+        [ctypes.c_double] * 4 + [vp] * 2
+    assert L.imago_populate_states(0, 1, 1, None, None, 0.0, 0.0, 0.0, 0.0, None, None) == 1
     L.imago_packed_traces.argtypes = [ctypes.c_int] * 3 + [vp, ctypes.c_int] + [vp] * 3
     assert L.imago_packed_traces(0, 1, 1, None, 1, None, None, None) == 1
     L.imago_intg_set_ham_mode.argtypes = [vp, ctypes.c_int]
