@@ -10,6 +10,7 @@
 !    call gaussOverlapDM(...)      -> call b200GaussOverlapDM(...)
 !    call gaussOverlapMM(...)      -> call b200GaussOverlapMM(...)
 !    call gaussKOverlap(...)       -> call b200GaussKOverlap(...)
+!    call populateStates           -> call b200PopulateStates
 !    call gaussOverlapNP(...)      -> call b200GaussOverlapNP(...)
 !    call elecPotGaussOverlap(...) -> call b200ElecPotGaussOverlap(...)
 !
@@ -34,7 +35,7 @@ module O_ImagoB200
    public :: b200Setup, b200GaussOverlapOL, b200GaussOverlapKE, &
          & b200GaussOverlapMV, b200GaussOverlapNP, b200ElecPotGaussOverlap, &
          & b200GaussOverlapHamPSCF, b200GaussOverlapDM, b200GaussOverlapMM, &
-         & b200GaussKOverlap, b200Cleanup
+         & b200GaussKOverlap, b200PopulateStates, b200Cleanup
 
    type, bind(C) :: imago_system
       real(c_double) :: real_vectors(9)
@@ -138,6 +139,15 @@ module O_ImagoB200
          type(c_ptr), value :: ctx
          real(c_double), intent(in) :: dk(9)
          real(c_double), intent(out) :: re(*), im(*)
+         integer(c_int) :: st
+      end function
+      function imago_populate_states(nk, spin, ns, eig, kw, ne, sigma, srange, &
+            & slimit, pop, info) bind(C, name="imago_populate_states") result(st)
+         import :: c_int, c_double
+         integer(c_int), value :: nk, spin, ns
+         real(c_double), intent(in) :: eig(*), kw(*)
+         real(c_double), value :: ne, sigma, srange, slimit
+         real(c_double), intent(out) :: pop(*), info(5)
          integer(c_int) :: st
       end function
       function imago_elec_pot_gauss_overlap(ctx, packed) &
@@ -570,6 +580,45 @@ contains
       enddo
       call markDone(aid)
    end subroutine b200GaussKOverlap
+
+   ! populateStates (populate.F90:150-187) through imago_populate_states:
+   ! the eigenvalues are handed over k-point by k-point, spin by spin,
+   ! state fastest (the order populateStandard lists them in), and
+   ! electronPopulation, occupiedEnergy, occupiedEnergyIndex, bandGap and
+   ! gapKindCode are set as the reference sets them.  The XANES core-hole
+   ! correction (excitedQN_n /= 0) is not handled: call populateStates then.
+   ! sortedEnergyEigenValues and indexEnergyEigenValues are not filled.
+   subroutine b200PopulateStates()
+      use O_KPoints, only: numKPoints, kPointWeight
+      use O_Potential, only: spin
+      use O_Input, only: numStates, numElectrons, thermalSigma, &
+            & maxThermalRange, fermiSearchLimit
+      use O_SecularEquation, only: energyEigenValues
+      use O_Populate, only: electronPopulation, occupiedEnergy, &
+            & occupiedEnergyIndex, bandGap, gapKindCode
+      real(c_double), allocatable :: eig(:,:,:)
+      real(c_double) :: info(5)
+      integer :: i, j
+      integer(c_int) :: st
+      allocate (eig(numStates, spin, numKPoints))
+      do i = 1, numKPoints
+         do j = 1, spin
+            eig(:,j,i) = energyEigenValues(1:numStates,i,j)
+         enddo
+      enddo
+      if (allocated(electronPopulation)) deallocate (electronPopulation)
+      allocate (electronPopulation(numStates*numKPoints*spin))
+      st = imago_populate_states(int(numKPoints, c_int), int(spin, c_int), &
+            & int(numStates, c_int), eig, kPointWeight, &
+            & real(numElectrons, c_double), thermalSigma, maxThermalRange, &
+            & fermiSearchLimit, electronPopulation, info)
+      if (st /= 0) call fail(st, 'populateStates')
+      occupiedEnergy = info(1)
+      bandGap = info(2)
+      gapKindCode = nint(info(3))
+      occupiedEnergyIndex = nint(info(4)) + 1
+      deallocate (eig)
+   end subroutine b200PopulateStates
 
    subroutine b200Cleanup()
       if (c_associated(ctx)) call imago_intg_destroy(ctx)
