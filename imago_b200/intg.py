@@ -280,7 +280,16 @@ class IntegralSetup:
             pass
 
     # -- host-output builds (reference layout, numpy) --
+    def _device_only(self, out, what):
+        """A device-output context's kernels write straight through the
+        output pointers, so host (numpy) memory there, or no output at all,
+        is refused before the library is called."""
+        if self.outputs_on_device and (out is None or isinstance(out, np.ndarray)):
+            raise ValueError(f"{what}: this context writes device memory; pass CUDA "
+                             "tensors or device pointers")
+
     def _packed(self, n=None):
+        self._device_only(None, "a host output")
         shape = (self.nk, self.npacked, 2) if n is None else (n, self.nk, self.npacked, 2)
         return np.zeros(shape)
 
@@ -311,6 +320,7 @@ class IntegralSetup:
         return out
 
     def _ptr(self, out):
+        self._device_only(out, "an output")
         if isinstance(out, int):
             return ctypes.cast(ctypes.c_void_p(out), _D)
         if hasattr(out, "data_ptr"):
@@ -351,8 +361,10 @@ class IntegralSetup:
         q = np.ascontiguousarray(dk, dtype=np.float64).reshape(9)
         shape = (3, self.nk, self.vale_dim, self.vale_dim)
         if re is None:
+            self._device_only(None, "gauss_koverlap re")
             re = np.zeros(shape)
         if im is None:
+            self._device_only(None, "gauss_koverlap im")
             im = np.zeros(shape)
         _check(lib().imago_gauss_koverlap(self._ctx, _p(q), self._ptr(re), self._ptr(im)),
                "gaussKOverlap")
@@ -372,6 +384,7 @@ class IntegralSetup:
         cf = np.ascontiguousarray(c.T)  # potCoeffs(potDim, spin) column-major
         if out is None:
             out = self._packed(spin)
+        self._device_only(out, "ham_pscf")
         ptr = (ctypes.cast(ctypes.c_void_p(out), _D) if isinstance(out, int) else
                ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D) if hasattr(out, "data_ptr")
                else _p(out))
@@ -390,6 +403,7 @@ class IntegralSetup:
         `out` a device pointer/tensor for outputs_on_device contexts."""
         if out is None:
             out = self._packed(count)
+        self._device_only(out, "elec_pot_gauss_overlap_range")
         ptr = (ctypes.cast(ctypes.c_void_p(out), _D) if isinstance(out, int) else
                ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D) if hasattr(out, "data_ptr")
                else _p(out))
@@ -418,6 +432,8 @@ class IntegralSetup:
                 out["ep_packed"] = self._packed(self.pot_dim)
             if which & IMAGO_MV:
                 out["mv_packed"] = self._packed()
+        for k, v in out.items():
+            self._device_only(v, k)
         s = _out_struct(out)
         _check(lib().imago_intg_build(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build")
@@ -428,6 +444,8 @@ class IntegralSetup:
         graph (outputs_on_device contexts; `out` maps names to device
         pointers or CUDA tensors).  The first call for an output set builds
         eagerly and captures, later calls replay."""
+        for k, v in out.items():
+            self._device_only(v, k)
         s = _out_struct(out)
         _check(lib().imago_intg_build_graph(self._ctx, which, ctypes.byref(s)),
                "imago_intg_build_graph")

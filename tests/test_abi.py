@@ -126,3 +126,27 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_intg_set_ham_mode(None, 0) == 1
     L.imago_secular_matrices_rel.argtypes = [ctypes.c_int] * 3 + [vp] * 9
     assert L.imago_secular_matrices_rel(0, 1, 0, *([None] * 9)) == 1
+
+
+def test_device_output_context_refuses_host_outputs():
+    # a context whose kernels write through the output pointers takes no
+    # numpy array (the check runs before the library is called, so an
+    # instance without a context shows it on the CPU)
+    import ctypes
+    import numpy as np
+    from imago_b200 import intg
+    g = object.__new__(intg.IntegralSetup)
+    g._ctx = ctypes.c_void_p()
+    g.outputs_on_device = True
+    g.nk, g.npacked, g.vale_dim, g.core_dim, g.pot_dim = 2, 3, 2, 0, 1
+    calls = [lambda: g.gauss_overlap_ke(), lambda: g.gauss_overlap_mm(),
+             lambda: g.gauss_overlap_dm([0.0, 0.0, 0.0]),
+             lambda: g.gauss_overlap_mm(out=np.zeros((3, 2, 3, 2))),
+             lambda: g.gauss_koverlap(np.zeros((3, 3))),
+             lambda: g.ham_pscf(np.zeros(1)),
+             lambda: g.elec_pot_gauss_overlap_range(0, 1, np.zeros((1, 2, 3, 2))),
+             lambda: g.build(intg.IMAGO_KE, {"ke_packed": np.zeros((2, 3, 2))}),
+             lambda: g.build(intg.IMAGO_KE)]
+    for call in calls:
+        with pytest.raises(ValueError):
+            call()
