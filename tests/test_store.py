@@ -173,3 +173,22 @@ def test_plane_wave_groups(tmp_path):
     assert st.build_checkpointed(f2, _store(tmp_path, f2), momentum=True,
                                  plane_wave=True) == []
     assert f2.calls == []
+
+
+def test_wave_vectors_follow_the_reference_reciprocal_lattice():
+    # recipVectors(:, i) = 2 pi (a_{i+1} x a_{i+2}) / (a_i . a_{i+1} x a_{i+2})
+    # with cyclic indices (lattice.f90:200-214), on a skewed cell, divided
+    # by numAxialKPoints(i)
+    from imago_b200 import configs, intg
+    s = configs.silicon_cubic8(kmesh=(2, 3, 4))
+    a = np.array([[10.2, 0.3, -0.4], [1.1, 9.7, 0.2], [-0.6, 0.8, 11.3]])
+    s.real_vectors = a
+    ref = np.zeros((3, 3))
+    for i in range(3):
+        b = np.cross(a[(i + 1) % 3], a[(i + 2) % 3])
+        ref[i] = 2.0 * np.pi * b / np.dot(a[i], b) / (2, 3, 4)[i]
+    got = intg.koverlap_wave_vectors(s)
+    assert np.allclose(got, ref, rtol=1e-14, atol=0)
+    # the reciprocal vectors themselves with one point per axis
+    assert np.allclose(intg.koverlap_wave_vectors(s, num_axial=(1, 1, 1)),
+                       ref * [[2], [3], [4]], rtol=1e-14, atol=0)
