@@ -21,8 +21,9 @@
 ! the reference does, writes the packed valence-valence datasets per
 ! k-point (and coreValeOL for the overlap) and sets the attribute.
 !
-! No Fortran compiler exists where this library is built, so this file is
-! not compiled there; INTEGRATION.md gives the build line.
+! Build line: compile this file with the reference's own sources (it uses
+! their modules) and link libimago_b200.so, e.g.
+!    h5fc -c imago_b200_bind.F90 && h5fc ... imago_b200_bind.o -limago_b200
 
 module O_ImagoB200
 
@@ -141,13 +142,15 @@ module O_ImagoB200
          real(c_double), intent(out) :: re(*), im(*)
          integer(c_int) :: st
       end function
-      function imago_populate_states(nk, spin, ns, eig, kw, ne, sigma, srange, &
-            & slimit, pop, info) bind(C, name="imago_populate_states") result(st)
+      function imago_populate_states_sorted(nk, spin, ns, eig, kw, ne, sigma, &
+            & srange, slimit, pop, info, sorted, idx) &
+            & bind(C, name="imago_populate_states_sorted") result(st)
          import :: c_int, c_double
          integer(c_int), value :: nk, spin, ns
          real(c_double), intent(in) :: eig(*), kw(*)
          real(c_double), value :: ne, sigma, srange, slimit
-         real(c_double), intent(out) :: pop(*), info(5)
+         real(c_double), intent(out) :: pop(*), info(5), sorted(*)
+         integer(c_int), intent(out) :: idx(*)
          integer(c_int) :: st
       end function
       function imago_elec_pot_gauss_overlap(ctx, packed) &
@@ -581,13 +584,16 @@ contains
       call markDone(aid)
    end subroutine b200GaussKOverlap
 
-   ! populateStates (populate.F90:150-187) through imago_populate_states:
-   ! the eigenvalues are handed over k-point by k-point, spin by spin,
-   ! state fastest (the order populateStandard lists them in), and
-   ! electronPopulation, occupiedEnergy, occupiedEnergyIndex, bandGap and
-   ! gapKindCode are set as the reference sets them.  The XANES core-hole
-   ! correction (excitedQN_n /= 0) is not handled: call populateStates then.
-   ! sortedEnergyEigenValues and indexEnergyEigenValues are not filled.
+   ! populateStates (populate.F90:150-187) through
+   ! imago_populate_states_sorted: the eigenvalues are handed over k-point by
+   ! k-point, spin by spin, state fastest (the order populateStandard lists
+   ! them in), and electronPopulation, occupiedEnergy, occupiedEnergyIndex,
+   ! bandGap and gapKindCode are set as the reference sets them.  The module
+   ! arrays sortedEnergyEigenValues and indexEnergyEigenValues (1-based
+   ! indices) are allocated and filled too, because cleanUpPopulation
+   ! (populate.F90:1230-1231), which makeValenceRho calls every iteration,
+   ! deallocates them unconditionally.  The XANES core-hole correction
+   ! (excitedQN_n /= 0) is not handled: call populateStates then.
    subroutine b200PopulateStates()
       use O_KPoints, only: numKPoints, kPointWeight
       use O_Potential, only: spin
@@ -595,11 +601,14 @@ contains
             & maxThermalRange, fermiSearchLimit
       use O_SecularEquation, only: energyEigenValues
       use O_Populate, only: electronPopulation, occupiedEnergy, &
-            & occupiedEnergyIndex, bandGap, gapKindCode
+            & occupiedEnergyIndex, bandGap, gapKindCode, &
+            & sortedEnergyEigenValues, indexEnergyEigenValues
       real(c_double), allocatable :: eig(:,:,:)
+      integer(c_int), allocatable :: idx(:)
       real(c_double) :: info(5)
-      integer :: i, j
+      integer :: i, j, n
       integer(c_int) :: st
+      n = numStates*numKPoints*spin
       allocate (eig(numStates, spin, numKPoints))
       do i = 1, numKPoints
          do j = 1, spin
@@ -607,17 +616,26 @@ contains
          enddo
       enddo
       if (allocated(electronPopulation)) deallocate (electronPopulation)
-      allocate (electronPopulation(numStates*numKPoints*spin))
-      st = imago_populate_states(int(numKPoints, c_int), int(spin, c_int), &
-            & int(numStates, c_int), eig, kPointWeight, &
+      if (allocated(sortedEnergyEigenValues)) &
+            & deallocate (sortedEnergyEigenValues)
+      if (allocated(indexEnergyEigenValues)) deallocate (indexEnergyEigenValues)
+      allocate (electronPopulation(n))
+      allocate (sortedEnergyEigenValues(n))
+      allocate (indexEnergyEigenValues(n))
+      allocate (idx(n))
+      st = imago_populate_states_sorted(int(numKPoints, c_int), &
+            & int(spin, c_int), int(numStates, c_int), eig, kPointWeight, &
             & real(numElectrons, c_double), thermalSigma, maxThermalRange, &
-            & fermiSearchLimit, electronPopulation, info)
+            & fermiSearchLimit, electronPopulation, info, &
+            & sortedEnergyEigenValues, idx)
       if (st /= 0) call fail(st, 'populateStates')
+      indexEnergyEigenValues(:) = idx(:) + 1
       occupiedEnergy = info(1)
       bandGap = info(2)
       gapKindCode = nint(info(3))
       occupiedEnergyIndex = nint(info(4)) + 1
       deallocate (eig)
+      deallocate (idx)
    end subroutine b200PopulateStates
 
    subroutine b200Cleanup()

@@ -1993,7 +1993,8 @@ int imago_prim_eval(int kind, int n, const double *params, const int *cls,
   if (!rc && kind != 4 &&
       cudaMemcpy(dc, cls, sizeof(int) * 2 * n, cudaMemcpyHostToDevice) != cudaSuccess)
     rc = IMAGO_ERR_CUDA;
-  if (!rc && kind == 4) cudaMemset(dc, 0, sizeof(int) * 2 * n);
+  if (!rc && kind == 4 && cudaMemset(dc, 0, sizeof(int) * 2 * n) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
   if (!rc) rc = launch_prim_eval(kind, n, dp, dc, ds, 0);
   if (!rc && cudaMemcpy(sh, ds, sizeof(double) * 256 * n,
                         cudaMemcpyDeviceToHost) != cudaSuccess)

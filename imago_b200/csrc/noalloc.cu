@@ -11,14 +11,13 @@
 //
 // The array is a module-scope __device__ variable: every GPU that loads
 // this library holds it (IMAGO_PRIM_STATIC_BYTES) until the process exits.
-// Its name is not a device address in host code, so the address is taken
-// with cudaGetSymbolAddress once per device, the first time the entry point
-// runs on that device (with that device current).  All calls share the
+// Its name is not a device address in host code, so every call takes the
+// address with cudaGetSymbolAddress on the current device (cheap next to
+// the copies; an address kept from an earlier call would go stale after a
+// cudaDeviceReset reloads the module elsewhere).  All calls share the
 // array and it keeps the last call's contents; calls that overlap on the
 // GPU (from several host threads, or on several streams) would overwrite
 // each other's records and must not be issued.
-#include <mutex>
-
 #include "intg.cuh"
 
 namespace {
@@ -36,30 +35,16 @@ static_assert(kBytes == IMAGO_PRIM_STATIC_BYTES,
 // Records in, class pairs in, 16x16 blocks out.
 static __device__ __align__(256) unsigned char g_prim_scratch[kBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-unsigned char *g_addr[kMaxDevices] = {};
-
-// Device address of g_prim_scratch on the current device, looked up on the
-// first call on that device.
+// Device address of g_prim_scratch on the current device, looked up on
+// every call.
 int scratch_address(unsigned char **out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_prim_scratch);
+  if (e != cudaSuccess || !p) {
     cudaGetLastError();
-    return IMAGO_ERR_NO_DEVICE;
+    return IMAGO_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) return IMAGO_ERR_RANGE;
-  std::lock_guard<std::mutex> guard(g_lock);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_prim_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return IMAGO_ERR_CUDA;
-    }
-    g_addr[dev] = static_cast<unsigned char *>(p);
-  }
-  *out = g_addr[dev];
+  *out = static_cast<unsigned char *>(p);
   return IMAGO_OK;
 }
 

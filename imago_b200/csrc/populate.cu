@@ -21,6 +21,7 @@
 // Host work over a few hundred thousand values at most: done where the
 // eigenvalues are read, with the reference's summation order.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <numeric>
 #include <vector>
@@ -41,16 +42,16 @@ double step_function(double x, double range) {
 
 }  // namespace
 
-extern "C" int imago_populate_states(int num_kpoints, int spin, int num_states,
-                                     const double *eigenvalues,
-                                     const double *kpoint_weights, double num_electrons,
-                                     double thermal_sigma, double max_thermal_range,
-                                     double fermi_search_limit, double *population,
-                                     double *info) {
+extern "C" int imago_populate_states_sorted(
+    int num_kpoints, int spin, int num_states, const double *eigenvalues,
+    const double *kpoint_weights, double num_electrons, double thermal_sigma,
+    double max_thermal_range, double fermi_search_limit, double *population, double *info,
+    double *sorted_energies, int *sort_index) {
   if (num_kpoints <= 0 || spin < 1 || spin > 2 || num_states <= 0 || !eigenvalues ||
       !population || !info || !(num_electrons >= 0.0) || !(thermal_sigma >= 0.0))
     return IMAGO_ERR_INVALID;
   const long long n = (long long)num_kpoints * spin * num_states;
+  if (sort_index && n > (long long)INT_MAX) return IMAGO_ERR_RANGE;
   const long long per_k = (long long)spin * num_states;
   std::vector<double> kw(num_kpoints);
   for (int k = 0; k < num_kpoints; ++k)
@@ -65,6 +66,11 @@ extern "C" int imago_populate_states(int num_kpoints, int spin, int num_states,
     srt[i] = eigenvalues[order[i]];
     w[i] = kw[order[i] / per_k] / (double)spin;
   }
+  // sortedEnergyEigenValues / indexEnergyEigenValues (populate.F90:250-287),
+  // the index 0-based here
+  if (sorted_energies) std::copy(srt.begin(), srt.end(), sorted_energies);
+  if (sort_index)
+    for (long long i = 0; i < n; ++i) sort_index[i] = (int)order[i];
   const double ne = num_electrons;
   std::fill(population, population + n, 0.0);
   double populated = 0.0;
@@ -135,4 +141,16 @@ extern "C" int imago_populate_states(int num_kpoints, int spin, int num_states,
   info[3] = (double)occ;
   info[4] = steps;
   return IMAGO_OK;
+}
+
+extern "C" int imago_populate_states(int num_kpoints, int spin, int num_states,
+                                     const double *eigenvalues,
+                                     const double *kpoint_weights, double num_electrons,
+                                     double thermal_sigma, double max_thermal_range,
+                                     double fermi_search_limit, double *population,
+                                     double *info) {
+  return imago_populate_states_sorted(num_kpoints, spin, num_states, eigenvalues,
+                                      kpoint_weights, num_electrons, thermal_sigma,
+                                      max_thermal_range, fermi_search_limit, population,
+                                      info, nullptr, nullptr);
 }

@@ -224,6 +224,23 @@ IMAGO_API int imago_populate_states(int num_kpoints, int spin, int num_states,
                                     double fermi_search_limit, double *population,
                                     double *info);
 
+/* populateStates as above, also returning the sorted list the reference
+ * keeps in module O_Populate (populate.F90:250-287) and frees in
+ * cleanUpPopulation (populate.F90:1230-1231): sorted_energies
+ * [nk * spin * numStates] receives sortedEnergyEigenValues (ascending,
+ * stable) and sort_index the 0-based position of each sorted value in
+ * `eigenvalues` (indexEnergyEigenValues minus 1).  Either may be NULL.
+ * IMAGO_ERR_RANGE when sort_index is given and nk * spin * numStates
+ * exceeds INT_MAX. */
+IMAGO_API int imago_populate_states_sorted(int num_kpoints, int spin, int num_states,
+                                           const double *eigenvalues,
+                                           const double *kpoint_weights,
+                                           double num_electrons, double thermal_sigma,
+                                           double max_thermal_range,
+                                           double fermi_search_limit, double *population,
+                                           double *info, double *sorted_energies,
+                                           int *sort_index);
+
 /* The traces of makeValenceRho (valeCharge.F90:218-291) on the device:
  *   traces[m * nrho + s] = sum over k of matrixElementMult(M_m(k), R_s(k))
  *     = sum_k [ 2 sum_{off-diagonal} (Re M Re R + Im M Im R)
@@ -434,10 +451,12 @@ IMAGO_API int imago_prim_eval(int kind, int n, const double *params, const int *
  * synchronisation of cudaMalloc/cudaFree.  Same arguments, layout and
  * results as imago_prim_eval; the records are staged in one fixed
  * module-scope device array instead of per-call buffers.  n above
- * IMAGO_PRIM_STATIC_MAX_RECORDS returns IMAGO_ERR_RANGE.  The first call on
- * a device looks up the array's device address (with that device current)
- * and should precede any stream capture on that device.  Calls share the
- * array: calls that overlap on the GPU race and must not be issued.
+ * IMAGO_PRIM_STATIC_MAX_RECORDS returns IMAGO_ERR_RANGE.  Every call looks
+ * up the array's device address on the current device
+ * (cudaGetSymbolAddress, whose first use on a device loads the module and
+ * should precede any stream capture there), so the address stays right
+ * after a cudaDeviceReset.  Calls share the array: calls that overlap on
+ * the GPU race and must not be issued.
  */
 IMAGO_API int imago_prim_eval_static(int kind, int n, const double *params,
                                      const int *cls, double *sh);

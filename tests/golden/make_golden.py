@@ -21,7 +21,7 @@ are kept:
 Run in a container that has the reference mounted (it is read here and
 nowhere else):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <root of the reference checkout>
 
 It writes `tests/golden/primitives.json`, which the tests read.  The
 fixture is committed; nothing at test time touches the reference.
@@ -395,7 +395,9 @@ def run_3c(ns, kern, la, lb, a1, a2, a3, A, B, C):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <root of the reference checkout>")
+    ref_root = sys.argv[1]
     ns = load_kernels(ref_root)
     rng = np.random.default_rng(20261203)
     records = []

@@ -57,3 +57,14 @@ def test_static_rejects_more_records_than_its_array_holds(imago_lib):
         0, n, params.ctypes.data_as(D),
         cls.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), out.ctypes.data_as(D))
     assert st == 8  # IMAGO_ERR_RANGE
+
+
+def test_static_at_its_record_limit(imago_lib, golden):
+    # exactly PRIM_STATIC_MAX_RECORDS records: the only size whose output
+    # blocks fill the array to its end
+    p, c = _records(golden, "kinetic")
+    n = intg.PRIM_STATIC_MAX_RECORDS
+    reps = -(-n // len(p))
+    p, c = np.tile(p, (reps, 1))[:n], np.tile(c, (reps, 1))[:n]
+    for _ in range(2):
+        _close(intg.prim_eval_static("kinetic", p, c), intg.prim_eval("kinetic", p, c))
