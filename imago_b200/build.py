@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "imago_b200")
 LIB = os.path.join(HERE, "libimago_b200.so")
 SOURCES = ["api.cu", "k_dense.cu", "k_prim.cu", "k_eval.cu", "noalloc.cu",
-           "k_secular.cu", "populate.cu"]
+           "k_secular.cu", "populate.cu", "scf.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
@@ -33,7 +33,7 @@ def nvcc():
 
 def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
-    hs.append(os.path.join(ROOT, "include", "imago_intg.h"))
+    hs += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     return hs
 
 

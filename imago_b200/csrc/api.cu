@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "intg.cuh"
+#include "lattice.cuh"
 
 using namespace imago;
 
@@ -373,20 +374,6 @@ double smallest_singular(const double *rv) {
   return std::sqrt(std::max(lmin, 0.0));
 }
 
-bool border_within(const double *rv, const double *t, double lim) {
-  double sh[3] = {0, 0, 0}, cur[3] = {t[0], t[1], t[2]};
-  for (int i = 0; i < 3; ++i)
-    for (int x = 0; x < 3; ++x) sh[x] += rv[3 * i + x];
-  // The seven other corners, walked as cellBorderCheck walks them.
-  const int ax[7] = {0, 1, 0, 2, 0, 1, 0};
-  const int sg[7] = {1, 1, -1, 1, 1, -1, -1};
-  for (int s = 0; s < 7; ++s) {
-    cur[ax[s]] += sg[s] * sh[ax[s]];
-    if (cur[0] * cur[0] + cur[1] * cur[1] + cur[2] * cur[2] < lim) return true;
-  }
-  return false;
-}
-
 int make_cells(imago_ctx *c, double min_atom_alpha, double min_pot_alpha) {
   double lim = c->T * std::max(2.0 / min_atom_alpha,
                                1.0 / min_pot_alpha + 0.5 / min_atom_alpha);
@@ -398,35 +385,8 @@ int make_cells(imago_ctx *c, double min_atom_alpha, double min_pot_alpha) {
   }
   lim = lim + 0.75 * maxsq + std::sqrt(3.0 * maxsq * lim);
   lim = std::max(lim, 2.0 * c->T / min_atom_alpha);
-  int reps[3];
-  for (int i = 0; i < 3; ++i)
-    reps[i] = 2 * (int)std::ceil(std::sqrt(lim) / std::sqrt(len2[i])) + 1;
-  struct Cell {
-    double size, d[3];
-    int idx;
-  };
-  std::vector<Cell> list;
-  for (int i = 1; i <= reps[0]; ++i)
-    for (int j = 1; j <= reps[1]; ++j)
-      for (int k = 1; k <= reps[2]; ++k) {
-        const int rep[3] = {i - (1 + reps[0]) / 2, j - (1 + reps[1]) / 2,
-                            k - (1 + reps[2]) / 2};
-        double t[3] = {0, 0, 0};
-        for (int l = 0; l < 3; ++l)
-          for (int m = 0; m < 3; ++m) t[m] = t[m] + c->rv[3 * l + m] * rep[l];
-        const double s = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
-        if (s > lim && !border_within(c->rv, t, lim)) continue;
-        list.push_back({s, {t[0], t[1], t[2]}, (int)list.size()});
-      }
-  std::stable_sort(list.begin(), list.end(),
-                   [](const Cell &a, const Cell &b) { return a.size < b.size; });
-  c->ncell = (int)list.size();
-  c->cells.resize(3 * list.size());
-  c->csize.resize(list.size());
-  for (size_t i = 0; i < list.size(); ++i) {
-    std::memcpy(&c->cells[3 * i], list[i].d, sizeof(double) * 3);
-    c->csize[i] = list[i].size;
-  }
+  lattice_points(c->rv, lim, c->cells, c->csize);
+  c->ncell = (int)c->csize.size();
   return IMAGO_OK;
 }
 
@@ -1946,6 +1906,8 @@ const char *imago_strerror(int status) {
     case IMAGO_ERR_TIMEOUT: return "a bounded device wait gave up";
     case IMAGO_ERR_NO_DEVICE: return "no CUDA device of compute capability 10.x";
     case IMAGO_ERR_RANGE: return "argument out of range";
+    case IMAGO_ERR_SCF:
+      return "Total energy is positive! Your structure might have a serious problem.";
     default: return "unknown status";
   }
 }

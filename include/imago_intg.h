@@ -63,7 +63,8 @@ enum imago_status {
   IMAGO_ERR_CUDA = 5,         /* a CUDA call failed */
   IMAGO_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
   IMAGO_ERR_NO_DEVICE = 7,    /* no CUDA device of compute capability 10.0 */
-  IMAGO_ERR_RANGE = 8         /* argument outside the supported range */
+  IMAGO_ERR_RANGE = 8,        /* argument outside the supported range */
+  IMAGO_ERR_SCF = 9           /* "Total energy is positive!", potentialUpdate.F90:1261-1272 */
 };
 
 /* Matrix selection bits for imago_intg_build. */

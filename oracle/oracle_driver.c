@@ -152,11 +152,38 @@ typedef struct {
   int idx;
 } cellkey;
 
-static int cellkey_cmp(const void *a, const void *b) {
-  const cellkey *x = a, *y = b;
-  if (x->size < y->size) return -1;
-  if (x->size > y->size) return 1;
-  return x->idx - y->idx; /* stable, as the reference's merge sort */
+/* mergeSort / mergeLists (sortSubs.f90:18-200): bottom-up merges of
+ * neighbouring runs, starting from runs of one; when the two heads are
+ * equal the head of the second run goes first (the comparison is a strict
+ * "<" on the first run), so equal sizes are not kept in input order. */
+static void reference_merge_sort(cellkey *k, int n) {
+  if (n < 2) return;
+  cellkey *tmp = malloc(sizeof(cellkey) * n);
+  int *bord = malloc(sizeof(int) * (n + 1));
+  for (int i = 0; i <= n; ++i) bord[i] = i;
+  cellkey *from = k, *to = tmp;
+  int nseg = n;
+  while (nseg > 1) {
+    int t = 0;
+    for (int s = 0; s < nseg / 2; ++s) {
+      int p1 = bord[2 * s], e1 = bord[2 * s + 1], p2 = e1, e2 = bord[2 * s + 2];
+      while (p1 < e1 && p2 < e2) to[t++] = (from[p1].size < from[p2].size) ? from[p1++] : from[p2++];
+      while (p1 < e1) to[t++] = from[p1++];
+      while (p2 < e2) to[t++] = from[p2++];
+      bord[s + 1] = e2;
+    }
+    if (nseg % 2) {
+      for (int i = t; i < bord[nseg]; ++i) to[i] = from[i];
+      bord[nseg / 2 + 1] = bord[nseg];
+    }
+    nseg = nseg / 2 + nseg % 2;
+    cellkey *sw = from;
+    from = to;
+    to = sw;
+  }
+  if (from != k) memcpy(k, from, sizeof(cellkey) * n);
+  free(tmp);
+  free(bord);
 }
 
 /* initializeLattice + makeLattice, lattice.f90:310-444, 571-690. */
@@ -198,7 +225,7 @@ static int make_lattice(orc_ctx *c, double min_atom_alpha,
         keys[n].idx = n;
         ++n;
       }
-  qsort(keys, n, sizeof(cellkey), cellkey_cmp);
+  reference_merge_sort(keys, n);
   c->ncell = n;
   c->cell = malloc(sizeof(double) * 3 * n);
   c->csize = malloc(sizeof(double) * n);
