@@ -1,0 +1,345 @@
+"""The learned SCF start: a per-atom perceptron that corrects the plain
+atomic-superposition start of Imago's SCF (initPotCoeffs,
+src/imago/potential.f90:433-563) from each atom's radial environment.
+
+Everything the network computes runs in the library's own CUDA kernels
+(include/imago_learned.h): the descriptors, the forward pass, the backward
+pass and Adam.  This module holds the host side:
+
+  descriptors(system)   32 radial Gaussians within 6 A of each atom and the
+                        one-hot of its species (C, Si, O)
+  PotBasis              per element, the L2-orthonormal coordinates of a
+                        potential correction: dc = U diag(lambda)^-1/2 z,
+                        U, lambda the eigenpairs of the potential Gaussians'
+                        self overlap (pi / (a_i + a_j))^3/2 above 1e-10 of
+                        the largest, so that |z| is the L2 norm of the
+                        potential change and the ill-conditioned directions
+                        of the even-tempered basis are left out
+  training_cells(...)   seeded strained and perturbed Si8 and diamond C16
+                        cells
+  make_dataset(...)     the plain SCF of each training cell on the GPU
+                        (imago_b200.scf.run_scf) and its converged potential
+                        as the target z of each of its atoms
+  train(...)            full-batch Adam on the masked mean squared error of
+                        the normalised z
+  LearnedStart          the trained network: start(system) gives the
+                        corrected coefficients, the per-atom predictions
+                        averaged over the atoms of each potential type (all
+                        sites of a type share its coefficients)
+  compare(...)          plain start against learned start on one system,
+                        the plain start being the judge: the learned start
+                        is discarded when its converged energy is more than
+                        1e-6 Ha from the plain start's or it needs more
+                        iterations
+"""
+
+import ctypes
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import configs, intg, scf
+
+ANGSTROM = configs.ANGSTROM
+SPECIES = (6, 14, 8)            # nuclear charges of the one-hot positions
+NRAD = 32
+CUTOFF = 6.0 * ANGSTROM         # 6 A in bohr
+WIDTH = 0.5 * ANGSTROM
+NHIDDEN = 128
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def _lib():
+    L = intg.lib()
+    if not hasattr(L, "_learned_ready"):
+        vp = ctypes.c_void_p
+        L.imago_mlp_create.argtypes = [ctypes.c_int] * 3 + [ctypes.c_ulonglong, ctypes.c_int,
+                                                            vp, ctypes.POINTER(vp)]
+        L.imago_mlp_destroy.argtypes = [vp]
+        L.imago_mlp_destroy.restype = None
+        L.imago_mlp_num_params.argtypes = [vp]
+        L.imago_mlp_num_params.restype = ctypes.c_longlong
+        L.imago_mlp_get_params.argtypes = [vp, vp]
+        L.imago_mlp_set_params.argtypes = [vp, vp]
+        L.imago_mlp_forward.argtypes = [vp, ctypes.c_int, vp, vp]
+        L.imago_mlp_loss_grad.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp]
+        L.imago_mlp_adam_step.argtypes = [vp] + [ctypes.c_float] * 4
+        L.imago_descriptors.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_double, ctypes.c_int, vp]
+        L._learned_ready = True
+    return L
+
+
+def _check(st, what):
+    if st:
+        raise intg.ImagoError(st, what)
+
+
+def descriptors(system, device=0):
+    """[natoms][NRAD + len(SPECIES)] float32 (imago_descriptors)."""
+    rv = np.ascontiguousarray(system.real_vectors, dtype=np.float64)
+    pos = np.ascontiguousarray(system.pot_site_pos, dtype=np.float64)
+    z = [int(round(system.pot_types[t - 1].nuc_charge)) for t in system.pot_site_type]
+    sp = np.array([SPECIES.index(x) for x in z], np.int32)
+    x = np.zeros((len(pos), NRAD + len(SPECIES)), np.float32)
+    _check(_lib().imago_descriptors(rv.ctypes.data, len(pos), pos.ctypes.data, sp.ctypes.data,
+                                    len(SPECIES), CUTOFF, NRAD, WIDTH, device, x.ctypes.data),
+           "imago_descriptors")
+    return x
+
+
+class PotBasis:
+    """L2-orthonormal coordinates of a potential correction, per element."""
+
+    def __init__(self, alphas):
+        a = np.asarray(alphas, float)
+        S = (np.pi / (a[:, None] + a[None, :])) ** 1.5
+        lam, U = np.linalg.eigh(S)
+        keep = lam > 1e-10 * lam.max()
+        self.lam, self.U = lam[keep], U[:, keep]
+        self.n = int(keep.sum())
+
+    def to_z(self, dc):
+        return np.sqrt(self.lam) * (self.U.T @ dc)
+
+    def to_dc(self, z):
+        return self.U @ (z[:self.n] / np.sqrt(self.lam))
+
+
+class Mlp:
+    """A network of the library (imago_mlp_*)."""
+
+    def __init__(self, n_in, n_out, n_hidden=NHIDDEN, seed=0, device=0):
+        self._ctx = ctypes.c_void_p()
+        _check(_lib().imago_mlp_create(n_in, n_hidden, n_out, seed, device, None,
+                                       ctypes.byref(self._ctx)), "imago_mlp_create")
+        self.n_in, self.n_out, self.n_hidden, self.device = n_in, n_out, n_hidden, device
+
+    def close(self):
+        if self._ctx:
+            _lib().imago_mlp_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self):
+        return int(_lib().imago_mlp_num_params(self._ctx))
+
+    def params(self):
+        p = np.zeros(self.num_params, np.float32)
+        _check(_lib().imago_mlp_get_params(self._ctx, p.ctypes.data), "imago_mlp_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params
+        _check(_lib().imago_mlp_set_params(self._ctx, p.ctypes.data), "imago_mlp_set_params")
+
+    def forward(self, x):
+        """x: torch float32 CUDA [n, n_in] -> [n, n_out]."""
+        import torch
+        y = torch.empty((x.shape[0], self.n_out), dtype=torch.float32, device=x.device)
+        torch.cuda.synchronize(x.device)
+        _check(_lib().imago_mlp_forward(self._ctx, x.shape[0], x.data_ptr(), y.data_ptr()),
+               "imago_mlp_forward")
+        torch.cuda.synchronize(x.device)
+        return y
+
+    def loss_grad(self, x, t, m, want_grad=False):
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.num_params, np.float32) if want_grad else None
+        _check(_lib().imago_mlp_loss_grad(self._ctx, x.shape[0], x.data_ptr(), t.data_ptr(),
+                                          m.data_ptr(), loss.ctypes.data,
+                                          g.ctypes.data if want_grad else None),
+               "imago_mlp_loss_grad")
+        return (float(loss[0]), g) if want_grad else float(loss[0])
+
+    def adam_step(self, lr, b1=0.9, b2=0.999, eps=1e-8):
+        _check(_lib().imago_mlp_adam_step(self._ctx, lr, b1, b2, eps), "imago_mlp_adam_step")
+
+
+# ------------------------------------------------------------ training set
+
+def training_cells(n=512, seed=11, strain=0.03, jitter=0.02):
+    """Half jittered, strained Si8 conventional cells, half diamond C16
+    (the conventional cell doubled along a), each with its own symmetric
+    strain (components within +-strain) and N(0, jitter A) displacements,
+    k-mesh 2x2x2 (the plain SCF that labels them is converged on it)."""
+    rng = np.random.default_rng(seed)
+    cells = []
+    for i in range(n):
+        e = rng.uniform(-strain, strain, size=(3, 3))
+        e = 0.5 * (e + e.T)
+        if i % 2 == 0:
+            s = configs.cubic_supercell("si", reps=(1, 1, 1), kmesh=(2, 2, 2),
+                                        seed=int(rng.integers(1 << 30)), strain=e,
+                                        jitter=jitter)
+        else:
+            s = configs.cubic_supercell("c", reps=(2, 1, 1), kmesh=(2, 2, 2),
+                                        seed=int(rng.integers(1 << 30)), strain=e,
+                                        jitter=jitter)
+        cells.append(s)
+    return cells
+
+
+def bases_for(systems):
+    """PotBasis per nuclear charge, from the potential types of the systems."""
+    out = {}
+    for s in systems:
+        for p in s.pot_types:
+            z = int(round(p.nuc_charge))
+            if z not in out:
+                out[z] = PotBasis(p.alphas)
+    return out
+
+
+def make_dataset(cells, params=None, device=0, log=None):
+    """Plain SCF of every cell on the GPU; returns descriptors x [atoms, n_in],
+    raw targets z [atoms, n_out] (the converged potential's correction to
+    the plain start of the atom's type), masks, and per-cell SCF records."""
+    p = params or scf.ScfParams()
+    bases = bases_for(cells)
+    nout = max(b.n for b in bases.values())
+    xs, ts, ms, recs = [], [], [], []
+    for i, s in enumerate(cells):
+        t0 = time.perf_counter()
+        start = scf.atomic_start(s)
+        r = scf.run_scf(s, start, p, device=device)
+        if r["positive_energy"] or not (r["converged"] or r["energy_converged"]):
+            continue
+        conv = r["pot_coeffs"]
+        x = descriptors(s, device)
+        off = 0
+        tz = {}
+        for ti, pt in enumerate(s.pot_types):
+            n = len(pt.alphas)
+            z = int(round(pt.nuc_charge))
+            tz[ti + 1] = bases[z].to_z(conv[off:off + n] - start[off:off + n])
+            off += n
+        t = np.zeros((len(x), nout), np.float32)
+        m = np.zeros((len(x), nout), np.float32)
+        for a, ti in enumerate(s.pot_site_type):
+            zz = tz[int(ti)]
+            t[a, :len(zz)] = zz
+            m[a, :len(zz)] = 1.0
+        xs.append(x)
+        ts.append(t)
+        ms.append(m)
+        recs.append({"iterations": r["iterations"], "energy": r["energies"][-1],
+                     "seconds": time.perf_counter() - t0})
+        if log and (i % 32 == 0):
+            log(f"cell {i}: {r['iterations']} iterations, E = {r['energies'][-1]:.8f}")
+    return np.concatenate(xs), np.concatenate(ts), np.concatenate(ms), recs
+
+
+def train(x, t, m, steps=3000, lr=1e-3, seed=0, device=0, log=None):
+    """Full-batch Adam on the normalised targets; returns (params, norm,
+    loss history)."""
+    import torch
+    dev = torch.device("cuda", device)
+    xm, xs = x.mean(axis=0), x.std(axis=0) + 1e-6
+    cnt = np.maximum(m.sum(axis=0), 1.0)
+    tm = (t * m).sum(axis=0) / cnt
+    ts = np.sqrt((((t - tm) * m) ** 2).sum(axis=0) / cnt) + 1e-8
+    xn = torch.as_tensor((x - xm) / xs, dtype=torch.float32, device=dev).contiguous()
+    tn = torch.as_tensor(((t - tm) / ts) * m, dtype=torch.float32, device=dev).contiguous()
+    mm = torch.as_tensor(m, dtype=torch.float32, device=dev).contiguous()
+    net = Mlp(x.shape[1], t.shape[1], seed=seed, device=device)
+    hist = []
+    torch.cuda.synchronize(dev)
+    for k in range(steps):
+        loss = net.loss_grad(xn, tn, mm)
+        net.adam_step(lr * 0.5 * (1.0 + math.cos(math.pi * k / steps)))
+        if k % 100 == 0 or k == steps - 1:
+            hist.append((k, loss))
+            if log:
+                log(f"step {k}: loss {loss:.6f}")
+    params = net.params()
+    net.close()
+    norm = {"x_mean": xm, "x_std": xs, "t_mean": tm, "t_std": ts}
+    return params, norm, hist
+
+
+class LearnedStart:
+    """A trained network and its normalisation."""
+
+    def __init__(self, params, norm, n_in, n_out, alphas, device=0):
+        self.net = Mlp(n_in, n_out, device=device)
+        self.net.set_params(params)
+        self.norm = {k: np.asarray(v, np.float64) for k, v in norm.items()}
+        self.bases = {int(z): PotBasis(a) for z, a in alphas.items()}
+        self.device = device
+
+    @classmethod
+    def load(cls, path=None, device=0):
+        path = path or os.path.join(DATA, "learned_start.npz")
+        d = np.load(path, allow_pickle=False)
+        alphas = {int(z): d[f"alphas_{int(z)}"] for z in d["elements"]}
+        norm = {k: d[k] for k in ("x_mean", "x_std", "t_mean", "t_std")}
+        return cls(d["params"], norm, int(d["n_in"]), int(d["n_out"]), alphas, device)
+
+    @staticmethod
+    def save(path, params, norm, n_in, n_out, alphas, extra=None):
+        kw = {"params": np.asarray(params, np.float32), "n_in": n_in, "n_out": n_out,
+              "elements": np.array(sorted(alphas), np.int64)}
+        kw.update({k: np.asarray(v) for k, v in norm.items()})
+        kw.update({f"alphas_{z}": np.asarray(a) for z, a in alphas.items()})
+        if extra:
+            kw.update({k: np.asarray(v) for k, v in extra.items()})
+        np.savez(path, **kw)
+
+    def start(self, system):
+        """The plain start plus the network's correction (per type, the
+        per-atom predictions averaged over the type's sites)."""
+        import torch
+        plain = scf.atomic_start(system)
+        x = descriptors(system, self.device).astype(np.float64)
+        xn = (x - self.norm["x_mean"]) / self.norm["x_std"]
+        xt = torch.as_tensor(xn, dtype=torch.float32,
+                             device=torch.device("cuda", self.device)).contiguous()
+        y = self.net.forward(xt).cpu().numpy().astype(np.float64)
+        z = y * self.norm["t_std"] + self.norm["t_mean"]
+        out = plain.copy()
+        off = 0
+        types = np.asarray(system.pot_site_type)
+        for ti, pt in enumerate(system.pot_types):
+            n = len(pt.alphas)
+            zz = z[types == ti + 1].mean(axis=0)
+            b = self.bases[int(round(pt.nuc_charge))]
+            out[off:off + n] = plain[off:off + n] + b.to_dc(zz)
+            off += n
+        return out
+
+
+def compare(system, learned, params=None, device=0):
+    """Plain start and learned start on one system, integrals and SCF set-up
+    shared and built once (their time is reported apart).  Returns the two
+    runs, the learned start's inference time and whether it is kept (the
+    plain start judges: within 1e-6 Ha of its energy, no more
+    iterations)."""
+    import torch
+    p = params or scf.ScfParams()
+    ints, t_int = scf.device_integrals(system, device)
+    t0 = time.perf_counter()
+    setup = scf.ScfSetup(system, p, device)
+    torch.cuda.synchronize(device)
+    t_setup = time.perf_counter() - t0
+    plain = scf.run_scf(system, scf.atomic_start(system), p, device, ints, setup)
+    t0 = time.perf_counter()
+    c = learned.start(system)
+    t_inf = time.perf_counter() - t0
+    lrn = scf.run_scf(system, c, p, device, ints, setup)
+    setup.close()
+    ok = (not lrn["positive_energy"] and (lrn["converged"] or lrn["energy_converged"])
+          and abs(lrn["energies"][-1] - plain["energies"][-1]) <= 1e-6
+          and lrn["iterations"] <= plain["iterations"])
+    return {"plain": plain, "learned": lrn, "inference_s": t_inf, "kept": bool(ok),
+            "integrals_s": t_int, "setup_s": t_setup}
