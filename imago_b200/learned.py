@@ -343,3 +343,87 @@ def compare(system, learned, params=None, device=0):
           and lrn["iterations"] <= plain["iterations"])
     return {"plain": plain, "learned": lrn, "inference_s": t_inf, "kept": bool(ok),
             "integrals_s": t_int, "setup_s": t_setup}
+
+
+def main(argv=None):
+    """python -m imago_b200.learned train|evaluate ...
+
+    train:    label the training cells with the plain SCF on the GPU, train
+              the network there, write the weights (npz) and a JSON record
+    evaluate: plain against learned start on the test cells (64-atom Si and
+              graphite at 4x4x4 k), JSON record"""
+    import argparse
+    ap = argparse.ArgumentParser(prog="imago_b200.learned")
+    ap.add_argument("mode", choices=("train", "evaluate"))
+    ap.add_argument("--cells", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--weights", default=os.path.join(DATA, "learned_start.npz"))
+    ap.add_argument("--record", default=None)
+    ap.add_argument("--kmesh", type=int, nargs=3, default=(4, 4, 4))
+    ap.add_argument("--systems", default="si64,graphite64")
+    args = ap.parse_args(argv)
+    log = lambda s: print(s, flush=True)
+    rec = {}
+    if args.mode == "train":
+        t0 = time.perf_counter()
+        cells = training_cells(args.cells)
+        x, t, m, recs = make_dataset(cells, log=log)
+        t1 = time.perf_counter()
+        params, norm, hist = train(x, t, m, steps=args.steps, lr=args.lr, log=log)
+        t2 = time.perf_counter()
+        alphas = {z: b for z, b in ((int(round(p.nuc_charge)), p.alphas)
+                                    for s in cells[:2] for p in s.pot_types)}
+        LearnedStart.save(args.weights, params, norm, x.shape[1], t.shape[1], alphas,
+                          extra={"loss_history": np.array(hist)})
+        rec = {"cells": len(recs), "atoms": int(len(x)),
+               "label_seconds": t1 - t0, "train_seconds": t2 - t1,
+               "plain_iterations_mean": float(np.mean([r["iterations"] for r in recs])),
+               "loss_first": hist[0][1], "loss_last": hist[-1][1]}
+    else:
+        ls = LearnedStart.load(args.weights)
+        out = {}
+        for name in args.systems.split(","):
+            s = test_system(name, tuple(args.kmesh))
+            r = compare(s, ls)
+            out[name] = {
+                "atoms": int(len(s.pot_site_type)), "kmesh": list(args.kmesh),
+                "integrals_s": r["integrals_s"], "setup_s": r["setup_s"],
+                "inference_s": r["inference_s"], "kept": r["kept"],
+                "plain": {k: r["plain"][k] for k in ("iterations", "converged",
+                                                     "energy_converged")},
+                "learned": {k: r["learned"][k] for k in ("iterations", "converged",
+                                                         "energy_converged")},
+                "plain_energy": r["plain"]["energies"][-1],
+                "learned_energy": r["learned"]["energies"][-1],
+                "plain_loop_s": r["plain"]["timings"]["loop_s"],
+                "learned_loop_s": r["learned"]["timings"]["loop_s"],
+                "plain_deltas": r["plain"]["deltas"], "learned_deltas": r["learned"]["deltas"]}
+            log(json.dumps({name: out[name]}))
+        rec = out
+    if args.record:
+        with open(args.record, "w") as fh:
+            json.dump(rec, fh, indent=1, default=float)
+    print(json.dumps(rec, default=float))
+
+
+def test_system(name, kmesh=(4, 4, 4), seed=21):
+    """The cells the learned start is measured on: 64-atom Si (the
+    conventional cell 2x2x2) and 64-atom AB graphite (the 4-atom cell 4x4x1),
+    each strained within +-3% and jittered by N(0, 0.02 A) from `seed`;
+    si16 (the conventional Si cell 2x1x1) is a small check case."""
+    rng = np.random.default_rng(seed)
+    e = rng.uniform(-0.03, 0.03, size=(3, 3))
+    e = 0.5 * (e + e.T)
+    if name == "si64":
+        return configs.cubic_supercell("si", reps=(2, 2, 2), kmesh=kmesh, seed=seed, strain=e)
+    if name == "graphite64":
+        return configs.graphite_cell(reps=(4, 4, 1), kmesh=kmesh, seed=seed, jitter=0.02,
+                                     strain=e)
+    if name == "si16":
+        return configs.cubic_supercell("si", reps=(2, 1, 1), kmesh=kmesh, seed=seed, strain=e)
+    raise ValueError(name)
+
+
+if __name__ == "__main__":
+    main()

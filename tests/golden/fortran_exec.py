@@ -208,6 +208,11 @@ def f_sum(x, dim=None):
     x = np.asarray(x).ravel(order="F")
     if x.dtype.kind in "iu":
         return int(x.sum())
+    if x.dtype.kind == "c":
+        c = 0.0 + 0.0j
+        for v in x:
+            c = c + complex(v)
+        return c
     s = 0.0
     for v in x:
         s = s + float(v)
@@ -260,6 +265,10 @@ def f_min(*a):
 
 def f_real(x, kind=None):
     x = _val(x)
+    if isinstance(x, complex):
+        x = x.real
+    if isinstance(x, np.ndarray) and x.dtype.kind == "c":
+        x = x.real
     if isinstance(x, np.ndarray):
         return x.astype(float) if kind is not None else x.astype(np.float32).astype(float)
     return float(x) if kind is not None else float(np.float32(x))
@@ -313,7 +322,33 @@ def f_allocated(x):
 
 
 def f_cmplx(re_, im_=0.0, kind=None):
-    return complex(_val(re_), _val(im_))
+    re_, im_ = _val(re_), _val(im_)
+    if isinstance(re_, np.ndarray) or isinstance(im_, np.ndarray):
+        return np.asarray(re_) + 1j * np.asarray(im_)
+    return complex(re_, im_)
+
+
+def f_aimag(x):
+    x = _val(x)
+    return x.imag if isinstance(x, np.ndarray) else complex(x).imag
+
+
+def f_conjg(x):
+    x = _val(x)
+    return np.conj(x) if isinstance(x, np.ndarray) else complex(x).conjugate()
+
+
+def f_transpose(x):
+    return np.asarray(_val(x)).T
+
+
+def f_ishft(a, n):
+    a, n = int(_val(a)), int(_val(n))
+    return a << n if n >= 0 else a >> -n
+
+
+def f_matmul(a, b):
+    return np.asarray(_val(a)) @ np.asarray(_val(b))
 
 
 def f_log10(x):
@@ -323,7 +358,7 @@ def f_log10(x):
 INTRINSICS = {"exp", "sqrt", "log", "cos", "sin", "acos", "erf", "abs", "sum",
               "dot_product", "maxval", "minval", "max", "min", "real", "dble",
               "int", "nint", "ceiling", "floor", "mod", "sign", "size", "allocated",
-              "cmplx", "log10"}
+              "cmplx", "log10", "aimag", "conjg", "transpose", "ishft", "matmul"}
 
 
 class FortranStop(RuntimeError):
@@ -463,7 +498,7 @@ class ExprParser:
 
     def mul(self):
         e = self.pow_()
-        while self.at("*", "/"):
+        while self.at("*", "/") and not (self.at("/") and self.peek(1)[1] == ")"):
             op = self.take()[1]
             r = self.pow_()
             e = f"({e} * {r})" if op == "*" else f"f_div({e}, {r})"
@@ -499,9 +534,25 @@ class ExprParser:
             if low in (".true.", ".false."):
                 self.take()
                 return "True" if low == ".true." else "False"
+        if val == "(" and self.peek(1)[1] == "/":
+            # array constructor (/ a, b, ... /)
+            self.take()
+            self.take()
+            items = [self.eqv()]
+            while self.at(","):
+                self.take()
+                items.append(self.eqv())
+            self.take("/")
+            self.take(")")
+            return f"np.array([{', '.join(items)}])"
         if val == "(":
             self.take()
             e = self.eqv()
+            if self.at(","):  # complex literal (re, im)
+                self.take()
+                im = self.eqv()
+                self.take(")")
+                return f"complex({e}, {im})"
             self.take(")")
             return f"({e})"
         if kind == "name":
@@ -572,10 +623,12 @@ class Ctx:
     """Names known to the translator: functions (called, not indexed),
     renames, and the scalar-dummy positions of translated subroutines."""
 
-    def __init__(self, functions=(), rename=None):
+    def __init__(self, functions=(), rename=None, types=None):
         self.functions = set(functions)
         self.rename = rename or {}
         self.sigs = {}
+        # types of module arrays allocated by the translated routines
+        self.types = types or {}
 
     def name(self, low):
         return self.rename.get(low, low)
@@ -587,10 +640,32 @@ def expr(src, ctx):
 
 # ------------------------------------------------------------- statements
 
+def preprocess(lines, defined=()):
+    """#ifdef / #ifndef / #else / #endif with the given macros defined (the
+    reference builds its complex engine without GAMMA)."""
+    out, stack = [], []
+    for raw in lines:
+        t = raw.strip()
+        m = re.match(r"#\s*(ifdef|ifndef)\s+(\w+)", t)
+        if m:
+            on = (m.group(2) in defined) == (m.group(1) == "ifdef")
+            stack.append(on)
+            continue
+        if re.match(r"#\s*else", t):
+            stack[-1] = not stack[-1]
+            continue
+        if re.match(r"#\s*endif", t):
+            stack.pop()
+            continue
+        if all(stack):
+            out.append(raw)
+    return out
+
+
 def join_lines(lines):
     """Free-form continuation and comments: one logical statement per item."""
     out, cur = [], ""
-    for raw in lines:
+    for raw in preprocess(lines):
         code = _strip_comment(raw.rstrip("\n"))
         if cur:
             s = code.lstrip()
@@ -692,6 +767,7 @@ def translate(stmts, ctx, hooks=None, record=False):
     params = [p.strip().lower() for p in (m.group(3) or "").split(",") if p.strip()]
     result = (m.group(4) or name).lower()
     decls = {}
+    inits = {}
     body = []
     for s in stmts[1:-1]:
         d = DECL.match(s)
@@ -702,11 +778,16 @@ def translate(stmts, ctx, hooks=None, record=False):
                 typ = "real4"
             dim = re.search(r"dimension\s*\(([^)]*)\)", attrs)
             for v in _split_top(d.group(3)):
-                v = v.split("=")[0].strip()
+                init = None
+                if "=" in v:
+                    v, init = v.split("=", 1)
+                v = v.strip()
                 vm = re.match(r"(\w+)\s*(?:\((.*)\))?", v)
                 vn = vm.group(1).lower()
                 vdims = vm.group(2) or (dim.group(1) if dim else None)
                 decls[vn] = (typ, vdims)
+                if init is not None:
+                    inits[vn] = init.strip()
             continue
         body.append(s)
     py = [f"def {ctx.name(name)}({', '.join(params)}):"]
@@ -732,6 +813,13 @@ def translate(stmts, ctx, hooks=None, record=False):
             py.append(f"    {v} = Arr(({shape},), {dt})")
         else:
             py.append(f"    {v} = None")
+    for v, init in inits.items():
+        typ, dims = decls[v]
+        if dims is None:
+            py.append(f"    {v} = {expr(init, ctx)}")
+        else:
+            dt = {"integer": "np.int64", "complex": "complex"}.get(typ, "float")
+            py.append(f"    {v} = Arr.of({expr(init, ctx)}, {dt})")
     if kind == "function" and result not in decls:
         py.append(f"    {result} = 0.0")
     ind = 1
@@ -789,7 +877,7 @@ def translate(stmts, ctx, hooks=None, record=False):
                 im = re.match(r"(\w+)\s*\((.*)\)$", item)
                 v = im.group(1).lower()
                 shape = ", ".join(f"int({expr(x, ctx)})" for x in _split_top(im.group(2)))
-                typ = decls.get(v, ("real", None))[0]
+                typ = decls.get(v, (ctx.types.get(v, "real"), None))[0]
                 dt = {"integer": "np.int64", "complex": "complex"}.get(typ, "float")
                 emit(f"{ctx.name(v)} = Arr(({shape},), {dt})")
             return
@@ -848,6 +936,34 @@ def translate(stmts, ctx, hooks=None, record=False):
             emit(f"if {expr(m.group(1), ctx)}:")
             stack.append(("if", None))
             ind += 1
+            continue
+        m = re.match(r"^select\s+case\s*\((.*)\)$", s, re.I)
+        if m:
+            sel = f"_sel{len(stack)}"
+            emit(f"{sel} = {expr(m.group(1), ctx)}")
+            emit("if False:")
+            emit("    pass")
+            stack.append(("select", sel))
+            ind += 1
+            continue
+        m = re.match(r"^case\s*(default|\((.*)\))$", s, re.I)
+        if m:
+            sel = stack[-1][1]
+            if m.group(1).lower() == "default":
+                py.append("    " * (ind - 1) + "else:")
+            else:
+                conds = []
+                for item in _split_top(m.group(2)):
+                    if ":" in item:
+                        lo, hi = item.split(":")
+                        conds.append(f"({expr(lo, ctx)} <= {sel} <= {expr(hi, ctx)})")
+                    else:
+                        conds.append(f"({sel} == {expr(item, ctx)})")
+                py.append("    " * (ind - 1) + f"elif {' or '.join(conds)}:")
+            continue
+        if re.fullmatch(r"end\s*select", low):
+            stack.pop()
+            ind -= 1
             continue
         m = re.match(r"^else\s*if\s*\((.*)\)\s*then$", s, re.I)
         if m:

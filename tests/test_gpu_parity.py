@@ -654,3 +654,20 @@ def test_koverlap_at_zero_wave_vector_is_the_overlap_quartz(imago_lib):
         # and the full matrix is Hermitian
         full = re[ax, 0] + 1j * im[ax, 0]
         assert np.abs(full - full.conj().T).max() <= 1e-10
+
+
+def test_driver_matches_reference_driver_executed(imago_lib):
+    # the reference's own integral driver, executed statement for statement
+    # (tests/golden/make_driver_golden.py: gaussOverlapOL / orthoOL,
+    # gaussOverlapKE / ortho with every routine they call) on the diamond
+    # primitive cell at 2x2x2 k
+    import os
+    from conftest import ROOT
+    g = np.load(os.path.join(ROOT, "tests", "golden", "driver_diamond.npz"))
+    with intg.IntegralSetup(configs.diamond_primitive(kmesh=(2, 2, 2))) as s:
+        ol, cre, cim = s.gauss_overlap_ol()
+        ke = s.gauss_overlap_ke()
+    _assert_all({"OL": packed_mismatch(ol, g["ol_packed"]),
+                 "KE": packed_mismatch(ke, g["ke_packed"]),
+                 "CVre": packed_mismatch(cre, g["ol_cv_re"]),
+                 "CVim": packed_mismatch(cim, g["ol_cv_im"])})

@@ -165,3 +165,23 @@ def test_koverlap_at_zero_wave_vector_is_the_overlap():
             # the packed overlap zeroes entries below 1e-10; the full planes
             # do not
             assert np.abs(kov[ax, k] - full).max() <= 1e-10
+
+
+def test_oracle_driver_matches_reference_driver_executed():
+    # the oracle's restatement of the integral driver against the
+    # reference's own driver executed statement for statement
+    # (tests/golden/make_driver_golden.py), OL with coreValeOL and KE on the
+    # diamond primitive cell at 2x2x2 k
+    import os
+    import numpy as np
+    import oracle
+    from conftest import ROOT, packed_mismatch
+    from imago_b200 import configs
+    g = np.load(os.path.join(ROOT, "tests", "golden", "driver_diamond.npz"))
+    ob = oracle.OracleBuild(configs.diamond_primitive(kmesh=(2, 2, 2)))
+    ol, cre, cim = ob.overlap()
+    ke = ob.kinetic()
+    assert np.array_equal(ob.kpoints_xyz(), g["kPointsXYZ"])
+    for a, b in ((ol, g["ol_packed"]), (ke, g["ke_packed"]), (cre, g["ol_cv_re"]),
+                 (cim, g["ol_cv_im"])):
+        assert packed_mismatch(a, b, atol=1e-13)[1] == 0
