@@ -482,6 +482,55 @@ def adjacent_builds(g, bufs, stream, torch, dev, reps=5, ham_mode="auto"):
     return out
 
 
+def scf_headline(local, torch, systems=("si8", "si64", "graphite64")):
+    """The metric's SCF half: Imago's SCF loop on the GPU (imago_b200.scf:
+    integrals, set-up, then secular equation / populations / density traces
+    / makeSCFPot per iteration) run to the reference's convergence test
+    (testableDelta < 1e-4) or two total energies within 1e-6 Ha, from the
+    plain atomic-superposition start and from the learned start
+    (imago_b200.learned, the network in imago_b200/data/learned_start.npz
+    trained on the GPU by the library's own kernels).  Wall seconds with the
+    device synchronised; the learned start is kept only when it reaches the
+    plain start's energy within 1e-6 Ha in no more iterations.
+    si8: the benched Si8 cell at 8x8x8 k (plain start only);
+    si64 / graphite64: the learned start's test cells at 4x4x4 k."""
+    from imago_b200 import learned, scf
+    out = {}
+    weights = os.path.join(ROOT, "imago_b200", "data", "learned_start.npz")
+    ls = learned.LearnedStart.load(weights, device=local) if os.path.exists(weights) else None
+    for name in systems:
+        s = system_for("si8") if name == "si8" else learned.test_system(name, (4, 4, 4))
+        if ls is None or name == "si8":
+            t0 = time.perf_counter()
+            r = scf.run_scf(s, scf.atomic_start(s), device=local)
+            torch.cuda.synchronize(local)
+            out[name] = {"atoms": int(len(s.pot_site_type)), "kpoints": int(len(s.kpoints_abc)),
+                         "plain_iterations": r["iterations"],
+                         "plain_energy": r["energies"][-1],
+                         "plain_converged": bool(r["converged"] or r["energy_converged"]),
+                         "integrals_s": r["timings"]["integrals_s"],
+                         "setup_s": r["timings"]["setup_s"],
+                         "plain_loop_s": r["timings"]["loop_s"],
+                         "plain_total_s": time.perf_counter() - t0}
+            continue
+        r = learned.compare(s, ls, device=local)
+        p, q = r["plain"], r["learned"]
+        shared = r["integrals_s"] + r["setup_s"]
+        lt = q["timings"]["loop_s"] + r["inference_s"]
+        out[name] = {
+            "atoms": int(len(s.pot_site_type)), "kpoints": int(len(s.kpoints_abc)),
+            "integrals_s": r["integrals_s"], "setup_s": r["setup_s"],
+            "plain_iterations": p["iterations"], "learned_iterations": q["iterations"],
+            "plain_energy": p["energies"][-1], "learned_energy": q["energies"][-1],
+            "plain_loop_s": p["timings"]["loop_s"], "learned_loop_s": lt,
+            "inference_s": r["inference_s"], "kept": r["kept"],
+            "plain_total_s": shared + p["timings"]["loop_s"],
+            "learned_total_s": shared + lt,
+            "learned_over_plain_total": (shared + lt) / (shared + p["timings"]["loop_s"]),
+            "learned_over_plain_loop": lt / p["timings"]["loop_s"]}
+    return out
+
+
 def silica_headline(args, local, stream, torch):
     """The 162-atom alpha-quartz build at Gamma (device time, end to end,
     the builds beside the SCF set, and the oracle on the host cores),
@@ -802,6 +851,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
         if world == 1 and args.workload == "si8" and not args.no_silica:
             line["silica_162"] = silica_headline(args, local, stream, torch)
+        if world == 1 and args.workload == "si8" and not args.no_scf:
+            line["scf"] = scf_headline(local, torch)
         print(json.dumps(line), flush=True)
     g.close()
     if world > 1:
@@ -838,6 +889,9 @@ def main():
                     help="how the PSCF Hamiltonian of the adjacent builds sums "
                          "its potential terms (profiling the fused kernel on a "
                          "small case)")
+    ap.add_argument("--no-scf", action="store_true",
+                    help="skip the SCF runs (plain and learned start) of the "
+                         "default line")
     ap.add_argument("--no-adjacent", action="store_true",
                     help="skip the timings of the mass-velocity, momentum, "
                          "dipole and PSCF Hamiltonian builds")

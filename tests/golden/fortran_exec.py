@@ -347,6 +347,24 @@ def f_ishft(a, n):
     return a << n if n >= 0 else a >> -n
 
 
+def f_bit_size(x):
+    return 64
+
+
+def f_btest(a, pos):
+    return bool((int(_val(a)) >> int(_val(pos))) & 1)
+
+
+def f_ibclr(a, pos):
+    v = int(_val(a)) & ~(1 << int(_val(pos)))
+    return v - (1 << 64) if v >= (1 << 63) else v
+
+
+def f_ibset(a, pos):
+    v = (int(_val(a)) | (1 << int(_val(pos)))) & ((1 << 64) - 1)
+    return v - (1 << 64) if v >= (1 << 63) else v
+
+
 def f_matmul(a, b):
     return np.asarray(_val(a)) @ np.asarray(_val(b))
 
@@ -358,7 +376,8 @@ def f_log10(x):
 INTRINSICS = {"exp", "sqrt", "log", "cos", "sin", "acos", "erf", "abs", "sum",
               "dot_product", "maxval", "minval", "max", "min", "real", "dble",
               "int", "nint", "ceiling", "floor", "mod", "sign", "size", "allocated",
-              "cmplx", "log10", "aimag", "conjg", "transpose", "ishft", "matmul"}
+              "cmplx", "log10", "aimag", "conjg", "transpose", "ishft", "matmul",
+              "bit_size", "btest", "ibclr", "ibset"}
 
 
 class FortranStop(RuntimeError):

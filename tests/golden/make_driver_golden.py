@@ -10,16 +10,18 @@ Executed from src/imago, statement for statement:
                        (getNumCells, makeLattice, cellBorderCheck; sortSubs'
                        mergeSort)
   kpoints.f90          convertKPointsToXYZ, computePhaseFactors
-  basis.f90            renormalizeBasis, initializeAtomSite
-  gaussRelations.f90   makeAlphaDist
-  integrals.F90        gaussOverlapOL, orthoOL, gaussOverlapKE, ortho
+  basis.f90            renormalizeBasis, initializeAtomSite, initializePotSite
+  gaussRelations.f90   makeAlphaDist, makeAlphaNucDist, makeAlphaPotDist
+  integrals.F90        gaussOverlapOL, orthoOL, gaussOverlapKE, gaussOverlapNP,
+                       nuclearPE, elecPotGaussOverlap, gaussOverlapEP,
+                       electronicPE, checkElecPotInteraction, ortho
   intgSaving.F90       multWithBasisFn1, applyPhaseFactors,
                        kPointLatticeOriginShift, saveCurrentPair and its
                        block savers
   intgOrtho.F90        valeCoreCoreValeOL, valeCoreCoreVale, coreValeCoreCore,
                        makeValeVale
-  gaussIntegrals.f90   overlap2CIntg, kinetic2CIntg (through make_golden.py's
-                       transliteration)
+  gaussIntegrals.f90   overlap2CIntg, kinetic2CIntg, nuclear3CIntg,
+                       electron3CIntg (through make_golden.py's transliteration)
 
 Supplied by this script: the module data of the synthetic systems
 (imago_b200.configs), findLatticeVector (a nearest lattice vector; the
@@ -29,8 +31,8 @@ LAPACK's zherk / zher2k (their definitions on the upper triangle in numpy,
 the diagonal's imaginary part set to zero as the routines specify).
 
 Fixture: driver_diamond.npz, the diamond primitive cell at 2x2x2 k: the
-packed OL and KE matrices per k-point and coreValeOL, as the reference
-hands them to HDF5.
+packed OL, KE, NP and every EP term per k-point and coreValeOL, as the
+reference hands them to HDF5.
 
 Run where the reference is mounted:
 
@@ -94,6 +96,21 @@ def kernel_hook(kns, name):
     return call
 
 
+def kernel3c_hook(kns, name):
+    """nuclear3CIntg / electron3CIntg(a1, a2, a3, A, B, C, code, sh) through
+    the transliterated generated kernel."""
+    def call(a1, a2, a3, A, B, C, code, sh):
+        f = make_golden.FArr("sh", [16, 16])
+        kns[name](float(a1), float(a2), float(a3), np.array(fe._val(A), float),
+                  np.array(fe._val(B), float), np.array(fe._val(C), float), int(code), f)
+        out = fe._val(sh)
+        out[...] = 0.0
+        for (i, j), v in f.d.items():
+            out[i - 1, j - 1] = v
+        return ()
+    return call
+
+
 def module_state(s, store, kns):
     ns = msg.module_state(s, store, 20)
     # atom sites and types (atomicSites.f90, atomicTypes.f90)
@@ -143,7 +160,14 @@ def module_state(s, store, kns):
     ns["corevale"] = None
     ns["valecore"] = None
     ns.update(zherk=zherk, zher2k=zher2k, overlap2cintg=kernel_hook(kns, "overlap2CIntg"),
-              kinetic2cintg=kernel_hook(kns, "kinetic2CIntg"))
+              kinetic2cintg=kernel_hook(kns, "kinetic2CIntg"),
+              nuclear3cintg=kernel3c_hook(kns, "nuclear3CIntg"),
+              electron3cintg=kernel3c_hook(kns, "electron3CIntg"))
+    for v in ("alphanucdist", "elementnucalpha", "alphapotdist", "anyelecpotinteraction",
+              "hsize_t_bitsize", "matrixindex", "cellindex", "currpottypenumber",
+              "curralphanumber", "currpotalpha", "currpotnumber", "currpotelement",
+              "currmultiplicity", "numelementpotalphas", "elementpotalphas"):
+        ns[v] = None
     return ns
 
 
@@ -168,20 +192,32 @@ ROUTINES = msg.ROUTINES[:9] + [
     ("integrals.F90", "subroutine", "ortho"),
     ("integrals.F90", "subroutine", "gaussOverlapOL"),
     ("integrals.F90", "subroutine", "gaussOverlapKE"),
+    ("gaussRelations.f90", "subroutine", "makeAlphaNucDist"),
+    ("basis.f90", "subroutine", "initializePotSite"),
+    ("integrals.F90", "subroutine", "nuclearPE"),
+    ("integrals.F90", "subroutine", "gaussOverlapNP"),
+    ("gaussRelations.f90", "subroutine", "makeAlphaPotDist"),
+    ("integrals.F90", "function", "checkElecPotInteraction"),
+    ("integrals.F90", "subroutine", "electronicPE"),
+    ("integrals.F90", "subroutine", "gaussOverlapEP"),
+    ("integrals.F90", "subroutine", "elecPotGaussOverlap"),
 ]
 
 
-def run(s, ref):
+def run(s, ref, with_ep=True):
     store = msg.Store()
     kns = make_golden.load_kernels(ref)
     ns = module_state(s, store, kns)
-    ctx = fe.Ctx(functions=["error_fn"],
+    ctx = fe.Ctx(functions=["error_fn", "checkelecpotinteraction"],
                  types={"phasefactor": "complex", "corevale": "complex",
                         "valecore": "complex", "lmindex": "integer",
-                        "lmalphaindex": "integer", "numelementatomicalphas": "integer"})
+                        "lmalphaindex": "integer", "numelementatomicalphas": "integer",
+                        "anyelecpotinteraction": "integer",
+                        "numelementpotalphas": "integer"})
     src = os.path.join(ref, "src", "imago")
     hooks = dict(msg.HOOK_ARGS)
-    hooks.update({"zherk": [], "zher2k": [], "overlap2cintg": [], "kinetic2cintg": []})
+    hooks.update({"zherk": [], "zher2k": [], "overlap2cintg": [], "kinetic2cintg": [],
+                  "nuclear3cintg": [], "electron3cintg": []})
     for f, k, n in ROUTINES:
         fe.load(os.path.join(src, f), k, n, ns, ctx, hooks)
     ns["findlatticevector"] = msg.nearest_lattice(ns)
@@ -203,13 +239,27 @@ def run(s, ref):
     t0 = time.time()
     ns["gaussoverlapke"](None, msg.names("ke", nk), "ke_aid")
     print(f"  KE executed in {time.time() - t0:.1f} s", flush=True)
+    ns["makealphanucdist"]()
+    t0 = time.time()
+    ns["gaussoverlapnp"](None, msg.names("np", nk), "np_aid")
+    print(f"  NP executed in {time.time() - t0:.1f} s", flush=True)
+    if with_ep:
+        ns["makealphapotdist"]()
+        P = ns["potdim"]
+        didp = fe.Arr.of(np.array([[f"ep_{t + 1}_{k + 1}" for t in range(P)] for k in range(nk)],
+                                  dtype=object), dtype=object)
+        t0 = time.time()
+        ns["elecpotgaussoverlap"](None, didp, msg.names("ep_aid", P))
+        print(f"  EP executed in {time.time() - t0:.1f} s", flush=True)
     V = ns["valedim"]
     npk = V * (V + 1) // 2
 
     def packed(prefix):
         return np.stack([np.asarray(store.d[f"{prefix}_{k + 1}"]).reshape(2, npk).T
                          for k in range(nk)])
-    out = {"ol_packed": packed("ol"), "ke_packed": packed("ke")}
+    out = {"ol_packed": packed("ol"), "ke_packed": packed("ke"), "np_packed": packed("np")}
+    if with_ep:
+        out["ep_packed"] = np.stack([packed(f"ep_{t + 1}") for t in range(ns["potdim"])])
     if ns["coredim"]:
         out["ol_cv_re"] = np.stack([np.asarray(store.d[f"olcv_re_{k + 1}"]).T
                                     for k in range(nk)])

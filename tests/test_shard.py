@@ -77,3 +77,73 @@ def test_two_ranks_gather_every_matrix(pot_dim, dst):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert results[0] and results[1]
+
+
+def test_cost_partition_balances_the_three_centre_builds():
+    from imago_b200 import configs
+    s = configs.quartz_supercell(gamma=True)
+    costs = shard.matrix_costs(s)
+    assert len(costs) == 2 + s.pot_dim
+    for world in (1, 2, 3, 4, 8):
+        parts = shard.partition(s.pot_dim, world, costs)
+        assert parts[0][0] == 0 and parts[-1][1] == 2 + s.pot_dim
+        assert all(a[1] == b[0] for a, b in zip(parts, parts[1:]))
+        assert all(hi > lo for lo, hi in parts)
+        loads = [sum(costs[lo:hi]) for lo, hi in parts]
+        # no rank above its share by more than its largest single matrix
+        assert max(loads) <= sum(costs) / world + max(costs)
+
+
+def _oracle_rank_main(rank, world, port, results):
+    # real builders on the CPU: the oracle's restatement of the driver
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import numpy as np
+    import oracle
+    from imago_b200 import configs
+    s = configs.small_test_system()
+    ob = oracle.OracleBuild(s, nthreads=1)
+
+    def overlap():
+        return {"ol_packed": torch.as_tensor(ob.overlap()[0])}
+
+    def builder(ids, shp):
+        out = torch.empty((len(ids),) + tuple(shp), dtype=torch.float64)
+        for i, m in enumerate(ids):
+            if m == shard.KE:
+                out[i] = torch.as_tensor(ob.kinetic())
+            elif m == shard.NP:
+                out[i] = torch.as_tensor(ob.nuclear())
+            else:
+                out[i] = torch.as_tensor(ob.elec_pot(m - 2, m - 1)[0])
+        return out
+
+    shape = ob.overlap()[0].shape
+    sb = shard.ShardedBuild(s.pot_dim, shape, builder, overlap, dst=0,
+                            costs=shard.matrix_costs(s))
+    got = sb.build()
+    if rank == 0:
+        ok = bool(np.array_equal(got["ke"].numpy(), ob.kinetic()))
+        ok &= bool(np.array_equal(got["np"].numpy(), ob.nuclear()))
+        ok &= bool(np.array_equal(got["ep"].numpy(), ob.elec_pot()))
+        results[rank] = ok
+    else:
+        results[rank] = got is None
+    ob.close()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_with_oracle_builders_reproduce_the_single_build():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    results = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_oracle_rank_main, args=(r, 2, port, results))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    assert results[0] and results[1]
