@@ -569,6 +569,54 @@ def silica_headline(args, local, stream, torch):
                                "kind": "port",
                                "sample": (f"oracle (CPU restatement, OpenMP over "
                                           f"atom pairs): {what}; {wall:.1f} s wall")}
+        if not args.no_full_cpu:
+            # the same build run once in full: every atom pair, every EP
+            # term's own orthogonalisation
+            t0 = time.perf_counter()
+            full = oracle_build_time(system, ncores)
+            out["cpu_full"] = {"value": full, "unit": UNIT, "cores": ncores, "kind": "port",
+                               "sample": "the full build, run once",
+                               "wall_s": time.perf_counter() - t0,
+                               "sampled_over_full": v / full}
+            out["speedup_vs_cpu_full"] = {"device": full / out["value"],
+                                          "e2e": full / out["e2e"]["value"]}
+    out["quartz_222"] = quartz_222(args, local, torch)
+    return out
+
+
+def quartz_222(args, local, torch):
+    """The same cell at 2x2x2 k (8 k-points): device time of the graph
+    replay, end to end, and the oracle on the host cores (sampled as for
+    Gamma: every 8th atom pair, the EP orthogonalisations timed on KE and
+    NP)."""
+    from imago_b200 import intg
+    wl = "quartz-222"
+    system = system_for(wl)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=local)
+    g = intg.IntegralSetup(system, device=local, outputs_on_device=True,
+                           stream=stream.cuda_stream)
+    bufs = device_outputs(g, torch, dev)
+    flush = torch.empty(512 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        g.build_graph({k: v.data_ptr() for k, v in bufs.items()})
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        step_s, kms, launches = time_device_builds(g, bufs, stream, 3, flush, torch)
+    out = {"workload": WORKLOADS[wl]["desc"], "value": float(np.mean(step_s)), "unit": UNIT,
+           "stage_ms": dict(zip(STAGES, [float(x) / 3 for x in kms])),
+           "gpu_launches": int(launches), "clocks": clk.summary()}
+    g.close()
+    out["e2e"] = time_e2e(system, local, stream, bufs, 2, torch)
+    del bufs, flush
+    torch.cuda.empty_cache()
+    if not args.skip_cpu:
+        ncores = os.cpu_count() or 1
+        v, wall, what = cpu_baseline(system, ncores, wl)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+                               "sample": (f"oracle (CPU restatement, OpenMP over "
+                                          f"atom pairs): {what}; {wall:.1f} s wall")}
+        out["speedup_vs_cpu"] = {"device": v / out["value"], "e2e": v / out["e2e"]["value"]}
     return out
 
 
@@ -889,6 +937,9 @@ def main():
                     help="how the PSCF Hamiltonian of the adjacent builds sums "
                          "its potential terms (profiling the fused kernel on a "
                          "small case)")
+    ap.add_argument("--no-full-cpu", action="store_true",
+                    help="skip the one unsampled oracle run of the quartz Gamma "
+                         "build in the default line")
     ap.add_argument("--no-scf", action="store_true",
                     help="skip the SCF runs (plain and learned start) of the "
                          "default line")

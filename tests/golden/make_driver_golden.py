@@ -168,6 +168,7 @@ def module_state(s, store, kns):
               "curralphanumber", "currpotalpha", "currpotnumber", "currpotelement",
               "currmultiplicity", "numelementpotalphas", "elementpotalphas"):
         ns[v] = None
+    ns["elecpotinteraction"] = 0
     return ns
 
 

@@ -8,9 +8,10 @@ Tolerances: the lattice lists are exact; the electrostatic operators and
 the mesh agree within 1e-12 relative to the largest element (the device's
 exp and the order of the sums over site pairs); the core charge fit and the
 next potential coefficients come out of ill-conditioned Gaussian fits
-(condition numbers near 1e10), so they are compared at 1e-9 relative, and
-what the physics depends on, the energies, at 1e-9 Hartree per iteration
-and 1e-7 Hartree at convergence.
+(condition numbers near 1e10), so they are compared at 1e-9 relative, the
+convergence measure (a norm of the difference of two coefficient sets) at
+1e-7 relative plus 1e-10, and what the physics depends on, the energies,
+at 1e-9 Hartree per iteration and 1e-7 Hartree at convergence.
 """
 import os
 
@@ -76,8 +77,11 @@ def _replay(update, g):
         for key in ("totalEnergy", "kineticEnergy", "elecStatEnergy", "exchCorrEnergy"):
             assert abs(r[key] - g["scf_" + key][it]) < 1e-9, (it, key)
         assert abs(r["electronDiff"] - g["scf_electronDiff"][it]) < 1e-9
+        # testableDelta is a norm of (new - used) coefficients, which cancel
+        # near convergence: its absolute error is that of the coefficients
+        # (1e-9 relative of their size, O(1..100)) times the mesh operator
         assert abs(r["testableDelta"] - g["scf_testableDelta"][it]) <= \
-            1e-7 * g["scf_testableDelta"][it] + 1e-12
+            1e-7 * g["scf_testableDelta"][it] + 1e-10
         assert r["converged"] == g["scf_converged"][it]
         assert _rel(nxt, g["scf_next"][it]) < 1e-9, it
 
