@@ -507,7 +507,7 @@ def scf_headline(local, torch, systems=("si8", "si64", "graphite64")):
             out[name] = {"atoms": int(len(s.pot_site_type)), "kpoints": int(len(s.kpoints_abc)),
                          "plain_iterations": r["iterations"],
                          "plain_energy": r["energies"][-1],
-                         "plain_converged": bool(r["converged"] or r["energy_converged"]),
+                         "plain_converged": bool(r["done"]),
                          "integrals_s": r["timings"]["integrals_s"],
                          "setup_s": r["timings"]["setup_s"],
                          "plain_loop_s": r["timings"]["loop_s"],

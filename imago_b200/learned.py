@@ -213,7 +213,7 @@ def make_dataset(cells, params=None, device=0, log=None):
         t0 = time.perf_counter()
         start = scf.atomic_start(s)
         r = scf.run_scf(s, start, p, device=device)
-        if r["positive_energy"] or not (r["converged"] or r["energy_converged"]):
+        if r["positive_energy"] or not r["done"]:
             continue
         conv = r["pot_coeffs"]
         x = descriptors(s, device)
@@ -338,7 +338,7 @@ def compare(system, learned, params=None, device=0):
     t_inf = time.perf_counter() - t0
     lrn = scf.run_scf(system, c, p, device, ints, setup)
     setup.close()
-    ok = (not lrn["positive_energy"] and (lrn["converged"] or lrn["energy_converged"])
+    ok = (not lrn["positive_energy"] and lrn["done"] and plain["done"]
           and abs(lrn["energies"][-1] - plain["energies"][-1]) <= 1e-6
           and lrn["iterations"] <= plain["iterations"])
     return {"plain": plain, "learned": lrn, "inference_s": t_inf, "kept": bool(ok),
@@ -391,9 +391,9 @@ def main(argv=None):
                 "integrals_s": r["integrals_s"], "setup_s": r["setup_s"],
                 "inference_s": r["inference_s"], "kept": r["kept"],
                 "plain": {k: r["plain"][k] for k in ("iterations", "converged",
-                                                     "energy_converged")},
+                                                     "energy_converged", "done")},
                 "learned": {k: r["learned"][k] for k in ("iterations", "converged",
-                                                         "energy_converged")},
+                                                         "energy_converged", "done")},
                 "plain_energy": r["plain"]["energies"][-1],
                 "learned_energy": r["learned"]["energies"][-1],
                 "plain_loop_s": r["plain"]["timings"]["loop_s"],

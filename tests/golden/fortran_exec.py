@@ -355,14 +355,17 @@ def f_btest(a, pos):
     return bool((int(_val(a)) >> int(_val(pos))) & 1)
 
 
-def f_ibclr(a, pos):
-    v = int(_val(a)) & ~(1 << int(_val(pos)))
+def _signed64(v):
+    v &= (1 << 64) - 1
     return v - (1 << 64) if v >= (1 << 63) else v
+
+
+def f_ibclr(a, pos):
+    return _signed64((int(_val(a)) & ((1 << 64) - 1)) & ~(1 << int(_val(pos))))
 
 
 def f_ibset(a, pos):
-    v = (int(_val(a)) | (1 << int(_val(pos)))) & ((1 << 64) - 1)
-    return v - (1 << 64) if v >= (1 << 63) else v
+    return _signed64((int(_val(a)) & ((1 << 64) - 1)) | (1 << int(_val(pos))))
 
 
 def f_matmul(a, b):
