@@ -554,7 +554,8 @@ def silica_headline(args, local, stream, torch):
            "stage_ms": dict(zip(STAGES, [float(x) / 5 for x in kms])),
            "vale_dim": g.vale_dim, "core_dim": g.core_dim, "pot_terms": g.pot_dim,
            "pair_images": g.num_pair_images, "shell_pairs": g.num_shell_pairs,
-           "gpu_launches": int(launches), "clocks": clk.summary()}
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "schedule": schedules(g, bufs, stream, flush, torch)}
     if not args.no_adjacent:
         out["adjacent_builds"] = adjacent_builds(g, bufs, stream, torch, dev, reps=3,
                                                  ham_mode=args.ham_mode)
@@ -584,6 +585,23 @@ def silica_headline(args, local, stream, torch):
     return out
 
 
+def schedules(g, bufs, stream, flush, torch, steps=3):
+    """The three-centre stage's two schedules on this build: per-class
+    launches against the persistent work-queue launch (device seconds of
+    whole builds replayed from graphs, and the primitive stage's ms with the
+    kinds serialised), the measured choice the context made, and back to
+    the measured choice."""
+    out = {"chosen": g.schedule()}
+    for mode in ("per_class", "queue"):
+        g.set_schedule(mode)
+        g.build_graph({k: v.data_ptr() for k, v in bufs.items()})
+        torch.cuda.synchronize()
+        step_s, kms, _ = time_device_builds(g, bufs, stream, steps, flush, torch)
+        out[mode] = {"build_s": float(np.mean(step_s)), "prim_ms": float(kms[0]) / steps}
+    g.set_schedule(out["chosen"]["schedule"])
+    return out
+
+
 def quartz_222(args, local, torch):
     """The same cell at 2x2x2 k (8 k-points): device time of the graph
     replay, end to end, and the oracle on the host cores (sampled as for
@@ -605,7 +623,8 @@ def quartz_222(args, local, torch):
         step_s, kms, launches = time_device_builds(g, bufs, stream, 3, flush, torch)
     out = {"workload": WORKLOADS[wl]["desc"], "value": float(np.mean(step_s)), "unit": UNIT,
            "stage_ms": dict(zip(STAGES, [float(x) / 3 for x in kms])),
-           "gpu_launches": int(launches), "clocks": clk.summary()}
+           "gpu_launches": int(launches), "clocks": clk.summary(),
+           "schedule": schedules(g, bufs, stream, flush, torch)}
     g.close()
     out["e2e"] = time_e2e(system, local, stream, bufs, 2, torch)
     del bufs, flush

@@ -179,6 +179,12 @@ struct imago_ctx {
   bool bloch_tuned = false;
   float bloch_ms[kNumBlochWidths] = {};
   int cls_beg[17];
+  // three-centre schedule: per-class launches (0) or one persistent launch
+  // fed by a work queue (1); mode -1 measures both on the first EP build
+  int sched_mode = -1, sched = 0;
+  bool sched_tuned = false;
+  float sched_ms[2] = {};
+  int queue_ctas = 0;
   long long blk_total = 0, m_total = 0;
   std::vector<Term3c> ep_terms;
 
@@ -195,6 +201,7 @@ struct imago_ctx {
   DBuf<DUnit> d_units;
   DBuf<DSp> d_sps;
   DBuf<Term3c> d_terms;
+  DBuf<unsigned long long> d_queue;  // one work-queue counter per lane
   DBuf<int2> d_btile, d_btile_w;
   DBuf<SiteImage> d_simg;
   DBuf<float> d_cl_d1;
@@ -276,6 +283,7 @@ struct imago_ctx {
     d_terms.release(st); d_btile.release(st); d_simg.release(st);
     d_btile_w.release(st);
     d_cl_d1.release(st);
+    d_queue.release(st);
     if (st) cudaStreamSynchronize(st);
     if (events)
       for (auto &e : ev) cudaEventDestroy(e);
@@ -841,6 +849,15 @@ int upload(imago_ctx *c) {
   UP(d_sps, c->sps) UP(d_sp_by_cls, c->sp_by_cls) UP(d_terms, c->ep_terms)
   UP(d_btile, c->btile) UP(d_btile_w, c->btile_w)
 #undef UP
+  if ((rc = c->d_queue.alloc(4, st))) return rc;
+  {
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
+      cudaGetLastError();
+      nsm = 148;
+    }
+    c->queue_ctas = nsm * prim3c_queue_ctas_per_sm();
+  }
   if ((rc = c->d_phase.alloc((size_t)c->ncell * c->nk, st))) return rc;
 
   DevSys &s = c->sys;
@@ -997,6 +1014,43 @@ int tune_bloch(imago_ctx *c, int nterm) {
   return rc;
 }
 
+int launch_prim3c_sched(imago_ctx *c, const DevSys &s, const DevWork &w,
+                        const Term3c *terms, int nterm, bool nuclear, double *blk,
+                        cudaStream_t st) {
+  if (c->sched)
+    return launch_prim3c_queue(s, w, c->cls_beg, terms, nterm, nuclear, blk,
+                               c->d_queue.p + c->lane, c->queue_ctas, st);
+  return launch_prim3c(s, w, c->cls_beg, terms, nterm, nuclear, blk, st);
+}
+
+// The three-centre schedule is picked by measurement, as the phase-sum
+// width: on the context's first EP build each schedule runs once on the
+// real terms (both write the same blocks) and the faster is kept.
+int tune_sched(imago_ctx *c, const DevSys &s, const DevWork &w, const Term3c *terms,
+               int nterm, double *blk, cudaStream_t st) {
+  cudaEvent_t e[3];
+  for (auto &x : e)
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_CUDA;
+    }
+  int rc = IMAGO_OK;
+  cudaEventRecord(e[0], st);
+  for (int k = 0; k < 2 && !rc; ++k) {
+    c->sched = k;
+    rc = launch_prim3c_sched(c, s, w, terms, nterm, false, blk, st);
+    cudaEventRecord(e[k + 1], st);
+  }
+  if (!rc && cudaEventSynchronize(e[2]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  for (int k = 0; k < 2 && !rc; ++k) cudaEventElapsedTime(&c->sched_ms[k], e[k], e[k + 1]);
+  for (auto &x : e) cudaEventDestroy(x);
+  cudaGetLastError();
+  c->sched = (!rc && c->sched_ms[1] < c->sched_ms[0]) ? 1 : 0;
+  c->launches += class_launches(c) + 1;
+  c->sched_tuned = !rc;
+  return rc;
+}
+
 int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
               double *packed_dev) {
   cudaStream_t st = c->cur();
@@ -1021,10 +1075,12 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   } else if (kind == KIND_MM || kind == KIND_DM) {
     rc = launch_prim2c_vec(s, w, c->cls_beg, kind == KIND_DM, c->dip_center, S.blk.p, st);
   } else if (kind == KIND_NP) {
-    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p, 1, true, S.blk.p, st);
+    rc = launch_prim3c_sched(c, s, w, c->d_terms.p, 1, true, S.blk.p, st);
   } else {
-    rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + term0, nterm, false,
-                       S.blk.p, st);
+    if (c->sched_mode < 0 && !c->sched_tuned && !c->capturing)
+      rc = tune_sched(c, s, w, c->d_terms.p + term0, nterm, S.blk.p, st);
+    if (!rc)
+      rc = launch_prim3c_sched(c, s, w, c->d_terms.p + term0, nterm, false, S.blk.p, st);
   }
   if (rc) return rc;
   mark(c);
@@ -1862,6 +1918,25 @@ int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) 
   if (bloch_width) *bloch_width = c->work.bw;
   if (trial_ms)
     for (int i = 0; i < kNumBlochWidths; ++i) trial_ms[i] = c->bloch_ms[i];
+  return IMAGO_OK;
+}
+
+int imago_intg_set_schedule(imago_ctx *c, int mode) {
+  if (!c || mode < -1 || mode > 1) return IMAGO_ERR_INVALID;
+  if (c->gexec) {  // a captured graph keeps the launches it was captured with
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  c->sched_mode = mode;
+  if (mode >= 0) c->sched = mode;
+  return IMAGO_OK;
+}
+
+int imago_intg_schedule(const imago_ctx *c, int *schedule, double trial_ms[2]) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (schedule) *schedule = c->sched;
+  if (trial_ms)
+    for (int i = 0; i < 2; ++i) trial_ms[i] = c->sched_ms[i];
   return IMAGO_OK;
 }
 

@@ -158,6 +158,24 @@ int launch_ortho_full(const DevSys &s, const double2 *vv, const double2 *cv,
 int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,
                       bool dipole, const double center[3], double *blk,
                       cudaStream_t st);
+// The classes of one three-centre build in work-queue order: class code
+// la * 4 + lb, first entry of its shell-pair list, count, and the first
+// queue item of each class (off[ncls] is the total).
+struct Prim3cQueue {
+  int ncls;
+  int cls[16], beg[16], n[16];
+  long long off[17];
+};
+
+// All classes of a three-centre build in one persistent launch of `ctas`
+// CTAs fed by a device counter (8 bytes at `counter`, zeroed here on the
+// stream before the launch).
+int launch_prim3c_queue(const DevSys &s, const DevWork &w, const int *cls_beg,
+                        const Term3c *terms_dev, int nterm, bool nuclear, double *blk,
+                        unsigned long long *counter, int ctas, cudaStream_t st);
+// CTAs of k_prim3c_queue resident per SM.
+int prim3c_queue_ctas_per_sm();
+
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
                   double *blk, cudaStream_t st);

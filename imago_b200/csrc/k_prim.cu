@@ -74,13 +74,13 @@ __global__ void __launch_bounds__(128)
 // site within threeAlphaDist of the overlap centre, in |R| order.
 // Registers: four CTAs per SM up to d-p (a few bytes of spill for d-p),
 // three for d-d, whose Hermite accumulator alone holds 35 doubles.
+// One item g < n * nterm of class (LA, LB): term g / n, shell pair g % n of
+// the class's list.  Shared by the per-class launches and the work queue.
 template <int LA, int LB, bool NUC>
-__global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
-    k_prim3c(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
-             int nterm, double *blk) {
+__device__ __forceinline__ void prim3c_item(const DevSys &s, const DevWork &w, int beg,
+                                            int n, const Term3c *terms, double *blk,
+                                            long long g) {
   constexpr int L = LA + LB;
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (long long)n * nterm) return;
   const int tl = (int)(g / n);
   const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
   const SpGeom q = sp_geom(s, w, sp);
@@ -166,6 +166,15 @@ __global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
   const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
   hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q,
                         blk + (long long)tl * w.blk_total + sp.boff);
+}
+
+template <int LA, int LB, bool NUC>
+__global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
+    k_prim3c(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
+             int nterm, double *blk) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * nterm) return;
+  prim3c_item<LA, LB, NUC>(s, w, beg, n, terms, blk, g);
 }
 
 // The potential terms of the PSCF Hamiltonian (gaussOverlapHamPSCF,
@@ -328,12 +337,10 @@ __global__ void __launch_bounds__(128)
 }
 
 template <bool NUC>
-__global__ void __launch_bounds__(128)
-    k_prim3c_rt(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
-                int nterm, int la, int lb, double *blk) {
+__device__ __noinline__ void prim3c_item_rt(const DevSys &s, const DevWork &w, int beg,
+                                            int n, const Term3c *terms, int la, int lb,
+                                            double *blk, long long g) {
   const int L = la + lb;
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (long long)n * nterm) return;
   const int tl = (int)(g / n);
   const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
   const SpGeom q = sp_geom(s, w, sp);
@@ -412,6 +419,63 @@ __global__ void __launch_bounds__(128)
   const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
   hermite_to_sh_rt(la, lb, q.A, q.B, q.a1, q.a2, pref, Q,
                    blk + (long long)tl * w.blk_total + sp.boff);
+}
+
+template <bool NUC>
+__global__ void __launch_bounds__(128)
+    k_prim3c_rt(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
+                int nterm, int la, int lb, double *blk) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * nterm) return;
+  prim3c_item_rt<NUC>(s, w, beg, n, terms, la, lb, blk, g);
+}
+
+// ------------------------------------------------------- work queue --
+// Every class of a three-centre build in one persistent launch: the items
+// of all classes are numbered one after another, the classes ordered by
+// their per-item cost (highest angular momentum first) so that the cheap
+// classes fill in behind the expensive ones, and each warp takes the next
+// 32 items with one atomicAdd on a counter the host zeroes before the
+// launch.  A warp's 32 items are consecutive items of one class (or of two
+// at a class boundary), the same groups the per-class launches form, and
+// every item writes only its own output block, so the results equal the
+// per-class launches bit for bit.  No warp waits on another: a warp leaves
+// as soon as the counter has passed the last item.
+template <int LA, int LB, bool NUC>
+__device__ __noinline__ void prim3c_item_q(const DevSys &s, const DevWork &w, int beg, int n,
+                                           const Term3c *terms, double *blk, long long g) {
+  prim3c_item<LA, LB, NUC>(s, w, beg, n, terms, blk, g);
+}
+
+template <bool NUC>
+__global__ void __launch_bounds__(128, 3)
+    k_prim3c_queue(DevSys s, DevWork w, Prim3cQueue qc, const Term3c *terms, double *blk,
+                   unsigned long long *counter) {
+  const int lane = threadIdx.x & 31;
+  const long long total = qc.off[qc.ncls];
+  while (true) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ULL);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((long long)base >= total) return;
+    const long long item = (long long)base + lane;
+    if (item >= total) continue;
+    int c = 0;
+    while (item >= qc.off[c + 1]) ++c;
+    const long long g = item - qc.off[c];
+    const int beg = qc.beg[c], n = qc.n[c];
+    switch (qc.cls[c]) {
+#define IMAGO_QC(a, b)                                                 \
+  case a * 4 + b:                                                      \
+    prim3c_item_q<a, b, NUC>(s, w, beg, n, terms, blk, g);             \
+    break;
+      IMAGO_QC(0, 0) IMAGO_QC(0, 1) IMAGO_QC(0, 2) IMAGO_QC(1, 0) IMAGO_QC(1, 1)
+      IMAGO_QC(1, 2) IMAGO_QC(2, 0) IMAGO_QC(2, 1) IMAGO_QC(2, 2)
+#undef IMAGO_QC
+      default:
+        prim3c_item_rt<NUC>(s, w, beg, n, terms, qc.cls[c] / 4, qc.cls[c] % 4, blk, g);
+    }
+  }
 }
 
 template <int LA, int LB>
@@ -606,6 +670,60 @@ int launch_prim_kov(const DevSys &s, const DevWork &w, const int *cls_beg,
     IMAGO_CUDA(cudaGetLastError());
   }
   return IMAGO_OK;
+}
+
+int launch_prim3c_queue(const DevSys &s, const DevWork &w, const int *cls_beg,
+                        const Term3c *terms_dev, int nterm, bool nuclear, double *blk,
+                        unsigned long long *counter, int ctas, cudaStream_t st) {
+  if (nterm <= 0) return IMAGO_OK;
+  Prim3cQueue qc{};
+  // highest l_a + l_b first, then the larger l_a
+  int order[16], m = 0;
+  for (int L = 6; L >= 0; --L)
+    for (int la = 3; la >= 0; --la) {
+      const int lb = L - la;
+      if (lb < 0 || lb > 3) continue;
+      order[m++] = la * 4 + lb;
+    }
+  long long off = 0;
+  for (int i = 0; i < m; ++i) {
+    const int c = order[i];
+    const int n = cls_beg[c + 1] - cls_beg[c];
+    if (n <= 0) continue;
+    qc.cls[qc.ncls] = c;
+    qc.beg[qc.ncls] = cls_beg[c];
+    qc.n[qc.ncls] = n;
+    qc.off[qc.ncls] = off;
+    off += (long long)n * nterm;
+    ++qc.ncls;
+  }
+  qc.off[qc.ncls] = off;
+  if (off == 0) return IMAGO_OK;
+  IMAGO_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+  const long long need = (off + 127) / 128;
+  const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(ctas, need));
+  if (nuclear)
+    k_prim3c_queue<true><<<grid, 128, 0, st>>>(s, w, qc, terms_dev, blk, counter);
+  else
+    k_prim3c_queue<false><<<grid, 128, 0, st>>>(s, w, qc, terms_dev, blk, counter);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
+int prim3c_queue_ctas_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_prim3c_queue<false>, 128, 0) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  int m = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_prim3c_queue<true>, 128, 0) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return std::max(1, n);
+  }
+  return std::max(1, std::min(n, m));
 }
 
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,

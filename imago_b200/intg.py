@@ -100,6 +100,10 @@ def lib():
         L.imago_intg_set_serial.restype = ctypes.c_int
         L.imago_intg_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         L.imago_intg_tuning.restype = ctypes.c_int
+        L.imago_intg_set_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.imago_intg_set_schedule.restype = ctypes.c_int
+        L.imago_intg_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
+        L.imago_intg_schedule.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
         L.imago_intg_build_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint,
@@ -326,6 +330,22 @@ class IntegralSetup:
         if hasattr(out, "data_ptr"):
             return ctypes.cast(ctypes.c_void_p(out.data_ptr()), _D)
         return _p(out)
+
+    def set_schedule(self, mode):
+        """How the three-centre primitive stage schedules its classes
+        (imago_intg_set_schedule): "auto" (both measured on the first EP
+        build, the faster kept), "per_class" (one launch per class) or
+        "queue" (one persistent launch fed by a device work queue)."""
+        m = {"auto": -1, "per_class": 0, "queue": 1}[mode]
+        _check(lib().imago_intg_set_schedule(self._ctx, m), "imago_intg_set_schedule")
+
+    def schedule(self):
+        """{"schedule": "per_class" | "queue", "trial_ms": [per class, queue]}"""
+        s = ctypes.c_int()
+        ms = np.zeros(2)
+        _check(lib().imago_intg_schedule(self._ctx, ctypes.byref(s), _p(ms)),
+               "imago_intg_schedule")
+        return {"schedule": ("per_class", "queue")[s.value], "trial_ms": ms.tolist()}
 
     def set_ham_mode(self, mode):
         """How ham_pscf sums the potential terms (imago_intg_set_ham_mode):

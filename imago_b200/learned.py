@@ -345,6 +345,11 @@ def compare(system, learned, params=None, device=0):
             "integrals_s": t_int, "setup_s": t_setup}
 
 
+def _plain(x):
+    """numpy scalars and arrays as JSON values."""
+    return x.tolist() if hasattr(x, "tolist") else float(x)
+
+
 def main(argv=None):
     """python -m imago_b200.learned train|evaluate ...
 
@@ -399,12 +404,12 @@ def main(argv=None):
                 "plain_loop_s": r["plain"]["timings"]["loop_s"],
                 "learned_loop_s": r["learned"]["timings"]["loop_s"],
                 "plain_deltas": r["plain"]["deltas"], "learned_deltas": r["learned"]["deltas"]}
-            log(json.dumps({name: out[name]}))
+            log(json.dumps({name: out[name]}, default=_plain))
         rec = out
     if args.record:
         with open(args.record, "w") as fh:
-            json.dump(rec, fh, indent=1, default=float)
-    print(json.dumps(rec, default=float))
+            json.dump(rec, fh, indent=1, default=_plain)
+    print(json.dumps(rec, default=_plain))
 
 
 def test_system(name, kmesh=(4, 4, 4), seed=21):

@@ -403,6 +403,19 @@ IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
 IMAGO_API int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
                                    double *vec, void *stream);
 
+/* No counterpart: how the three-centre primitive stage of NP and EP
+ * schedules its shell-pair classes.  mode 0: one launch per class
+ * (k_prim3c<la, lb>); mode 1: all classes in one persistent launch whose
+ * warps take 32 items at a time from a device work queue (one atomic
+ * counter), the classes ordered by cost so that the cheap ones fill in
+ * behind the expensive ones; mode -1 (the default): both run once on the
+ * context's first EP build and the faster is kept.  The results are the
+ * same bit for bit.  A captured graph of the context is dropped. */
+IMAGO_API int imago_intg_set_schedule(imago_ctx *ctx, int mode);
+/* The schedule in use (0 per class, 1 work queue) and the trial times of
+ * the measurement (ms, per class then work queue; zero when not measured). */
+IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double trial_ms[2]);
+
 /* No counterpart in the reference.  The builds of one call run each kind
  * (OL, KE, NP, EP) on a stream of its own, concurrently; serial != 0 runs
  * them one after another on the context's stream instead, which gives each

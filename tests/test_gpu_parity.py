@@ -671,3 +671,28 @@ def test_driver_matches_reference_driver_executed(imago_lib):
                  "KE": packed_mismatch(ke, g["ke_packed"]),
                  "CVre": packed_mismatch(cre, g["ol_cv_re"]),
                  "CVim": packed_mismatch(cim, g["ol_cv_im"])})
+
+
+@pytest.mark.parametrize("make", [configs.small_test_system, configs.f_test_system,
+                                  lambda: configs.silicon_cubic8(kmesh=(2, 2, 2))])
+def test_work_queue_schedule_equals_per_class_launches(imago_lib, make):
+    # the persistent work-queue launch of the three-centre stage computes
+    # every item as the per-class launches do and writes the same blocks:
+    # NP and every EP term bit for bit, and the measured choice is one of
+    # the two
+    s = make()
+    out = {}
+    for mode in ("per_class", "queue", "auto"):
+        with intg.IntegralSetup(s) as g:
+            g.set_schedule(mode)
+            g.gauss_overlap_ol()
+            out[mode] = (g.gauss_overlap_np(), g.elec_pot_gauss_overlap())
+            sch = g.schedule()
+        if mode == "auto":
+            assert sch["schedule"] in ("per_class", "queue")
+            assert min(sch["trial_ms"]) > 0.0
+        else:
+            assert sch["schedule"] == mode
+    for mode in ("queue", "auto"):
+        assert np.array_equal(out[mode][0], out["per_class"][0])
+        assert np.array_equal(out[mode][1], out["per_class"][1])
