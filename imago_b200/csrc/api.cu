@@ -185,6 +185,12 @@ struct imago_ctx {
   bool sched_tuned = false;
   float sched_ms[2] = {};
   int queue_ctas = 0;
+  // orthogonalisation of multi-term builds: per-(k, term) CTAs (0) or the
+  // persistent TMA-fed kernel (1); mode -1 measures both on the first
+  // EP build
+  int ortho_mode = -1, ortho = 0;
+  bool ortho_tuned = false;
+  float ortho_ms[2] = {};
   long long blk_total = 0, m_total = 0;
   std::vector<Term3c> ep_terms;
 
@@ -202,6 +208,7 @@ struct imago_ctx {
   DBuf<DSp> d_sps;
   DBuf<Term3c> d_terms;
   DBuf<unsigned long long> d_queue;  // one work-queue counter per lane
+  DBuf<int> d_flag;                  // DevSys::flag
   DBuf<int2> d_btile, d_btile_w;
   DBuf<SiteImage> d_simg;
   DBuf<float> d_cl_d1;
@@ -284,6 +291,7 @@ struct imago_ctx {
     d_btile_w.release(st);
     d_cl_d1.release(st);
     d_queue.release(st);
+    d_flag.release(st);
     if (st) cudaStreamSynchronize(st);
     if (events)
       for (auto &e : ev) cudaEventDestroy(e);
@@ -850,6 +858,8 @@ int upload(imago_ctx *c) {
   UP(d_btile, c->btile) UP(d_btile_w, c->btile_w)
 #undef UP
   if ((rc = c->d_queue.alloc(4, st))) return rc;
+  if ((rc = c->d_flag.alloc(1, st))) return rc;
+  IMAGO_CUDA(cudaMemsetAsync(c->d_flag.p, 0, sizeof(int), st));
   {
     int nsm = 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
@@ -884,6 +894,7 @@ int upload(imago_ctx *c) {
   s.psite_pos = c->d_psite_pos.p; s.psite_ptype = c->d_psite_ptype.p;
   s.cell = c->d_cell.p; s.csize = c->d_csize.p; s.kxyz = c->d_kxyz.p;
   s.phase = c->d_phase.p;
+  s.flag = c->d_flag.p;
   DevWork &w = c->work;
   w.npairs = (int)c->pairs.size();
   w.nunits = (int)c->units.size();
@@ -1051,6 +1062,35 @@ int tune_sched(imago_ctx *c, const DevSys &s, const DevWork &w, const Term3c *te
   return rc;
 }
 
+// The orthogonalisation of a multi-term build is picked by measurement
+// too: on the context's first EP build both kernels run once on the real
+// blocks (they write the same packed output) and the faster is kept.
+int tune_ortho(imago_ctx *c, const DevSys &s, int nterm, double *packed_dev,
+               cudaStream_t st) {
+  imago_ctx::Scratch &S = c->scr[c->lane];
+  cudaEvent_t e[3];
+  for (auto &x : e)
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_CUDA;
+    }
+  int rc = IMAGO_OK;
+  cudaEventRecord(e[0], st);
+  for (int m = 0; m < 2 && !rc; ++m) {
+    rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p, packed_dev, st,
+                      m == 1);
+    cudaEventRecord(e[m + 1], st);
+  }
+  if (!rc && cudaEventSynchronize(e[2]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  for (int m = 0; m < 2 && !rc; ++m) cudaEventElapsedTime(&c->ortho_ms[m], e[m], e[m + 1]);
+  for (auto &x : e) cudaEventDestroy(x);
+  cudaGetLastError();
+  c->ortho = (!rc && c->ortho_ms[1] < c->ortho_ms[0]) ? 1 : 0;
+  c->launches += 2;
+  c->ortho_tuned = !rc;
+  return rc;
+}
+
 int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
               double *packed_dev) {
   cudaStream_t st = c->cur();
@@ -1105,9 +1145,14 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   if (kind == KIND_DM)
     rc = launch_ortho_general(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
                               packed_dev, st);
-  else
-    rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p,
-                      packed_dev, st);
+  else {
+    const bool multi = kind == KIND_EP && nterm > 1 && ortho_pipe_fits(c->core_dim, c->vale_dim);
+    if (multi && c->ortho_mode < 0 && !c->ortho_tuned && !c->capturing)
+      rc = tune_ortho(c, s, nterm, packed_dev, st);
+    if (!rc)
+      rc = launch_ortho(s, nterm, S.vv.p, S.cv.p, S.cc.p, c->s_cv.p, S.y.p, packed_dev, st,
+                        multi && c->ortho == 1);
+  }
   mark(c);
   return rc;
 }
@@ -1426,6 +1471,14 @@ int finish(imago_ctx *c, int rc) {
   for (cudaStream_t k : c->kst)
     if (k) IMAGO_CUDA(cudaStreamSynchronize(k));
   if (c->copy_stream) IMAGO_CUDA(cudaStreamSynchronize(c->copy_stream));
+  if (c->d_flag.p && c->ortho == 1) {  // the only kernel with device waits
+    int f = 0;
+    IMAGO_CUDA(cudaMemcpy(&f, c->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) {
+      IMAGO_CUDA(cudaMemset(c->d_flag.p, 0, sizeof(int)));
+      return f;
+    }
+  }
   for (int k = 0; k < 4; ++k) c->kernel_ms[k] = 0.0;
   for (int b = 0; b + 4 < c->kev_used; b += 5)
     for (int k = 0; k < 4; ++k) {
@@ -1937,6 +1990,25 @@ int imago_intg_schedule(const imago_ctx *c, int *schedule, double trial_ms[2]) {
   if (schedule) *schedule = c->sched;
   if (trial_ms)
     for (int i = 0; i < 2; ++i) trial_ms[i] = c->sched_ms[i];
+  return IMAGO_OK;
+}
+
+int imago_intg_set_ortho_schedule(imago_ctx *c, int mode) {
+  if (!c || mode < -1 || mode > 1) return IMAGO_ERR_INVALID;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  c->ortho_mode = mode;
+  if (mode >= 0) c->ortho = mode;
+  return IMAGO_OK;
+}
+
+int imago_intg_ortho_schedule(const imago_ctx *c, int *schedule, double trial_ms[2]) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (schedule) *schedule = c->ortho;
+  if (trial_ms)
+    for (int i = 0; i < 2; ++i) trial_ms[i] = c->ortho_ms[i];
   return IMAGO_OK;
 }
 

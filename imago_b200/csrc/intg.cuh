@@ -45,6 +45,9 @@ struct DevSys {
   const double *csize;    // [n]
   const double *kxyz;     // [nk*3]
   const double2 *phase;   // [cell * nk + k]  exp(i k.R)
+  // device status word: a kernel whose bounded wait ran out records
+  // IMAGO_ERR_TIMEOUT here (first failure wins); read after each call
+  int *flag;
 };
 
 // Atom pair (i <= j) that passes the nearest-image screen.
@@ -183,9 +186,12 @@ int launch_contract(const DevSys &s, const DevWork &w, int nterm,
                     const double *blk, double *M, cudaStream_t st);
 int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
                  double2 *vv, double2 *cv, double2 *cc, cudaStream_t st);
+// pipe: the persistent TMA-fed kernel where it applies (several terms,
+// S and two X_cv buffers in shared memory), the per-(k, term) CTAs else.
 int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  const double2 *cv, const double2 *cc, const double2 *s_cv,
-                 double2 *y, double *packed, cudaStream_t st);
+                 double2 *y, double *packed, cudaStream_t st, bool pipe = false);
+bool ortho_pipe_fits(int C, int V);
 // The same for a matrix whose core-core block is not Hermitian (dipole):
 // the reference's zher2k-then-makeValeVale sequence as it stands.
 int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,

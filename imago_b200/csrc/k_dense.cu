@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "intg.cuh"
+#include "tma.cuh"
 
 namespace imago {
 
@@ -859,6 +860,397 @@ __global__ void __launch_bounds__(kFThreads, 1)
   }
 }
 
+// ----------------------------------------------------- ortho, piped --
+// The fused orthogonalisation for builds of several terms as a persistent
+// kernel: one CTA per SM walks a contiguous range of (k, term) items in
+// k-major order.  S(k) stays in shared memory while k is unchanged, and
+// X_cv of the next item comes in by one TMA tensor copy (completing on an
+// mbarrier) into the second of two buffers while the current item's Y and
+// W are formed, so the fill hides behind the tensor-core work.  X_cc is
+// read from L2 by the Y step's fragments.  Shared arrays keep the global
+// layout, core index fastest, in rows of ld complex values with
+// ld = 4 mod 8: the TMA box writes them as they are (its columns beyond C
+// zero-filled), and the fragment reads of a quarter warp (two rows, four
+// k) fall on distinct banks.  Rows v >= V are not stored; their fragments
+// read zero.
+struct PipeDims {
+  int C4, C16, V16, ld;
+  size_t buf;  // bytes of one V x ld array, a multiple of 128
+};
+
+__host__ __device__ inline PipeDims pipe_dims(int C, int V) {
+  PipeDims d;
+  d.C4 = (C + 3) / 4 * 4;
+  d.C16 = (C + 15) / 16 * 16;
+  d.V16 = (V + 15) / 16 * 16;
+  d.ld = d.C4 % 8 == 0 ? d.C4 + 4 : d.C4;
+  d.buf = ((size_t)V * d.ld * sizeof(double2) + 127) / 128 * 128;
+  return d;
+}
+
+// dynamic shared memory of k_ortho_pipe at most: 227 KB less room for its
+// static shared state
+constexpr size_t kPipeMaxSmem = 227 * 1024 - 1024;
+
+inline size_t pipe_smem(int C, int V) { return 3 * pipe_dims(C, V).buf + 64; }
+
+bool ortho_pipe_fits(int C, int V) {
+  const PipeDims d = pipe_dims(C, V);
+  return C > 0 && V > 0 && V <= 256 && 2 * d.ld <= 256 && pipe_smem(C, V) <= kPipeMaxSmem;
+}
+
+// One warp's 16x16 complex subtile of op(A)^T B over k in [0, nk4), A and B
+// stored [index][k] with row stride ld; rows at or beyond na (A) or nb (B)
+// read as zero.  3M form as fused_tile.
+template <bool CONJ, bool REAL>
+__device__ __forceinline__ void pipe_tile(const double2 *A, int na, int r0, const double2 *B,
+                                          int nb, int c0, int ld, int nk4, bool skip_lower,
+                                          double t1[2][2][2], double t2[2][2][2],
+                                          double t3[2][2][2], int lane) {
+  const int ra0 = r0 + (lane >> 2), cb0 = c0 + (lane >> 2);
+  const bool va[2] = {ra0 < na, ra0 + 8 < na}, vb[2] = {cb0 < nb, cb0 + 8 < nb};
+  const double2 *pa[2] = {A + (long long)ra0 * ld, A + (long long)(ra0 + 8) * ld};
+  const double2 *pb[2] = {B + (long long)cb0 * ld, B + (long long)(cb0 + 8) * ld};
+  for (int ks = 0; ks < nk4; ks += 4) {
+    const int kk = ks + (lane & 3);
+    double2 a[2], b[2];
+    double as[2], bs[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      a[t] = va[t] ? pa[t][kk] : make_double2(0.0, 0.0);
+      b[t] = vb[t] ? pb[t][kk] : make_double2(0.0, 0.0);
+      as[t] = CONJ ? a[t].x - a[t].y : a[t].x + a[t].y;
+      bs[t] = b[t].x + b[t].y;
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        if (skip_lower && mt > nt) continue;
+        dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        if (REAL) continue;
+        dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
+        dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
+      }
+  }
+}
+
+// The Y step's product X_cc S: A(l, c) = X_cc(c, l) = XC[l * C + c] from
+// global memory (L2), B(l, v) = S(l, v) from the shared [v][l] array.
+template <bool REAL>
+__device__ __forceinline__ void pipe_y_tile(const double2 *__restrict__ XC, int C, int r0,
+                                            const double2 *S, int V, int c0, int ld, int nk4,
+                                            double t1[2][2][2], double t2[2][2][2],
+                                            double t3[2][2][2], int lane) {
+  const int ra0 = r0 + (lane >> 2), cb0 = c0 + (lane >> 2);
+  const bool vb[2] = {cb0 < V, cb0 + 8 < V};
+  const double2 *pb[2] = {S + (long long)cb0 * ld, S + (long long)(cb0 + 8) * ld};
+  for (int ks = 0; ks < nk4; ks += 4) {
+    const int kk = ks + (lane & 3);
+    double2 a[2], b[2];
+    double as[2], bs[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int c = ra0 + 8 * t;
+      a[t] = (c < C && kk < C) ? __ldg(XC + (long long)kk * C + c) : make_double2(0.0, 0.0);
+      b[t] = vb[t] ? pb[t][kk] : make_double2(0.0, 0.0);
+      as[t] = a[t].x + a[t].y;
+      bs[t] = b[t].x + b[t].y;
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
+        if (REAL) continue;
+        dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
+        dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
+      }
+  }
+}
+
+// What every thread of a k_ortho_pipe CTA reads (kept in shared memory,
+// written once by thread 0).
+struct PipeCta {
+  const double2 *vv, *cc;
+  double *packed;
+  double2 *Ss, *Xb[2];
+  uint64_t *bar;       // S, X buffer 0, X buffer 1
+  int *ctr;            // task counters, one per phase parity
+  int V, C, nk, nterm, ld, C4, nup, ny, yr;
+  long long np, i0;
+};
+
+// One W tile (J <= I, the upper 16x16 subtiles of S^H Y + Y^H S) of item q:
+// subtracted from VV and packed.
+template <bool REAL>
+__device__ __forceinline__ void pipe_w_task(const PipeCta &p, long long q, int tile, int lane) {
+  const int V = p.V;
+  const long long tk = (long long)(q % p.nterm) * p.nk + q / p.nterm;
+  const double2 *Ys = p.Xb[(q - p.i0) & 1];
+  const double2 *VVt = p.vv + tk * V * V;
+  double *out = p.packed + 2 * tk * p.np;
+  int t = tile, I = 0;
+  while (t > I) {
+    t -= I + 1;
+    ++I;
+  }
+  const int J = t, r0 = J * 16, c0 = I * 16;
+  // VV is read in the epilogue: other warps' products cover its latency
+  double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
+  pipe_tile<true, REAL>(p.Ss, V, r0, Ys, V, c0, p.ld, p.C4, J == I, t1, t2, t3, lane);
+  pipe_tile<true, REAL>(Ys, V, r0, p.Ss, V, c0, p.ld, p.C4, J == I, t1, t2, t3, lane);
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int row = r0 + 8 * mt + (lane >> 2);
+        const int col = c0 + 8 * nt + 2 * (lane & 3) + e;
+        if (row >= V || col >= V || row > col) continue;
+        double2 v = VVt[(long long)col * V + row];
+        const double2 d = ocombine<true, REAL>(t1[mt][nt][e], t2[mt][nt][e], t3[mt][nt][e]);
+        v.x -= d.x;
+        v.y -= d.y;
+        if (row == col) v.y = 0.0;
+        if (fabs(v.x) < kPackThresh) v.x = 0.0;
+        if (fabs(v.y) < kPackThresh) v.y = 0.0;
+        store_packed(out, (long long)col * (col + 1) / 2 + row, v);
+      }
+}
+
+// One Y tile (16 core x 16 valence) of item q: Y = X_cv - X_cc S / 2 in place.
+template <bool REAL>
+__device__ __forceinline__ void pipe_y_task(const PipeCta &p, long long q, int tile, int lane) {
+  const int C = p.C, V = p.V;
+  const long long tk = (long long)(q % p.nterm) * p.nk + q / p.nterm;
+  double2 *Ys = p.Xb[(q - p.i0) & 1];
+  const double2 *XC = p.cc + tk * C * C;
+  const int r0 = (tile % p.yr) * 16, c0 = (tile / p.yr) * 16;
+  double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
+  pipe_y_tile<REAL>(XC, C, r0, p.Ss, V, c0, p.ld, p.C4, t1, t2, t3, lane);
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = r0 + 8 * mt + (lane >> 2);
+        const int v = c0 + 8 * nt + 2 * (lane & 3) + e;
+        if (c >= C || v >= V) continue;
+        const double2 d = ocombine<false, REAL>(t1[mt][nt][e], t2[mt][nt][e], t3[mt][nt][e]);
+        double2 &y = Ys[v * p.ld + c];
+        y.x -= 0.5 * d.x;
+        y.y -= 0.5 * d.y;
+      }
+}
+
+// One phase between two CTA barriers: the W tiles of item wq (wq < 0: none)
+// first, then the Y tiles of item yq (yq < 0: none), handed to warps one
+// tile at a time from the phase's counter so that the two kinds balance.
+// Y tiles wait (bounded) for their item's X_cv copy.  At the start, the
+// counter of the next phase is cleared, and X_cv of item xq (xq < 0: none)
+// is sent for into its buffer, whose last reader ended at the barrier
+// before.  px holds the parity of each X barrier's next completion.
+// False (on every thread) when a copy did not land in time.
+template <bool REAL>
+__device__ __forceinline__ bool pipe_phase(const PipeCta &p, unsigned px[2], int &ph,
+                                           long long wq, long long yq, long long xq,
+                                           const CUtensorMap *map_x) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) {
+    p.ctr[ph ^ 1] = 0;
+    if (xq >= 0) {
+      const int b = (int)((xq - p.i0) & 1);
+      fence_proxy_async();
+      mbar_expect_tx(&p.bar[1 + b], (unsigned)(16 * p.ld) * (unsigned)p.V);
+      tma_load_3d(p.Xb[b], map_x, &p.bar[1 + b], 0, 0,
+                  (int)((xq % p.nterm) * p.nk + xq / p.nterm));
+    }
+  }
+  const int nw = wq >= 0 ? p.nup : 0, ntask = nw + (yq >= 0 ? p.ny : 0);
+  const int yb = yq >= 0 ? (int)((yq - p.i0) & 1) : 0;
+  bool ready = false, fail = false;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = atomicAdd(&p.ctr[ph], 1);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    if (task >= ntask) break;
+    if (task < nw) {
+      pipe_w_task<REAL>(p, wq, task, lane);
+      continue;
+    }
+    if (!ready) {
+      ready = __all_sync(0xffffffffu, mbar_wait_bounded(&p.bar[1 + yb], px[yb]));
+      if (!ready) {
+        fail = true;
+        break;
+      }
+    }
+    pipe_y_task<REAL>(p, yq, task - nw, lane);
+  }
+  ph ^= 1;
+  const bool bad = __syncthreads_or(fail);
+  if (yq >= 0 && !bad) px[yb] ^= 1u;
+  return !bad;
+}
+
+template <bool REAL>
+__global__ void __launch_bounds__(kFThreads, 1)
+    k_ortho_pipe(DevSys s, const __grid_constant__ CUtensorMap map_x,
+                 const __grid_constant__ CUtensorMap map_s, const double2 *vv,
+                 const double2 *cc, int nterm, double *packed) {
+  extern __shared__ __align__(128) unsigned char psm[];
+  const int V = s.vale_dim, C = s.core_dim, nk = s.nk;
+  const PipeDims d = pipe_dims(C, V);
+  const long long N = (long long)nk * nterm;
+  const long long i0 = N * blockIdx.x / gridDim.x, i1 = N * (blockIdx.x + 1) / gridDim.x;
+  if (i0 >= i1) return;
+  __shared__ PipeCta p;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    p.vv = vv;
+    p.cc = cc;
+    p.packed = packed;
+    p.Ss = reinterpret_cast<double2 *>(psm);
+    p.Xb[0] = reinterpret_cast<double2 *>(psm + d.buf);
+    p.Xb[1] = reinterpret_cast<double2 *>(psm + 2 * d.buf);
+    p.bar = reinterpret_cast<uint64_t *>(psm + 3 * d.buf);
+    p.ctr = reinterpret_cast<int *>(p.bar + 3);
+    p.V = V;
+    p.C = C;
+    p.nk = nk;
+    p.nterm = nterm;
+    p.ld = d.ld;
+    p.C4 = d.C4;
+    const int nt16 = d.V16 / 16;
+    p.nup = nt16 * (nt16 + 1) / 2;
+    p.yr = d.C16 / 16;
+    p.ny = p.yr * nt16;
+    p.np = (long long)V * (V + 1) / 2;
+    p.i0 = i0;
+    for (int b = 0; b < 3; ++b) mbar_init(&p.bar[b], 1);
+    p.ctr[0] = p.ctr[1] = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const unsigned tx = (unsigned)(16 * d.ld) * (unsigned)V;
+  unsigned ps = 0, px[2] = {0u, 0u};
+  int ph = 0;
+  int k = (int)(i0 / nterm);
+  if (tid == 0) {
+    mbar_expect_tx(&p.bar[0], tx);
+    tma_load_3d(p.Ss, &map_s, &p.bar[0], 0, 0, k);
+  }
+  // S(k): waited for by every thread; on a timeout the copy in flight gets
+  // one more bounded wait before the CTA leaves
+  auto load_s_wait = [&]() -> bool {
+    const bool ok = mbar_wait_bounded(&p.bar[0], ps);
+    ps ^= 1u;
+    if (!__syncthreads_or(!ok)) return true;
+    if (tid == 0) {
+      report_status(s.flag, IMAGO_ERR_TIMEOUT);
+      mbar_wait_bounded(&p.bar[0], ps ^ 1u);
+    }
+    return false;
+  };
+  bool ok = load_s_wait();
+  // item i0: its Y tiles alone
+  ok = ok && pipe_phase<REAL>(p, px, ph, -1, i0, i0, &map_x);
+  for (long long q = i0 + 1; ok && q < i1; ++q) {
+    const int kq = (int)(q / nterm);
+    if (kq == k) {
+      ok = pipe_phase<REAL>(p, px, ph, q - 1, q, q, &map_x);
+      continue;
+    }
+    // a new k: the previous item's W tiles, then S(kq), then this item's Y
+    ok = pipe_phase<REAL>(p, px, ph, q - 1, -1, q, &map_x);
+    if (!ok) break;
+    k = kq;
+    if (tid == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&p.bar[0], tx);
+      tma_load_3d(p.Ss, &map_s, &p.bar[0], 0, 0, k);
+    }
+    ok = load_s_wait() && pipe_phase<REAL>(p, px, ph, -1, q, -1, &map_x);
+  }
+  if (ok) ok = pipe_phase<REAL>(p, px, ph, i1 - 1, -1, -1, &map_x);
+  if (!ok && tid == 0) {
+    report_status(s.flag, IMAGO_ERR_TIMEOUT);
+    // copies still in flight get one more bounded wait before the CTA leaves
+    for (int b = 0; b < 2; ++b) mbar_wait_bounded(&p.bar[1 + b], px[b]);
+  }
+  __syncthreads();
+}
+
+bool encode_tensor_map_f64_3d(CUtensorMap *map, const void *base, const uint64_t dims[3],
+                              const uint64_t strides[2], const uint32_t box[3]) {
+  using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                              const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                              const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode fn = []() -> Encode {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<Encode>(p);
+  }();
+  if (!fn || ((uintptr_t)base & 15) || (strides[0] & 15) || (strides[1] & 15)) return false;
+  const cuuint64_t gd[3] = {dims[0], dims[1], dims[2]};
+  const cuuint64_t gs[2] = {strides[0], strides[1]};
+  const cuuint32_t bx[3] = {box[0], box[1], box[2]};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), gd, gs, bx, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The piped orthogonalisation when it applies (several terms, the three
+// arrays in shared memory, tensor maps accepted); *launched says whether it
+// ran.
+int launch_ortho_pipe(const DevSys &s, int nterm, const double2 *vv, const double2 *cv,
+                      const double2 *cc, const double2 *s_cv, double *packed, bool *launched,
+                      cudaStream_t st) {
+  *launched = false;
+  const int V = s.vale_dim, C = s.core_dim;
+  if (nterm < 2 || !ortho_pipe_fits(C, V)) return IMAGO_OK;
+  const PipeDims d = pipe_dims(C, V);
+  CUtensorMap mx, ms;
+  const uint64_t dx[3] = {2ull * C, (uint64_t)V, (uint64_t)nterm * s.nk};
+  const uint64_t ds[3] = {2ull * C, (uint64_t)V, (uint64_t)s.nk};
+  const uint64_t str[2] = {16ull * C, 16ull * V * C};
+  const uint32_t box[3] = {2u * d.ld, (uint32_t)V, 1u};
+  if (!encode_tensor_map_f64_3d(&mx, cv, dx, str, box) ||
+      !encode_tensor_map_f64_3d(&ms, s_cv, ds, str, box))
+    return IMAGO_OK;
+  int dev = 0, nsm = 0;
+  IMAGO_CUDA(cudaGetDevice(&dev));
+  IMAGO_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  static bool attr_set[2][64] = {};
+  const size_t smem = pipe_smem(C, V);
+  if (dev >= 0 && dev < 64 && !attr_set[s.real_k][dev]) {
+    IMAGO_CUDA(cudaFuncSetAttribute(s.real_k ? k_ortho_pipe<true> : k_ortho_pipe<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kPipeMaxSmem));
+    attr_set[s.real_k][dev] = true;
+  }
+  const long long N = (long long)nterm * s.nk;
+  const unsigned grid = (unsigned)std::min<long long>(nsm, N);
+  if (s.real_k)
+    k_ortho_pipe<true><<<grid, kFThreads, smem, st>>>(s, mx, ms, vv, cc, nterm, packed);
+  else
+    k_ortho_pipe<false><<<grid, kFThreads, smem, st>>>(s, mx, ms, vv, cc, nterm, packed);
+  IMAGO_CUDA(cudaGetLastError());
+  *launched = true;
+  return IMAGO_OK;
+}
+
 // coreDim == 0: the reference packs valeVale as it is (integrals.F90:3657-3676).
 __global__ void __launch_bounds__(256)
     k_pack_plain(DevSys s, const double2 *vv, double *packed) {
@@ -881,7 +1273,7 @@ __global__ void __launch_bounds__(256)
 
 int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  const double2 *cv, const double2 *cc, const double2 *s_cv,
-                 double2 *y, double *packed, cudaStream_t st) {
+                 double2 *y, double *packed, cudaStream_t st, bool pipe) {
   const int V = s.vale_dim, C = s.core_dim;
   if (nterm == 0) return IMAGO_OK;
   if (C == 0) {
@@ -890,6 +1282,11 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
     k_pack_plain<<<g, 256, 0, st>>>(s, vv, packed);
     IMAGO_CUDA(cudaGetLastError());
     return IMAGO_OK;
+  }
+  if (pipe) {
+    bool launched = false;
+    const int rc = launch_ortho_pipe(s, nterm, vv, cv, cc, s_cv, packed, &launched, st);
+    if (rc || launched) return rc;
   }
   const size_t smem = fused_smem(C, V);
   if (smem <= kFusedMaxSmem) {

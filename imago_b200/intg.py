@@ -104,6 +104,11 @@ def lib():
         L.imago_intg_set_schedule.restype = ctypes.c_int
         L.imago_intg_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), _D]
         L.imago_intg_schedule.restype = ctypes.c_int
+        L.imago_intg_set_ortho_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.imago_intg_set_ortho_schedule.restype = ctypes.c_int
+        L.imago_intg_ortho_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                                _D]
+        L.imago_intg_ortho_schedule.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
         L.imago_intg_build_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint,
@@ -346,6 +351,24 @@ class IntegralSetup:
         _check(lib().imago_intg_schedule(self._ctx, ctypes.byref(s), _p(ms)),
                "imago_intg_schedule")
         return {"schedule": ("per_class", "queue")[s.value], "trial_ms": ms.tolist()}
+
+    def set_ortho_schedule(self, mode):
+        """How EP builds of several terms run the core orthogonalisation
+        (imago_intg_set_ortho_schedule): "auto" (both measured on the first
+        EP build, the faster kept), "per_item" (one CTA per k-point and
+        term) or "piped" (one persistent CTA per SM, the overlap block
+        resident, the next term's block brought in by TMA meanwhile)."""
+        m = {"auto": -1, "per_item": 0, "piped": 1}[mode]
+        _check(lib().imago_intg_set_ortho_schedule(self._ctx, m),
+               "imago_intg_set_ortho_schedule")
+
+    def ortho_schedule(self):
+        """{"schedule": "per_item" | "piped", "trial_ms": [per item, piped]}"""
+        s = ctypes.c_int()
+        ms = np.zeros(2)
+        _check(lib().imago_intg_ortho_schedule(self._ctx, ctypes.byref(s), _p(ms)),
+               "imago_intg_ortho_schedule")
+        return {"schedule": ("per_item", "piped")[s.value], "trial_ms": ms.tolist()}
 
     def set_ham_mode(self, mode):
         """How ham_pscf sums the potential terms (imago_intg_set_ham_mode):

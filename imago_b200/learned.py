@@ -319,14 +319,24 @@ class LearnedStart:
         return out
 
 
+def metric_params():
+    """The SCF settings both starts are measured with: makeinput.py's
+    defaults with the convergence test one decade tighter (1e-5) and the
+    1e-6 Ha energy stop.  At the default 1e-4 the stopped energy of a run
+    still lies up to 3e-6 Ha from its fixed point (measured on the 16- and
+    64-atom Si cells), so two runs that stop there cannot be compared to
+    1e-6 Ha; at 1e-5 both stop within 3e-7 Ha of it."""
+    return scf.ScfParams(convergence_test=1.0e-5)
+
+
 def compare(system, learned, params=None, device=0):
     """Plain start and learned start on one system, integrals and SCF set-up
-    shared and built once (their time is reported apart).  Returns the two
-    runs, the learned start's inference time and whether it is kept (the
-    plain start judges: within 1e-6 Ha of its energy, no more
-    iterations)."""
+    shared and built once (their time is reported apart), with
+    metric_params() unless `params` is given.  Returns the two runs, the
+    learned start's inference time and whether it is kept (the plain start
+    judges: within 1e-6 Ha of its energy, no more iterations)."""
     import torch
-    p = params or scf.ScfParams()
+    p = params or metric_params()
     ints, t_int = scf.device_integrals(system, device)
     t0 = time.perf_counter()
     setup = scf.ScfSetup(system, p, device)

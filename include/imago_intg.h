@@ -416,6 +416,21 @@ IMAGO_API int imago_intg_set_schedule(imago_ctx *ctx, int mode);
  * the measurement (ms, per class then work queue; zero when not measured). */
 IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double trial_ms[2]);
 
+/* No counterpart in the reference (the orthogonalisation of
+ * makeValeVale/coreValeCoreCore, intgOrtho.F90:23-213, as scheduled on the
+ * GPU).  For EP builds of several terms whose overlap blocks fit in shared
+ * memory, mode 1 runs the persistent kernel that keeps S(k) resident and
+ * brings each term's core-valence block in by TMA while the previous one
+ * is reduced, mode 0 one CTA per (k, term); -1 (the default) times both on
+ * the first EP build and keeps the faster.  Results are identical.  A
+ * copy that does not land within its bound (1 s) makes the call return
+ * IMAGO_ERR_TIMEOUT. */
+IMAGO_API int imago_intg_set_ortho_schedule(imago_ctx *ctx, int mode);
+/* The orthogonalisation schedule in use (0 or 1) and the trial times of the
+ * measurement (ms, mode 0 then mode 1; zero when not measured). */
+IMAGO_API int imago_intg_ortho_schedule(const imago_ctx *ctx, int *schedule,
+                                        double trial_ms[2]);
+
 /* No counterpart in the reference.  The builds of one call run each kind
  * (OL, KE, NP, EP) on a stream of its own, concurrently; serial != 0 runs
  * them one after another on the context's stream instead, which gives each

@@ -659,7 +659,8 @@ def test_koverlap_at_zero_wave_vector_is_the_overlap_quartz(imago_lib):
 def test_driver_matches_reference_driver_executed(imago_lib):
     # the reference's own integral driver, executed statement for statement
     # (tests/golden/make_driver_golden.py: gaussOverlapOL / orthoOL,
-    # gaussOverlapKE / ortho with every routine they call) on the diamond
+    # gaussOverlapKE, gaussOverlapNP and elecPotGaussOverlap with every
+    # routine they call, and the orthogonalisations) on the diamond
     # primitive cell at 2x2x2 k
     import os
     from conftest import ROOT
@@ -667,10 +668,16 @@ def test_driver_matches_reference_driver_executed(imago_lib):
     with intg.IntegralSetup(configs.diamond_primitive(kmesh=(2, 2, 2))) as s:
         ol, cre, cim = s.gauss_overlap_ol()
         ke = s.gauss_overlap_ke()
+        npk = s.gauss_overlap_np()
+        ep = s.elec_pot_gauss_overlap()
+    assert ep.shape == g["ep_packed"].shape
     _assert_all({"OL": packed_mismatch(ol, g["ol_packed"]),
                  "KE": packed_mismatch(ke, g["ke_packed"]),
+                 "NP": packed_mismatch(npk, g["np_packed"]),
                  "CVre": packed_mismatch(cre, g["ol_cv_re"]),
-                 "CVim": packed_mismatch(cim, g["ol_cv_im"])})
+                 "CVim": packed_mismatch(cim, g["ol_cv_im"]),
+                 **{f"EP{t}": packed_mismatch(ep[t], g["ep_packed"][t])
+                    for t in range(ep.shape[0])}})
 
 
 @pytest.mark.parametrize("make", [configs.small_test_system, configs.f_test_system,
@@ -696,3 +703,27 @@ def test_work_queue_schedule_equals_per_class_launches(imago_lib, make):
     for mode in ("queue", "auto"):
         assert np.array_equal(out[mode][0], out["per_class"][0])
         assert np.array_equal(out[mode][1], out["per_class"][1])
+
+
+@pytest.mark.parametrize("make", [configs.small_test_system,
+                                  lambda: configs.silicon_cubic8(kmesh=(2, 2, 2)),
+                                  lambda: configs.silicon_cubic8(kmesh=(1, 1, 1))])
+def test_piped_orthogonalisation_equals_per_item(imago_lib, make):
+    # the persistent TMA-fed orthogonalisation of EP builds forms the same
+    # products in the same order as the per-(k, term) kernel: every packed
+    # element equal, at general k and at Gamma (real arithmetic)
+    s = make()
+    out = {}
+    for mode in ("per_item", "piped", "auto"):
+        with intg.IntegralSetup(s) as g:
+            g.set_ortho_schedule(mode)
+            g.gauss_overlap_ol()
+            out[mode] = g.elec_pot_gauss_overlap()
+            sch = g.ortho_schedule()
+        if mode == "auto":
+            assert sch["schedule"] in ("per_item", "piped")
+            assert min(sch["trial_ms"]) > 0.0
+        else:
+            assert sch["schedule"] == mode
+    assert np.array_equal(out["piped"], out["per_item"])
+    assert np.array_equal(out["auto"], out["per_item"])

@@ -170,8 +170,8 @@ def test_koverlap_at_zero_wave_vector_is_the_overlap():
 def test_oracle_driver_matches_reference_driver_executed():
     # the oracle's restatement of the integral driver against the
     # reference's own driver executed statement for statement
-    # (tests/golden/make_driver_golden.py), OL with coreValeOL and KE on the
-    # diamond primitive cell at 2x2x2 k
+    # (tests/golden/make_driver_golden.py): OL with coreValeOL, KE, NP and
+    # the 16 EP terms on the diamond primitive cell at 2x2x2 k
     import os
     import numpy as np
     import oracle
@@ -181,7 +181,10 @@ def test_oracle_driver_matches_reference_driver_executed():
     ob = oracle.OracleBuild(configs.diamond_primitive(kmesh=(2, 2, 2)))
     ol, cre, cim = ob.overlap()
     ke = ob.kinetic()
+    npk = ob.nuclear()
+    ep = ob.elec_pot()
     assert np.array_equal(ob.kpoints_xyz(), g["kPointsXYZ"])
+    assert ep.shape == g["ep_packed"].shape
     for a, b in ((ol, g["ol_packed"]), (ke, g["ke_packed"]), (cre, g["ol_cv_re"]),
-                 (cim, g["ol_cv_im"])):
+                 (cim, g["ol_cv_im"]), (npk, g["np_packed"]), (ep, g["ep_packed"])):
         assert packed_mismatch(a, b, atol=1e-13)[1] == 0
