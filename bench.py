@@ -335,6 +335,51 @@ def time_device_builds(g, bufs, stream, steps, flush, torch):
     return step_s, kms, launches
 
 
+# Algorithmic FP64 flops of one primitive three-centre evaluation by class
+# (l_a, l_b), larger l first: the binary + - * of the reference's generated
+# recursions (src/imago/gaussIntegrals.f90 electron3CIntg / nuclear3CIntg
+# class blocks, counted over the statements; ranges between the two orders
+# taken at their middle), prefactor exp / erf / pow not included.
+EP_FLOPS = {(0, 0): 0, (1, 0): 3, (1, 1): 21, (2, 0): 19, (2, 1): 91, (2, 2): 320,
+            (3, 0): 54, (3, 1): 248, (3, 2): 819, (3, 3): 2022}
+NP_FLOPS = {(0, 0): 0, (1, 0): 9, (1, 1): 63, (2, 0): 49, (2, 1): 241, (2, 2): 797,
+            (3, 0): 137, (3, 1): 610, (3, 2): 1916, (3, 3): 4499}
+
+
+def prim3c_roofline(g, bufs, stream, flush, torch, peak, steps=3):
+    """FP64 roofline of the three-centre primitive stage: the screened
+    (shell pair, site, image) triples of the NP build and every EP term per
+    class (imago_intg_count_triples) times the per-class flops above, over
+    the k_prim3c time of NP + EP builds run alone (kinds serialised, L2
+    flushed before each), against the measured FP64 peak."""
+    from imago_b200 import intg
+    cnp = g.count_triples(intg.IMAGO_NP)
+    cep = g.count_triples(intg.IMAGO_EP)
+    if (cnp < 0).any() or (cep < 0).any():
+        return None
+    flops = 0.0
+    for la in range(4):
+        for lb in range(4):
+            key = (max(la, lb), min(la, lb))
+            flops += cnp[la, lb] * NP_FLOPS[key] + cep[la, lb] * EP_FLOPS[key]
+    out = {k: v.data_ptr() for k, v in bufs.items()}
+    g.set_serial(True)
+    ms = 0.0
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        g.build(which=intg.IMAGO_NP | intg.IMAGO_EP, out=out)
+        ms += g.kernel_stats()[0][0]
+    g.set_serial(False)
+    ms /= steps
+    achieved = flops / (ms / 1e3) / 1e12
+    return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak else None, "kernel": "k_prim3c (NP + EP)",
+            "kernel_ms": ms, "algorithmic_flops": flops,
+            "triples_np": int(cnp.sum()), "triples_ep": int(cep.sum()),
+            "flops_source": "reference recursion flops per class x screened triples"}
+
+
 def time_e2e(system, local, stream, bufs, steps, torch):
     """End to end through the C ABI with host buffers, wall clock: create
     (host set-up, H2D of the system, device tables) + one build of every
@@ -556,7 +601,9 @@ def silica_headline(args, local, stream, torch):
            "vale_dim": g.vale_dim, "core_dim": g.core_dim, "pot_terms": g.pot_dim,
            "pair_images": g.num_pair_images, "shell_pairs": g.num_shell_pairs,
            "gpu_launches": int(launches), "clocks": clk.summary(),
-           "schedule": schedules(g, bufs, stream, flush, torch)}
+           "schedule": schedules(g, bufs, stream, flush, torch),
+           "prim3c_roofline": prim3c_roofline(g, bufs, stream, flush, torch,
+                                              fp64_peak_tflops(torch))}
     if not args.no_adjacent:
         out["adjacent_builds"] = adjacent_builds(g, bufs, stream, torch, dev, reps=3,
                                                  ham_mode=args.ham_mode)
@@ -867,6 +914,7 @@ def run_ours(args):
 
     flops = algorithmic_flops(g)
     fp64 = fp64_peak_tflops(torch) if rank == 0 else None
+    prim3c = prim3c_roofline(g, bufs, stream, flush, torch, fp64) if rank == 0 else None
     top = int(np.argmax(kms))
     top_name = STAGES[top]
     roofline = None
@@ -905,6 +953,7 @@ def run_ours(args):
             "stage_ms": dict(zip(STAGES, [float(x) for x in kms])),
             "shell_pairs_per_s": g.num_shell_pairs * (3 + P) / value,
             "roofline": roofline,
+            "prim3c_roofline": prim3c if rank == 0 else None,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "tuning": tuning,

@@ -20,6 +20,8 @@
 #include <atomic>
 #include <mutex>
 #include <thread>
+#include <array>
+#include <map>
 #include <numeric>
 #include <vector>
 
@@ -212,6 +214,7 @@ struct imago_ctx {
   DBuf<int2> d_btile, d_btile_w;
   DBuf<SiteImage> d_simg;
   DBuf<float> d_cl_d1;
+  DBuf<int> d_site_rank;
 
   // scratch
   // Each build kind (OL, KE, NP, EP) has its own scratch and stream (a
@@ -290,6 +293,7 @@ struct imago_ctx {
     d_terms.release(st); d_btile.release(st); d_simg.release(st);
     d_btile_w.release(st);
     d_cl_d1.release(st);
+    d_site_rank.release(st);
     d_queue.release(st);
     d_flag.release(st);
     if (st) cudaStreamSynchronize(st);
@@ -908,17 +912,21 @@ int upload(imago_ctx *c) {
   set_bloch_width(c, kNumBlochWidths - 1);
   w.simg = nullptr;
   w.cl_d1 = nullptr;
+  w.site_rank = nullptr;
   w.ncl = (c->nps + kSiteCluster - 1) / kSiteCluster;
   if ((rc = launch_phase(s, c->d_phase.p, st))) return rc;
-  // midpoint images of the potential sites, and their cluster bounds, for
-  // the three-centre screens, when the table fits in kMaxSiteImageBytes;
-  // without it every site is searched in full
+  // midpoint images of the potential sites, their cluster bounds and each
+  // unit's sites by distance, for the three-centre screens, when the
+  // tables fit in kMaxSiteImageBytes; without them every site is searched
+  // in full
   const size_t nb = (size_t)w.nunits * c->nps;
-  if (nb > 0 && nb * sizeof(SiteImage) <= kMaxSiteImageBytes &&
+  if (nb > 0 && nb * (sizeof(SiteImage) + sizeof(int)) <= kMaxSiteImageBytes &&
       c->d_simg.alloc(nb, st) == IMAGO_OK &&
-      c->d_cl_d1.alloc((size_t)w.nunits * w.ncl, st) == IMAGO_OK) {
+      c->d_cl_d1.alloc((size_t)w.nunits * w.ncl, st) == IMAGO_OK &&
+      c->d_site_rank.alloc(nb, st) == IMAGO_OK) {
     w.simg = c->d_simg.p;
     w.cl_d1 = c->d_cl_d1.p;
+    w.site_rank = c->d_site_rank.p;
     rc = launch_site_images(s, w, c->d_simg.p, c->d_cl_d1.p, st);
   }
   return rc;
@@ -1025,6 +1033,64 @@ int tune_bloch(imago_ctx *c, int nterm) {
   return rc;
 }
 
+// Measured choices of the autotuned stages (phase-sum width, three-centre
+// schedule, orthogonalisation schedule), kept for the process per device
+// and workload shape, so that a later context of the same system (a
+// rebuilt SCF set-up, an end-to-end call) starts tuned instead of timing
+// the alternatives again.
+struct TuneRecord {
+  int bloch = -1, sched = -1, ortho = -1;
+  float bloch_ms[kNumBlochWidths] = {}, sched_ms[2] = {}, ortho_ms[2] = {};
+};
+using TuneKey = std::array<long long, 10>;
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneRecord> g_tune;
+
+TuneKey tune_key(const imago_ctx *c) {
+  return {c->device,       c->vale_dim,          c->core_dim,        c->nk,
+          c->pot_dim,      (long long)c->units.size(), (long long)c->sps.size(),
+          c->ncell,        c->nps,               c->sys.real_k};
+}
+
+void tune_store(const imago_ctx *c) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  TuneRecord &r = g_tune[tune_key(c)];
+  if (c->bloch_tuned) {
+    r.bloch = (c->work.bw - bloch_width(0)) / (bloch_width(1) - bloch_width(0));
+    std::copy(c->bloch_ms, c->bloch_ms + kNumBlochWidths, r.bloch_ms);
+  }
+  if (c->sched_tuned) {
+    r.sched = c->sched;
+    std::copy(c->sched_ms, c->sched_ms + 2, r.sched_ms);
+  }
+  if (c->ortho_tuned) {
+    r.ortho = c->ortho;
+    std::copy(c->ortho_ms, c->ortho_ms + 2, r.ortho_ms);
+  }
+}
+
+void tune_apply(imago_ctx *c) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  const auto it = g_tune.find(tune_key(c));
+  if (it == g_tune.end()) return;
+  const TuneRecord &r = it->second;
+  if (r.bloch >= 0) {
+    set_bloch_width(c, r.bloch);
+    std::copy(r.bloch_ms, r.bloch_ms + kNumBlochWidths, c->bloch_ms);
+    c->bloch_tuned = true;
+  }
+  if (r.sched >= 0 && c->sched_mode < 0) {
+    c->sched = r.sched;
+    std::copy(r.sched_ms, r.sched_ms + 2, c->sched_ms);
+    c->sched_tuned = true;
+  }
+  if (r.ortho >= 0 && c->ortho_mode < 0) {
+    c->ortho = r.ortho;
+    std::copy(r.ortho_ms, r.ortho_ms + 2, c->ortho_ms);
+    c->ortho_tuned = true;
+  }
+}
+
 int launch_prim3c_sched(imago_ctx *c, const DevSys &s, const DevWork &w,
                         const Term3c *terms, int nterm, bool nuclear, double *blk,
                         cudaStream_t st) {
@@ -1059,6 +1125,7 @@ int tune_sched(imago_ctx *c, const DevSys &s, const DevWork &w, const Term3c *te
   c->sched = (!rc && c->sched_ms[1] < c->sched_ms[0]) ? 1 : 0;
   c->launches += class_launches(c) + 1;
   c->sched_tuned = !rc;
+  if (!rc) tune_store(c);
   return rc;
 }
 
@@ -1088,6 +1155,7 @@ int tune_ortho(imago_ctx *c, const DevSys &s, int nterm, double *packed_dev,
   c->ortho = (!rc && c->ortho_ms[1] < c->ortho_ms[0]) ? 1 : 0;
   c->launches += 2;
   c->ortho_tuned = !rc;
+  if (!rc) tune_store(c);
   return rc;
 }
 
@@ -1126,9 +1194,10 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   mark(c);
   if ((rc = launch_contract(s, w, nterm, S.blk.p, S.M.p, st))) return rc;
   mark(c);
-  if (!c->bloch_tuned && !c->capturing && s.nk > kBlochSmallNk &&
-      (rc = tune_bloch(c, nterm)))
-    return rc;
+  if (!c->bloch_tuned && !c->capturing && s.nk > kBlochSmallNk) {
+    if ((rc = tune_bloch(c, nterm))) return rc;
+    tune_store(c);
+  }
   if ((rc = launch_bloch(s, w, nterm, S.M.p, S.vv.p, S.cv.p, S.cc.p, st)))
     return rc;
   mark(c);
@@ -1435,7 +1504,10 @@ int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packe
   mark(c);
   if ((rc = launch_contract(s, w, spin, c->ham_blk.p, S.M.p, st))) return rc;
   mark(c);
-  if (!c->bloch_tuned && s.nk > kBlochSmallNk && (rc = tune_bloch(c, spin))) return rc;
+  if (!c->bloch_tuned && s.nk > kBlochSmallNk) {
+    if ((rc = tune_bloch(c, spin))) return rc;
+    tune_store(c);
+  }
   if ((rc = launch_bloch(s, w, spin, S.M.p, S.vv.p, S.cv.p, S.cc.p, st))) return rc;
   mark(c);
   const size_t npd = packed_doubles(c) * spin;
@@ -1640,6 +1712,7 @@ int imago_intg_create(const imago_system *sys, const imago_opts *opts,
     c->events = true;
     rc = upload(c);
   }
+  if (!rc) tune_apply(c);
   if (!rc) rc = finish(c, rc);
   if (rc) {
     delete c;
@@ -2010,6 +2083,58 @@ int imago_intg_ortho_schedule(const imago_ctx *c, int *schedule, double trial_ms
   if (trial_ms)
     for (int i = 0; i < 2; ++i) trial_ms[i] = c->ortho_ms[i];
   return IMAGO_OK;
+}
+
+int imago_intg_count_triples(imago_ctx *c, unsigned which, long long counts[16]) {
+  if (!c || !counts || (which != IMAGO_NP && which != IMAGO_EP)) return IMAGO_ERR_INVALID;
+  int rc = set_device(c);
+  if (rc) return rc;
+  unsigned long long *d = nullptr;
+  if (cudaMalloc(&d, 16 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return IMAGO_ERR_NOMEM;
+  }
+  unsigned long long h[16] = {};
+  cudaStream_t st = c->stream;
+  const bool nuc = which == IMAGO_NP;
+  if (cudaMemsetAsync(d, 0, sizeof h, st) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  if (!rc)
+    rc = launch_prim3c_count(c->sys, c->work, c->cls_beg, c->d_terms.p, nuc ? 1 : c->pot_dim,
+                             nuc, d, st);
+  if (!rc && (cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+              cudaStreamSynchronize(st) != cudaSuccess))
+    rc = IMAGO_ERR_CUDA;
+  cudaFree(d);
+  cudaGetLastError();
+  if (rc) return rc;
+  for (int k = 0; k < 16; ++k) {
+    const bool f = k / 4 == 3 || k % 4 == 3;
+    counts[k] = (f && c->cls_beg[k + 1] > c->cls_beg[k]) ? -1 : (long long)h[k];
+  }
+  return IMAGO_OK;
+}
+
+int imago_wait_check(int device, double limit_ms, int *status) {
+  if (!status || !(limit_ms > 0.0) || limit_ms > 1000.0) return IMAGO_ERR_INVALID;
+  *status = IMAGO_OK;
+  int prev = 0;
+  IMAGO_CUDA(cudaGetDevice(&prev));
+  IMAGO_CUDA(cudaSetDevice(device));
+  int *flag = nullptr;
+  int rc = IMAGO_OK;
+  if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    rc = IMAGO_ERR_NOMEM;
+  }
+  if (!rc && cudaMemset(flag, 0, sizeof(int)) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  if (!rc) rc = launch_wait_check(flag, limit_ms, nullptr);
+  if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  if (!rc && cudaMemcpy(status, flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = IMAGO_ERR_CUDA;
+  if (flag) cudaFree(flag);
+  cudaGetLastError();
+  cudaSetDevice(prev);
+  return rc;
 }
 
 int imago_intg_set_ham_mode(imago_ctx *c, int mode) {

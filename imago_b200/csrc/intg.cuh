@@ -94,6 +94,10 @@ struct DevWork {
   // with simg)
   const float *cl_d1;
   int ncl;
+  // [unit * nps + first site of type + r]: the r-th site of the type in
+  // ascending d1 for that unit, as an offset within the type (null with
+  // simg)
+  const int *site_rank;
 };
 
 // Consecutive potential sites screened together before their own tests.
@@ -178,6 +182,11 @@ int launch_prim3c_queue(const DevSys &s, const DevWork &w, const int *cls_beg,
                         unsigned long long *counter, int ctas, cudaStream_t st);
 // CTAs of k_prim3c_queue resident per SM.
 int prim3c_queue_ctas_per_sm();
+// Screened (shell pair, site, image) triples of the s/p/d classes into
+// count16[la * 4 + lb] (added), by the count-only form of k_prim3c.
+int launch_prim3c_count(const DevSys &s, const DevWork &w, const int *cls_beg,
+                        const Term3c *terms_dev, int nterm, bool nuclear,
+                        unsigned long long *count16, cudaStream_t st);
 
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
@@ -192,6 +201,9 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
                  const double2 *cv, const double2 *cc, const double2 *s_cv,
                  double2 *y, double *packed, cudaStream_t st, bool pipe = false);
 bool ortho_pipe_fits(int C, int V);
+// One CTA waiting (bounded, limit_ms) on a barrier nothing completes; it
+// records IMAGO_ERR_TIMEOUT in *flag.
+int launch_wait_check(int *flag, double limit_ms, cudaStream_t st);
 // The same for a matrix whose core-core block is not Hermitian (dipole):
 // the reference's zher2k-then-makeValeVale sequence as it stands.
 int launch_ortho_general(const DevSys &s, int nterm, const double2 *vv,

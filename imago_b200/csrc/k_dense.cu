@@ -1184,6 +1184,26 @@ __global__ void __launch_bounds__(kFThreads, 1)
   __syncthreads();
 }
 
+// The bounded wait of k_ortho_pipe on a barrier that nothing completes:
+// every thread gives up after limit_ns and the status word records it.
+__global__ void k_wait_check(int *flag, unsigned long long limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) report_status(flag, IMAGO_ERR_TIMEOUT);
+}
+
+int launch_wait_check(int *flag, double limit_ms, cudaStream_t st) {
+  const unsigned long long ns = (unsigned long long)(limit_ms * 1e6);
+  k_wait_check<<<1, 128, 0, st>>>(flag, ns);
+  IMAGO_CUDA(cudaGetLastError());
+  return IMAGO_OK;
+}
+
 bool encode_tensor_map_f64_3d(CUtensorMap *map, const void *base, const uint64_t dims[3],
                               const uint64_t strides[2], const uint32_t box[3]) {
   using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,

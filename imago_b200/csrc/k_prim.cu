@@ -76,10 +76,12 @@ __global__ void __launch_bounds__(128)
 // three for d-d, whose Hermite accumulator alone holds 35 doubles.
 // One item g < n * nterm of class (LA, LB): term g / n, shell pair g % n of
 // the class's list.  Shared by the per-class launches and the work queue.
-template <int LA, int LB, bool NUC>
+// CNT: the same loops, counting the screened (site, image) triples into
+// *ntrip instead of integrating (nothing is written).
+template <int LA, int LB, bool NUC, bool CNT = false>
 __device__ __forceinline__ void prim3c_item(const DevSys &s, const DevWork &w, int beg,
                                             int n, const Term3c *terms, double *blk,
-                                            long long g) {
+                                            long long g, unsigned *ntrip = nullptr) {
   constexpr int L = LA + LB;
   const int tl = (int)(g / n);
   const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
@@ -136,36 +138,57 @@ __device__ __forceinline__ void prim3c_item(const DevSys &s, const DevWork &w, i
     }
     const float tf = __double2float_ru(t);
     const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
-    // clusters of kSiteCluster sites first: one bound rules out all of them
-    for (int cb = s0 - s0 % kSiteCluster; cb < s1; cb += kSiteCluster) {
-      if (w.cl_d1 &&
-          beyond(w.cl_d1[(long long)sp.unit * w.ncl + cb / kSiteCluster], pmf, tf))
-        continue;
-      const int lo = max(cb, s0), hi = min(cb + kSiteCluster, s1);
-      for (int site = lo; site < hi; ++site) {
-        double L2[3], v[3], c0;
-        if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
-        const double *C = s.psite_pos + 3 * site;
-        const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
-        for (int nc = 0; nc < s.ncell; ++nc) {
-          if (s.csize[nc] > maxr) break;
-          const double *R = s.cell + 3 * nc;
-          const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
-          if (dx * dx + dy * dy + dz * dz > t) continue;
-          double X[3];
-#pragma unroll
-          for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-          if (NUC)
-            accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
-          else
-            accumulate_overlap_q<L>(X, mu, 1.0, Q);
+    // the type's sites nearest the unit first (with the site tables): the
+    // first one beyond reach ends the walk; without them, every site
+    const long long ub = (long long)sp.unit * s.nps;
+    for (int r = 0; r < s1 - s0; ++r) {
+      int site = s0 + r;
+      if (w.site_rank) {
+        site = s0 + w.site_rank[ub + s0 + r];
+        if (beyond(w.simg[ub + site].d1, pmf, tf)) break;
+      }
+      double L2[3], v[3], c0;
+      if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+      const double *C = s.psite_pos + 3 * site;
+      const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+      for (int nc = 0; nc < s.ncell; ++nc) {
+        if (s.csize[nc] > maxr) break;
+        const double *R = s.cell + 3 * nc;
+        const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+        if (dx * dx + dy * dy + dz * dz > t) continue;
+        if (CNT) {
+          ++*ntrip;
+          continue;
         }
+        double X[3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+        if (NUC)
+          accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
+        else
+          accumulate_overlap_q<L>(X, mu, 1.0, Q);
       }
     }
   }
+  if (CNT) return;
   const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
   hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q,
                         blk + (long long)tl * w.blk_total + sp.boff);
+}
+
+// Screened primitive triples (shell pair, potential site, lattice image) of
+// one class's items: what the reference's nuclearPE / electronicPE loops
+// evaluate (integrals.F90:2533-2698, 2700-2858), summed into *count.
+template <int LA, int LB, bool NUC>
+__global__ void __launch_bounds__(128)
+    k_prim3c_count(DevSys s, DevWork w, int beg, int n, const Term3c *terms, int nterm,
+                   unsigned long long *count) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned c = 0;
+  if (g < (long long)n * nterm)
+    prim3c_item<LA, LB, NUC, true>(s, w, beg, n, terms, nullptr, g, &c);
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
 
 template <int LA, int LB, bool NUC>
@@ -510,6 +533,28 @@ static int prim3c_one(const DevSys &s, const DevWork &w, int beg, int end,
 #define IMAGO_FOR_SPD_CLASSES(M) \
   M(0, 0) M(0, 1) M(0, 2) M(1, 0) M(1, 1) M(1, 2) M(2, 0) M(2, 1) M(2, 2)
 
+int launch_prim3c_count(const DevSys &s, const DevWork &w, const int *cls_beg,
+                        const Term3c *terms_dev, int nterm, bool nuclear,
+                        unsigned long long *count16, cudaStream_t st) {
+#define IMAGO_PC(a, b)                                                               \
+  {                                                                                 \
+    const int beg = cls_beg[a * 4 + b], n = cls_beg[a * 4 + b + 1] - beg;           \
+    if (n > 0 && nterm > 0) {                                                       \
+      const unsigned grid = (unsigned)(((long long)n * nterm + 127) / 128);         \
+      if (nuclear)                                                                  \
+        k_prim3c_count<a, b, true><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev,   \
+                                                         nterm, count16 + a * 4 + b); \
+      else                                                                          \
+        k_prim3c_count<a, b, false><<<grid, 128, 0, st>>>(s, w, beg, n, terms_dev,  \
+                                                          nterm, count16 + a * 4 + b); \
+      IMAGO_CUDA(cudaGetLastError());                                               \
+    }                                                                               \
+  }
+  IMAGO_FOR_SPD_CLASSES(IMAGO_PC)
+#undef IMAGO_PC
+  return IMAGO_OK;
+}
+
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   int op, double *blk, cudaStream_t st) {
   int rc = IMAGO_OK;
@@ -774,6 +819,32 @@ __global__ void k_cluster_bounds(DevSys s, DevWork w, const SiteImage *simg,
   }
 }
 
+// For each unit and potential type, the type's sites in ascending order
+// of d1, the lower bound of their distance from the unit's midpoint, as
+// offsets within the type (ties by site index).  One warp per (unit, type),
+// each lane ranking its sites by counting the smaller ones.
+__global__ void k_site_rank(DevSys s, DevWork w, const SiteImage *simg, int *rank) {
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const long long n = (long long)w.nunits * s.npt;
+  for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < n;
+       i += nw) {
+    const int unit = (int)(i / s.npt), pt = (int)(i % s.npt);
+    const int s0 = s.ptype_first_site[pt], m = s.ptype_mult[pt];
+    const SiteImage *si = simg + (long long)unit * s.nps + s0;
+    int *out = rank + (long long)unit * s.nps + s0;
+    for (int r = lane; r < m; r += 32) {
+      const float d = si[r].d1;
+      int pos = 0;
+      for (int q = 0; q < m; ++q) {
+        const float e = si[q].d1;
+        pos += (e < d) || (e == d && q < r);
+      }
+      out[pos] = r;
+    }
+  }
+}
+
 int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
                        float *cl_d1, cudaStream_t st) {
   const long long n = (long long)w.nunits * s.nps;
@@ -785,6 +856,12 @@ int launch_site_images(const DevSys &s, const DevWork &w, SiteImage *simg,
   if (cl_d1 && nc > 0) {
     k_cluster_bounds<<<(unsigned)std::min<long long>((nc + 255) / 256, 148 * 16),
                        256, 0, st>>>(s, w, simg, cl_d1);
+    IMAGO_CUDA(cudaGetLastError());
+  }
+  const long long nr = (long long)w.nunits * s.npt;
+  if (w.site_rank && nr > 0) {
+    k_site_rank<<<(unsigned)std::min<long long>((nr + 7) / 8, 148 * 16), 256, 0, st>>>(
+        s, w, simg, const_cast<int *>(w.site_rank));
     IMAGO_CUDA(cudaGetLastError());
   }
   return IMAGO_OK;

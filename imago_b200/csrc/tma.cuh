@@ -73,18 +73,19 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Wait for phase `parity` of `bar` to complete, for at most about
-// kWaitLimitNs (and never more than kWaitPolls polls).  False when the
-// bound ran out.
+// Wait for phase `parity` of `bar` to complete, for at most about limit_ns
+// (kWaitLimitNs unless given, and never more than kWaitPolls polls).
+// False when the bound ran out.
 constexpr unsigned long long kWaitLimitNs = 1000000000ULL;  // 1 s
 constexpr unsigned kWaitPolls = 1u << 26;
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (unsigned it = 1; it < kWaitPolls; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0 && global_ns() - t0 > kWaitLimitNs) return false;
+    if ((it & 255u) == 0 && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }

@@ -111,6 +111,12 @@ def lib():
         L.imago_intg_ortho_schedule.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
+        L.imago_intg_count_triples.argtypes = [ctypes.c_void_p, ctypes.c_uint,
+                                               ctypes.POINTER(ctypes.c_longlong)]
+        L.imago_intg_count_triples.restype = ctypes.c_int
+        L.imago_wait_check.argtypes = [ctypes.c_int, ctypes.c_double,
+                                       ctypes.POINTER(ctypes.c_int)]
+        L.imago_wait_check.restype = ctypes.c_int
         L.imago_intg_build_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint,
                                              ctypes.POINTER(ImagoOutC)]
         L.imago_intg_build_graph.restype = ctypes.c_int
@@ -157,6 +163,17 @@ def trim_memory(device=0):
     """Hand the unused memory of the library's device pool back to the
     driver (contexts keep taking scratch from the pool afterwards)."""
     _check(lib().imago_trim_memory(device), "imago_trim_memory")
+
+
+def wait_check(device=0, limit_ms=5.0):
+    """The library's bounded device wait run out on purpose
+    (imago_wait_check): a barrier that nothing completes, given up after
+    limit_ms.  Returns the status the kernel recorded (IMAGO_ERR_TIMEOUT, 6,
+    when the bound works)."""
+    st = ctypes.c_int(-1)
+    _check(lib().imago_wait_check(device, float(limit_ms), ctypes.byref(st)),
+           "imago_wait_check")
+    return st.value
 
 
 def kpoint_mesh(n, shift=(0.0, 0.0, 0.0)):
@@ -369,6 +386,16 @@ class IntegralSetup:
         _check(lib().imago_intg_ortho_schedule(self._ctx, ctypes.byref(s), _p(ms)),
                "imago_intg_ortho_schedule")
         return {"schedule": ("per_item", "piped")[s.value], "trial_ms": ms.tolist()}
+
+    def count_triples(self, which):
+        """Screened primitive triples (shell pair, site, image) per class of
+        the NP build (which=IMAGO_NP) or of every EP term (IMAGO_EP), as an
+        int64 [4, 4] array indexed (l_a, l_b); -1 for f classes present."""
+        c = np.zeros(16, dtype=np.int64)
+        _check(lib().imago_intg_count_triples(
+            self._ctx, which, c.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))),
+            "imago_intg_count_triples")
+        return c.reshape(4, 4)
 
     def set_ham_mode(self, mode):
         """How ham_pscf sums the potential terms (imago_intg_set_ham_mode):

@@ -426,6 +426,22 @@ IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double tr
  * copy that does not land within its bound (1 s) makes the call return
  * IMAGO_ERR_TIMEOUT. */
 IMAGO_API int imago_intg_set_ortho_schedule(imago_ctx *ctx, int mode);
+/* No counterpart in the reference.  Runs the bounded device wait that the
+ * TMA-fed orthogonalisation uses on a barrier that nothing completes, with
+ * a limit of limit_ms (0 < limit_ms <= 1000), on `device`'s default stream:
+ * *status receives IMAGO_ERR_TIMEOUT when the wait gave up as designed and
+ * the device stays usable.  Returns IMAGO_OK unless the check itself could
+ * not run. */
+IMAGO_API int imago_wait_check(int device, double limit_ms, int *status);
+
+/* No counterpart in the reference.  The screened primitive triples that a
+ * build evaluates -- (shell pair, potential site, lattice image) passing
+ * the screens of nuclearPE (which = IMAGO_NP) or electronicPE over every
+ * potential term (IMAGO_EP), integrals.F90:2533-2858 -- per shell-pair
+ * class, counts[la * 4 + lb] for l = 0..3 (s, p, d, f).  Classes with f
+ * are not counted (-1 where the system has them).  Synchronous on the
+ * context's stream; used for the primitive stage's roofline. */
+IMAGO_API int imago_intg_count_triples(imago_ctx *ctx, unsigned which, long long counts[16]);
 /* The orthogonalisation schedule in use (0 or 1) and the trial times of the
  * measurement (ms, mode 0 then mode 1; zero when not measured). */
 IMAGO_API int imago_intg_ortho_schedule(const imago_ctx *ctx, int *schedule,

@@ -727,3 +727,36 @@ def test_piped_orthogonalisation_equals_per_item(imago_lib, make):
             assert sch["schedule"] == mode
     assert np.array_equal(out["piped"], out["per_item"])
     assert np.array_equal(out["auto"], out["per_item"])
+
+
+def test_bounded_device_wait_gives_up_and_the_device_stays_usable(imago_lib):
+    # the TMA-fed orthogonalisation waits on mbarriers with a bound; here
+    # that wait runs on a barrier nothing completes: it must give up within
+    # its limit, record IMAGO_ERR_TIMEOUT, and leave the device usable
+    import time
+    t0 = time.perf_counter()
+    assert intg.wait_check(0, limit_ms=5.0) == 6
+    assert time.perf_counter() - t0 < 5.0
+    with intg.IntegralSetup(configs.small_test_system()) as g:
+        ol, _, _ = g.gauss_overlap_ol()
+    assert np.isfinite(ol).all()
+
+
+@pytest.mark.parametrize("make", [configs.small_test_system,
+                                  lambda: configs.silicon_cubic8(kmesh=(1, 1, 1))])
+def test_screened_triple_counts_match_the_oracle_loops(imago_lib, make):
+    # the count-only form of the three-centre kernel walks the same screens
+    # as the integrating one: its total per build equals the number of
+    # (shell pair, site, image) evaluations of the oracle's restatement of
+    # nuclearPE / electronicPE
+    s = make()
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    with intg.IntegralSetup(s) as g:
+        cnp = g.count_triples(intg.IMAGO_NP)
+        cep = g.count_triples(intg.IMAGO_EP)
+    assert (cnp >= 0).all() and (cep >= 0).all()
+    ob.nuclear()
+    assert int(cnp.sum()) == ob.last_counts()[2]
+    ob.elec_pot()
+    assert int(cep.sum()) == ob.last_counts()[2]
