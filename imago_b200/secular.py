@@ -77,14 +77,56 @@ def hermitian_eigvals(a):
     return w
 
 
+_EIGH_LANES = 8
+_EIGH_POOL = None
+_EIGH_STREAMS = {}
+
+
+def _eigh_lanes(a):
+    """torch.linalg.eigh (cuSOLVER syevd) of each matrix of the batch, the
+    matrices dealt to _EIGH_LANES host threads with a CUDA stream each:
+    syevd synchronises with the host inside every call, so one stream runs
+    the batch one matrix at a time.  Measured on one B200 for 64 matrices:
+    n = 832 743 -> 577 ms, n = 256 190 -> 124 ms, n = 208 161 -> 102 ms."""
+    global _EIGH_POOL
+    import concurrent.futures
+    b = a.shape[0]
+    lanes = min(_EIGH_LANES, b)
+    dev = a.device
+    if _EIGH_POOL is None:
+        _EIGH_POOL = concurrent.futures.ThreadPoolExecutor(_EIGH_LANES)
+    streams = _EIGH_STREAMS.setdefault(dev, [torch.cuda.Stream(dev)
+                                             for _ in range(_EIGH_LANES)])
+    w = torch.empty(a.shape[:-1], dtype=torch.float64, device=dev)
+    v = torch.empty_like(a)
+    cur = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(cur)
+
+    def lane(i):
+        st = streams[i]
+        st.wait_event(ready)
+        with torch.cuda.device(dev), torch.cuda.stream(st):
+            for j in range(i, b, lanes):
+                wj, vj = torch.linalg.eigh(a[j])
+                w[j].copy_(wj)
+                v[j].copy_(vj)
+
+    list(_EIGH_POOL.map(lane, range(lanes)))
+    for st in streams[:lanes]:
+        cur.wait_stream(st)
+    return w, v
+
+
 def hermitian_eigh(a):
     """Ascending eigenvalues [b, n] and unit eigenvectors [b, n, n] (in
     columns) of a batch of Hermitian matrices [b, n, n] (complex128, CUDA):
     imago_hermitian_eigh (the Jacobi kernel accumulating its rotations) up
-    to n = 112, cuSOLVER through torch beyond."""
+    to n = 112, cuSOLVER through torch beyond (one host thread and stream
+    per lane of matrices, _eigh_lanes)."""
     b, n = a.shape[0], a.shape[-1]
     if n > JACOBI_MAX_N:
-        return torch.linalg.eigh(a)
+        return _eigh_lanes(a) if b > 1 else torch.linalg.eigh(a)
     a = a.contiguous()
     w = torch.empty((b, n), dtype=torch.float64, device=a.device)
     v = torch.empty((b, n, n), dtype=torch.complex128, device=a.device)
