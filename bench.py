@@ -634,13 +634,14 @@ def silica_headline(args, local, stream, torch):
 
 
 def schedules(g, bufs, stream, flush, torch, steps=3):
-    """The three-centre stage's two schedules on this build: per-class
-    launches against the persistent work-queue launch (device seconds of
+    """The three-centre stage's schedules on this build: per-class
+    launches, the persistent work-queue launch and per-class launches with
+    two EP terms per thread (device seconds of
     whole builds replayed from graphs, and the primitive stage's ms with the
     kinds serialised), the measured choice the context made, and back to
     the measured choice."""
     out = {"chosen": g.schedule()}
-    for mode in ("per_class", "queue"):
+    for mode in ("per_class", "queue", "pairs"):
         g.set_schedule(mode)
         g.build_graph({k: v.data_ptr() for k, v in bufs.items()})
         torch.cuda.synchronize()

@@ -150,6 +150,8 @@ struct HPType {
 
 }  // namespace
 
+constexpr int kNumSchedules = 3;  // three-centre schedules, imago_intg_set_schedule
+
 struct imago_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -181,11 +183,12 @@ struct imago_ctx {
   bool bloch_tuned = false;
   float bloch_ms[kNumBlochWidths] = {};
   int cls_beg[17];
-  // three-centre schedule: per-class launches (0) or one persistent launch
-  // fed by a work queue (1); mode -1 measures both on the first EP build
+  // three-centre schedule: per-class launches (0), one persistent launch
+  // fed by a work queue (1), or per-class launches with two EP terms of a
+  // type per thread (2); mode -1 measures all on the first EP build
   int sched_mode = -1, sched = 0;
   bool sched_tuned = false;
-  float sched_ms[2] = {};
+  float sched_ms[kNumSchedules] = {};
   int queue_ctas = 0;
   // orthogonalisation of multi-term builds: per-(k, term) CTAs (0) or the
   // persistent TMA-fed kernel (1); mode -1 measures both on the first
@@ -1040,7 +1043,7 @@ int tune_bloch(imago_ctx *c, int nterm) {
 // the alternatives again.
 struct TuneRecord {
   int bloch = -1, sched = -1, ortho = -1;
-  float bloch_ms[kNumBlochWidths] = {}, sched_ms[2] = {}, ortho_ms[2] = {};
+  float bloch_ms[kNumBlochWidths] = {}, sched_ms[kNumSchedules] = {}, ortho_ms[2] = {};
 };
 using TuneKey = std::array<long long, 10>;
 std::mutex g_tune_mu;
@@ -1061,7 +1064,7 @@ void tune_store(const imago_ctx *c) {
   }
   if (c->sched_tuned) {
     r.sched = c->sched;
-    std::copy(c->sched_ms, c->sched_ms + 2, r.sched_ms);
+    std::copy(c->sched_ms, c->sched_ms + kNumSchedules, r.sched_ms);
   }
   if (c->ortho_tuned) {
     r.ortho = c->ortho;
@@ -1081,7 +1084,7 @@ void tune_apply(imago_ctx *c) {
   }
   if (r.sched >= 0 && c->sched_mode < 0) {
     c->sched = r.sched;
-    std::copy(r.sched_ms, r.sched_ms + 2, c->sched_ms);
+    std::copy(r.sched_ms, r.sched_ms + kNumSchedules, c->sched_ms);
     c->sched_tuned = true;
   }
   if (r.ortho >= 0 && c->ortho_mode < 0) {
@@ -1094,18 +1097,23 @@ void tune_apply(imago_ctx *c) {
 int launch_prim3c_sched(imago_ctx *c, const DevSys &s, const DevWork &w,
                         const Term3c *terms, int nterm, bool nuclear, double *blk,
                         cudaStream_t st) {
-  if (c->sched)
+  if (c->sched == 1)
     return launch_prim3c_queue(s, w, c->cls_beg, terms, nterm, nuclear, blk,
                                c->d_queue.p + c->lane, c->queue_ctas, st);
-  return launch_prim3c(s, w, c->cls_beg, terms, nterm, nuclear, blk, st);
+  // the same terms on the host, for the pairing of EP terms
+  const Term3c *th = c->sched != 2 || nuclear || c->ep_terms.empty()
+                         ? nullptr
+                         : c->ep_terms.data() + (terms - c->d_terms.p);
+  return launch_prim3c(s, w, c->cls_beg, terms, nterm, nuclear, blk, st, th);
 }
 
 // The three-centre schedule is picked by measurement, as the phase-sum
 // width: on the context's first EP build each schedule runs once on the
-// real terms (both write the same blocks) and the faster is kept.
+// real terms (all write the same blocks, to rounding) and the fastest is
+// kept.
 int tune_sched(imago_ctx *c, const DevSys &s, const DevWork &w, const Term3c *terms,
                int nterm, double *blk, cudaStream_t st) {
-  cudaEvent_t e[3];
+  cudaEvent_t e[kNumSchedules + 1];
   for (auto &x : e)
     if (cudaEventCreate(&x) != cudaSuccess) {
       cudaGetLastError();
@@ -1113,17 +1121,21 @@ int tune_sched(imago_ctx *c, const DevSys &s, const DevWork &w, const Term3c *te
     }
   int rc = IMAGO_OK;
   cudaEventRecord(e[0], st);
-  for (int k = 0; k < 2 && !rc; ++k) {
+  for (int k = 0; k < kNumSchedules && !rc; ++k) {
     c->sched = k;
     rc = launch_prim3c_sched(c, s, w, terms, nterm, false, blk, st);
     cudaEventRecord(e[k + 1], st);
   }
-  if (!rc && cudaEventSynchronize(e[2]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
-  for (int k = 0; k < 2 && !rc; ++k) cudaEventElapsedTime(&c->sched_ms[k], e[k], e[k + 1]);
+  if (!rc && cudaEventSynchronize(e[kNumSchedules]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  for (int k = 0; k < kNumSchedules && !rc; ++k)
+    cudaEventElapsedTime(&c->sched_ms[k], e[k], e[k + 1]);
   for (auto &x : e) cudaEventDestroy(x);
   cudaGetLastError();
-  c->sched = (!rc && c->sched_ms[1] < c->sched_ms[0]) ? 1 : 0;
-  c->launches += class_launches(c) + 1;
+  int best = 0;
+  for (int k = 1; k < kNumSchedules && !rc; ++k)
+    if (c->sched_ms[k] < c->sched_ms[best]) best = k;
+  c->sched = best;
+  c->launches += 2 * class_launches(c) + 1;
   c->sched_tuned = !rc;
   if (!rc) tune_store(c);
   return rc;
@@ -1484,7 +1496,8 @@ int do_ham(imago_ctx *c, int spin, const double *coeffs, bool rel, double *packe
   } else {
     for (int t0 = 0; t0 < c->pot_dim; t0 += chunk) {
       const int nt = std::min(chunk, c->pot_dim - t0);
-      if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + t0, nt, false, S.blk.p, st)))
+      if ((rc = launch_prim3c(s, w, c->cls_beg, c->d_terms.p + t0, nt, false, S.blk.p, st,
+                              c->ep_terms.data() + t0)))
         return rc;
       if ((rc = launch_block_axpy(S.blk.p, nt, n, c->ham_w.p + t0, c->pot_dim, spin,
                                   c->ham_blk.p, st)))
@@ -2048,7 +2061,7 @@ int imago_intg_tuning(const imago_ctx *c, int *bloch_width, double trial_ms[3]) 
 }
 
 int imago_intg_set_schedule(imago_ctx *c, int mode) {
-  if (!c || mode < -1 || mode > 1) return IMAGO_ERR_INVALID;
+  if (!c || mode < -1 || mode >= kNumSchedules) return IMAGO_ERR_INVALID;
   if (c->gexec) {  // a captured graph keeps the launches it was captured with
     cudaGraphExecDestroy(c->gexec);
     c->gexec = nullptr;
@@ -2058,11 +2071,11 @@ int imago_intg_set_schedule(imago_ctx *c, int mode) {
   return IMAGO_OK;
 }
 
-int imago_intg_schedule(const imago_ctx *c, int *schedule, double trial_ms[2]) {
+int imago_intg_schedule(const imago_ctx *c, int *schedule, double trial_ms[3]) {
   if (!c) return IMAGO_ERR_INVALID;
   if (schedule) *schedule = c->sched;
   if (trial_ms)
-    for (int i = 0; i < 2; ++i) trial_ms[i] = c->sched_ms[i];
+    for (int i = 0; i < kNumSchedules; ++i) trial_ms[i] = c->sched_ms[i];
   return IMAGO_OK;
 }
 

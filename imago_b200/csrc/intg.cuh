@@ -168,6 +168,19 @@ int launch_prim2c_vec(const DevSys &s, const DevWork &w, const int *cls_beg,
 // The classes of one three-centre build in work-queue order: class code
 // la * 4 + lb, first entry of its shell-pair list, count, and the first
 // queue item of each class (off[ncls] is the total).
+// Consecutive EP terms of one potential type evaluated by one thread, so
+// that they share the site and image walk: group g is terms first[g] ..
+// first[g] + count[g] - 1 of a launch's term list.
+constexpr int kMaxTermGroups = 64;
+struct TermGroups {
+  int n;
+  unsigned short first[kMaxTermGroups];
+  unsigned char count[kMaxTermGroups];
+};
+// Pairs of consecutive terms of one type (a single term where a type's
+// count is odd); n = 0 when there would be more than kMaxTermGroups.
+TermGroups term_pairs(const Term3c *terms_host, int nterm);
+
 struct Prim3cQueue {
   int ncls;
   int cls[16], beg[16], n[16];
@@ -188,9 +201,11 @@ int launch_prim3c_count(const DevSys &s, const DevWork &w, const int *cls_beg,
                         const Term3c *terms_dev, int nterm, bool nuclear,
                         unsigned long long *count16, cudaStream_t st);
 
+// terms_host (the same list on the host): EP classes up to d-p run two
+// terms of a type per thread (k_prim3c_pair); null: one term per thread.
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
-                  double *blk, cudaStream_t st);
+                  double *blk, cudaStream_t st, const Term3c *terms_host = nullptr);
 int launch_contract(const DevSys &s, const DevWork &w, int nterm,
                     const double *blk, double *M, cudaStream_t st);
 int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,

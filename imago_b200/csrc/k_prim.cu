@@ -176,6 +176,110 @@ __device__ __forceinline__ void prim3c_item(const DevSys &s, const DevWork &w, i
                         blk + (long long)tl * w.blk_total + sp.boff);
 }
 
+// The Hermite-to-spherical transform of one term of a pair, as a call: the
+// other term's accumulators wait in memory meanwhile instead of crowding
+// the transform's registers.
+template <int LA, int LB>
+__device__ __noinline__ void pair_to_sh(const double *A, const double *B, double a1, double a2,
+                                        double pref, const double *Q, double *out) {
+  double Qr[nherm(LA + LB)];
+#pragma unroll
+  for (int i = 0; i < nherm(LA + LB); ++i) Qr[i] = Q[i];
+  hermite_to_sh<LA, LB>(A, B, a1, a2, pref, Qr, out);
+}
+
+// Two EP terms of one potential type per thread (group g / n of tg): the
+// sites and images are walked once with the larger of the two screening
+// radii and each image is accumulated into the terms whose own radius it
+// passes, so each term gets exactly the triples of its own walk (the set
+// of images within a radius does not depend on the lattice vector the
+// enumeration starts from).
+template <int LA, int LB>
+__device__ __forceinline__ void prim3c_item2(const DevSys &s, const DevWork &w, int beg,
+                                             int n, const Term3c *terms,
+                                             const TermGroups &tg, double *blk, long long g) {
+  constexpr int L = LA + LB;
+  const int gi = (int)(g / n);
+  const int t0 = tg.first[gi], cnt = tg.count[gi];
+  const DSp sp = w.sps[w.sp_by_cls[beg + (int)(g % n)]];
+  const SpGeom q = sp_geom(s, w, sp);
+  const double cen = q.a1s / (q.a1s + q.a2s);
+  const double adist = s.T / q.a2s / cen;
+  const double frac = 1 - q.r2 / adist;
+  double Ps[3], Pt[3];
+  const double zeta = q.a1 + q.a2, xi = q.a1 * q.a2 / zeta;
+  double pm = 0.0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    Ps[x] = cen * (q.A[x] - q.B[x]) + q.B[x];
+    Pt[x] = (q.a1 * q.A[x] + q.a2 * q.B[x]) / zeta;
+    const double e = Ps[x] - 0.5 * (q.A[x] + q.B[x]);
+    pm += e * e;
+  }
+  pm = sqrt(pm);
+  const int pt = terms[t0].ptype;
+  double tc[2], mu[2], a3[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const Term3c tm = terms[t0 + (j < cnt ? j : 0)];
+    a3[j] = s.palpha[s.ptype_alpha_off[pt] + tm.j];
+    const double a3s = s.palpha[s.ptype_alpha_off[s.ptype_screen[pt]] + tm.j];
+    // alphaPotDist (gaussRelations.f90:187-196); a missing second term
+    // takes no image
+    tc[j] = j < cnt ? frac * (s.T * (q.a1s + q.a2s + a3s) / (q.a1s + q.a2s) / a3s) : -1.0;
+    mu[j] = zeta * a3[j] / (zeta + a3[j]);
+  }
+  const double t = fmax(tc[0], tc[1]);
+  const float tf = __double2float_ru(t), pmf = __double2float_ru(pm);
+  double Q[2][nherm(L)];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int i = 0; i < nherm(L); ++i) Q[j][i] = 0.0;
+  const int s0 = s.ptype_first_site[pt], s1 = s0 + s.ptype_mult[pt];
+  const long long ub = (long long)sp.unit * s.nps;
+  for (int r = 0; r < s1 - s0; ++r) {
+    int site = s0 + r;
+    if (w.site_rank) {
+      site = s0 + w.site_rank[ub + s0 + r];
+      if (beyond(w.simg[ub + site].d1, pmf, tf)) break;
+    }
+    double L2[3], v[3], c0;
+    if (!site_search(s, w, sp.unit, site, Ps, pmf, t, tf, L2, v, c0)) continue;
+    const double *C = s.psite_pos + 3 * site;
+    const double maxr = c0 + t + 2.0 * sqrt(c0 * t);
+    for (int nc = 0; nc < s.ncell; ++nc) {
+      if (s.csize[nc] > maxr) break;
+      const double *R = s.cell + 3 * nc;
+      const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 > t) continue;
+      double X[3];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+      if (d2 <= tc[0]) accumulate_overlap_q<L>(X, mu[0], 1.0, Q[0]);
+      if (d2 <= tc[1]) accumulate_overlap_q<L>(X, mu[1], 1.0, Q[1]);
+    }
+  }
+  const double ex = exp(-xi * q.r2);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (j >= cnt) break;
+    const double pref = pow(kPi / (zeta + a3[j]), 1.5) * ex;
+    pair_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q[j],
+                       blk + (long long)(t0 + j) * w.blk_total + sp.boff);
+  }
+}
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(128, LA + LB >= 3 ? 3 : 4)
+    k_prim3c_pair(DevSys s, DevWork w, int beg, int n, const Term3c *terms, TermGroups tg,
+                  double *blk) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * tg.n) return;
+  prim3c_item2<LA, LB>(s, w, beg, n, terms, tg, blk, g);
+}
+
 // Screened primitive triples (shell pair, potential site, lattice image) of
 // one class's items: what the reference's nuclearPE / electronicPE loops
 // evaluate (integrals.F90:2533-2698, 2700-2858), summed into *count.
@@ -192,7 +296,7 @@ __global__ void __launch_bounds__(128)
 }
 
 template <int LA, int LB, bool NUC>
-__global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : 4)
+__global__ void __launch_bounds__(128, LA + LB >= 4 ? 3 : (LA + LB >= 3 ? 4 : (LA + LB == 2 ? 5 : 6)))
     k_prim3c(DevSys s, DevWork w, int beg, int n, const Term3c *terms,
              int nterm, double *blk) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -514,12 +618,38 @@ static int prim2c_one(const DevSys &s, const DevWork &w, int beg, int end,
   return IMAGO_OK;
 }
 
+TermGroups term_pairs(const Term3c *terms_host, int nterm) {
+  TermGroups tg{};
+  for (int i = 0; i < nterm;) {
+    if (tg.n == kMaxTermGroups) {
+      tg.n = 0;
+      return tg;
+    }
+    const int c = (i + 1 < nterm && terms_host[i + 1].ptype == terms_host[i].ptype) ? 2 : 1;
+    tg.first[tg.n] = (unsigned short)i;
+    tg.count[tg.n] = (unsigned char)c;
+    ++tg.n;
+    i += c;
+  }
+  return tg;
+}
+
 template <int LA, int LB>
 static int prim3c_one(const DevSys &s, const DevWork &w, int beg, int end,
-                      const Term3c *terms, int nterm, bool nuc, double *blk,
-                      cudaStream_t st) {
+                      const Term3c *terms, int nterm, bool nuc, const TermGroups *tg,
+                      double *blk, cudaStream_t st) {
   const int n = end - beg, tb = 128;
   if (n <= 0 || nterm <= 0) return IMAGO_OK;
+  // EP classes up to d-p: two terms per thread share the walk (d-d keeps
+  // one: its two accumulators would not fit the registers)
+  if constexpr (LA + LB <= 3) {
+    if (!nuc && tg && tg->n > 0 && tg->n < nterm) {
+      const unsigned grid = (unsigned)(((long long)n * tg->n + tb - 1) / tb);
+      k_prim3c_pair<LA, LB><<<grid, tb, 0, st>>>(s, w, beg, n, terms, *tg, blk);
+      IMAGO_CUDA(cudaGetLastError());
+      return IMAGO_OK;
+    }
+  }
   const long long tot = (long long)n * nterm;
   const unsigned grid = (unsigned)((tot + tb - 1) / tb);
   if (nuc)
@@ -773,12 +903,14 @@ int prim3c_queue_ctas_per_sm() {
 
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
-                  double *blk, cudaStream_t st) {
+                  double *blk, cudaStream_t st, const Term3c *terms_host) {
   int rc = IMAGO_OK;
+  TermGroups tg{};
+  if (!nuclear && terms_host) tg = term_pairs(terms_host, nterm);
 #define IMAGO_P3(a, b)                                                        \
   if (rc == IMAGO_OK)                                                        \
     rc = prim3c_one<a, b>(s, w, cls_beg[a * 4 + b], cls_beg[a * 4 + b + 1],  \
-                          terms_dev, nterm, nuclear, blk, st);
+                          terms_dev, nterm, nuclear, &tg, blk, st);
   IMAGO_FOR_SPD_CLASSES(IMAGO_P3)
 #undef IMAGO_P3
   for (int c = 0; c < 16 && rc == IMAGO_OK; ++c) {

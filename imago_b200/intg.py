@@ -355,19 +355,21 @@ class IntegralSetup:
 
     def set_schedule(self, mode):
         """How the three-centre primitive stage schedules its classes
-        (imago_intg_set_schedule): "auto" (both measured on the first EP
-        build, the faster kept), "per_class" (one launch per class) or
-        "queue" (one persistent launch fed by a device work queue)."""
-        m = {"auto": -1, "per_class": 0, "queue": 1}[mode]
+        (imago_intg_set_schedule): "auto" (all measured on the first EP
+        build, the fastest kept), "per_class" (one launch per class),
+        "queue" (one persistent launch fed by a device work queue) or
+        "pairs" (one launch per class, two EP terms of a type per thread)."""
+        m = {"auto": -1, "per_class": 0, "queue": 1, "pairs": 2}[mode]
         _check(lib().imago_intg_set_schedule(self._ctx, m), "imago_intg_set_schedule")
 
     def schedule(self):
-        """{"schedule": "per_class" | "queue", "trial_ms": [per class, queue]}"""
+        """{"schedule": "per_class" | "queue" | "pairs",
+        "trial_ms": [per class, queue, pairs]}"""
         s = ctypes.c_int()
-        ms = np.zeros(2)
+        ms = np.zeros(3)
         _check(lib().imago_intg_schedule(self._ctx, ctypes.byref(s), _p(ms)),
                "imago_intg_schedule")
-        return {"schedule": ("per_class", "queue")[s.value], "trial_ms": ms.tolist()}
+        return {"schedule": ("per_class", "queue", "pairs")[s.value], "trial_ms": ms.tolist()}
 
     def set_ortho_schedule(self, mode):
         """How EP builds of several terms run the core orthogonalisation

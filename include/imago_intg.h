@@ -405,16 +405,21 @@ IMAGO_API int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
 
 /* No counterpart: how the three-centre primitive stage of NP and EP
  * schedules its shell-pair classes.  mode 0: one launch per class
- * (k_prim3c<la, lb>); mode 1: all classes in one persistent launch whose
- * warps take 32 items at a time from a device work queue (one atomic
- * counter), the classes ordered by cost so that the cheap ones fill in
- * behind the expensive ones; mode -1 (the default): both run once on the
- * context's first EP build and the faster is kept.  The results are the
- * same bit for bit.  A captured graph of the context is dropped. */
+ * (k_prim3c<la, lb>), one (shell pair, term) per thread; mode 1: all
+ * classes in one persistent launch whose warps take 32 items at a time
+ * from a device work queue (one atomic counter), the classes ordered by
+ * cost so that the cheap ones fill in behind the expensive ones; mode 2:
+ * one launch per class with two EP terms of a potential type per thread
+ * for the classes up to d-p (k_prim3c_pair), which walk the sites and
+ * images once for both; mode -1 (the default): all run once on the
+ * context's first EP build and the fastest is kept.  NP is the same bit for
+ * bit under every mode, EP the same to rounding (mode 2 may enumerate an
+ * item's images from another lattice vector).  A captured graph of the
+ * context is dropped. */
 IMAGO_API int imago_intg_set_schedule(imago_ctx *ctx, int mode);
-/* The schedule in use (0 per class, 1 work queue) and the trial times of
- * the measurement (ms, per class then work queue; zero when not measured). */
-IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double trial_ms[2]);
+/* The schedule in use (0, 1 or 2) and the trial times of the measurement
+ * (ms, in mode order; zero when not measured). */
+IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double trial_ms[3]);
 
 /* No counterpart in the reference (the orthogonalisation of
  * makeValeVale/coreValeCoreCore, intgOrtho.F90:23-213, as scheduled on the

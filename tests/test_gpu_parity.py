@@ -684,25 +684,28 @@ def test_driver_matches_reference_driver_executed(imago_lib):
                                   lambda: configs.silicon_cubic8(kmesh=(2, 2, 2))])
 def test_work_queue_schedule_equals_per_class_launches(imago_lib, make):
     # the persistent work-queue launch of the three-centre stage computes
-    # every item as the per-class launches do and writes the same blocks:
-    # NP and every EP term bit for bit, and the measured choice is one of
-    # the two
+    # every item as the per-class launches do: NP bit for bit; EP to
+    # rounding, since the per-class launches walk the sites of two terms at
+    # once (the same triples, their images enumerated from another lattice
+    # vector where the walk's radius changes which image comes first); and
+    # the measured choice is one of the two
     s = make()
     out = {}
-    for mode in ("per_class", "queue", "auto"):
+    for mode in ("per_class", "queue", "pairs", "auto"):
         with intg.IntegralSetup(s) as g:
             g.set_schedule(mode)
             g.gauss_overlap_ol()
             out[mode] = (g.gauss_overlap_np(), g.elec_pot_gauss_overlap())
             sch = g.schedule()
         if mode == "auto":
-            assert sch["schedule"] in ("per_class", "queue")
+            assert sch["schedule"] in ("per_class", "queue", "pairs")
             assert min(sch["trial_ms"]) > 0.0
         else:
             assert sch["schedule"] == mode
-    for mode in ("queue", "auto"):
+    for mode in ("queue", "pairs", "auto"):
         assert np.array_equal(out[mode][0], out["per_class"][0])
-        assert np.array_equal(out[mode][1], out["per_class"][1])
+        ref = out["per_class"][1]
+        assert np.abs(out[mode][1] - ref).max() <= 1e-14 * np.abs(ref).max()
 
 
 @pytest.mark.parametrize("make", [configs.small_test_system,
