@@ -167,3 +167,43 @@ def test_gpu_setup_matches_oracle_on_si8(imago_lib):
         n, w, op = st.mesh()
         assert np.array_equal(n, o.site_points)
         assert _rel(op, o.op) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_scf_matches_the_oracle_loop_on_si8_2x2x2(imago_lib):
+    # the whole SCF on the jittered Si8 cell at 2x2x2 k (8 k-points, one
+    # type, 20 terms), GPU against the CPU oracle's loop (the oracle's
+    # integrals, LAPACK eigh(H, S), populateStandard, makeValenceRho's
+    # traces and makeSCFPot restated): the same iterations, every total
+    # energy within 1e-7 Ha, and the last iteration's eigenvalues within
+    # 1e-8 Ha
+    import oracle
+    from oracle import scf as oscf
+    from imago_b200 import scf, secular
+    s = configs.silicon_cubic8(kmesh=(2, 2, 2))
+    nsv = 12
+    ne = scf.valence_electrons(s)
+    ob = oracle.OracleBuild(s)
+    ol, _, _ = ob.overlap()
+    ke, npk, ep = ob.kinetic(), ob.nuclear(), ob.elec_pot()
+    o = oscf.ScfOracle(s, num_sample_vectors=nsv)
+    o.reset()
+    coeffs = scf.atomic_start(s)
+    V = ol.shape[1]
+    V = int((int((8 * V + 1) ** 0.5) - 1) // 2)
+    energies, last_ev = [], None
+    for _ in range(30):
+        r = oracle.valence_rho(npk, ke, ep, ol, coeffs, ne, V)
+        last_ev = r["eigenvalues"][:, 0, :]
+        coeffs, res = o.make_scf_pot(r["potRho"][:, 0], r["nucPotTrace"][0],
+                                     r["kineticEnergyTrace"][0], coeffs, ne)
+        energies.append(res["totalEnergy"])
+        if res["converged"]:
+            break
+    p = scf.ScfParams(num_sample_vectors=nsv, energy_tol=0.0)
+    ints, _ = scf.device_integrals(s)
+    g = scf.run_scf(s, scf.atomic_start(s), p, integrals=ints)
+    assert g["converged"] and g["iterations"] == len(energies)
+    assert np.abs(np.array(g["energies"]) - np.array(energies)).max() < 1e-7
+    ev = secular.secular_eigenvalues(ints, g["pot_coeffs"]).cpu().numpy()
+    assert np.abs(ev - last_ev).max() < 1e-8
