@@ -755,6 +755,37 @@ __device__ __forceinline__ void fused_tile(const double2 *A, int lda, int r0,
   }
 }
 
+// One warp's 8x16 complex subtile of A^T B (plain, 3M form) over k in
+// [0, nk4) from k-major shared arrays: one row fragment, two column ones.
+template <bool REAL>
+__device__ __forceinline__ void fused_tile8(const double2 *A, int lda, int r0,
+                                            const double2 *B, int ldb, int c0, int nk4,
+                                            double t1[2][2], double t2[2][2],
+                                            double t3[2][2], int lane) {
+  for (int ks = 0; ks < nk4; ks += 4) {
+    const int kk = ks + (lane & 3);
+    const double2 a = A[kk * lda + r0 + (lane >> 2)];
+    const double as = a.x + a.y;
+    double2 b[2];
+    double bs[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      b[t] = B[kk * ldb + c0 + 8 * t + (lane >> 2)];
+      bs[t] = b[t].x + b[t].y;
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      dmma(t1[nt][0], t1[nt][1], a.x, b[nt].x);
+      if (REAL) continue;
+      dmma(t2[nt][0], t2[nt][1], a.y, b[nt].y);
+      dmma(t3[nt][0], t3[nt][1], as, bs[nt]);
+    }
+  }
+}
+
+// Y tiles of 8 core x 16 valence indices held per warp before X_cv lands
+constexpr int kFYTilesPerWarp = 3;
+
 template <bool REAL>
 __global__ void __launch_bounds__(kFThreads, 1)
     k_ortho_fused(DevSys s, const double2 *vv, const double2 *cv,
@@ -769,15 +800,14 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const double2 *X = cv + tk * V * C;
   const double2 *XC = cc + tk * C * C;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // S(l, v) and X_cv(l, v), l fastest in memory, to [l][v]; X_cc(c, l), c
-  // fastest, to [l][c]: asynchronous 16-byte copies, all in flight at once,
-  // the padding zero-filled
+  // S(l, v) and X_cc(c, l) first (S to [l][v], X_cc to [l][c], l and c
+  // fastest in memory), then X_cv(l, v) to [l][v] in a second group that
+  // lands while the products of the Y step run: asynchronous 16-byte
+  // copies, the padding zero-filled
   for (int i = tid; i < d.C4 * d.V16; i += kFThreads) {
     const int l = i % d.C4, v = i / d.C4;
     const bool in = l < C && v < V;
-    const long long g = in ? (long long)v * C + l : 0;
-    cp_async16(&Ss[l * d.Vp + v], S + g, in);
-    cp_async16(&Ys[l * d.Vp + v], X + g, in);
+    cp_async16(&Ss[l * d.Vp + v], S + (in ? (long long)v * C + l : 0), in);
   }
   for (int i = tid; i < d.C4 * d.C16; i += kFThreads) {
     const int c = i % d.C16, l = i / d.C16;
@@ -785,28 +815,50 @@ __global__ void __launch_bounds__(kFThreads, 1)
     cp_async16(&Xs[l * d.Cp + c], XC + (in ? (long long)l * C + c : 0), in);
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (int i = tid; i < d.C4 * d.V16; i += kFThreads) {
+    const int l = i % d.C4, v = i / d.C4;
+    const bool in = l < C && v < V;
+    cp_async16(&Ys[l * d.Vp + v], X + (in ? (long long)v * C + l : 0), in);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  __syncthreads();
+  // Y = X_cv - X_cc S / 2 on tiles of 8 core x 16 valence indices (C = 40
+  // gives 5 row tiles, no padding): each warp forms the products of its
+  // tiles (at most kFYTilesPerWarp) in registers, then, once X_cv is in,
+  // subtracts them
+  const int yr = (C + 7) / 8, ny = yr * (d.V16 / 16);
+  double y1[kFYTilesPerWarp][2][2], y2[kFYTilesPerWarp][2][2], y3[kFYTilesPerWarp][2][2];
+#pragma unroll
+  for (int q = 0; q < kFYTilesPerWarp; ++q) {
+    const int tile = warp + q * kFWarps;
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) y1[q][nt][i] = y2[q][nt][i] = y3[q][nt][i] = 0.0;
+    if (tile < ny)
+      fused_tile8<REAL>(Xs, d.Cp, (tile % yr) * 8, Ss, d.Vp, (tile / yr) * 16, d.C4, y1[q],
+                        y2[q], y3[q], lane);
+  }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
-  // Y = X_cv - X_cc S / 2, subtiles of 16 core x 16 valence indices
-  const int yr = d.C16 / 16, ny = yr * (d.V16 / 16);
-  for (int tile = warp; tile < ny; tile += kFWarps) {
-    const int r0 = (tile % yr) * 16, c0 = (tile / yr) * 16;
-    double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
-    fused_tile<false, REAL>(Xs, d.Cp, r0, Ss, d.Vp, c0, d.C4, false, t1, t2, t3, lane);
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+  for (int q = 0; q < kFYTilesPerWarp; ++q) {
+    const int tile = warp + q * kFWarps;
+    if (tile >= ny) continue;
+    const int r0 = (tile % yr) * 8, c0 = (tile / yr) * 16;
 #pragma unroll
-      for (int nt = 0; nt < 2; ++nt)
+    for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int c = r0 + 8 * mt + (lane >> 2);
-          const int v = c0 + 8 * nt + 2 * (lane & 3) + i;
-          if (c >= C || v >= V) continue;
-          const double2 p = ocombine<false, REAL>(t1[mt][nt][i], t2[mt][nt][i], t3[mt][nt][i]);
-          double2 &y = Ys[c * d.Vp + v];
-          y.x -= 0.5 * p.x;
-          y.y -= 0.5 * p.y;
-        }
+      for (int i = 0; i < 2; ++i) {
+        const int c = r0 + (lane >> 2);
+        const int v = c0 + 8 * nt + 2 * (lane & 3) + i;
+        if (c >= C || v >= V) continue;
+        const double2 p = ocombine<false, REAL>(y1[q][nt][i], y2[q][nt][i], y3[q][nt][i]);
+        double2 &y = Ys[c * d.Vp + v];
+        y.x -= 0.5 * p.x;
+        y.y -= 0.5 * p.y;
+      }
   }
   __syncthreads();
   // upper subtiles (J <= I) of S^H Y + Y^H S over the stacked k = 2 C4
@@ -1309,7 +1361,8 @@ int launch_ortho(const DevSys &s, int nterm, const double2 *vv,
     if (rc || launched) return rc;
   }
   const size_t smem = fused_smem(C, V);
-  if (smem <= kFusedMaxSmem) {
+  const int fused_y_tiles = (C + 7) / 8 * ((V + 15) / 16);
+  if (smem <= kFusedMaxSmem && fused_y_tiles <= kFYTilesPerWarp * kFWarps) {
     static bool attr_set[2][64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
