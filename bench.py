@@ -602,6 +602,7 @@ def silica_headline(args, local, stream, torch):
            "pair_images": g.num_pair_images, "shell_pairs": g.num_shell_pairs,
            "gpu_launches": int(launches), "clocks": clk.summary(),
            "schedule": schedules(g, bufs, stream, flush, torch),
+           "contract": g.contract_tuning(),
            "prim3c_roofline": prim3c_roofline(g, bufs, stream, flush, torch,
                                               fp64_peak_tflops(torch))}
     if not args.no_adjacent:
@@ -904,6 +905,7 @@ def run_ours(args):
     tuning = g.tuning()
     tuning["prim3c"] = g.schedule()
     tuning["ortho"] = g.ortho_schedule()
+    tuning["contract"] = g.contract_tuning()
     secular_s = time_secular(bufs, P, stream, torch)
     # the valence-charge step as measured on the Si8 mesh (V = 104, the
     # Jacobi eigenvectors); the quartz cells' V = 1566 is beyond that kernel

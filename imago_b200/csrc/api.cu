@@ -196,6 +196,10 @@ struct imago_ctx {
   int ortho_mode = -1, ortho = 0;
   bool ortho_tuned = false;
   float ortho_ms[2] = {};
+  // EP terms per contraction CTA (4 or 8), measured on the first EP build
+  int contract_tpc = 4;
+  bool contract_tuned = false;
+  float contract_ms[2] = {};
   long long blk_total = 0, m_total = 0;
   std::vector<Term3c> ep_terms;
 
@@ -1042,8 +1046,9 @@ int tune_bloch(imago_ctx *c, int nterm) {
 // rebuilt SCF set-up, an end-to-end call) starts tuned instead of timing
 // the alternatives again.
 struct TuneRecord {
-  int bloch = -1, sched = -1, ortho = -1;
-  float bloch_ms[kNumBlochWidths] = {}, sched_ms[kNumSchedules] = {}, ortho_ms[2] = {};
+  int bloch = -1, sched = -1, ortho = -1, contract = -1;
+  float bloch_ms[kNumBlochWidths] = {}, sched_ms[kNumSchedules] = {}, ortho_ms[2] = {},
+        contract_ms[2] = {};
 };
 using TuneKey = std::array<long long, 10>;
 std::mutex g_tune_mu;
@@ -1070,6 +1075,10 @@ void tune_store(const imago_ctx *c) {
     r.ortho = c->ortho;
     std::copy(c->ortho_ms, c->ortho_ms + 2, r.ortho_ms);
   }
+  if (c->contract_tuned) {
+    r.contract = c->contract_tpc;
+    std::copy(c->contract_ms, c->contract_ms + 2, r.contract_ms);
+  }
 }
 
 void tune_apply(imago_ctx *c) {
@@ -1092,6 +1101,39 @@ void tune_apply(imago_ctx *c) {
     std::copy(r.ortho_ms, r.ortho_ms + 2, c->ortho_ms);
     c->ortho_tuned = true;
   }
+  if (r.contract > 0) {
+    c->contract_tpc = r.contract;
+    std::copy(r.contract_ms, r.contract_ms + 2, c->contract_ms);
+    c->contract_tuned = true;
+  }
+}
+
+// EP terms per contraction CTA by measurement, on the context's first
+// build of more than four terms: 4 and 8 each run once on the real blocks
+// (the same values) and the faster is kept.
+int tune_contract(imago_ctx *c, const DevSys &s, const DevWork &w, int nterm,
+                  const double *blk, double *M, cudaStream_t st) {
+  cudaEvent_t e[3];
+  for (auto &x : e)
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      cudaGetLastError();
+      return IMAGO_ERR_CUDA;
+    }
+  int rc = IMAGO_OK;
+  cudaEventRecord(e[0], st);
+  for (int k = 0; k < 2 && !rc; ++k) {
+    rc = launch_contract(s, w, nterm, blk, M, st, k ? 8 : 4);
+    cudaEventRecord(e[k + 1], st);
+  }
+  if (!rc && cudaEventSynchronize(e[2]) != cudaSuccess) rc = IMAGO_ERR_CUDA;
+  for (int k = 0; k < 2 && !rc; ++k) cudaEventElapsedTime(&c->contract_ms[k], e[k], e[k + 1]);
+  for (auto &x : e) cudaEventDestroy(x);
+  cudaGetLastError();
+  c->contract_tpc = (!rc && c->contract_ms[1] < c->contract_ms[0]) ? 8 : 4;
+  c->launches += 2;
+  c->contract_tuned = !rc;
+  if (!rc) tune_store(c);
+  return rc;
 }
 
 int launch_prim3c_sched(imago_ctx *c, const DevSys &s, const DevWork &w,
@@ -1204,7 +1246,10 @@ int run_build(imago_ctx *c, Kind kind, int term0, int nterm,
   }
   if (rc) return rc;
   mark(c);
-  if ((rc = launch_contract(s, w, nterm, S.blk.p, S.M.p, st))) return rc;
+  if (nterm > 4 && !c->contract_tuned && !c->capturing &&
+      (rc = tune_contract(c, s, w, nterm, S.blk.p, S.M.p, st)))
+    return rc;
+  if ((rc = launch_contract(s, w, nterm, S.blk.p, S.M.p, st, c->contract_tpc))) return rc;
   mark(c);
   if (!c->bloch_tuned && !c->capturing && s.nk > kBlochSmallNk) {
     if ((rc = tune_bloch(c, nterm))) return rc;
@@ -2148,6 +2193,14 @@ int imago_wait_check(int device, double limit_ms, int *status) {
   cudaGetLastError();
   cudaSetDevice(prev);
   return rc;
+}
+
+int imago_intg_contract_tuning(const imago_ctx *c, int *terms_per_cta, double trial_ms[2]) {
+  if (!c) return IMAGO_ERR_INVALID;
+  if (terms_per_cta) *terms_per_cta = c->contract_tpc;
+  if (trial_ms)
+    for (int i = 0; i < 2; ++i) trial_ms[i] = c->contract_ms[i];
+  return IMAGO_OK;
 }
 
 int imago_intg_set_ham_mode(imago_ctx *c, int mode) {

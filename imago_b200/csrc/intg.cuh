@@ -206,8 +206,9 @@ int launch_prim3c_count(const DevSys &s, const DevWork &w, const int *cls_beg,
 int launch_prim3c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   const Term3c *terms_dev, int nterm, bool nuclear,
                   double *blk, cudaStream_t st, const Term3c *terms_host = nullptr);
+// terms_per_cta: 4 or 8 EP terms per CTA (builds of up to 4 terms use 4)
 int launch_contract(const DevSys &s, const DevWork &w, int nterm,
-                    const double *blk, double *M, cudaStream_t st);
+                    const double *blk, double *M, cudaStream_t st, int terms_per_cta = 4);
 int launch_bloch(const DevSys &s, const DevWork &w, int nterm, const double *M,
                  double2 *vv, double2 *cv, double2 *cc, cudaStream_t st);
 // pipe: the persistent TMA-fed kernel where it applies (several terms,

@@ -73,16 +73,19 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
 // chunks of whole shell pairs with coalesced loads, together with the
 // chunk's shell-pair list and both atoms' coefficient tables; the
 // coefficient product of an (element, shell pair) serves every term of
-// the group.
-constexpr int kTermsPerCta = 4;
+// the group.  T = 4 or 8 terms per CTA, picked by measurement: eight halve
+// the per-(element, shell pair) work of a many-term build but give fewer
+// CTAs and a smaller staging chunk.
 constexpr int kContractThreads = 128;
 constexpr int kElemsPerThread = 3;          // n_i n_j <= 384 per pass
 constexpr int kSpStage = 256;               // shell pairs staged at a time
-constexpr int kBlkStage = 768;              // block doubles per term staged
 constexpr int kCoefMax = 1024;              // alphas x states per atom
 
+template <int T>
 __global__ void __launch_bounds__(kContractThreads, 4)
     k_contract(DevSys s, DevWork w, int nterm, const double *blk, double *M) {
+  constexpr int kTermsPerCta = T;
+  constexpr int kBlkStage = T >= 8 ? 384 : 768;  // block doubles per term staged
   __shared__ int sp_ab[kSpStage];            // a | b << 16
   __shared__ int sp_cls[kSpStage];           // nsh(la) | nsh(lb) << 8
   __shared__ int sp_rel[kSpStage];           // block offset from the chunk's
@@ -181,11 +184,15 @@ __global__ void __launch_bounds__(kContractThreads, 4)
 }
 
 int launch_contract(const DevSys &s, const DevWork &w, int nterm,
-                    const double *blk, double *M, cudaStream_t st) {
+                    const double *blk, double *M, cudaStream_t st, int terms_per_cta) {
   if (w.nunits == 0 || nterm == 0) return IMAGO_OK;
-  const int ntg = (nterm + kTermsPerCta - 1) / kTermsPerCta;
-  const long long grid = (long long)w.nunits * ntg;
-  k_contract<<<(unsigned)grid, kContractThreads, 0, st>>>(s, w, nterm, blk, M);
+  if (terms_per_cta >= 8 && nterm > 4) {
+    const long long grid = (long long)w.nunits * ((nterm + 7) / 8);
+    k_contract<8><<<(unsigned)grid, kContractThreads, 0, st>>>(s, w, nterm, blk, M);
+  } else {
+    const long long grid = (long long)w.nunits * ((nterm + 3) / 4);
+    k_contract<4><<<(unsigned)grid, kContractThreads, 0, st>>>(s, w, nterm, blk, M);
+  }
   IMAGO_CUDA(cudaGetLastError());
   return IMAGO_OK;
 }

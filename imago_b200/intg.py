@@ -111,6 +111,9 @@ def lib():
         L.imago_intg_ortho_schedule.restype = ctypes.c_int
         L.imago_trim_memory.argtypes = [ctypes.c_int]
         L.imago_trim_memory.restype = ctypes.c_int
+        L.imago_intg_contract_tuning.argtypes = [ctypes.c_void_p,
+                                                 ctypes.POINTER(ctypes.c_int), _D]
+        L.imago_intg_contract_tuning.restype = ctypes.c_int
         L.imago_intg_count_triples.argtypes = [ctypes.c_void_p, ctypes.c_uint,
                                                ctypes.POINTER(ctypes.c_longlong)]
         L.imago_intg_count_triples.restype = ctypes.c_int
@@ -388,6 +391,15 @@ class IntegralSetup:
         _check(lib().imago_intg_ortho_schedule(self._ctx, ctypes.byref(s), _p(ms)),
                "imago_intg_ortho_schedule")
         return {"schedule": ("per_item", "piped")[s.value], "trial_ms": ms.tolist()}
+
+    def contract_tuning(self):
+        """{"terms_per_cta": 4 | 8, "trial_ms": [4, 8]}: the contraction's
+        measured terms per CTA (imago_intg_contract_tuning)."""
+        n = ctypes.c_int()
+        ms = np.zeros(2)
+        _check(lib().imago_intg_contract_tuning(self._ctx, ctypes.byref(n), _p(ms)),
+               "imago_intg_contract_tuning")
+        return {"terms_per_cta": n.value, "trial_ms": ms.tolist()}
 
     def count_triples(self, which):
         """Screened primitive triples (shell pair, site, image) per class of

@@ -431,6 +431,11 @@ IMAGO_API int imago_intg_schedule(const imago_ctx *ctx, int *schedule, double tr
  * copy that does not land within its bound (1 s) makes the call return
  * IMAGO_ERR_TIMEOUT. */
 IMAGO_API int imago_intg_set_ortho_schedule(imago_ctx *ctx, int mode);
+/* No counterpart: the EP terms each contraction CTA handles (4 or 8),
+ * measured on the context's first build of more than four terms, and the
+ * trial times (ms, 4 then 8; zero when not measured). */
+IMAGO_API int imago_intg_contract_tuning(const imago_ctx *ctx, int *terms_per_cta,
+                                         double trial_ms[2]);
 /* No counterpart in the reference.  Runs the bounded device wait that the
  * TMA-fed orthogonalisation uses on a barrier that nothing completes, with
  * a limit of limit_ms (0 < limit_ms <= 1000), on `device`'s default stream:

@@ -763,3 +763,19 @@ def test_screened_triple_counts_match_the_oracle_loops(imago_lib, make):
     assert int(cnp.sum()) == ob.last_counts()[2]
     ob.elec_pot()
     assert int(cep.sum()) == ob.last_counts()[2]
+
+
+def test_contraction_terms_per_cta_is_measured_and_exact(imago_lib):
+    # the contraction runs 4 or 8 EP terms per CTA, chosen by timing both on
+    # the first build of more than four terms; either gives the same blocks,
+    # so the EP matrices equal the oracle's within the usual bar
+    s = configs.silicon_cubic8(kmesh=(1, 1, 1))
+    with intg.IntegralSetup(s) as g:
+        g.gauss_overlap_ol()
+        ep = g.elec_pot_gauss_overlap()
+        tun = g.contract_tuning()
+    assert tun["terms_per_cta"] in (4, 8) and min(tun["trial_ms"]) > 0.0
+    ob = oracle.OracleBuild(s)
+    ob.overlap()
+    ref = ob.elec_pot()
+    _assert_all({f"EP{t}": packed_mismatch(ep[t], ref[t]) for t in range(ep.shape[0])})
