@@ -21,6 +21,8 @@
 #include <mutex>
 #include <thread>
 #include <array>
+#include <cstdlib>
+#include <string>
 #include <map>
 #include <numeric>
 #include <vector>
@@ -1108,6 +1110,50 @@ void tune_apply(imago_ctx *c) {
   }
 }
 
+// IMAGO_TUNING fixes measured choices in every context, for profiling
+// runs (a profiler's serialised replays distort the trial timings): a
+// comma-separated list of bloch=32|48|64, sched=per_class|queue|pairs,
+// ortho=per_item|piped, contract=4|8.  Unknown entries are ignored.
+void tune_from_env(imago_ctx *c) {
+  const char *env = std::getenv("IMAGO_TUNING");
+  if (!env) return;
+  std::string all(env);
+  size_t pos = 0;
+  while (pos <= all.size()) {
+    size_t end = all.find(',', pos);
+    if (end == std::string::npos) end = all.size();
+    const std::string item = all.substr(pos, end - pos);
+    pos = end + 1;
+    const size_t eq = item.find('=');
+    if (eq == std::string::npos) continue;
+    const std::string k = item.substr(0, eq), v = item.substr(eq + 1);
+    if (k == "bloch") {
+      for (int wi = 0; wi < kNumBlochWidths; ++wi)
+        if (v == std::to_string(bloch_width(wi))) {
+          set_bloch_width(c, wi);
+          c->bloch_tuned = true;
+        }
+    } else if (k == "sched") {
+      const int m = v == "per_class" ? 0 : v == "queue" ? 1 : v == "pairs" ? 2 : -1;
+      if (m >= 0) {
+        c->sched = m;
+        c->sched_tuned = true;
+      }
+    } else if (k == "ortho") {
+      const int m = v == "per_item" ? 0 : v == "piped" ? 1 : -1;
+      if (m >= 0) {
+        c->ortho = m;
+        c->ortho_tuned = true;
+      }
+    } else if (k == "contract") {
+      if (v == "4" || v == "8") {
+        c->contract_tpc = v == "8" ? 8 : 4;
+        c->contract_tuned = true;
+      }
+    }
+  }
+}
+
 // EP terms per contraction CTA by measurement, on the context's first
 // build of more than four terms: 4 and 8 each run once on the real blocks
 // (the same values) and the faster is kept.
@@ -1770,7 +1816,10 @@ int imago_intg_create(const imago_system *sys, const imago_opts *opts,
     c->events = true;
     rc = upload(c);
   }
-  if (!rc) tune_apply(c);
+  if (!rc) {
+    tune_apply(c);
+    tune_from_env(c);
+  }
   if (!rc) rc = finish(c, rc);
   if (rc) {
     delete c;
