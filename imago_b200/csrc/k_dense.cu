@@ -290,9 +290,16 @@ __global__ void __launch_bounds__(4 * BC, (KOV ? 128 : 256) / BC)
             double2 *cc) {
   constexpr int T = 4 * BC, NWC = BC / 16;
   constexpr int PH = (kBU * kBK + T - 1) / T, ML = kBU * BC / T;
-  // two stages: the next 16 images load (cp.async) during this stage's MMAs
-  __shared__ double2 ph_s[2][kBU][kBKP];
-  __shared__ double m_s[2][kBU][BC + 4];
+  // two stages: the next 16 images load (cp.async) during this stage's MMAs;
+  // the epilogue reuses the same shared memory for the output tile
+  constexpr size_t kPhBytes = 2 * kBU * kBKP * sizeof(double2);
+  constexpr size_t kMBytes = 2 * kBU * (BC + 4) * sizeof(double);
+  constexpr size_t kOutBytes = kBK * (BC + 1) * sizeof(double2);
+  constexpr size_t kSmBytes =
+      kPhBytes + kMBytes > kOutBytes ? kPhBytes + kMBytes : kOutBytes;
+  __shared__ __align__(16) unsigned char bsm[kSmBytes];
+  auto ph_s = reinterpret_cast<double2(*)[kBU][kBKP]>(bsm);
+  auto m_s = reinterpret_cast<double(*)[kBU][BC + 4]>(bsm + kPhBytes);
   const int2 bt = w.btile_w[blockIdx.x];
   const DPair p = w.pairs[bt.x];
   const int ne = p.ni * p.nj, c0 = bt.y * BC;
@@ -358,7 +365,42 @@ __global__ void __launch_bounds__(4 * BC, (KOV ? 128 : 256) / BC)
   }
   }
   // epilogue: origin shift (kPointLatticeOriginShift, intgSaving.F90:241-292,
-  // skipped when |k.L0| < smallThresh) and the scatter
+  // skipped when |k.L0| < smallThresh) and the scatter.  The plain form
+  // stages the 32 k x BC tile through shared memory (the stages' buffers,
+  // free after the last barrier) so that consecutive threads store
+  // consecutive block elements of one k-point.
+  if constexpr (!KOV) {
+    auto out_s = reinterpret_cast<double2(*)[BC + 1]>(bsm);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      const int kl = wk + mt * 8 + (lane >> 2), k = k0 + kl;
+      double sn = 0.0, cs = 1.0;
+      if (k < nk) {
+        const double *kv = s.kxyz + 3 * k;
+        const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
+        if (fabs(dot) >= kSmallThresh) sincos(dot, &sn, &cs);
+      }
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const double re = ar[0][mt][nt][i], im = ai[0][mt][nt][i];
+          const double xr = cs * re - sn * im, xi = cs * im + sn * re;
+          out_s[kl][wc + nt * 8 + 2 * (lane & 3) + i] =
+              s.minus_i ? make_double2(xi, -xr) : make_double2(xr, xi);
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kBK * BC; idx += T) {
+      const int kl = idx / BC, el = idx - kl * BC;
+      const int k = k0 + kl, e = c0 + el;
+      if (k >= nk || e >= ne) continue;
+      const int m2 = e / p.ni, m1 = e - m2 * p.ni;
+      const double2 v = out_s[kl][el];
+      scatter(s, p, (long long)term * nk + k, m1, m2, v.x, v.y, vv, cv, cc);
+    }
+    return;
+  }
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
     const int k = k0 + wk + mt * 8 + (lane >> 2);
