@@ -666,6 +666,8 @@ def test_driver_matches_reference_driver_executed(imago_lib):
     from conftest import ROOT
     g = np.load(os.path.join(ROOT, "tests", "golden", "driver_diamond.npz"))
     with intg.IntegralSetup(configs.diamond_primitive(kmesh=(2, 2, 2))) as s:
+        # numCellsReal as the reference's initializeLattice counts it
+        assert s.num_cells == g["phaseFactor"].shape[0]
         ol, cre, cim = s.gauss_overlap_ol()
         ke = s.gauss_overlap_ke()
         npk = s.gauss_overlap_np()

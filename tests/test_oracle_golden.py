@@ -188,3 +188,20 @@ def test_oracle_driver_matches_reference_driver_executed():
     for a, b in ((ol, g["ol_packed"]), (ke, g["ke_packed"]), (cre, g["ol_cv_re"]),
                  (cim, g["ol_cv_im"]), (npk, g["np_packed"]), (ep, g["ep_packed"])):
         assert packed_mismatch(a, b, atol=1e-13)[1] == 0
+
+
+def test_oracle_cell_list_gives_the_reference_phase_factors():
+    # computePhaseFactors (kpoints.f90:578-609) executed over the
+    # reference's own cell list (initializeLattice): the oracle's integral
+    # cell list, in its order, reproduces every exp(i k.R) of it
+    import os
+    import numpy as np
+    import oracle
+    from conftest import ROOT
+    from imago_b200 import configs
+    g = np.load(os.path.join(ROOT, "tests", "golden", "driver_diamond.npz"))
+    ob = oracle.OracleBuild(configs.diamond_primitive(kmesh=(2, 2, 2)))
+    cells, _ = ob.cells()
+    assert cells.shape[0] == g["phaseFactor"].shape[0]
+    ph = np.exp(1j * (cells @ ob.kpoints_xyz().T))
+    assert np.abs(ph - g["phaseFactor"]).max() < 1e-14
