@@ -399,35 +399,35 @@ __global__ void __launch_bounds__(4 * BC, (KOV ? 128 : 256) / BC)
       const double2 v = out_s[kl][el];
       scatter(s, p, (long long)term * nk + k, m1, m2, v.x, v.y, vv, cv, cc);
     }
-    return;
-  }
+  } else {
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int k = k0 + wk + mt * 8 + (lane >> 2);
-    if (k >= nk) continue;
-    const double *kv = s.kxyz + 3 * k;
-    const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
-    double sn = 0.0, cs = 1.0;
-    if (fabs(dot) >= kSmallThresh) sincos(dot, &sn, &cs);
-    const long long tk = (long long)term * nk + k;
+    for (int mt = 0; mt < 2; ++mt) {
+      const int k = k0 + wk + mt * 8 + (lane >> 2);
+      if (k >= nk) continue;
+      const double *kv = s.kxyz + 3 * k;
+      const double dot = kv[0] * p.L0[0] + kv[1] * p.L0[1] + kv[2] * p.L0[2];
+      double sn = 0.0, cs = 1.0;
+      if (fabs(dot) >= kSmallThresh) sincos(dot, &sn, &cs);
+      const long long tk = (long long)term * nk + k;
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
+      for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int e = c0 + wc + nt * 8 + 2 * (lane & 3) + i;
-        if (e >= ne) continue;
-        // KOV: (phase) x (Mr + i Mi)
-        const double re = KOV ? ar[0][mt][nt][i] - ai[NP - 1][mt][nt][i] : ar[0][mt][nt][i];
-        const double im = KOV ? ai[0][mt][nt][i] + ar[NP - 1][mt][nt][i] : ai[0][mt][nt][i];
-        const int m2 = e / p.ni, m1 = e - m2 * p.ni;
-        const double xr = cs * re - sn * im, xi = cs * im + sn * re;
-        if (KOV)
-          scatter_full(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
-        else if (s.minus_i)
-          scatter(s, p, tk, m1, m2, xi, -xr, vv, cv, cc);
-        else
-          scatter(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
-      }
+        for (int i = 0; i < 2; ++i) {
+          const int e = c0 + wc + nt * 8 + 2 * (lane & 3) + i;
+          if (e >= ne) continue;
+          // KOV: (phase) x (Mr + i Mi)
+          const double re = KOV ? ar[0][mt][nt][i] - ai[NP - 1][mt][nt][i] : ar[0][mt][nt][i];
+          const double im = KOV ? ai[0][mt][nt][i] + ar[NP - 1][mt][nt][i] : ai[0][mt][nt][i];
+          const int m2 = e / p.ni, m1 = e - m2 * p.ni;
+          const double xr = cs * re - sn * im, xi = cs * im + sn * re;
+          if (KOV)
+            scatter_full(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
+          else if (s.minus_i)
+            scatter(s, p, tk, m1, m2, xi, -xr, vv, cv, cc);
+          else
+            scatter(s, p, tk, m1, m2, xr, xi, vv, cv, cc);
+        }
+    }
   }
 }
 
@@ -964,19 +964,21 @@ __global__ void __launch_bounds__(kFThreads, 1)
 // ----------------------------------------------------- ortho, piped --
 // The fused orthogonalisation for builds of several terms as a persistent
 // kernel: one CTA per SM walks a contiguous range of (k, term) items in
-// k-major order.  S(k) stays in shared memory while k is unchanged, and
-// X_cv of the next item comes in by one TMA tensor copy (completing on an
-// mbarrier) into the second of two buffers while the current item's Y and
-// W are formed, so the fill hides behind the tensor-core work.  X_cc is
-// read from L2 by the Y step's fragments.  Shared arrays keep the global
-// layout, core index fastest, in rows of ld complex values with
-// ld = 4 mod 8: the TMA box writes them as they are (its columns beyond C
-// zero-filled), and the fragment reads of a quarter warp (two rows, four
-// k) fall on distinct banks.  Rows v >= V are not stored; their fragments
-// read zero.
+// k-major order.  S(k) stays in shared memory while k is unchanged; X_cv
+// and X_cc of the next item come in by TMA tensor copies (completing on an
+// mbarrier) into the second of two X_cv buffers and the X_cc buffer while
+// the current item's products run, so the fills hide behind the
+// tensor-core work.  S and X_cv are stored in groups of four core indices:
+// element (v, k) at ((k / 4) V + v) 4 + k % 4, one 64-byte TMA box row per
+// (v, group), which puts the two rows and four k of a quarter warp's
+// fragment read on eight distinct 16-byte bank groups without padding;
+// X_cc keeps the global layout (core index c fastest) in rows of ld = 2 mod
+// 8 complex values, conflict-free for the same reads.  Rows v >= V are not
+// stored; their fragments read zero.
 struct PipeDims {
-  int C4, C16, V16, ld;
-  size_t buf;  // bytes of one V x ld array, a multiple of 128
+  int C4, C16, V16, ld, nbox;
+  size_t buf;   // bytes of one S or X_cv array (V x C4 complex), 1024-aligned
+  size_t xbuf;  // bytes of the X_cc array (C4 rows of ld complex)
 };
 
 __host__ __device__ inline PipeDims pipe_dims(int C, int V) {
@@ -984,8 +986,10 @@ __host__ __device__ inline PipeDims pipe_dims(int C, int V) {
   d.C4 = (C + 3) / 4 * 4;
   d.C16 = (C + 15) / 16 * 16;
   d.V16 = (V + 15) / 16 * 16;
-  d.ld = d.C4 % 8 == 0 ? d.C4 + 4 : d.C4;
-  d.buf = ((size_t)V * d.ld * sizeof(double2) + 127) / 128 * 128;
+  d.nbox = d.C4 / 4;
+  d.ld = d.C4 + ((2 - d.C4 % 8) + 8) % 8;
+  d.buf = ((size_t)V * d.C4 * sizeof(double2) + 1023) / 1024 * 1024;
+  d.xbuf = ((size_t)d.C4 * d.ld * sizeof(double2) + 127) / 128 * 128;
   return d;
 }
 
@@ -993,33 +997,37 @@ __host__ __device__ inline PipeDims pipe_dims(int C, int V) {
 // static shared state
 constexpr size_t kPipeMaxSmem = 227 * 1024 - 1024;
 
-inline size_t pipe_smem(int C, int V) { return 3 * pipe_dims(C, V).buf + 64; }
+inline size_t pipe_smem(int C, int V) {
+  const PipeDims d = pipe_dims(C, V);
+  return 3 * d.buf + d.xbuf + 64;
+}
 
 bool ortho_pipe_fits(int C, int V) {
   const PipeDims d = pipe_dims(C, V);
-  return C > 0 && V > 0 && V <= 256 && 2 * d.ld <= 256 && pipe_smem(C, V) <= kPipeMaxSmem;
+  return C > 0 && V > 0 && V <= 256 && d.C4 <= 256 && 2 * d.ld <= 256 &&
+         pipe_smem(C, V) <= kPipeMaxSmem;
 }
 
+// Element (v, k) of an S or X_cv array in groups of four k.
+__device__ __forceinline__ int pv(int V, int v, int k) { return (((k >> 2) * V + v) << 2) + (k & 3); }
+
 // One warp's 16x16 complex subtile of op(A)^T B over k in [0, nk4), A and B
-// stored [index][k] with row stride ld; rows at or beyond na (A) or nb (B)
-// read as zero.  3M form as fused_tile.
+// grouped arrays (rows v); rows at or beyond V read as zero.  3M form as
+// fused_tile.
 template <bool CONJ, bool REAL>
-__device__ __forceinline__ void pipe_tile(const double2 *A, int na, int r0, const double2 *B,
-                                          int nb, int c0, int ld, int nk4, bool skip_lower,
-                                          double t1[2][2][2], double t2[2][2][2],
-                                          double t3[2][2][2], int lane) {
+__device__ __forceinline__ void pipe_tile(const double2 *A, int r0, const double2 *B, int c0,
+                                          int V, int nk4, bool skip_lower, double t1[2][2][2],
+                                          double t2[2][2][2], double t3[2][2][2], int lane) {
   const int ra0 = r0 + (lane >> 2), cb0 = c0 + (lane >> 2);
-  const bool va[2] = {ra0 < na, ra0 + 8 < na}, vb[2] = {cb0 < nb, cb0 + 8 < nb};
-  const double2 *pa[2] = {A + (long long)ra0 * ld, A + (long long)(ra0 + 8) * ld};
-  const double2 *pb[2] = {B + (long long)cb0 * ld, B + (long long)(cb0 + 8) * ld};
+  const bool va[2] = {ra0 < V, ra0 + 8 < V}, vb[2] = {cb0 < V, cb0 + 8 < V};
   for (int ks = 0; ks < nk4; ks += 4) {
     const int kk = ks + (lane & 3);
     double2 a[2], b[2];
     double as[2], bs[2];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      a[t] = va[t] ? pa[t][kk] : make_double2(0.0, 0.0);
-      b[t] = vb[t] ? pb[t][kk] : make_double2(0.0, 0.0);
+      a[t] = va[t] ? A[pv(V, ra0 + 8 * t, kk)] : make_double2(0.0, 0.0);
+      b[t] = vb[t] ? B[pv(V, cb0 + 8 * t, kk)] : make_double2(0.0, 0.0);
       as[t] = CONJ ? a[t].x - a[t].y : a[t].x + a[t].y;
       bs[t] = b[t].x + b[t].y;
     }
@@ -1036,49 +1044,47 @@ __device__ __forceinline__ void pipe_tile(const double2 *A, int na, int r0, cons
   }
 }
 
-// The Y step's product X_cc S: A(l, c) = X_cc(c, l) = XC[l * C + c] from
-// global memory (L2), B(l, v) = S(l, v) from the shared [v][l] array.
+// The Y step's product X_cc S on an 8 core x 16 valence tile: A(l, c) =
+// X_cc(c, l) from the shared [l][c] array (row pitch ld), B(l, v) = S(l, v)
+// from the grouped array.
 template <bool REAL>
-__device__ __forceinline__ void pipe_y_tile(const double2 *__restrict__ XC, int C, int r0,
-                                            const double2 *S, int V, int c0, int ld, int nk4,
-                                            double t1[2][2][2], double t2[2][2][2],
-                                            double t3[2][2][2], int lane) {
-  const int ra0 = r0 + (lane >> 2), cb0 = c0 + (lane >> 2);
-  const bool vb[2] = {cb0 < V, cb0 + 8 < V};
-  const double2 *pb[2] = {S + (long long)cb0 * ld, S + (long long)(cb0 + 8) * ld};
+__device__ __forceinline__ void pipe_y_tile(const double2 *XC, int ld, int C, int r0,
+                                            const double2 *S, int V, int c0, int nk4,
+                                            double t1[2][2], double t2[2][2], double t3[2][2],
+                                            int lane) {
+  const int ra = r0 + (lane >> 2), cb0 = c0 + (lane >> 2);
+  const bool va = ra < C, vb[2] = {cb0 < V, cb0 + 8 < V};
   for (int ks = 0; ks < nk4; ks += 4) {
     const int kk = ks + (lane & 3);
-    double2 a[2], b[2];
-    double as[2], bs[2];
+    const double2 a = va ? XC[kk * ld + ra] : make_double2(0.0, 0.0);
+    const double as = a.x + a.y;
+    double2 b[2];
+    double bs[2];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      const int c = ra0 + 8 * t;
-      a[t] = (c < C && kk < C) ? __ldg(XC + (long long)kk * C + c) : make_double2(0.0, 0.0);
-      b[t] = vb[t] ? pb[t][kk] : make_double2(0.0, 0.0);
-      as[t] = a[t].x + a[t].y;
+      b[t] = vb[t] ? S[pv(V, cb0 + 8 * t, kk)] : make_double2(0.0, 0.0);
       bs[t] = b[t].x + b[t].y;
     }
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) {
-        dmma(t1[mt][nt][0], t1[mt][nt][1], a[mt].x, b[nt].x);
-        if (REAL) continue;
-        dmma(t2[mt][nt][0], t2[mt][nt][1], a[mt].y, b[nt].y);
-        dmma(t3[mt][nt][0], t3[mt][nt][1], as[mt], bs[nt]);
-      }
+    for (int nt = 0; nt < 2; ++nt) {
+      dmma(t1[nt][0], t1[nt][1], a.x, b[nt].x);
+      if (REAL) continue;
+      dmma(t2[nt][0], t2[nt][1], a.y, b[nt].y);
+      dmma(t3[nt][0], t3[nt][1], as, bs[nt]);
+    }
   }
 }
 
 // What every thread of a k_ortho_pipe CTA reads (kept in shared memory,
 // written once by thread 0).
 struct PipeCta {
-  const double2 *vv, *cc;
+  const double2 *vv;
   double *packed;
-  double2 *Ss, *Xb[2];
+  double2 *Ss, *Xb[2], *Xc;
   uint64_t *bar;       // S, X buffer 0, X buffer 1
   int *ctr;            // task counters, one per phase parity
-  int V, C, nk, nterm, ld, C4, nup, ny, yr;
+  int V, C, nk, nterm, ld, C4, nbox, nup, ny, yr;
+  unsigned tx_s, tx_x; // bytes of the S copy; of one item's X_cv and X_cc copies
   long long np, i0;
 };
 
@@ -1099,8 +1105,8 @@ __device__ __forceinline__ void pipe_w_task(const PipeCta &p, long long q, int t
   const int J = t, r0 = J * 16, c0 = I * 16;
   // VV is read in the epilogue: other warps' products cover its latency
   double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
-  pipe_tile<true, REAL>(p.Ss, V, r0, Ys, V, c0, p.ld, p.C4, J == I, t1, t2, t3, lane);
-  pipe_tile<true, REAL>(Ys, V, r0, p.Ss, V, c0, p.ld, p.C4, J == I, t1, t2, t3, lane);
+  pipe_tile<true, REAL>(p.Ss, r0, Ys, c0, V, p.C4, J == I, t1, t2, t3, lane);
+  pipe_tile<true, REAL>(Ys, r0, p.Ss, c0, V, p.C4, J == I, t1, t2, t3, lane);
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -1121,54 +1127,68 @@ __device__ __forceinline__ void pipe_w_task(const PipeCta &p, long long q, int t
       }
 }
 
-// One Y tile (16 core x 16 valence) of item q: Y = X_cv - X_cc S / 2 in place.
+// One Y tile (8 core x 16 valence) of item q: Y = X_cv - X_cc S / 2 in
+// place, X_cc from the shared copy of the item.
 template <bool REAL>
 __device__ __forceinline__ void pipe_y_task(const PipeCta &p, long long q, int tile, int lane) {
   const int C = p.C, V = p.V;
-  const long long tk = (long long)(q % p.nterm) * p.nk + q / p.nterm;
   double2 *Ys = p.Xb[(q - p.i0) & 1];
-  const double2 *XC = p.cc + tk * C * C;
-  const int r0 = (tile % p.yr) * 16, c0 = (tile / p.yr) * 16;
-  double t1[2][2][2] = {}, t2[2][2][2] = {}, t3[2][2][2] = {};
-  pipe_y_tile<REAL>(XC, C, r0, p.Ss, V, c0, p.ld, p.C4, t1, t2, t3, lane);
+  const int r0 = (tile % p.yr) * 8, c0 = (tile / p.yr) * 16;
+  double t1[2][2] = {}, t2[2][2] = {}, t3[2][2] = {};
+  pipe_y_tile<REAL>(p.Xc, p.ld, C, r0, p.Ss, V, c0, p.C4, t1, t2, t3, lane);
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
+  for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int c = r0 + 8 * mt + (lane >> 2);
-        const int v = c0 + 8 * nt + 2 * (lane & 3) + e;
-        if (c >= C || v >= V) continue;
-        const double2 d = ocombine<false, REAL>(t1[mt][nt][e], t2[mt][nt][e], t3[mt][nt][e]);
-        double2 &y = Ys[v * p.ld + c];
-        y.x -= 0.5 * d.x;
-        y.y -= 0.5 * d.y;
-      }
+    for (int e = 0; e < 2; ++e) {
+      const int c = r0 + (lane >> 2);
+      const int v = c0 + 8 * nt + 2 * (lane & 3) + e;
+      if (c >= C || v >= V) continue;
+      const double2 d = ocombine<false, REAL>(t1[nt][e], t2[nt][e], t3[nt][e]);
+      double2 &y = Ys[pv(V, v, c)];
+      y.x -= 0.5 * d.x;
+      y.y -= 0.5 * d.y;
+    }
+}
+
+// The copies of item q's X_cv (nbox boxes of four core indices) into buffer
+// b and of its X_cc into the X_cc buffer, all completing on bar[1 + b].
+__device__ __forceinline__ void pipe_issue_x(const PipeCta &p, long long q, int b,
+                                             const CUtensorMap *map_x,
+                                             const CUtensorMap *map_c) {
+  const int z = (int)((q % p.nterm) * p.nk + q / p.nterm);
+  fence_proxy_async();
+  mbar_expect_tx(&p.bar[1 + b], p.tx_x);
+  for (int g = 0; g < p.nbox; ++g)
+    tma_load_3d(p.Xb[b] + (size_t)g * p.V * 4, map_x, &p.bar[1 + b], 8 * g, 0, z);
+  tma_load_3d(p.Xc, map_c, &p.bar[1 + b], 0, 0, z);
+}
+
+// S(k) into its buffer (nbox boxes), completing on bar[0].
+__device__ __forceinline__ void pipe_issue_s(const PipeCta &p, int k, const CUtensorMap *map_s) {
+  fence_proxy_async();
+  mbar_expect_tx(&p.bar[0], p.tx_s);
+  for (int g = 0; g < p.nbox; ++g)
+    tma_load_3d(p.Ss + (size_t)g * p.V * 4, map_s, &p.bar[0], 8 * g, 0, k);
 }
 
 // One phase between two CTA barriers: the W tiles of item wq (wq < 0: none)
 // first, then the Y tiles of item yq (yq < 0: none), handed to warps one
 // tile at a time from the phase's counter so that the two kinds balance.
-// Y tiles wait (bounded) for their item's X_cv copy.  At the start, the
-// counter of the next phase is cleared, and X_cv of item xq (xq < 0: none)
-// is sent for into its buffer, whose last reader ended at the barrier
-// before.  px holds the parity of each X barrier's next completion.
-// False (on every thread) when a copy did not land in time.
+// Y tiles wait (bounded) for their item's copies.  At the start, the
+// counter of the next phase is cleared, and the copies of item xq (xq < 0:
+// none) are sent for: its X_cv buffer and the X_cc buffer were last read by
+// the phase before, which ended at a barrier.  px holds the parity of each
+// X barrier's next completion.  False (on every thread) when a copy did not
+// land in time.
 template <bool REAL>
 __device__ __forceinline__ bool pipe_phase(const PipeCta &p, unsigned px[2], int &ph,
                                            long long wq, long long yq, long long xq,
-                                           const CUtensorMap *map_x) {
+                                           const CUtensorMap *map_x,
+                                           const CUtensorMap *map_c) {
   const int tid = threadIdx.x, lane = tid & 31;
   if (tid == 0) {
     p.ctr[ph ^ 1] = 0;
-    if (xq >= 0) {
-      const int b = (int)((xq - p.i0) & 1);
-      fence_proxy_async();
-      mbar_expect_tx(&p.bar[1 + b], (unsigned)(16 * p.ld) * (unsigned)p.V);
-      tma_load_3d(p.Xb[b], map_x, &p.bar[1 + b], 0, 0,
-                  (int)((xq % p.nterm) * p.nk + xq / p.nterm));
-    }
+    if (xq >= 0) pipe_issue_x(p, xq, (int)((xq - p.i0) & 1), map_x, map_c);
   }
   const int nw = wq >= 0 ? p.nup : 0, ntask = nw + (yq >= 0 ? p.ny : 0);
   const int yb = yq >= 0 ? (int)((yq - p.i0) & 1) : 0;
@@ -1200,9 +1220,10 @@ __device__ __forceinline__ bool pipe_phase(const PipeCta &p, unsigned px[2], int
 template <bool REAL>
 __global__ void __launch_bounds__(kFThreads, 1)
     k_ortho_pipe(DevSys s, const __grid_constant__ CUtensorMap map_x,
-                 const __grid_constant__ CUtensorMap map_s, const double2 *vv,
-                 const double2 *cc, int nterm, double *packed) {
-  extern __shared__ __align__(128) unsigned char psm[];
+                 const __grid_constant__ CUtensorMap map_c,
+                 const __grid_constant__ CUtensorMap map_s, const double2 *vv, int nterm,
+                 double *packed) {
+  extern __shared__ __align__(1024) unsigned char psm[];
   const int V = s.vale_dim, C = s.core_dim, nk = s.nk;
   const PipeDims d = pipe_dims(C, V);
   const long long N = (long long)nk * nterm;
@@ -1212,12 +1233,12 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const int tid = threadIdx.x;
   if (tid == 0) {
     p.vv = vv;
-    p.cc = cc;
     p.packed = packed;
     p.Ss = reinterpret_cast<double2 *>(psm);
     p.Xb[0] = reinterpret_cast<double2 *>(psm + d.buf);
     p.Xb[1] = reinterpret_cast<double2 *>(psm + 2 * d.buf);
-    p.bar = reinterpret_cast<uint64_t *>(psm + 3 * d.buf);
+    p.Xc = reinterpret_cast<double2 *>(psm + 3 * d.buf);
+    p.bar = reinterpret_cast<uint64_t *>(psm + 3 * d.buf + d.xbuf);
     p.ctr = reinterpret_cast<int *>(p.bar + 3);
     p.V = V;
     p.C = C;
@@ -1225,10 +1246,13 @@ __global__ void __launch_bounds__(kFThreads, 1)
     p.nterm = nterm;
     p.ld = d.ld;
     p.C4 = d.C4;
+    p.nbox = d.nbox;
     const int nt16 = d.V16 / 16;
     p.nup = nt16 * (nt16 + 1) / 2;
-    p.yr = d.C16 / 16;
+    p.yr = (C + 7) / 8;  // Y tiles of 8 core indices
     p.ny = p.yr * nt16;
+    p.tx_s = (unsigned)(d.nbox * V * 64);
+    p.tx_x = p.tx_s + (unsigned)(d.C4 * d.ld * 16);
     p.np = (long long)V * (V + 1) / 2;
     p.i0 = i0;
     for (int b = 0; b < 3; ++b) mbar_init(&p.bar[b], 1);
@@ -1236,14 +1260,10 @@ __global__ void __launch_bounds__(kFThreads, 1)
     mbar_init_fence();
   }
   __syncthreads();
-  const unsigned tx = (unsigned)(16 * d.ld) * (unsigned)V;
   unsigned ps = 0, px[2] = {0u, 0u};
   int ph = 0;
   int k = (int)(i0 / nterm);
-  if (tid == 0) {
-    mbar_expect_tx(&p.bar[0], tx);
-    tma_load_3d(p.Ss, &map_s, &p.bar[0], 0, 0, k);
-  }
+  if (tid == 0) pipe_issue_s(p, k, &map_s);
   // S(k): waited for by every thread; on a timeout the copy in flight gets
   // one more bounded wait before the CTA leaves
   auto load_s_wait = [&]() -> bool {
@@ -1258,25 +1278,21 @@ __global__ void __launch_bounds__(kFThreads, 1)
   };
   bool ok = load_s_wait();
   // item i0: its Y tiles alone
-  ok = ok && pipe_phase<REAL>(p, px, ph, -1, i0, i0, &map_x);
+  ok = ok && pipe_phase<REAL>(p, px, ph, -1, i0, i0, &map_x, &map_c);
   for (long long q = i0 + 1; ok && q < i1; ++q) {
     const int kq = (int)(q / nterm);
     if (kq == k) {
-      ok = pipe_phase<REAL>(p, px, ph, q - 1, q, q, &map_x);
+      ok = pipe_phase<REAL>(p, px, ph, q - 1, q, q, &map_x, &map_c);
       continue;
     }
     // a new k: the previous item's W tiles, then S(kq), then this item's Y
-    ok = pipe_phase<REAL>(p, px, ph, q - 1, -1, q, &map_x);
+    ok = pipe_phase<REAL>(p, px, ph, q - 1, -1, q, &map_x, &map_c);
     if (!ok) break;
     k = kq;
-    if (tid == 0) {
-      fence_proxy_async();
-      mbar_expect_tx(&p.bar[0], tx);
-      tma_load_3d(p.Ss, &map_s, &p.bar[0], 0, 0, k);
-    }
-    ok = load_s_wait() && pipe_phase<REAL>(p, px, ph, -1, q, -1, &map_x);
+    if (tid == 0) pipe_issue_s(p, k, &map_s);
+    ok = load_s_wait() && pipe_phase<REAL>(p, px, ph, -1, q, -1, &map_x, &map_c);
   }
-  if (ok) ok = pipe_phase<REAL>(p, px, ph, i1 - 1, -1, -1, &map_x);
+  if (ok) ok = pipe_phase<REAL>(p, px, ph, i1 - 1, -1, -1, &map_x, &map_c);
   if (!ok && tid == 0) {
     report_status(s.flag, IMAGO_ERR_TIMEOUT);
     // copies still in flight get one more bounded wait before the CTA leaves
@@ -1332,9 +1348,8 @@ bool encode_tensor_map_f64_3d(CUtensorMap *map, const void *base, const uint64_t
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// The piped orthogonalisation when it applies (several terms, the three
-// arrays in shared memory, tensor maps accepted); *launched says whether it
-// ran.
+// The piped orthogonalisation when it applies (several terms, the arrays in
+// shared memory, tensor maps accepted); *launched says whether it ran.
 int launch_ortho_pipe(const DevSys &s, int nterm, const double2 *vv, const double2 *cv,
                       const double2 *cc, const double2 *s_cv, double *packed, bool *launched,
                       cudaStream_t st) {
@@ -1342,13 +1357,20 @@ int launch_ortho_pipe(const DevSys &s, int nterm, const double2 *vv, const doubl
   const int V = s.vale_dim, C = s.core_dim;
   if (nterm < 2 || !ortho_pipe_fits(C, V)) return IMAGO_OK;
   const PipeDims d = pipe_dims(C, V);
-  CUtensorMap mx, ms;
+  CUtensorMap mx, mc, ms;
+  // X_cv and S: rows of 2C doubles (v), boxes of 8 doubles (four core
+  // indices) x V rows; X_cc: rows of 2C doubles (l), one box of 2 ld
+  // doubles x C4 rows.  Beyond C, zero fill.
   const uint64_t dx[3] = {2ull * C, (uint64_t)V, (uint64_t)nterm * s.nk};
   const uint64_t ds[3] = {2ull * C, (uint64_t)V, (uint64_t)s.nk};
-  const uint64_t str[2] = {16ull * C, 16ull * V * C};
-  const uint32_t box[3] = {2u * d.ld, (uint32_t)V, 1u};
-  if (!encode_tensor_map_f64_3d(&mx, cv, dx, str, box) ||
-      !encode_tensor_map_f64_3d(&ms, s_cv, ds, str, box))
+  const uint64_t dc[3] = {2ull * C, (uint64_t)C, (uint64_t)nterm * s.nk};
+  const uint64_t sv[2] = {16ull * C, 16ull * V * C};
+  const uint64_t sc[2] = {16ull * C, 16ull * C * C};
+  const uint32_t bv[3] = {8u, (uint32_t)V, 1u};
+  const uint32_t bc[3] = {2u * d.ld, (uint32_t)d.C4, 1u};
+  if (!encode_tensor_map_f64_3d(&mx, cv, dx, sv, bv) ||
+      !encode_tensor_map_f64_3d(&ms, s_cv, ds, sv, bv) ||
+      !encode_tensor_map_f64_3d(&mc, cc, dc, sc, bc))
     return IMAGO_OK;
   int dev = 0, nsm = 0;
   IMAGO_CUDA(cudaGetDevice(&dev));
@@ -1364,9 +1386,9 @@ int launch_ortho_pipe(const DevSys &s, int nterm, const double2 *vv, const doubl
   const long long N = (long long)nterm * s.nk;
   const unsigned grid = (unsigned)std::min<long long>(nsm, N);
   if (s.real_k)
-    k_ortho_pipe<true><<<grid, kFThreads, smem, st>>>(s, mx, ms, vv, cc, nterm, packed);
+    k_ortho_pipe<true><<<grid, kFThreads, smem, st>>>(s, mx, mc, ms, vv, nterm, packed);
   else
-    k_ortho_pipe<false><<<grid, kFThreads, smem, st>>>(s, mx, ms, vv, cc, nterm, packed);
+    k_ortho_pipe<false><<<grid, kFThreads, smem, st>>>(s, mx, mc, ms, vv, nterm, packed);
   IMAGO_CUDA(cudaGetLastError());
   *launched = true;
   return IMAGO_OK;
