@@ -635,7 +635,7 @@ def silica_headline(args, local, stream, torch):
 
 
 def schedules(g, bufs, stream, flush, torch, steps=3):
-    """The three-centre stage's schedules on this build: per-class
+    """The three-centre stage's schedules on the context's build: per-class
     launches, the persistent work-queue launch and per-class launches with
     two EP terms per thread (device seconds of
     whole builds replayed from graphs, and the primitive stage's ms with the

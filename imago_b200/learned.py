@@ -27,7 +27,7 @@ pass and Adam.  This module holds the host side:
                         averaged over the atoms of each potential type (all
                         sites of a type share its coefficients)
   compare(...)          plain start against learned start on one system,
-                        the plain start being the judge: the learned start
+                        the plain start being the reference: the learned start
                         is discarded when its converged energy is more than
                         1e-6 Ha from the plain start's or it needs more
                         iterations
@@ -333,8 +333,8 @@ def compare(system, learned, params=None, device=0):
     """Plain start and learned start on one system, integrals and SCF set-up
     shared and built once (their time is reported apart), with
     metric_params() unless `params` is given.  Returns the two runs, the
-    learned start's inference time and whether it is kept (the plain start
-    judges: within 1e-6 Ha of its energy, no more iterations)."""
+    learned start's inference time and whether it is kept (measured against
+    the plain start: within 1e-6 Ha of its energy, no more iterations)."""
     import torch
     p = params or metric_params()
     ints, t_int = scf.device_integrals(system, device)

@@ -8,7 +8,7 @@
  * (src/imago/potential.f90:433-563).  The learned start maps each atom's
  * radial environment to a correction of that start; the caller (the Python
  * host, imago_b200/learned.py) averages the corrections over the atoms of
- * each potential type, keeps the plain start as the fallback and judge, and
+ * each potential type, keeps the plain start as the fallback and the yardstick, and
  * discards a learned start that does not reach the plain start's energy or
  * takes more iterations.
  *
