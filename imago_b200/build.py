@@ -61,7 +61,7 @@ def build(verbose=False):
     with concurrent.futures.ThreadPoolExecutor(len(SOURCES)) as ex:
         objs = list(ex.map(_compile, SOURCES))
     if _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -152,6 +152,9 @@ struct HPType {
 
 }  // namespace
 
+// The library's device scratch pool for code outside this file.
+cudaMemPool_t imago::device_scratch_pool() { return scratch_pool(); }
+
 constexpr int kNumSchedules = 3;  // three-centre schedules, imago_intg_set_schedule
 
 struct imago_ctx {

@@ -132,6 +132,10 @@ struct Term3c {
 // Two-centre primitive operators of launch_prim2c.
 enum { kPrim2cOverlap = 0, kPrim2cKinetic = 1, kPrim2cMassVel = 2 };
 
+// The library's stream-ordered device memory pool of the current device
+// (freed memory stays in it until imago_trim_memory); null if none.
+cudaMemPool_t device_scratch_pool();
+
 // Launchers (kernels.cu).  All take the stream to run on.
 int launch_prim2c(const DevSys &s, const DevWork &w, const int *cls_beg,
                   int op, double *blk, cudaStream_t st);

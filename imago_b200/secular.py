@@ -55,15 +55,15 @@ def secular_matrices(out, pot_coeffs, stream=None):
 
 
 JACOBI_MAX_N = 112
+_ERR_RANGE = 8  # IMAGO_ERR_RANGE
 
 
 def hermitian_eigvals(a):
     """Ascending eigenvalues of a batch of Hermitian matrices [b, n, n]
     (complex128, CUDA): imago_hermitian_eigvals (one CTA per matrix, cyclic
-    Jacobi in shared memory) up to n = 112, cuSOLVER through torch beyond."""
+    Jacobi in shared memory) up to n = 112, cuSOLVER's batched solver
+    through the library beyond (torch's eigvalsh if that is absent)."""
     b, n = a.shape[0], a.shape[-1]
-    if n > JACOBI_MAX_N:
-        return torch.linalg.eigvalsh(a)
     a = a.contiguous()
     w = torch.empty((b, n), dtype=torch.float64, device=a.device)
     L = intg.lib()
@@ -72,6 +72,8 @@ def hermitian_eigvals(a):
     L.imago_hermitian_eigvals.restype = ctypes.c_int
     rc = L.imago_hermitian_eigvals(n, b, a.data_ptr(), w.data_ptr(),
                                    torch.cuda.current_stream().cuda_stream)
+    if rc == _ERR_RANGE and n > JACOBI_MAX_N:  # no batched cuSOLVER in the process
+        return torch.linalg.eigvalsh(a)
     if rc:
         raise intg.ImagoError(rc, "imago_hermitian_eigvals")
     return w
@@ -122,11 +124,9 @@ def hermitian_eigh(a):
     """Ascending eigenvalues [b, n] and unit eigenvectors [b, n, n] (in
     columns) of a batch of Hermitian matrices [b, n, n] (complex128, CUDA):
     imago_hermitian_eigh (the Jacobi kernel accumulating its rotations) up
-    to n = 112, cuSOLVER through torch beyond (one host thread and stream
-    per lane of matrices, _eigh_lanes)."""
+    to n = 112, cuSOLVER's batched solver through the library beyond (one
+    call for the batch; _eigh_lanes if the process has no batched solver)."""
     b, n = a.shape[0], a.shape[-1]
-    if n > JACOBI_MAX_N:
-        return _eigh_lanes(a) if b > 1 else torch.linalg.eigh(a)
     a = a.contiguous()
     w = torch.empty((b, n), dtype=torch.float64, device=a.device)
     v = torch.empty((b, n, n), dtype=torch.complex128, device=a.device)
@@ -135,6 +135,8 @@ def hermitian_eigh(a):
     L.imago_hermitian_eigh.restype = ctypes.c_int
     rc = L.imago_hermitian_eigh(n, b, a.data_ptr(), w.data_ptr(), v.data_ptr(),
                                 torch.cuda.current_stream().cuda_stream)
+    if rc == _ERR_RANGE and n > JACOBI_MAX_N:  # no batched cuSOLVER in the process
+        return _eigh_lanes(a) if b > 1 else torch.linalg.eigh(a)
     if rc:
         raise intg.ImagoError(rc, "imago_hermitian_eigh")
     return w, v

@@ -387,8 +387,8 @@ IMAGO_API int imago_secular_matrices_rel(int vale_dim, int num_kpoints, int pot_
 /*
  * Eigenvalues of `batch` Hermitian n x n matrices (device memory, (re, im)
  * interleaved, either storage order) into w [batch][n], ascending, by a
- * cyclic Jacobi method with each matrix in shared memory (n up to 112,
- * IMAGO_ERR_RANGE beyond).  The eigenvalue step of the secular equation
+ * cyclic Jacobi method with each matrix in shared memory (n up to 112;
+ * beyond, cuSOLVER's batched solver as below).  The eigenvalue step of the secular equation
  * (zhegv after its Cholesky reduction, interfaces.F90:73-120).
  */
 IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
@@ -398,8 +398,12 @@ IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
  * a[b][row][col], and vec [batch][n][n] (device, (re, im) interleaved)
  * receives vec[b][row][j], the row-th component of the unit eigenvector of
  * w[b][j] (the columns of V with A V = V diag(w)), accumulated from the
- * Jacobi rotations.  The eigenvector step of zhegv(1, 'V', 'U') after its
- * Cholesky reduction (interfaces.F90:73-120). */
+ * Jacobi rotations.  Above n = 112 both functions hand the batch to
+ * cuSOLVER's batched Hermitian eigensolver (cusolverDnXsyevBatched, loaded
+ * from the process's libcusolver.so.11; IMAGO_ERR_RANGE when it is absent)
+ * under the same contract, synchronising the stream to check its status.
+ * The eigenvector step of zhegv(1, 'V', 'U') after its Cholesky reduction
+ * (interfaces.F90:73-120). */
 IMAGO_API int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
                                    double *vec, void *stream);
 

@@ -142,3 +142,27 @@ def test_mass_velocity_shifts_the_oracle_eigenvalues():
     b = oracle.secular_eigenvalues(npm, ke, ep, w, ol, mv_packed=mv)
     assert np.all(b <= a + 1e-12)
     assert np.all(a - b <= 0.05 * (np.abs(a) + 1.0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [113, 208])
+def test_batched_eigensolver_beyond_the_jacobi_kernel(imago_lib, n):
+    # above n = 112 imago_hermitian_eigh hands the batch to cuSOLVER's
+    # batched solver under the same contract: ascending eigenvalues equal to
+    # LAPACK's, unit eigenvectors in columns with A V = V diag(w)
+    import torch
+    from imago_b200 import secular
+    rng = np.random.default_rng(n)
+    x = rng.normal(size=(3, n, n)) + 1j * rng.normal(size=(3, n, n))
+    a = (x + np.conj(np.transpose(x, (0, 2, 1)))) / 2
+    at = torch.tensor(a, device="cuda")
+    w, v = secular.hermitian_eigh(at)
+    w, v = w.cpu().numpy(), v.cpu().numpy()
+    ref = np.linalg.eigvalsh(a)
+    assert np.abs(w - ref).max() < 1e-10 * np.abs(ref).max()
+    for b in range(3):
+        r = a[b] @ v[b] - v[b] * w[b][None, :]
+        assert np.abs(r).max() < 1e-10 * np.abs(ref[b]).max()
+        assert np.abs(np.conj(v[b].T) @ v[b] - np.eye(n)).max() < 1e-10
+    assert np.abs(secular.hermitian_eigvals(at).cpu().numpy() - ref).max() < \
+        1e-10 * np.abs(ref).max()
