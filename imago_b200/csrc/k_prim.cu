@@ -156,24 +156,25 @@ __device__ __forceinline__ void prim3c_item(const DevSys &s, const DevWork &w, i
         const double *R = s.cell + 3 * nc;
         const double dx = v[0] - R[0], dy = v[1] - R[1], dz = v[2] - R[2];
         if (dx * dx + dy * dy + dz * dz > t) continue;
-        if (CNT) {
+        if constexpr (CNT) {
           ++*ntrip;
-          continue;
-        }
-        double X[3];
+        } else {
+          double X[3];
 #pragma unroll
-        for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
-        if (NUC)
-          accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
-        else
-          accumulate_overlap_q<L>(X, mu, 1.0, Q);
+          for (int x = 0; x < 3; ++x) X[x] = Pt[x] - (C[x] + L2[x] + R[x]);
+          if (NUC)
+            accumulate_nuclear_q<L>(X, mu, nu, w0, Q);
+          else
+            accumulate_overlap_q<L>(X, mu, 1.0, Q);
+        }
       }
     }
   }
-  if (CNT) return;
-  const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
-  hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q,
-                        blk + (long long)tl * w.blk_total + sp.boff);
+  if constexpr (!CNT) {
+    const double pref = NUC ? exp(-xi * q.r2) : pow(kPi / z3e, 1.5) * exp(-xi * q.r2);
+    hermite_to_sh<LA, LB>(q.A, q.B, q.a1, q.a2, pref, Q,
+                          blk + (long long)tl * w.blk_total + sp.boff);
+  }
 }
 
 // The Hermite-to-spherical transform of one term of a pair, as a call: the
