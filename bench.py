@@ -431,6 +431,66 @@ def time_secular(bufs, pot_dim, stream, torch, steps=3):
     return float(np.median(ts))
 
 
+def _event_ms(fn, stream, torch, steps=3):
+    fn()
+    ts = []
+    for _ in range(steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def time_reduction(out, w, pop, stream, torch):
+    """Device milliseconds (median of 3, CUDA events) of the library's
+    Cholesky reduction (A = L^-1 H L^-H), back-transformation (c = L^-H y for
+    the populated states' count of vectors) and packed density for every
+    k-point, each beside the cuSOLVER / cuBLAS calls through torch that do
+    the same work (batched Cholesky and triangular solves; a complex GEMM
+    and the packing gather), on the same matrices."""
+    from imago_b200 import charge, secular
+    hs, ss = secular._secular_storage(out, w)
+    nk, n = hs.shape[0], hs.shape[-1]
+    h, s = hs.transpose(-2, -1), ss.transpose(-2, -1)
+    f = torch.as_tensor(pop, dtype=torch.float64, device=hs.device)
+    ns = int(torch.nonzero((f != 0).any(dim=0)).flatten()[-1]) + 1
+    res = {"n": n, "num_kpoints": nk, "states": ns}
+    with torch.cuda.stream(stream):
+        a, lfac, _ = secular.cholesky_reduce(hs, ss, factor=True)
+        _, vec = secular.hermitian_eigh(a)
+        res["reduce_ms"] = _event_ms(lambda: secular.cholesky_reduce(hs, ss, factor=True),
+                                     stream, torch)
+
+        def lib_reduce():
+            lo = torch.linalg.cholesky(s)
+            y = torch.linalg.solve_triangular(lo, h, upper=False)
+            return lo, torch.linalg.solve_triangular(lo, y.mH, upper=False)
+        res["cusolver_reduce_ms"] = _event_ms(lib_reduce, stream, torch)
+        lo, _ = lib_reduce()
+        res["back_ms"] = _event_ms(lambda: secular.back_transform(lfac, vec, ns), stream, torch)
+        res["cusolver_back_ms"] = _event_ms(
+            lambda: torch.linalg.solve_triangular(lo.mH, vec[:, :, :ns], upper=True),
+            stream, torch)
+        c = secular.back_transform(lfac, vec, ns)
+        fs = f[:, :ns].contiguous()
+        res["density_ms"] = _event_ms(lambda: charge.packed_density(c, fs), stream, torch)
+        cols = torch.repeat_interleave(torch.arange(n), torch.arange(1, n + 1)).to(hs.device)
+        rows = torch.arange(n * (n + 1) // 2, device=hs.device) - cols * (cols + 1) // 2
+        cc = c.contiguous()
+
+        def lib_density():
+            full = (cc * fs[:, None, :].to(cc.dtype)) @ cc.mH
+            return torch.view_as_real(full[:, rows, cols].contiguous())
+        res["cublas_density_ms"] = _event_ms(lib_density, stream, torch)
+        res["density_max_diff"] = float((charge.packed_density(c, fs) - lib_density())
+                                        .abs().max())
+    return res
+
+
 def time_valence_rho(bufs, pot_dim, stream, torch, steps=3):
     """One SCF step's valence charge from the resident builds
     (imago_b200.charge): eigenvalues and eigenvectors, the populations (host,
@@ -459,6 +519,7 @@ def time_valence_rho(bufs, pot_dim, stream, torch, steps=3):
             if rep:
                 ts.append(time.perf_counter() - t0)
         rho = charge.packed_density(c, pop["population"][:, 0, :])[None]
+        reduction = time_reduction(out, w, pop["population"][:, 0, :], stream, torch)
         charge.packed_traces(out["ep_packed"], rho, nk, V)
         kt = []
         for _ in range(steps):
@@ -475,6 +536,7 @@ def time_valence_rho(bufs, pot_dim, stream, torch, steps=3):
             "charge_trace": float(r["chargeDensityTrace"][0]),
             "trace_kernel_ms": kms, "trace_bytes": nbytes,
             "trace_gbs": nbytes / (kms * 1e-3) / 1e9,
+            "reduction": reduction,
             "stat": f"median of {steps}"}
 
 

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "imago_b200")
 LIB = os.path.join(HERE, "libimago_b200.so")
 SOURCES = ["api.cu", "k_dense.cu", "k_prim.cu", "k_eval.cu", "noalloc.cu",
-           "k_secular.cu", "populate.cu", "scf.cu", "learned.cu"]
+           "k_secular.cu", "k_reduce.cu", "populate.cu", "scf.cu", "learned.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]

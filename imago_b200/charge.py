@@ -9,8 +9,9 @@ populate_states is populateStates (populate.F90:150-620: the standard
 population and the thermal smearing) in the library's host code
 (imago_populate_states), over the sorted eigenvalues as in the reference.  valence_rho is the trace part of
 makeValenceRho (valeCharge.F90:34-526): per k-point the density
-rho = sum_j f_j c_j c_j^H of the occupied states (a batched complex GEMM,
-cuBLAS through torch), packed like the integrals, and its traces against
+rho = sum_j f_j c_j c_j^H of the occupied states (the library's packed
+density kernel, imago_packed_density), packed like the integrals, and its
+traces against
 the packed OL, NP, KE, MV and every EP_j matrix by the library's trace
 kernel (imago_packed_traces), which reads each integral matrix once from
 HBM.  Energies in Hartree.
@@ -86,28 +87,35 @@ def populate_smearing(eigenvalues, num_electrons, thermal_sigma, max_thermal_ran
             "charge": float(r["population"].sum())}
 
 
-_PACK_CACHE = {}
-
-
-def _pack_index(V, device):
-    key = (V, str(device))
-    if key not in _PACK_CACHE:
-        cols = torch.repeat_interleave(torch.arange(V), torch.arange(1, V + 1))
-        starts = cols * (cols + 1) // 2
-        rows = torch.arange(V * (V + 1) // 2) - starts
-        _PACK_CACHE[key] = (rows.to(device), cols.to(device))
-    return _PACK_CACHE[key]
-
-
 def packed_density(eigenvectors, population):
     """rho = sum_j f_j c_j c_j^H per k-point (the zher updates of
-    valeCharge.F90:187-192) for populations [nk, numStates], packed as
-    packMatrix does (matrixSubs.F90:506-533): [nk, V(V+1)/2, 2]."""
+    valeCharge.F90:187-192, in state order, the diagonal real) for
+    eigenvectors [nk, V, numStates] (complex128, CUDA; state-major storage,
+    as secular_eigensystem returns it, is read in place) and populations
+    [nk, numStates], packed as packMatrix does (matrixSubs.F90:506-533):
+    [nk, V(V+1)/2, 2], by imago_packed_density.  The states after the last
+    one populated at any k-point are not read."""
     c = eigenvectors
-    f = torch.as_tensor(population, dtype=torch.float64, device=c.device)
-    full = (c * f[:, None, :].to(c.dtype)) @ c.mH
-    rows, cols = _pack_index(c.shape[1], c.device)
-    return torch.view_as_real(full[:, rows, cols].contiguous()).contiguous()
+    if c.dtype != torch.complex128:
+        raise TypeError("eigenvectors must be complex128")
+    nk, V, ns = c.shape
+    ct = c.transpose(-2, -1)
+    if not ct.is_contiguous():
+        ct = ct.contiguous()
+    f = torch.as_tensor(population, dtype=torch.float64).to(c.device).contiguous()
+    if tuple(f.shape) != (nk, ns):
+        raise ValueError(f"population shape {tuple(f.shape)} for {nk} k-points x {ns} states")
+    occ = torch.nonzero((f != 0).any(dim=0)).flatten()
+    used = int(occ[-1]) + 1 if occ.numel() else 0
+    rho = torch.empty((nk, V * (V + 1) // 2, 2), dtype=torch.float64, device=c.device)
+    L = intg.lib()
+    L.imago_packed_density.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4
+    L.imago_packed_density.restype = ctypes.c_int
+    rc = L.imago_packed_density(V, nk, ns, used, ct.data_ptr(), f.data_ptr(), rho.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise intg.ImagoError(rc, "imago_packed_density")
+    return rho
 
 
 def packed_traces(mats, rho, nk, V):

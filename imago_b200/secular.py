@@ -9,10 +9,12 @@ the potDim coefficients of the current SCF potential (potCoeffs in the
 reference).  H and S are assembled and unpacked on the device by
 imago_secular_matrices, then the generalised Hermitian problem
 H c = E S c, which the reference hands to LAPACK zhegv(1, 'V', 'U')
-(interfaces.F90:73-120), is reduced by the Cholesky factor of S (cuSOLVER
-through torch.linalg) and the eigenvalues of the reduced matrices come
-from the library's batched Jacobi kernel.  Eigenvalues come back ascending per
-k-point, in Hartree.
+(interfaces.F90:73-120), is reduced by the Cholesky factor of S and the
+eigenvalues of the reduced matrices come from the library's batched Jacobi
+kernel.  Up to n = 128 the reduction and the back-transformation of the
+vectors are the library's own kernels (imago_secular_reduce / _back, one
+CTA per k-point); beyond, cuSOLVER through torch.linalg.  Eigenvalues come
+back ascending per k-point, in Hartree.
 """
 
 import ctypes
@@ -26,6 +28,14 @@ def secular_matrices(out, pot_coeffs, stream=None):
     """Full Hermitian H and S [nk, V, V] (complex128, CUDA) for every k;
     with out["mv_packed"] (a scalar-relativistic run) H includes the mass
     velocity, added after KE as the reference does."""
+    h, s = _secular_storage(out, pot_coeffs, stream)
+    # stored [k][col][row]: the matrix is the transpose of each slice
+    return h.transpose(-2, -1), s.transpose(-2, -1)
+
+
+def _secular_storage(out, pot_coeffs, stream=None):
+    """H and S as imago_secular_matrices_rel writes them: contiguous
+    [nk, V, V], column-major per k-point."""
     npk = out["np_packed"]
     nk, npacked = npk.shape[0], npk.shape[1]
     V = int((int((8 * npacked + 1) ** 0.5) - 1) // 2)
@@ -50,8 +60,56 @@ def secular_matrices(out, pot_coeffs, stream=None):
         out["ol_packed"].data_ptr(), h.data_ptr(), s.data_ptr(), st)
     if rc:
         raise intg.ImagoError(rc, "imago_secular_matrices_rel")
-    # stored [k][col][row]: the matrix is the transpose of each slice
-    return h.transpose(-2, -1), s.transpose(-2, -1)
+    return h, s
+
+
+REDUCE_MAX_N = 128
+
+
+def cholesky_reduce(h_store, s_store, factor=False):
+    """imago_secular_reduce: A = L^-1 H L^-H [nk, n, n] (row-major,
+    complex128) with S = L L^H, from H and S stored column-major per k-point
+    (_secular_storage); with factor, also L packed by columns [nk,
+    n(n+1)/2] for back_transform.  Raises ValueError, as zhegv stops, when S
+    of some k-point is not positive definite."""
+    nk, n = h_store.shape[0], h_store.shape[-1]
+    a = torch.empty_like(h_store)
+    lfac = (torch.empty((nk, n * (n + 1) // 2), dtype=torch.complex128, device=h_store.device)
+            if factor else None)
+    info = torch.zeros(nk, dtype=torch.int32, device=h_store.device)
+    L = intg.lib()
+    L.imago_secular_reduce.argtypes = [ctypes.c_int] * 2 + [ctypes.c_void_p] * 6
+    L.imago_secular_reduce.restype = ctypes.c_int
+    rc = L.imago_secular_reduce(n, nk, h_store.data_ptr(), s_store.data_ptr(), a.data_ptr(),
+                                lfac.data_ptr() if factor else None, info.data_ptr(),
+                                torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise intg.ImagoError(rc, "imago_secular_reduce")
+    return a, lfac, info
+
+
+def _check_info(info):
+    bad = torch.nonzero(info).flatten()
+    if bad.numel():
+        k = int(bad[0])
+        raise ValueError(f"overlap matrix of k-point {k} is not positive definite "
+                         f"(leading minor {int(info[k])})")
+
+
+def back_transform(lfac, vec, num_states):
+    """imago_secular_back: c = L^-H y for the first num_states columns of vec
+    [nk, n, n] (hermitian_eigh's eigenvectors); returns [nk, n, num_states]
+    as a view of state-major storage [nk, num_states, n]."""
+    nk, n = vec.shape[0], vec.shape[-1]
+    ct = torch.empty((nk, num_states, n), dtype=torch.complex128, device=vec.device)
+    L = intg.lib()
+    L.imago_secular_back.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 4
+    L.imago_secular_back.restype = ctypes.c_int
+    rc = L.imago_secular_back(n, nk, num_states, lfac.data_ptr(), vec.contiguous().data_ptr(),
+                              ct.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise intg.ImagoError(rc, "imago_secular_back")
+    return ct.transpose(-2, -1)
 
 
 JACOBI_MAX_N = 112
@@ -144,13 +202,20 @@ def hermitian_eigh(a):
 
 def secular_eigenvalues(out, pot_coeffs, num_states=None):
     """Eigenvalues of H c = E S c per k-point, ascending, [nk, num_states]:
-    the Cholesky factor L of S (cuSOLVER, batched), A = L^-1 H L^-H, and the
-    eigenvalues of A (hermitian_eigvals)."""
-    h, s = secular_matrices(out, pot_coeffs)
-    lo = torch.linalg.cholesky(s)
-    y = torch.linalg.solve_triangular(lo, h, upper=False)          # L^-1 H
-    a = torch.linalg.solve_triangular(lo, y.mH, upper=False)       # L^-1 H L^-H
-    ev = hermitian_eigvals(a)
+    the Cholesky factor L of S, A = L^-1 H L^-H (cholesky_reduce up to n =
+    128, cuSOLVER through torch.linalg beyond), and the eigenvalues of A
+    (hermitian_eigvals)."""
+    hs, ss = _secular_storage(out, pot_coeffs)
+    if hs.shape[-1] <= REDUCE_MAX_N:
+        a, _, info = cholesky_reduce(hs, ss)
+        ev = hermitian_eigvals(a)
+        _check_info(info)
+    else:
+        h, s = hs.transpose(-2, -1), ss.transpose(-2, -1)
+        lo = torch.linalg.cholesky(s)
+        y = torch.linalg.solve_triangular(lo, h, upper=False)          # L^-1 H
+        a = torch.linalg.solve_triangular(lo, y.mH, upper=False)       # L^-1 H L^-H
+        ev = hermitian_eigvals(a)
     return ev if num_states is None else ev[:, :num_states]
 
 
@@ -159,8 +224,19 @@ def secular_eigensystem(out, pot_coeffs, num_states=None):
     [nk, V, num_states] of H c = E S c per k-point, the vectors normalised
     as zhegv(1, 'V', 'U') returns them (c^H S c = 1): A = L^-1 H L^-H is
     diagonalised by hermitian_eigh and the vectors taken back by
-    c = L^-H y."""
-    h, s = secular_matrices(out, pot_coeffs)
+    c = L^-H y (cholesky_reduce and back_transform up to n = 128, the
+    vectors then a view of state-major storage; cuSOLVER through
+    torch.linalg beyond)."""
+    hs, ss = _secular_storage(out, pot_coeffs)
+    n = hs.shape[-1]
+    if n <= REDUCE_MAX_N:
+        a, lfac, info = cholesky_reduce(hs, ss, factor=True)
+        ev, vec = hermitian_eigh(a)
+        ns = n if num_states is None else num_states
+        c = back_transform(lfac, vec, ns)
+        _check_info(info)
+        return ev[:, :ns], c
+    h, s = hs.transpose(-2, -1), ss.transpose(-2, -1)
     lo = torch.linalg.cholesky(s)
     y = torch.linalg.solve_triangular(lo, h, upper=False)
     a = torch.linalg.solve_triangular(lo, y.mH, upper=False)

@@ -407,6 +407,45 @@ IMAGO_API int imago_hermitian_eigvals(int n, int batch, const double *a,
 IMAGO_API int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
                                    double *vec, void *stream);
 
+/* The Cholesky reduction of zhegv(1, 'V', 'U') (interfaces.F90:73-120:
+ * zpotrf, then zhegst) for every k-point: S = L L^H (L = U^H, zpotrf's
+ * factor) and A = L^-1 H L^-H.  h_full and s_full as
+ * imago_secular_matrices writes them (column-major per k-point, both
+ * triangles); a [num_kpoints][n][n] receives A row-major, the layout
+ * imago_hermitian_eigvals/eigh take; l_packed (may be NULL)
+ * [num_kpoints][n(n+1)/2] (re, im) the factor, column by column from the
+ * diagonal down (L(r, j), r >= j, at j n - j (j - 1) / 2 + r - j), for
+ * imago_secular_back; info [num_kpoints] (device, may be NULL) zpotrf's
+ * info per k-point: 0, or the order of the first leading minor of S that
+ * is not positive definite (A of that k-point is then zero).  One
+ * CTA per k-point with the factor in shared memory: n up to 128
+ * (IMAGO_ERR_RANGE beyond).  a must not overlap h_full or s_full.
+ * Asynchronous on `stream`. */
+IMAGO_API int imago_secular_reduce(int n, int num_kpoints, const double *h_full,
+                                   const double *s_full, double *a, double *l_packed,
+                                   int *info, void *stream);
+
+/* The back-transformation of zhegv(1, 'V', ...) (ztrsm with the upper
+ * factor): c = L^-H y for the first num_states eigenvectors y of A, vec as
+ * imago_hermitian_eigh writes it (vec[k][row][j]), l_packed from
+ * imago_secular_reduce; c [num_kpoints][num_states][n] state-major
+ * (c[k][j][row]), each vector normalised as zhegv's (c^H S c = 1).  n up to
+ * 128 (IMAGO_ERR_RANGE beyond).  Asynchronous on `stream`. */
+IMAGO_API int imago_secular_back(int n, int num_kpoints, int num_states,
+                                 const double *l_packed, const double *vec, double *c,
+                                 void *stream);
+
+/* The valence density of makeValenceRho (valeCharge.F90:181-192): per
+ * k-point rho = sum_j f_j c_j c_j^H over the first num_states states, the
+ * zher updates in state order, packed as packMatrix leaves the upper
+ * triangle ((r, q), r <= q, at q (q + 1) / 2 + r; the diagonal real).  c
+ * state-major [num_kpoints][ld_states][n] (imago_secular_back's layout),
+ * population [num_kpoints][ld_states] (device), rho
+ * [num_kpoints][n(n+1)/2] (re, im).  Asynchronous on `stream`. */
+IMAGO_API int imago_packed_density(int n, int num_kpoints, int ld_states, int num_states,
+                                   const double *c, const double *population, double *rho,
+                                   void *stream);
+
 /* No counterpart: how the three-centre primitive stage of NP and EP
  * schedules its shell-pair classes.  mode 0: one launch per class
  * (k_prim3c<la, lb>), one (shell pair, term) per thread; mode 1: all

@@ -126,6 +126,20 @@ def test_added_entry_points_reject_bad_arguments(imago_lib):
     assert L.imago_intg_set_ham_mode(None, 0) == 1
     L.imago_secular_matrices_rel.argtypes = [ctypes.c_int] * 3 + [vp] * 9
     assert L.imago_secular_matrices_rel(0, 1, 0, *([None] * 9)) == 1
+    L.imago_secular_reduce.argtypes = [ctypes.c_int] * 2 + [vp] * 6
+    assert L.imago_secular_reduce(0, 1, *([None] * 6)) == 1
+    dummy = [vp(16), vp(32), vp(48)]
+    # one CTA per k-point holds the factor: n above 128 is out of range
+    assert L.imago_secular_reduce(129, 1, *dummy, None, None, None) == 8
+    # the reduced matrix may not overwrite H or S
+    assert L.imago_secular_reduce(8, 1, dummy[0], dummy[1], dummy[0], None, None, None) == 1
+    L.imago_secular_back.argtypes = [ctypes.c_int] * 3 + [vp] * 4
+    assert L.imago_secular_back(0, 1, 1, *([None] * 4)) == 1
+    assert L.imago_secular_back(8, 1, 9, *dummy, None) == 1
+    assert L.imago_secular_back(129, 1, 4, *dummy, None) == 8
+    L.imago_packed_density.argtypes = [ctypes.c_int] * 4 + [vp] * 4
+    assert L.imago_packed_density(0, 1, 1, 1, *([None] * 4)) == 1
+    assert L.imago_packed_density(8, 1, 2, 3, *dummy, None) == 1
 
 
 def test_device_output_context_refuses_host_outputs():
