@@ -29,7 +29,7 @@ namespace {
 constexpr int kRedThreads = 256;
 constexpr int kRedWarps = kRedThreads / 32;
 constexpr int kRedMaxN = 128;  // 4 rows per lane in the substitutions
-constexpr int kRedCols = 2;    // right-hand sides a warp carries at once
+constexpr int kRedCols = 4;    // right-hand sides a warp carries at once
 
 // Column-packed lower storage: L(r, j), r >= j, at pcol(n, j) + r - j.
 __device__ __forceinline__ int pcol(int n, int j) { return j * n - (j * (j - 1)) / 2; }
@@ -50,8 +50,9 @@ __device__ __forceinline__ double2 shfl2(double2 v, int l) {
 
 // The pivot of column q, whose update is complete (the calling warp made
 // it): L_qq = sqrt(a_qq) and the rows below scaled by its reciprocal, as
-// zpotf2 scales by 1 / ajj.  False on every lane when a_qq is not positive.
-__device__ __forceinline__ bool pivot_column(double2 *Lp, double *ldiag, int n, int q,
+// zpotf2 scales by 1 / ajj, which linv[q] keeps for the substitutions.
+// False on every lane when a_qq is not positive.
+__device__ __forceinline__ bool pivot_column(double2 *Lp, double *linv, int n, int q,
                                              int lane) {
   const int pq = pcol(n, q) - q;
   const double d = Lp[pq + q].x;
@@ -64,30 +65,33 @@ __device__ __forceinline__ bool pivot_column(double2 *Lp, double *ldiag, int n, 
   }
   if (lane == 0) {
     Lp[pq + q] = make_double2(sd, 0.0);
-    ldiag[q] = sd;
+    linv[q] = inv;
   }
   return true;
 }
 
 // Forward substitution L x = b for NC right-hand sides carried by one
 // warp, row r = lane + 32 m in w[c][m] (zero beyond n).  Column form, as
-// ztrsm('L', 'L', 'N', 'N') runs it: x_j = b_j / L_jj, then
-// b_r <- b_r - L_rj x_j for r > j.
+// ztrsm('L', 'L', 'N', 'N') runs it, but with x_j = b_j (1 / L_jj) (a
+// multiplication where ztrsm divides: the division sat on the critical
+// path of every step), then b_r <- b_r - L_rj x_j for r > j.  Each step
+// waits on the previous one through one lane's row, so a warp carries
+// several right-hand sides to have independent work in flight.
 template <int M, int NC>
-__device__ __forceinline__ void lower_solve(const double2 *Lp, const double *ldiag, int n,
+__device__ __forceinline__ void lower_solve(const double2 *Lp, const double *linv, int n,
                                             double2 (&w)[NC][M], int lane) {
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     for (int l = 0; l < 32; ++l) {
       const int j = 32 * m + l;
       if (j >= n) break;
-      const double dj = ldiag[j];
+      const double dj = linv[j];
       const int pj = pcol(n, j) - j;
       double2 x[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const double2 b = shfl2(w[c][m], l);
-        x[c] = make_double2(b.x / dj, b.y / dj);
+        x[c] = make_double2(b.x * dj, b.y * dj);
         if (lane == l) w[c][m] = x[c];
       }
 #pragma unroll
@@ -105,23 +109,23 @@ __device__ __forceinline__ void lower_solve(const double2 *Lp, const double *ldi
 
 // Backward substitution L^H x = b (the upper factor U = L^H of zpotrf), L
 // row-packed: L(j, i), i <= j, at j (j + 1) / 2 + i.  Column form, as
-// ztrsm('L', 'U', 'N', 'N') runs it: x_j = b_j / L_jj from the last row
-// up, then b_r <- b_r - conj(L_jr) x_j for r < j.
+// ztrsm('L', 'U', 'N', 'N') runs it (again multiplying by 1 / L_jj): x_j
+// from the last row up, then b_r <- b_r - conj(L_jr) x_j for r < j.
 template <int M, int NC>
-__device__ __forceinline__ void upper_solve(const double2 *Lr, const double *ldiag, int n,
+__device__ __forceinline__ void upper_solve(const double2 *Lr, const double *linv, int n,
                                             double2 (&w)[NC][M], int lane) {
 #pragma unroll
   for (int m = M - 1; m >= 0; --m) {
     for (int l = 31; l >= 0; --l) {
       const int j = 32 * m + l;
       if (j >= n) continue;
-      const double dj = ldiag[j];
+      const double dj = linv[j];
       const int rj = j * (j + 1) / 2;
       double2 x[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         const double2 b = shfl2(w[c][m], l);
-        x[c] = make_double2(b.x / dj, b.y / dj);
+        x[c] = make_double2(b.x * dj, b.y * dj);
         if (lane == l) w[c][m] = x[c];
       }
 #pragma unroll
@@ -158,7 +162,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   extern __shared__ __align__(16) unsigned char rsm[];
   const int np = n * (n + 1) / 2;
   double2 *Lp = reinterpret_cast<double2 *>(rsm);
-  double *ldiag = reinterpret_cast<double *>(Lp + np);
+  double *linv = reinterpret_cast<double *>(Lp + np);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long base = (long long)blockIdx.x * n * n;
   // column j of S from row j down is contiguous in both layouts
@@ -168,7 +172,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   }
   __syncthreads();
   int failed = 0;  // 1 + the failing pivot, on the lanes of the warp that met it
-  if (warp == 0 && !pivot_column(Lp, ldiag, n, 0, lane)) failed = 1;
+  if (warp == 0 && !pivot_column(Lp, linv, n, 0, lane)) failed = 1;
   bool stop = __syncthreads_or(failed);
   for (int j = 0; j + 1 < n && !stop; ++j) {
     const int pj = pcol(n, j) - j;
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
       for (int r = q + lane; r < n; r += 32) Lp[pq + r] = csub_mulc(Lp[pq + r], Lp[pj + r], lq);
       if (q == j + 1) {
         __syncwarp();
-        if (!pivot_column(Lp, ldiag, n, q, lane)) failed = q + 1;
+        if (!pivot_column(Lp, linv, n, q, lane)) failed = q + 1;
       }
     }
     stop = __syncthreads_or(failed);
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
         const int r = lane + 32 * m, col = c0 + c;
         w[c][m] = (r < n && col < n) ? h[base + (long long)col * n + r] : make_double2(0.0, 0.0);
       }
-    lower_solve<M, NC>(Lp, ldiag, n, w, lane);
+    lower_solve<M, NC>(Lp, linv, n, w, lane);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
         const int r = lane + 32 * m, col = c0 + c;
         w[c][m] = (r < n && col < n) ? a[base + (long long)col * n + r] : make_double2(0.0, 0.0);
       }
-    lower_solve<M, NC>(Lp, ldiag, n, w, lane);
+    lower_solve<M, NC>(Lp, linv, n, w, lane);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -243,13 +247,13 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   extern __shared__ __align__(16) unsigned char rsm[];
   const int np = n * (n + 1) / 2;
   double2 *Lr = reinterpret_cast<double2 *>(rsm);
-  double *ldiag = reinterpret_cast<double *>(Lr + np);
+  double *linv = reinterpret_cast<double *>(Lr + np);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double2 *lk = lfac + (long long)blockIdx.x * np;
   for (int j = warp; j < n; j += kRedWarps) {
     const int pj = pcol(n, j) - j;
     for (int r = j + lane; r < n; r += 32) Lr[r * (r + 1) / 2 + j] = lk[pj + r];
-    if (lane == 0) ldiag[j] = lk[pj + j].x;
+    if (lane == 0) linv[j] = 1.0 / lk[pj + j].x;
   }
   __syncthreads();
   const long long vbase = (long long)blockIdx.x * n * n;
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(kRedThreads, 2)
         const int r = lane + 32 * m, col = c0 + c;
         w[c][m] = (r < n && col < ns) ? vec[vbase + (long long)r * n + col] : make_double2(0.0, 0.0);
       }
-    upper_solve<M, NC>(Lr, ldiag, n, w, lane);
+    upper_solve<M, NC>(Lr, linv, n, w, lane);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll

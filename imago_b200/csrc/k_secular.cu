@@ -16,6 +16,7 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include <cusolverDn.h>
@@ -340,13 +341,15 @@ size_t jacobi_smem(int n) {
          sizeof(double2) * (m / 2) + sizeof(int2) * (m / 2);
 }
 
-// ------------------------------------------------- larger matrices --
-// Above the Jacobi kernel's n = 112 the eigenproblems go to cuSOLVER's
-// batched Hermitian eigensolver (cusolverDnXsyevBatched; one call for the
-// whole batch, 150 ms for 64 matrices of n = 832 against 743 ms for one
-// syevd per matrix on one B200; its time varies with the matrices).  It is reached through dlopen, so the
-// library does not link cuSOLVER and uses the copy the process already
-// holds; without it the caller gets IMAGO_ERR_RANGE as before.
+// ------------------------------------------ the batched library solver --
+// cuSOLVER's batched Hermitian eigensolver (cusolverDnXsyevBatched, one
+// call for the whole batch) is the default wherever it loads: measured on
+// one B200 it takes 6.1 ms (eigenvalues) / 7.8 ms (with vectors) for 512
+// matrices of n = 104, where the Jacobi kernel above takes 22.5 / 33.6 ms,
+// and 150 ms for 64 matrices of n = 832 against 743 ms for one syevd per
+// matrix.  It is reached through dlopen, so the library does not link
+// cuSOLVER and uses the copy the process already holds; without it the
+// Jacobi kernel serves n up to 112 and larger n get IMAGO_ERR_RANGE.
 struct SyevApi {
   decltype(&cusolverDnCreate) create = nullptr;
   decltype(&cusolverDnSetStream) set_stream = nullptr;
@@ -477,12 +480,31 @@ int hermitian_eigh_batched(int n, int batch, const double2 *a, double *w, double
 
 }  // namespace imago
 
+namespace {
+// 0: the batched library solver where it loads, else the Jacobi kernel;
+// 1: the Jacobi kernel up to n = 112; 2: the batched library solver only
+std::atomic<int> g_eig_solver{0};
+}  // namespace
+
+extern "C" int imago_hermitian_set_solver(int mode) {
+  if (mode < 0 || mode > 2) return IMAGO_ERR_INVALID;
+  g_eig_solver.store(mode);
+  return IMAGO_OK;
+}
+
+extern "C" int imago_hermitian_solver(int *mode) {
+  if (!mode) return IMAGO_ERR_INVALID;
+  *mode = g_eig_solver.load();
+  return IMAGO_OK;
+}
+
 extern "C" int imago_hermitian_eigh(int n, int batch, const double *a, double *w,
                                     double *vec, void *stream) {
   if (n <= 0 || batch < 0 || !a || !w) return IMAGO_ERR_INVALID;
   if (batch == 0) return IMAGO_OK;
   const size_t smem = imago::jacobi_smem(n);
-  if (smem > imago::kJacobiMaxSmem)
+  const int mode = g_eig_solver.load();
+  if (smem > imago::kJacobiMaxSmem || mode == 2 || (mode == 0 && imago::syev_api().ok))
     return imago::hermitian_eigh_batched(n, batch, reinterpret_cast<const double2 *>(a), w,
                                          reinterpret_cast<double2 *>(vec),
                                          (cudaStream_t)stream);

@@ -11,10 +11,11 @@ imago_secular_matrices, then the generalised Hermitian problem
 H c = E S c, which the reference hands to LAPACK zhegv(1, 'V', 'U')
 (interfaces.F90:73-120), is reduced by the Cholesky factor of S and the
 eigenvalues of the reduced matrices come from the library's batched Jacobi
-kernel.  Up to n = 128 the reduction and the back-transformation of the
-vectors are the library's own kernels (imago_secular_reduce / _back, one
-CTA per k-point); beyond, cuSOLVER through torch.linalg.  Eigenvalues come
-back ascending per k-point, in Hartree.
+kernel or cuSOLVER's batched solver (set_eigensolver).  Up to n = 128 the
+reduction and the back-transformation of the vectors are the library's own
+kernels (imago_secular_reduce / _back, one CTA per k-point); beyond,
+cuSOLVER through torch.linalg.  Eigenvalues come back ascending per
+k-point, in Hartree.
 """
 
 import ctypes
@@ -114,13 +115,43 @@ def back_transform(lfac, vec, num_states):
 
 JACOBI_MAX_N = 112
 _ERR_RANGE = 8  # IMAGO_ERR_RANGE
+_SOLVERS = {"auto": 0, "jacobi": 1, "batched": 2}
+
+
+def set_eigensolver(name):
+    """The solver behind hermitian_eigvals / hermitian_eigh for the whole
+    process (imago_hermitian_set_solver): "auto" (the default) cuSOLVER's
+    batched Hermitian solver where it loads, else the library's Jacobi
+    kernel; "jacobi" the Jacobi kernel up to n = 112; "batched" the batched
+    solver only."""
+    L = intg.lib()
+    L.imago_hermitian_set_solver.argtypes = [ctypes.c_int]
+    L.imago_hermitian_set_solver.restype = ctypes.c_int
+    if name not in _SOLVERS:
+        raise ValueError(f"eigensolver must be one of {sorted(_SOLVERS)}")
+    rc = L.imago_hermitian_set_solver(_SOLVERS[name])
+    if rc:
+        raise intg.ImagoError(rc, "imago_hermitian_set_solver")
+
+
+def eigensolver():
+    """The name set by set_eigensolver."""
+    L = intg.lib()
+    L.imago_hermitian_solver.argtypes = [ctypes.c_void_p]
+    L.imago_hermitian_solver.restype = ctypes.c_int
+    m = ctypes.c_int(0)
+    rc = L.imago_hermitian_solver(ctypes.byref(m))
+    if rc:
+        raise intg.ImagoError(rc, "imago_hermitian_solver")
+    return {v: k for k, v in _SOLVERS.items()}[m.value]
 
 
 def hermitian_eigvals(a):
     """Ascending eigenvalues of a batch of Hermitian matrices [b, n, n]
-    (complex128, CUDA): imago_hermitian_eigvals (one CTA per matrix, cyclic
-    Jacobi in shared memory) up to n = 112, cuSOLVER's batched solver
-    through the library beyond (torch's eigvalsh if that is absent)."""
+    (complex128, CUDA): imago_hermitian_eigvals, cuSOLVER's batched solver
+    through the library or the library's Jacobi kernel (one CTA per matrix,
+    cyclic Jacobi in shared memory, n up to 112) as set_eigensolver chooses
+    (torch's eigvalsh beyond n = 112 if the batched solver is absent)."""
     b, n = a.shape[0], a.shape[-1]
     a = a.contiguous()
     w = torch.empty((b, n), dtype=torch.float64, device=a.device)
@@ -181,9 +212,10 @@ def _eigh_lanes(a):
 def hermitian_eigh(a):
     """Ascending eigenvalues [b, n] and unit eigenvectors [b, n, n] (in
     columns) of a batch of Hermitian matrices [b, n, n] (complex128, CUDA):
-    imago_hermitian_eigh (the Jacobi kernel accumulating its rotations) up
-    to n = 112, cuSOLVER's batched solver through the library beyond (one
-    call for the batch; _eigh_lanes if the process has no batched solver)."""
+    imago_hermitian_eigh, cuSOLVER's batched solver through the library (one
+    call for the batch) or the Jacobi kernel accumulating its rotations (n
+    up to 112) as set_eigensolver chooses; _eigh_lanes beyond n = 112 if the
+    process has no batched solver."""
     b, n = a.shape[0], a.shape[-1]
     a = a.contiguous()
     w = torch.empty((b, n), dtype=torch.float64, device=a.device)

@@ -68,9 +68,28 @@ def test_secular_eigenvalues_match_oracle(imago_lib, name, rel):
     assert np.abs(ev - ref).max() <= EV_TOL, np.abs(ev - ref).max()
 
 
+@pytest.fixture(params=["jacobi", "batched"])
+def eigensolver(request):
+    # each solver behind imago_hermitian_eigvals/eigh in turn, the default
+    # restored after the test
+    from imago_b200 import secular
+    before = secular.eigensolver()
+    secular.set_eigensolver(request.param)
+    yield request.param
+    secular.set_eigensolver(before)
+
+
+def test_eigensolver_choice_is_validated(imago_lib):
+    from imago_b200 import secular
+    assert secular.eigensolver() == "auto"
+    with pytest.raises(ValueError):
+        secular.set_eigensolver("qr")
+    assert imago_lib.imago_hermitian_set_solver(3) == 1
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 5, 33, 104, 112])
-def test_batched_jacobi_eigenvalues(imago_lib, n):
+def test_batched_jacobi_eigenvalues(imago_lib, eigensolver, n):
     # imago_hermitian_eigvals against LAPACK, including degenerate spectra
     import torch
     from imago_b200 import secular
@@ -88,7 +107,7 @@ def test_batched_jacobi_eigenvalues(imago_lib, n):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 5, 33, 104, 112])
-def test_batched_jacobi_eigenvectors(imago_lib, n):
+def test_batched_jacobi_eigenvectors(imago_lib, eigensolver, n):
     # imago_hermitian_eigh: A V = V diag(w), V unitary, w as LAPACK's, on
     # random and degenerate spectra
     import torch
