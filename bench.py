@@ -600,7 +600,8 @@ def scf_headline(local, torch, systems=("si8", "si64", "graphite64")):
     trained on the GPU by the library's own kernels).  Wall seconds with the
     device synchronised; the learned start is kept only when it reaches the
     plain start's energy within 1e-6 Ha in no more iterations.
-    si8: the benched Si8 cell at 8x8x8 k (plain start only);
+    si8: the benched Si8 cell at 8x8x8 k (plain start only, after one
+    untimed run);
     si64 / graphite64: the learned start's test cells at 4x4x4 k."""
     from imago_b200 import learned, scf
     out = {}
@@ -609,6 +610,11 @@ def scf_headline(local, torch, systems=("si8", "si64", "graphite64")):
     for name in systems:
         s = system_for("si8") if name == "si8" else learned.test_system(name, (4, 4, 4))
         if ls is None or name == "si8":
+            # one untimed run first: the process's first SCF pays one-time
+            # costs (kernel loading, pool growth) that a user's steady state
+            # does not
+            scf.run_scf(s, scf.atomic_start(s), learned.metric_params(), device=local)
+            torch.cuda.synchronize(local)
             t0 = time.perf_counter()
             r = scf.run_scf(s, scf.atomic_start(s), learned.metric_params(), device=local)
             torch.cuda.synchronize(local)
@@ -1036,6 +1042,8 @@ def run_ours(args):
         if world == 1 and args.workload == "si8" and not args.no_silica:
             line["silica_162"] = silica_headline(args, local, stream, torch)
         if world == 1 and args.workload == "si8" and not args.no_scf:
+            torch.cuda.synchronize(local)
+            torch.cuda.empty_cache()
             line["scf"] = scf_headline(local, torch)
         print(json.dumps(line), flush=True)
     g.close()
