@@ -176,11 +176,26 @@ __global__ void __launch_bounds__(kRedThreads, 2)
   bool stop = __syncthreads_or(failed);
   for (int j = 0; j + 1 < n && !stop; ++j) {
     const int pj = pcol(n, j) - j;
-    // columns q > j: A(r, q) -= L(r, j) conj(L(q, j)), r >= q
+    // columns q > j: A(r, q) -= L(r, j) conj(L(q, j)), r >= q; a lane's
+    // rows (at most M, n <= 32 M) loaded together so that their updates
+    // overlap
     for (int q = j + 1 + warp; q < n; q += kRedWarps) {
       const double2 lq = Lp[pj + q];
       const int pq = pcol(n, q) - q;
-      for (int r = q + lane; r < n; r += 32) Lp[pq + r] = csub_mulc(Lp[pq + r], Lp[pj + r], lq);
+      double2 av[M], lv[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int r = q + lane + 32 * m;
+        if (r < n) {
+          av[m] = Lp[pq + r];
+          lv[m] = Lp[pj + r];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int r = q + lane + 32 * m;
+        if (r < n) Lp[pq + r] = csub_mulc(av[m], lv[m], lq);
+      }
       if (q == j + 1) {
         __syncwarp();
         if (!pivot_column(Lp, linv, n, q, lane)) failed = q + 1;
