@@ -93,8 +93,11 @@ def packed_density(eigenvectors, population):
     eigenvectors [nk, V, numStates] (complex128, CUDA; state-major storage,
     as secular_eigensystem returns it, is read in place) and populations
     [nk, numStates], packed as packMatrix does (matrixSubs.F90:506-533):
-    [nk, V(V+1)/2, 2], by imago_packed_density.  The states after the last
-    one populated at any k-point are not read."""
+    [nk, V(V+1)/2, 2], by imago_packed_density.  With host populations
+    (numpy, as populate_states returns them) the states after the last one
+    populated at any k-point are not read and the call does not wait for
+    the device; device populations are used as they are (every state read,
+    the unpopulated ones adding nothing)."""
     c = eigenvectors
     if c.dtype != torch.complex128:
         raise TypeError("eigenvectors must be complex128")
@@ -102,11 +105,16 @@ def packed_density(eigenvectors, population):
     ct = c.transpose(-2, -1)
     if not ct.is_contiguous():
         ct = ct.contiguous()
-    f = torch.as_tensor(population, dtype=torch.float64).to(c.device).contiguous()
+    if isinstance(population, torch.Tensor):
+        f = population.to(device=c.device, dtype=torch.float64).contiguous()
+        used = ns
+    else:
+        fh = np.ascontiguousarray(population, dtype=np.float64)
+        occ = np.flatnonzero((fh != 0).any(axis=0)) if fh.ndim == 2 else []
+        used = int(occ[-1]) + 1 if len(occ) else 0
+        f = torch.from_numpy(fh).pin_memory().to(c.device, non_blocking=True)
     if tuple(f.shape) != (nk, ns):
         raise ValueError(f"population shape {tuple(f.shape)} for {nk} k-points x {ns} states")
-    occ = torch.nonzero((f != 0).any(dim=0)).flatten()
-    used = int(occ[-1]) + 1 if occ.numel() else 0
     rho = torch.empty((nk, V * (V + 1) // 2, 2), dtype=torch.float64, device=c.device)
     L = intg.lib()
     L.imago_packed_density.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4

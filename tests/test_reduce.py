@@ -120,10 +120,13 @@ def test_packed_density_matches_zher(n, ns, used):
     rows, cols = np.triu_indices(n)
     order = np.lexsort((rows, cols))
     ref = full[:, rows[order], cols[order]]
-    # state-major storage (secular_eigensystem's) and a plain [nk, V, ns] tensor
+    # state-major storage (secular_eigensystem's) and a plain [nk, V, ns]
+    # tensor; host populations (the unpopulated tail not read) and device ones
     ct = torch.as_tensor(np.ascontiguousarray(c.transpose(0, 2, 1)), device="cuda")
-    for cv in (ct.transpose(-2, -1), torch.as_tensor(c, device="cuda")):
-        rho = charge.packed_density(cv, f).cpu().numpy()
+    cases = [(ct.transpose(-2, -1), f), (torch.as_tensor(c, device="cuda"), f),
+             (ct.transpose(-2, -1), torch.as_tensor(f, device="cuda"))]
+    for cv, fv in cases:
+        rho = charge.packed_density(cv, fv).cpu().numpy()
         got = rho[..., 0] + 1j * rho[..., 1]
         assert _rel(got, ref) < 1e-13
         diag = [q * (q + 1) // 2 + q for q in range(n)]
