@@ -105,16 +105,17 @@ def packed_density(eigenvectors, population):
     ct = c.transpose(-2, -1)
     if not ct.is_contiguous():
         ct = ct.contiguous()
+    shape = tuple(population.shape) if hasattr(population, "shape") else np.shape(population)
+    if tuple(shape) != (nk, ns):
+        raise ValueError(f"population shape {tuple(shape)} for {nk} k-points x {ns} states")
     if isinstance(population, torch.Tensor):
         f = population.to(device=c.device, dtype=torch.float64).contiguous()
         used = ns
     else:
         fh = np.ascontiguousarray(population, dtype=np.float64)
-        occ = np.flatnonzero((fh != 0).any(axis=0)) if fh.ndim == 2 else []
+        occ = np.flatnonzero((fh != 0).any(axis=0))
         used = int(occ[-1]) + 1 if len(occ) else 0
         f = torch.from_numpy(fh).pin_memory().to(c.device, non_blocking=True)
-    if tuple(f.shape) != (nk, ns):
-        raise ValueError(f"population shape {tuple(f.shape)} for {nk} k-points x {ns} states")
     rho = torch.empty((nk, V * (V + 1) // 2, 2), dtype=torch.float64, device=c.device)
     L = intg.lib()
     L.imago_packed_density.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 4

@@ -140,3 +140,13 @@ def test_packed_density_of_no_occupied_state_is_zero():
     rho = charge.packed_density(c, np.zeros((2, 4)))
     assert rho.shape == (2, 45, 2)
     assert torch.count_nonzero(rho).item() == 0
+
+
+def test_packed_density_checks_its_arguments(imago_lib):
+    # shape and type errors surface before any device work
+    from imago_b200 import charge
+    c = torch.zeros((2, 5, 3), dtype=torch.complex128)
+    with pytest.raises(ValueError, match="population shape"):
+        charge.packed_density(c, np.zeros((2, 4)))
+    with pytest.raises(TypeError):
+        charge.packed_density(c.to(torch.complex64), np.zeros((2, 3)))

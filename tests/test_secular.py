@@ -1,7 +1,8 @@
 """The secular equation of one SCF step (secularEqnSCF) from the integral
 builds: H = NP + KE + sum_j w_j EP_j and S = OL unpacked and solved as the
-generalised Hermitian problem.  Eigenvalues on the GPU (own assembly
-kernel, cuSOLVER through torch) against the CPU oracle (numpy assembly,
+generalised Hermitian problem.  Eigenvalues on the GPU (the library's
+assembly and Cholesky-reduction kernels, then cuSOLVER's batched solver or
+the library's Jacobi kernel) against the CPU oracle (numpy assembly,
 LAPACK), within the 1e-8 Hartree of the target."""
 
 import numpy as np
