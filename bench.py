@@ -288,6 +288,8 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if args.workload == "si8" and list(args.kmesh) != [8, 8, 8]:
+        line["note"] = f"k-mesh {args.kmesh} (profiling case, not the measured workload)"
     print(json.dumps(line), flush=True)
 
 
