@@ -29,3 +29,23 @@ def test_reference_arm_prints_one_contract_line():
                         "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]
     assert "k-mesh [2, 2, 2]" in d["note"]
+
+
+def test_reference_arm_under_two_ranks_prints_once():
+    # launched as the driver launches it for N > 1: rank 0 alone runs and
+    # prints, the other rank exits 0 without work
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                        "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "0", "--kmesh", "2", "2", "2"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2
