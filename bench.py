@@ -978,8 +978,8 @@ def run_ours(args):
     tuning["ortho"] = g.ortho_schedule()
     tuning["contract"] = g.contract_tuning()
     secular_s = time_secular(bufs, P, stream, torch)
-    # the valence-charge step as measured on the Si8 mesh (V = 104, the
-    # Jacobi eigenvectors); the quartz cells' V = 1566 is beyond that kernel
+    # the valence-charge step as measured on the Si8 mesh (V = 104, within
+    # the library's reduction kernels); the SCF cells beyond are in `scf`
     valence = time_valence_rho(bufs, P, stream, torch) if args.workload == "si8" else None
     adjacent = None
     if world == 1 and args.workload == "si8" and not args.no_adjacent:

@@ -5,8 +5,9 @@
 Every iteration runs, as the reference does:
 
   secularEqnSCF   H = NP + KE + sum_j potCoeffs_j EP_j and S = OL from the
-                  device-resident integral builds, Cholesky reduction and
-                  the batched Jacobi eigensolver (imago_b200.secular);
+                  device-resident integral builds, the Cholesky reduction,
+                  the batched eigensolver and the back-transformation
+                  (imago_b200.secular);
   populateStates  the populations (imago_populate_states, host);
   makeValenceRho  the density of the occupied states and its traces
                   against OL, NP, KE and every EP_j (imago_b200.charge);
